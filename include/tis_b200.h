@@ -1,0 +1,252 @@
+/*
+ * tis_b200.h -- C-ABI of the B200 (sm_100a) force-and-integrate library for
+ * the TIS coarse-grained RNA engine (DT15 model).
+ *
+ * Every array crossing this boundary is caller-owned HOST memory laid out the
+ * way the Fortran host keeps it (column-major, xyz fastest), indices inside
+ * topology arrays are 1-based bead numbers, and replica arguments are 1-based
+ * (`irep`), exactly as the Fortran module globals of the reference:
+ *
+ *   xyz_mp_rep(3, nmp_all, nrep), velo_mp(3, nmp_real, nrep),
+ *   accel_mp(3, nmp_real, nrep), force_mp(3, nmp_all), energy(E_TYPE%MAX)
+ *   (src/var_struct.F90, src/var_simu.F90 of the reference).
+ *
+ * Return codes: 0 ok, >0 warning count (force clamps at DE_MAX), <0 fatal
+ * (see TIS_E_* below).  The library never calls exit().  One context per
+ * host thread; calls on one context are not reentrant.
+ */
+#ifndef TIS_B200_H
+#define TIS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ enums */
+/* Values of the reference's enums (src/const_index.F90:88-97, 99-145, 225-241). */
+enum {
+  TIS_CLASS_RNA = 2,
+  TIS_CLASS_LIG = 3,
+  TIS_CLASS_ION = 4
+};
+enum {
+  TIS_MP_RNA_PHOS = 2,
+  TIS_MP_RNA_BASE = 3,
+  TIS_MP_RNA_SUGAR = 4,
+  TIS_MP_ION_MG = 5,
+  TIS_MP_ION_CA2 = 6,
+  TIS_MP_ION_NA = 7,
+  TIS_MP_ION_K = 8,
+  TIS_MP_ION_CL = 9
+};
+/* E_TYPE (1-based in Fortran; index E-1 in C arrays of length TIS_ETYPE_MAX). */
+enum {
+  TIS_E_TOTAL = 1, TIS_E_VELO = 2, TIS_E_BOND = 3, TIS_E_BANGLE = 4,
+  TIS_E_ELE = 8, TIS_E_STACK_DTRNA = 16, TIS_E_HBOND_DTRNA = 17,
+  TIS_E_EXV_DT15 = 18, TIS_E_TSTACK_DTRNA = 19, TIS_E_THBOND_DTRNA = 20,
+  TIS_E_WCA_REP = 23, TIS_E_WCA_ATT = 24,
+  TIS_ETYPE_MAX = 25
+};
+/* i_simulate_type values used here (src/const_index.F90 SIM). */
+enum { TIS_SIM_LANGEVIN = 1, TIS_SIM_BROWNIAN_HI = 6 };
+/* electrostatics: 0 none, DH = i_function_form 0, EWALD = i_function_form 2 */
+enum { TIS_ELE_NONE = 0, TIS_ELE_DH = 1, TIS_ELE_EWALD = 2 };
+/* arithmetic of the force terms */
+enum { TIS_PREC_FP64 = 0, TIS_PREC_MIXED = 1 };
+
+/* error codes */
+#define TIS_OK 0
+#define TIS_E_ARG (-1)
+#define TIS_E_CUDA (-2)
+#define TIS_E_LIST_OVERFLOW (-3)
+#define TIS_E_NOT_SPD (-4)
+#define TIS_E_TIMEOUT (-5)
+#define TIS_E_NOISE_EXHAUSTED (-6)
+#define TIS_E_UNSUPPORTED (-7)
+#define TIS_E_NAN (-8)
+
+/* -------------------------------------------------------------- topology */
+/* One system (unit list + DT15 interaction tables) as read_nativeinfo and
+ * setp_dtrna15 leave it (src/read_nativeinfo.F90:121-620,833-986,
+ * src/setp_dtrna15.F90:40-174).  All index arrays hold 1-based bead numbers. */
+typedef struct tis_topology {
+  int32_t nmp;                     /* nmp_all (= nmp_real: no virtual beads) */
+  int32_t nunit;
+  const int32_t *lunit2mp;         /* (2, nunit) first/last bead of each unit */
+  const int32_t *iclass_unit;      /* (nunit) TIS_CLASS_* */
+  const int32_t *imp2type;         /* (nmp) TIS_MP_* */
+  const double *cmass;             /* (nmp) cmass_mp */
+  const double *fric;              /* (nmp) fric_mp (mass-divided for Langevin) */
+  const double *exv_radius;        /* (nmp) exv_radius_mp */
+  const double *exv_epsilon;       /* (nmp) exv_epsilon_mp = sqrt(eps) */
+  int32_t ncharge;
+  const int32_t *icharge2mp;       /* (ncharge), increasing */
+  const double *coef_charge;       /* (ncharge) */
+  int32_t nbd;                     /* harmonic bonds */
+  const int32_t *ibd2mp;           /* (2, nbd) */
+  const double *bd_nat;            /* (nbd) */
+  const double *coef_bd;           /* (nbd) */
+  int32_t nba;                     /* harmonic angles */
+  const int32_t *iba2mp;           /* (3, nba) */
+  const double *ba_nat;            /* (nba) radians */
+  const double *coef_ba;           /* (nba) */
+  int32_t nst;                     /* DT consecutive stacks */
+  const int32_t *idtrna_st2mp;     /* (7, nst) B1 B2 P1 S1 P2 S2 P3 */
+  const double *dtrna_st_nat;      /* (3, nst) dist, dih1, dih2 (rad) */
+  const double *coef_dtrna_st;     /* (3, nst) coef 1..3 */
+  const double *dtrna_st_hsTm;     /* (3, nst) h, s, Tm for U0(T) */
+  int32_t nhb;                     /* DT15 hydrogen bonds */
+  const int32_t *idtrna_hb2mp;     /* (6, nhb) */
+  const double *dtrna_hb_nat;      /* (6, nhb) dist, 2 angles, 3 dihedrals (rad) */
+  const double *coef_dtrna_hb;     /* (7, nhb) index 0 = U0, 1..6 */
+  const int32_t *idtrna_hb2hbsite; /* (3, 2, nhb) 0 = unused slot */
+  int32_t nhbsite;
+  const int32_t *nvalence_hbsite;  /* (nhbsite) */
+  int32_t nfene;                   /* FENE bonds (Brownian-HI chains) */
+  const int32_t *ifene2mp;         /* (2, nfene) */
+  const double *fene_nat;          /* (nfene) */
+  const double *coef_fene;         /* (nfene) */
+  const double *dist2_fene;        /* (nfene) */
+  int32_t nwca;                    /* WCA pairs (Brownian-HI chains) */
+  const int32_t *iwca2mp;          /* (2, nwca) */
+  const double *wca_nat;           /* (nwca) sigma */
+  const double *coef_wca;          /* (nwca, 2): repulsive, attractive */
+} tis_topology;
+
+/* ---------------------------------------------------------------- params */
+/* The inputs the reference reads from the .inp and para/ files for this
+ * path (src/var_setp.F90 inperi/insimu/inele/indtrna, para/rna.para:325-416,
+ * para/general.para). */
+typedef struct tis_params {
+  int32_t i_periodic;              /* 0 or 1 */
+  double psize[3];                 /* periodic box (cubic for Ewald) */
+  double neigh_margin;             /* Verlet skin, 8.0 */
+  int32_t n_step_neighbor;         /* 0: skin rule (i_neigh_dynamic=1); k>0: rebuild when mod(istep,k)==1 */
+  double exv_dist, exv_dist_PS, exv_adjust, exv_inf;
+  int32_t n_sep_nlocal_P, n_sep_nlocal_S, n_sep_nlocal_B;
+  double hb_cutoff_dist;
+  int32_t i_ele;                   /* TIS_ELE_* */
+  int32_t i_diele;                 /* 0 constant (diele_water), 1 Malmberg-Maryott */
+  double diele_water;
+  double ionic_strength;           /* mol/L */
+  double cutoff_ele;               /* DH: in Debye lengths; Ewald: Angstrom */
+  int32_t i_DH_cutoff_type;        /* energy only; the force always scales */
+  double ewld_alpha, ewld_hmax;
+  int32_t i_simulate_type;         /* TIS_SIM_* */
+  double tstep;
+  double viscosity;                /* Brownian-HI, internal units */
+  double wca_coef_cutoff;          /* Brownian-HI WCA cutoff factor */
+  int32_t precision;               /* TIS_PREC_* */
+  int32_t hb_beta_global;          /* 1: reference quirk (one beta_hbond15 for all replicas) */
+  uint64_t seed;                   /* counter-based noise key */
+} tis_params;
+
+/* ---------------------------------------------------------------- status */
+typedef struct tis_status_t {
+  int64_t step;                    /* istep of replica 1 */
+  int64_t n_rebuild;               /* neighbour rebuilds since init (all replicas) */
+  int64_t n_clamp;                 /* DE_MAX clamps since last tis_status */
+  int32_t list_overflow;           /* any list capacity exceeded */
+  int32_t nan_seen;                /* non-finite force or coordinate seen */
+  int32_t wait_timeout;            /* a bounded device wait gave up */
+  int32_t not_spd;                 /* Brownian-HI Cholesky pivot <= 0 */
+  int32_t last_error;              /* last TIS_E_* returned */
+  int32_t exv_pairs_max;           /* largest exv half list among replicas */
+  int32_t ele_pairs_max;           /* largest ele half list among replicas */
+} tis_status_t;
+
+typedef struct tis_ctx tis_ctx;
+
+/* Builds the device context for one topology and nrep replicas whose
+ * temperatures are tempk[0..nrep-1].  Replaces the allocate_xxx / setp_xxx
+ * and per-stage preparation calls before mloop_simulator
+ * (src/main.F90:44-58, src/main_loop.F90:89-109, src/mloop_dtrna.F90:149-155,
+ * src/mloop_neigh_dist.F90:28-149, src/simu_ele_set.F90, src/simu_set_dtrna.F90). */
+int tis_init(const tis_topology *top, const tis_params *par, int32_t nrep,
+             const double *tempk, tis_ctx **out);
+
+/* Uneven batch: ntop independent systems, system k replicated nrep[k] times
+ * with temperatures tempk[sum(nrep[0..k-1]) ...].  No reference counterpart
+ * beyond running the systems as separate processes (MXUNIT = 20). */
+int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_params *par,
+                   const int32_t *nrep, const double *tempk, tis_ctx **out);
+
+void tis_destroy(tis_ctx *ctx);
+
+/* Number of replicas (lanes) and beads of lane irep (1-based). */
+int tis_nrep(const tis_ctx *ctx);
+int tis_nmp(const tis_ctx *ctx, int32_t irep);
+
+/* Copy state in / out.  xyz is xyz_mp_rep(3, nmp, nrep); pxyz_mp_rep is set
+ * equal to xyz (src/simu_initial.F90); velo/accel may be NULL (zeros in,
+ * skipped out).  For a batch the replicas are concatenated in lane order. */
+int tis_set_state(tis_ctx *ctx, const double *xyz, const double *velo, const double *accel);
+int tis_get_state(tis_ctx *ctx, double *xyz, double *velo, double *accel);
+/* Periodic (wrapped) coordinates pxyz_mp_rep. */
+int tis_get_pxyz(tis_ctx *ctx, double *pxyz);
+
+/* Parity injection.  noise: r_boxmuller(3, nmp, nrep) for nsteps consecutive
+ * steps (step-major); uniforms: for each replica a stream of n_uniform draws
+ * consumed in order by the hydrogen-bond valence pruning
+ * (src/force_dtrna_hbond15.F90:390-509).  Pass noise == NULL / uniforms ==
+ * NULL to return to the counter-based generator. */
+int tis_set_noise(tis_ctx *ctx, const double *noise, int32_t nsteps,
+                  const double *uniforms, int32_t n_uniform);
+
+/* neighbor(irep): exv, ele and hbond lists (src/neighbor.F90:13-142).
+ * irep = -1 rebuilds every replica. */
+int tis_neighbor(tis_ctx *ctx, int32_t irep);
+
+/* Read the lists back in the reference's layout and order:
+ * iexv2mp(3, nexv) = (i, j, imirror), iele2mp(4, nele) = (i, j, imirror, ipmf)
+ * with coef_ele(nele), ineigh2hb(nhbneigh).  *n receives the count; returns
+ * TIS_E_LIST_OVERFLOW when cap is too small (n still set). */
+int tis_get_exv_list(tis_ctx *ctx, int32_t irep, int32_t *iexv2mp, int32_t cap, int32_t *n);
+int tis_get_ele_list(tis_ctx *ctx, int32_t irep, int32_t *iele2mp, double *coef_ele,
+                     int32_t cap, int32_t *n);
+int tis_get_hb_list(tis_ctx *ctx, int32_t irep, int32_t *ineigh2hb, int32_t cap, int32_t *n);
+
+/* force_sumup(force_mp, irep) (src/force_sumup.F90:15-593). */
+int tis_force_sumup(tis_ctx *ctx, int32_t irep, double *force_mp);
+
+/* energy_sumup(irep, ...) -> energy(E_TYPE%MAX) (src/energy_sumup.F90:11-530). */
+int tis_energy_sumup(tis_ctx *ctx, int32_t irep, double *energy);
+
+/* time_integral_pre (src/time_integral_pre.F90:75-180): neighbour lists of
+ * every replica, dxyz = 0, forces and a(0) = F/m + rlan_const(1)*xi. */
+int tis_time_integral_pre(tis_ctx *ctx);
+
+/* nsteps calls of time_integral (src/time_integral.F90:13-473): neighbour
+ * trigger, noise, x update, force_sumup, v/a update, for every replica. */
+int tis_step(tis_ctx *ctx, int64_t nsteps);
+
+/* Replica exchange over temperature labels (src/energy_allrep.F90:123-260 and
+ * src/simu_replica_exchange.F90:18-300): energies at the own and the partner
+ * label's temperature, Metropolis with uniform u[k] for the k-th pair, label
+ * swap and velocity rescale, then the alternation of odd/even pairs.
+ * u == NULL draws counter-based uniforms.  n_accept receives the number of
+ * accepted swaps. */
+int tis_replica_exchange(tis_ctx *ctx, const double *u, int32_t *n_accept);
+/* rep2lab(nrep), 1-based labels. */
+int tis_get_labels(tis_ctx *ctx, int32_t *rep2lab);
+
+int tis_status(tis_ctx *ctx, tis_status_t *st);
+
+/* Milliseconds of the last tis_step measured with CUDA events on the
+ * library's stream. */
+double tis_last_step_ms(tis_ctx *ctx);
+
+/* Device timer on the library's stream: op 0 records the start event; op 1
+ * records the stop event, waits for it and writes the elapsed milliseconds
+ * to *ms.  Lets a caller time a sequence of library calls on the device. */
+int tis_timer(tis_ctx *ctx, int32_t op, double *ms);
+
+/* Human-readable text of the last error on this context. */
+const char *tis_last_error(const tis_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TIS_B200_H */

@@ -1,0 +1,924 @@
+// api.cu -- host side of the C-ABI (include/tis_b200.h): context set-up,
+// temperature-dependent parameters, buffer management and launches.
+//
+// Host-side parameter set-up restates, in the same FP64 operation order:
+//   simu_ele_set.F90:46-226 (dielectric, Bjerrum coefficient, Debye length),
+//   simu_set_dtrna.F90:43-58 (stack U0(T), beta_hbond15),
+//   time_integral_pre.F90:160-171 (rlan_const), simu_para.F90:26-27,
+//   mloop_neigh_dist.F90:28-149, mloop_dtrna.F90:149-152,
+//   setp_periodic.F90:78-113, neighbor_list_ele.F90:73-89.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/tis_b200.h"
+#include "common.cuh"
+
+namespace tis {
+size_t smem_bytes_host(int N, bool periodic, bool skin, int real_size, int nunit);
+cudaError_t lane_kernel_set_smem(bool mixed, int bytes);
+cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
+cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
+                              const double *scale);
+}  // namespace tis
+
+using namespace tis;
+
+namespace {
+
+const double F_PI = 3.14159265358979323846264338e0;
+const double EPSI_0 = 8.854187817e-12;
+const double ELE = 1.6021766208e-19;
+const double BOLTZ_J = 1.38064852e-23;
+const double N_AVO = 6.022140857e23;
+const double KCAL2JOUL = 4184.0;
+const double JOUL2KCAL = 1.0 / KCAL2JOUL;
+const double JOUL2KCAL_MOL = JOUL2KCAL * N_AVO;
+const double BOLTZ_KCAL_MOL = BOLTZ_J * JOUL2KCAL_MOL;
+
+template <typename T> struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    free();
+    n = count;
+    if (count == 0) count = 1;
+    return cudaMalloc((void **)&p, count * sizeof(T));
+  }
+  cudaError_t upload(const std::vector<T> &v) {
+    cudaError_t e = alloc(v.size());
+    if (e != cudaSuccess) return e;
+    if (!v.empty()) e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct HostTop {   // host copy of one topology with derived tables
+  TopDesc d;
+  std::vector<int> lunit, uclass;
+  std::vector<double> rneigh2;
+  int ncharge;
+};
+
+}  // namespace
+
+struct tis_ctx {
+  tis_params par;
+  int nlane = 0, ntop = 0, nlabel = 0;
+  int nbead_total = 0;
+  int threads = 256, group = 2;
+  size_t smem = 0;
+  std::vector<TopDesc> tops;
+  std::vector<LaneDesc> lanes;
+  std::vector<int> lane_nmp;
+  std::vector<int> label_top;        // topology of each label
+  std::vector<double> lab_T;
+  std::vector<int> top_first_label;
+  std::vector<int> rep2lab;          // per lane, global label index
+  std::vector<int> lab2rep;          // per label, lane
+  int idx_pair = 1;                  // odd/even alternation (var_replica.F90:134,165-183)
+  bool hb_energy_valid = false;      // flg_hb_energy
+  double beta_global = 0.0;
+  // device buffers
+  DBuf<TopDesc> d_tops;
+  DBuf<LaneDesc> d_lanes;
+  DBuf<LaneState> d_lstate;
+  DBuf<int8_t> b_type, b_class;
+  DBuf<int16_t> b_unit;
+  DBuf<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4;
+  DBuf<int> u_lunit, u_class;
+  DBuf<double> rneigh2;
+  DBuf<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot;
+  DBuf<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
+  DBuf<double> lab_Td, lab_coef, lab_cdist, lab_beta, lab_rele2, lab_u0, lab_c1;
+  DBuf<int> lab_u0off, lab_c1off, elabel;
+  DBuf<double> xyz, pxyz, velo, accel, dxyz, out_force, out_energy, scale, ebeta;
+  unsigned long long rex_counter = 0;
+  DBuf<uint32_t> nbr, mask;
+  DBuf<int> rowcnt, site_exc;
+  DBuf<uint8_t> mirror, hb_flag;
+  DBuf<double> hb_ene;
+  DBuf<unsigned char> slots;
+  DBuf<double> noise, unif;
+  int noise_nsteps = 0, noise_base = 0, n_unif = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
+  double last_ms = 0.0;
+  std::string err;
+  int last_error = 0;
+  int wait_timeout = 0, not_spd = 0;
+  std::vector<long long> clamp_seen;
+};
+
+namespace {
+
+int fail(tis_ctx *c, int code, const std::string &msg) {
+  if (c) {
+    c->err = msg;
+    c->last_error = code;
+  }
+  return code;
+}
+
+#define CK(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(c, TIS_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+// simu_ele_set.F90:46-226 (i_temp_independent = 0, i_charge = 0)
+void ele_params(const tis_params &p, double tempk, double &ek, double &coef, double &cdist) {
+  const double MM_A = 87.740e0, MM_B = -0.4008e0, MM_C = 9.398e-4, MM_D = -1.410e-6;
+  if (p.i_diele == 0) {
+    ek = p.diele_water;
+  } else {
+    double Tc = tempk - 273.15e0;
+    ek = MM_A + MM_B * Tc + MM_C * Tc * Tc + MM_D * Tc * Tc * Tc;
+  }
+  coef = JOUL2KCAL_MOL * 1.0e10 * (ELE * ELE) / (4.0e0 * F_PI * EPSI_0 * ek);
+  cdist = 1.0e10 * std::sqrt((1.0e-3 * EPSI_0 * ek * BOLTZ_J) / (2.0 * N_AVO * (ELE * ELE))) *
+          std::sqrt(tempk / p.ionic_strength);
+}
+
+template <typename T>
+void append(std::vector<T> &dst, const T *src, size_t n) {
+  if (n) dst.insert(dst.end(), src, src + n);
+}
+
+int choose_threads(int maxN) { return maxN <= 96 ? 128 : (maxN <= 200 ? 256 : 512); }
+
+int choose_group(int threads, int maxN) {
+  const char *env = std::getenv("TIS_GROUP");
+  if (env) {
+    int g = std::atoi(env);
+    if (g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) return g;
+  }
+  int g = 1;
+  while (g < 8 && (threads / (2 * g)) >= maxN) g *= 2;
+  return g;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------- init
+extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_params *par,
+                              const int32_t *nrep, const double *tempk, tis_ctx **out) {
+  if (!out || !tops || !par || !nrep || !tempk || ntop <= 0) return TIS_E_ARG;
+  *out = nullptr;
+  tis_ctx *c = new tis_ctx();
+  c->par = *par;
+  const tis_params &p = *par;
+  if (p.i_simulate_type != TIS_SIM_LANGEVIN) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+  if (p.i_ele == TIS_ELE_EWALD) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+  const bool periodic = p.i_periodic == 1;
+  const bool skin = p.n_step_neighbor <= 0;
+  c->ntop = ntop;
+  // ---- topology tables
+  std::vector<int8_t> b_type, b_class;
+  std::vector<int16_t> b_unit;
+  std::vector<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4;
+  std::vector<int> u_lunit, u_class;
+  std::vector<double> rneigh2;
+  std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot;
+  std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
+  std::vector<double> st_hsTm_all;
+  int maxN = 0;
+  for (int k = 0; k < ntop; ++k) {
+    const tis_topology &t = tops[k];
+    if (t.nmp <= 0 || t.nmp > 65535 || t.nunit <= 0) { tis_destroy(c); return TIS_E_ARG; }
+    TopDesc d{};
+    d.nmp = t.nmp;
+    d.nunit = t.nunit;
+    d.bead0 = (int)b_type.size();
+    d.unit0 = (int)u_class.size();
+    d.rn0 = (int)rneigh2.size();
+    d.bd0 = (int)bd_nat.size(); d.nbd = t.nbd;
+    d.ba0 = (int)ba_nat.size(); d.nba = t.nba;
+    d.st0 = (int)(st_nat.size() / 3); d.nst = t.nst;
+    d.hb0 = (int)(hb_nat.size() / 6); d.nhb = t.nhb;
+    d.site0 = (int)site_val.size(); d.nsite = t.nhbsite;
+    d.sitehb0 = (int)site_hb.size();
+    d.inc0 = (int)inc_ptr.size();
+    d.slot_ba = 2 * t.nbd;
+    d.slot_st = d.slot_ba + 3 * t.nba;
+    d.slot_hb = d.slot_st + 7 * t.nst;
+    d.nslot = d.slot_hb + 6 * t.nhb;
+    maxN = std::max(maxN, t.nmp);
+    // beads
+    std::vector<int> imp2unit(t.nmp, 0);
+    for (int u = 0; u < t.nunit; ++u) {
+      int a0 = t.lunit2mp[2 * u] - 1, a1 = t.lunit2mp[2 * u + 1] - 1;
+      if (a0 < 0 || a1 >= t.nmp || a1 < a0) { tis_destroy(c); return TIS_E_ARG; }
+      for (int i = a0; i <= a1; ++i) imp2unit[i] = u;
+      u_lunit.push_back(a0);
+      u_lunit.push_back(a1);
+      u_class.push_back(t.iclass_unit[u]);
+    }
+    std::vector<double> q(t.nmp, 0.0);
+    for (int i = 0; i < t.ncharge; ++i) q[t.icharge2mp[i] - 1] = t.coef_charge[i];
+    for (int i = 0; i < t.nmp; ++i) {
+      b_type.push_back((int8_t)t.imp2type[i]);
+      b_class.push_back((int8_t)t.iclass_unit[imp2unit[i]]);
+      b_unit.push_back((int16_t)imp2unit[i]);
+      b_cmass.push_back(t.cmass[i]);
+      b_rcmass.push_back(1.0e0 / t.cmass[i]);
+      b_fric.push_back(t.fric[i]);
+      b_radius.push_back(t.exv_radius[i]);
+      b_eps.push_back(t.exv_epsilon[i]);
+      b_charge.push_back(q[i]);
+      // time_integral_pre.F90:162-170
+      double tfh = 0.5e0 * p.tstep * t.fric[i];
+      double u1 = 1.0e0 - tfh;
+      double u2 = 1.0e0 - tfh + tfh * tfh;
+      b_c2.push_back(u1 * u2);
+      b_c3.push_back((0.5e0 * p.tstep) * u1);
+      b_c4.push_back(p.tstep * u1);
+    }
+    // mloop_neigh_dist.F90:28-149
+    for (int u = 0; u < t.nunit; ++u)
+      for (int v = 0; v < t.nunit; ++v) {
+        double max_cut = 0.0;
+        if (t.iclass_unit[u] == TIS_CLASS_RNA && t.iclass_unit[v] == TIS_CLASS_RNA) {
+          if (p.exv_dist > max_cut) max_cut = p.exv_dist;
+          if (p.exv_dist_PS > max_cut) max_cut = p.exv_dist_PS;
+        } else {
+          for (int i = t.lunit2mp[2 * u] - 1; i <= t.lunit2mp[2 * u + 1] - 1; ++i)
+            for (int j = t.lunit2mp[2 * v] - 1; j <= t.lunit2mp[2 * v + 1] - 1; ++j) {
+              double cut = t.exv_radius[i] + t.exv_radius[j];
+              if (cut > max_cut) max_cut = cut;
+            }
+        }
+        double r = max_cut + p.neigh_margin;
+        rneigh2.push_back(r * r);
+      }
+    for (int i = 0; i < 2 * t.nbd; ++i) bd_idx.push_back(t.ibd2mp[i] - 1);
+    append(bd_nat, t.bd_nat, t.nbd);
+    append(bd_coef, t.coef_bd, t.nbd);
+    for (int i = 0; i < 3 * t.nba; ++i) ba_idx.push_back(t.iba2mp[i] - 1);
+    append(ba_nat, t.ba_nat, t.nba);
+    append(ba_coef, t.coef_ba, t.nba);
+    for (int i = 0; i < 7 * t.nst; ++i) st_idx.push_back(t.idtrna_st2mp[i] - 1);
+    append(st_nat, t.dtrna_st_nat, 3 * (size_t)t.nst);
+    append(st_coef, t.coef_dtrna_st, 3 * (size_t)t.nst);
+    append(st_hsTm_all, t.dtrna_st_hsTm, 3 * (size_t)t.nst);
+    for (int i = 0; i < 6 * t.nhb; ++i) hb_idx.push_back(t.idtrna_hb2mp[i] - 1);
+    append(hb_nat, t.dtrna_hb_nat, 6 * (size_t)t.nhb);
+    append(hb_coef, t.coef_dtrna_hb, 7 * (size_t)t.nhb);
+    for (int i = 0; i < 6 * t.nhb; ++i) hb_site.push_back(t.idtrna_hb2hbsite[i] - 1);
+    for (int h = 0; h < t.nhb; ++h) {   // mloop_dtrna.F90:151
+      double r = t.dtrna_hb_nat[6 * h] + p.hb_cutoff_dist + p.neigh_margin;
+      hb_nd2.push_back(r * r);
+    }
+    for (int s = 0; s < t.nhbsite; ++s) site_val.push_back(t.nvalence_hbsite[s]);
+    // per-site hbond lists in list_hb_at_hbsite order (neighbor_list_hb.F90:394-410)
+    std::vector<std::vector<int>> at(t.nhbsite);
+    for (int h = 0; h < t.nhb; ++h)
+      for (int i = 0; i < 3; ++i) {
+        int s1 = t.idtrna_hb2hbsite[6 * h + i], s2 = t.idtrna_hb2hbsite[6 * h + 3 + i];
+        if (s1 > 0) at[s1 - 1].push_back(h);
+        if (s2 > 0) at[s2 - 1].push_back(h);
+      }
+    int cnt = 0;
+    for (int s = 0; s < t.nhbsite; ++s) {
+      site_ptr.push_back(cnt);
+      for (int h : at[s]) site_hb.push_back(h);
+      cnt += (int)at[s].size();
+    }
+    site_ptr.push_back(cnt);
+    // incidence lists: bead -> slots, ascending slot id
+    std::vector<std::vector<int>> inc(t.nmp);
+    for (int b = 0; b < t.nbd; ++b)
+      for (int q2 = 0; q2 < 2; ++q2) inc[t.ibd2mp[2 * b + q2] - 1].push_back(2 * b + q2);
+    for (int b = 0; b < t.nba; ++b)
+      for (int q2 = 0; q2 < 3; ++q2) inc[t.iba2mp[3 * b + q2] - 1].push_back(d.slot_ba + 3 * b + q2);
+    for (int b = 0; b < t.nst; ++b)
+      for (int q2 = 0; q2 < 7; ++q2) inc[t.idtrna_st2mp[7 * b + q2] - 1].push_back(d.slot_st + 7 * b + q2);
+    for (int b = 0; b < t.nhb; ++b)
+      for (int q2 = 0; q2 < 6; ++q2) inc[t.idtrna_hb2mp[6 * b + q2] - 1].push_back(d.slot_hb + 6 * b + q2);
+    int ip = (int)inc_slot.size();
+    for (int i = 0; i < t.nmp; ++i) {
+      inc_ptr.push_back(ip);
+      for (int sl : inc[i]) inc_slot.push_back(sl);
+      ip += (int)inc[i].size();
+    }
+    inc_ptr.push_back(ip);
+    c->tops.push_back(d);
+  }
+  // ---- lanes and labels
+  int nlane = 0;
+  for (int k = 0; k < ntop; ++k) {
+    if (nrep[k] <= 0) { tis_destroy(c); return TIS_E_ARG; }
+    nlane += nrep[k];
+  }
+  c->nlane = nlane;
+  c->nlabel = nlane;
+  std::vector<double> lab_T(nlane), lab_coef(nlane), lab_cdist(nlane), lab_beta(nlane), lab_rele2(nlane);
+  std::vector<int> lab_u0off(nlane), lab_c1off(nlane);
+  std::vector<double> lab_u0, lab_c1;
+  c->label_top.resize(nlane);
+  c->rep2lab.resize(nlane);
+  c->lab2rep.resize(nlane);
+  size_t nbr_off = 0, rowcnt_off = 0, mask_off = 0, slot_off = 0;
+  long long mirror_off = 0;
+  int hb_off = 0, site_off = 0, state_off = 0;
+  int lane = 0;
+  for (int k = 0; k < ntop; ++k) {
+    TopDesc &d = c->tops[k];
+    d.nlabel = nrep[k];
+    c->top_first_label.push_back(lane);
+    const int N = d.nmp;
+    for (int r = 0; r < nrep[k]; ++r, ++lane) {
+      const double T = tempk[lane];
+      double ek, coef, cdist;
+      ele_params(p, T, ek, coef, cdist);
+      lab_T[lane] = T;
+      lab_coef[lane] = coef;
+      lab_cdist[lane] = cdist;
+      lab_beta[lane] = 1.0e0 / (T * BOLTZ_KCAL_MOL);
+      double rr = (p.i_ele == TIS_ELE_DH) ? (p.neigh_margin + p.cutoff_ele * cdist) : (p.neigh_margin + p.cutoff_ele);
+      lab_rele2[lane] = rr * rr;
+      lab_u0off[lane] = (int)lab_u0.size();
+      for (int s = 0; s < d.nst; ++s) {   // simu_set_dtrna.F90:48-53
+        const double *hst = &st_hsTm_all[3 * (size_t)(d.st0 + s)];
+        lab_u0.push_back(-hst[0] + BOLTZ_KCAL_MOL * (T - hst[2]) * hst[1]);
+      }
+      lab_c1off[lane] = (int)lab_c1.size();
+      for (int i = 0; i < N; ++i) {   // time_integral_pre.F90:166-167
+        const int b = d.bead0 + i;
+        lab_c1.push_back(std::sqrt(2.0e0 * b_fric[b] * BOLTZ_KCAL_MOL * T / (p.tstep * b_cmass[b])));
+      }
+      c->label_top[lane] = k;
+      c->rep2lab[lane] = lane;
+      c->lab2rep[lane] = lane;
+      LaneDesc L{};
+      L.top = k;
+      L.state0 = state_off;
+      L.nbr0 = (int)nbr_off;
+      L.rowcnt0 = (int)rowcnt_off;
+      L.mask0 = (int)mask_off;
+      L.mirror0 = mirror_off;
+      L.slot0 = (int)slot_off;
+      L.hb0 = hb_off;
+      L.site0 = site_off;
+      L.unif0 = 0;
+      state_off += N;
+      nbr_off += (size_t)N * (N > 1 ? N - 1 : 1);
+      rowcnt_off += N;
+      mask_off += 2 * (size_t)N * ((N + 31) / 32);
+      if (periodic) mirror_off += (long long)N * N;
+      slot_off += d.nslot;
+      hb_off += d.nhb;
+      site_off += d.nsite;
+      c->lanes.push_back(L);
+      c->lane_nmp.push_back(N);
+    }
+  }
+  if (nbr_off > 0x7fffffffULL || mask_off > 0x7fffffffULL || slot_off > 0x7fffffffULL) {
+    tis_destroy(c);
+    return TIS_E_ARG;
+  }
+  c->nbead_total = state_off;
+  c->lab_T = lab_T;
+  // the global beta_hbond15 is the value set for the last replica (simu_set_dtrna.F90:58)
+  c->beta_global = lab_beta[nlane - 1];
+  c->threads = choose_threads(maxN);
+  c->group = choose_group(c->threads, maxN);
+  const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
+  size_t smem = 0;
+  for (auto &d : c->tops) smem = std::max(smem, smem_bytes_host(d.nmp, periodic, skin, real_size, d.nunit));
+  c->smem = smem;
+
+  // ---- device
+  CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&c->ev0));
+  CK(cudaEventCreate(&c->ev1));
+  CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem));
+  CK(c->d_tops.upload(c->tops));
+  CK(c->d_lanes.upload(c->lanes));
+  std::vector<LaneState> ls(nlane);
+  for (int i = 0; i < nlane; ++i) { std::memset(&ls[i], 0, sizeof(LaneState)); ls[i].label = i; }
+  CK(c->d_lstate.upload(ls));
+  CK(c->b_type.upload(b_type)); CK(c->b_class.upload(b_class)); CK(c->b_unit.upload(b_unit));
+  CK(c->b_rcmass.upload(b_rcmass)); CK(c->b_cmass.upload(b_cmass)); CK(c->b_fric.upload(b_fric));
+  CK(c->b_radius.upload(b_radius)); CK(c->b_eps.upload(b_eps)); CK(c->b_charge.upload(b_charge));
+  CK(c->b_c2.upload(b_c2)); CK(c->b_c3.upload(b_c3)); CK(c->b_c4.upload(b_c4));
+  CK(c->u_lunit.upload(u_lunit)); CK(c->u_class.upload(u_class)); CK(c->rneigh2.upload(rneigh2));
+  CK(c->bd_idx.upload(bd_idx)); CK(c->bd_nat.upload(bd_nat)); CK(c->bd_coef.upload(bd_coef));
+  CK(c->ba_idx.upload(ba_idx)); CK(c->ba_nat.upload(ba_nat)); CK(c->ba_coef.upload(ba_coef));
+  CK(c->st_idx.upload(st_idx)); CK(c->st_nat.upload(st_nat)); CK(c->st_coef.upload(st_coef));
+  CK(c->hb_idx.upload(hb_idx)); CK(c->hb_nat.upload(hb_nat)); CK(c->hb_coef.upload(hb_coef));
+  CK(c->hb_site.upload(hb_site)); CK(c->hb_nd2.upload(hb_nd2));
+  CK(c->site_val.upload(site_val)); CK(c->site_ptr.upload(site_ptr)); CK(c->site_hb.upload(site_hb));
+  CK(c->inc_ptr.upload(inc_ptr)); CK(c->inc_slot.upload(inc_slot));
+  CK(c->lab_Td.upload(lab_T)); CK(c->lab_coef.upload(lab_coef)); CK(c->lab_cdist.upload(lab_cdist));
+  CK(c->lab_beta.upload(lab_beta)); CK(c->lab_rele2.upload(lab_rele2));
+  CK(c->lab_u0off.upload(lab_u0off)); CK(c->lab_u0.upload(lab_u0));
+  CK(c->lab_c1off.upload(lab_c1off)); CK(c->lab_c1.upload(lab_c1));
+  size_t n3 = 3 * (size_t)state_off;
+  CK(c->xyz.alloc(n3)); CK(c->pxyz.alloc(n3)); CK(c->velo.alloc(n3)); CK(c->accel.alloc(n3));
+  CK(c->dxyz.alloc(n3)); CK(c->out_force.alloc(n3));
+  CK(cudaMemset(c->xyz.p, 0, n3 * 8)); CK(cudaMemset(c->pxyz.p, 0, n3 * 8));
+  CK(cudaMemset(c->velo.p, 0, n3 * 8)); CK(cudaMemset(c->accel.p, 0, n3 * 8));
+  CK(cudaMemset(c->dxyz.p, 0, n3 * 8));
+  CK(c->out_energy.alloc((size_t)nlane * N_ETYPE));
+  CK(c->scale.alloc(nlane));
+  CK(c->ebeta.alloc(nlane));
+  CK(c->elabel.alloc(nlane));
+  CK(c->nbr.alloc(nbr_off)); CK(c->rowcnt.alloc(rowcnt_off)); CK(c->mask.alloc(mask_off));
+  CK(cudaMemset(c->rowcnt.p, 0, std::max<size_t>(rowcnt_off, 1) * sizeof(int)));
+  CK(c->mirror.alloc(periodic ? (size_t)mirror_off : 1));
+  CK(c->slots.alloc(slot_off * 3 * real_size));
+  CK(c->hb_flag.alloc(hb_off)); CK(c->hb_ene.alloc(hb_off)); CK(c->site_exc.alloc(site_off));
+  CK(cudaMemset(c->hb_flag.p, 0, std::max(hb_off, 1)));
+  CK(cudaMemset(c->hb_ene.p, 0, std::max(hb_off, 1) * sizeof(double)));
+  c->clamp_seen.assign(nlane, 0);
+  *out = c;
+  return TIS_OK;
+}
+
+extern "C" int tis_init(const tis_topology *top, const tis_params *par, int32_t nrep, const double *tempk,
+                        tis_ctx **out) {
+  if (nrep <= 0) return TIS_E_ARG;
+  return tis_init_batch(1, top, par, &nrep, tempk, out);
+}
+
+extern "C" void tis_destroy(tis_ctx *c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->d_tops.free(); c->d_lanes.free(); c->d_lstate.free();
+  c->b_type.free(); c->b_class.free(); c->b_unit.free();
+  c->b_rcmass.free(); c->b_cmass.free(); c->b_fric.free(); c->b_radius.free(); c->b_eps.free(); c->b_charge.free();
+  c->b_c2.free(); c->b_c3.free(); c->b_c4.free();
+  c->u_lunit.free(); c->u_class.free(); c->rneigh2.free();
+  c->bd_idx.free(); c->ba_idx.free(); c->st_idx.free(); c->hb_idx.free(); c->hb_site.free();
+  c->site_val.free(); c->site_ptr.free(); c->site_hb.free(); c->inc_ptr.free(); c->inc_slot.free();
+  c->bd_nat.free(); c->bd_coef.free(); c->ba_nat.free(); c->ba_coef.free(); c->st_nat.free(); c->st_coef.free();
+  c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free();
+  c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
+  c->lab_u0.free(); c->lab_c1.free(); c->lab_u0off.free(); c->lab_c1off.free(); c->elabel.free();
+  c->ebeta.free();
+  c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free();
+  c->out_force.free(); c->out_energy.free(); c->scale.free();
+  c->nbr.free(); c->mask.free(); c->rowcnt.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
+  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->tev0) cudaEventDestroy(c->tev0);
+  if (c->tev1) cudaEventDestroy(c->tev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+extern "C" int tis_nrep(const tis_ctx *c) { return c ? c->nlane : TIS_E_ARG; }
+extern "C" int tis_nmp(const tis_ctx *c, int32_t irep) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  return c->lane_nmp[irep - 1];
+}
+
+// ------------------------------------------------------------------- state
+extern "C" int tis_set_state(tis_ctx *c, const double *xyz, const double *velo, const double *accel) {
+  if (!c || !xyz) return TIS_E_ARG;
+  size_t n = 3 * (size_t)c->nbead_total * sizeof(double);
+  CK(cudaMemcpyAsync(c->xyz.p, xyz, n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->pxyz.p, xyz, n, cudaMemcpyHostToDevice, c->stream));
+  if (velo) CK(cudaMemcpyAsync(c->velo.p, velo, n, cudaMemcpyHostToDevice, c->stream));
+  else CK(cudaMemsetAsync(c->velo.p, 0, n, c->stream));
+  if (accel) CK(cudaMemcpyAsync(c->accel.p, accel, n, cudaMemcpyHostToDevice, c->stream));
+  else CK(cudaMemsetAsync(c->accel.p, 0, n, c->stream));
+  CK(cudaMemsetAsync(c->dxyz.p, 0, n, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TIS_OK;
+}
+
+extern "C" int tis_get_state(tis_ctx *c, double *xyz, double *velo, double *accel) {
+  if (!c) return TIS_E_ARG;
+  size_t n = 3 * (size_t)c->nbead_total * sizeof(double);
+  if (xyz) CK(cudaMemcpyAsync(xyz, c->xyz.p, n, cudaMemcpyDeviceToHost, c->stream));
+  if (velo) CK(cudaMemcpyAsync(velo, c->velo.p, n, cudaMemcpyDeviceToHost, c->stream));
+  if (accel) CK(cudaMemcpyAsync(accel, c->accel.p, n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TIS_OK;
+}
+
+extern "C" int tis_get_pxyz(tis_ctx *c, double *pxyz) {
+  if (!c || !pxyz) return TIS_E_ARG;
+  CK(cudaMemcpy(pxyz, c->pxyz.p, 3 * (size_t)c->nbead_total * sizeof(double), cudaMemcpyDeviceToHost));
+  return TIS_OK;
+}
+
+extern "C" int tis_set_noise(tis_ctx *c, const double *noise, int32_t nsteps, const double *uniforms, int32_t n_uniform) {
+  if (!c) return TIS_E_ARG;
+  if (noise && nsteps > 0) {
+    std::vector<double> tmp(noise, noise + 3 * (size_t)c->nbead_total * nsteps);
+    CK(c->noise.upload(tmp));
+    c->noise_nsteps = nsteps;
+  } else {
+    c->noise.free();
+    c->noise_nsteps = 0;
+  }
+  c->noise_base = 0;
+  if (uniforms && n_uniform > 0) {
+    std::vector<double> tmp(uniforms, uniforms + (size_t)n_uniform * c->nlane);
+    CK(c->unif.upload(tmp));
+    c->n_unif = n_uniform;
+    for (int i = 0; i < c->nlane; ++i) c->lanes[i].unif0 = i * n_uniform;
+  } else {
+    c->unif.free();
+    c->n_unif = 0;
+    for (int i = 0; i < c->nlane; ++i) c->lanes[i].unif0 = 0;
+  }
+  CK(cudaMemcpy(c->d_lanes.p, c->lanes.data(), c->lanes.size() * sizeof(LaneDesc), cudaMemcpyHostToDevice));
+  // reset the per-lane uniform positions
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpy(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost));
+  for (auto &s : ls) { s.unif_pos = 0; s.flags &= ~(LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED); }
+  CK(cudaMemcpy(c->d_lstate.p, ls.data(), ls.size() * sizeof(LaneState), cudaMemcpyHostToDevice));
+  return TIS_OK;
+}
+
+// -------------------------------------------------------------- launches
+namespace {
+
+KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
+  const tis_params &p = c->par;
+  KArgs a{};
+  a.nlane = c->nlane;
+  a.nsteps = nsteps;
+  a.mode = mode;
+  a.only_lane = only_lane;
+  a.group = c->group;
+  a.periodic = p.i_periodic == 1;
+  for (int d = 0; d < 3; ++d) { a.psize[d] = p.psize[d]; a.psizeh[d] = p.psize[d] / 2.0; }
+  a.neigh_margin = p.neigh_margin;
+  a.n_step_neighbor = p.n_step_neighbor;
+  a.exv_dist = p.exv_dist; a.exv_dist_PS = p.exv_dist_PS; a.exv_adjust = p.exv_adjust;
+  a.nsep[0] = p.n_sep_nlocal_P; a.nsep[1] = p.n_sep_nlocal_S; a.nsep[2] = p.n_sep_nlocal_B;
+  a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : 0;
+  a.cutoff_ele = p.cutoff_ele;
+  a.i_DH_cutoff_type = p.i_DH_cutoff_type;
+  a.hb_cutoff_dist = p.hb_cutoff_dist;
+  a.max_abscos = std::cos((double)(0.57f / 180.0f) * F_PI);
+  a.tstep = p.tstep; a.tstep2 = 0.5e0 * p.tstep * p.tstep; a.tsteph = 0.5e0 * p.tstep;
+  a.beta_hbond15 = c->beta_global;
+  a.hb_beta_global = p.hb_beta_global;
+  a.seed = p.seed;
+  a.tops = c->d_tops.p; a.lanes = c->d_lanes.p; a.lstate = c->d_lstate.p;
+  a.b_type = c->b_type.p; a.b_class = c->b_class.p; a.b_unit = c->b_unit.p;
+  a.b_rcmass = c->b_rcmass.p; a.b_cmass = c->b_cmass.p; a.b_fric = c->b_fric.p; a.b_radius = c->b_radius.p;
+  a.b_eps = c->b_eps.p; a.b_charge = c->b_charge.p;
+  a.u_lunit = c->u_lunit.p; a.u_class = c->u_class.p; a.rneigh2 = c->rneigh2.p;
+  a.bd_idx = c->bd_idx.p; a.bd_nat = c->bd_nat.p; a.bd_coef = c->bd_coef.p;
+  a.ba_idx = c->ba_idx.p; a.ba_nat = c->ba_nat.p; a.ba_coef = c->ba_coef.p;
+  a.st_idx = c->st_idx.p; a.st_nat = c->st_nat.p; a.st_coef = c->st_coef.p;
+  a.hb_idx = c->hb_idx.p; a.hb_nat = c->hb_nat.p; a.hb_coef = c->hb_coef.p; a.hb_site = c->hb_site.p;
+  a.hb_nd2 = c->hb_nd2.p;
+  a.site_val = c->site_val.p; a.site_ptr = c->site_ptr.p; a.site_hb = c->site_hb.p;
+  a.inc_ptr = c->inc_ptr.p; a.inc_slot = c->inc_slot.p;
+  a.lab_T = c->lab_Td.p; a.lab_coef = c->lab_coef.p; a.lab_cdist = c->lab_cdist.p; a.lab_beta = c->lab_beta.p;
+  a.lab_rele2 = c->lab_rele2.p; a.lab_u0off = c->lab_u0off.p; a.lab_u0 = c->lab_u0.p;
+  a.lab_c1off = c->lab_c1off.p; a.lab_c1 = c->lab_c1.p;
+  a.b_c2 = c->b_c2.p; a.b_c3 = c->b_c3.p; a.b_c4 = c->b_c4.p;
+  a.xyz = c->xyz.p; a.pxyz = c->pxyz.p; a.velo = c->velo.p; a.accel = c->accel.p; a.dxyz = c->dxyz.p;
+  a.nbr = c->nbr.p; a.rowcnt = c->rowcnt.p; a.mask = c->mask.p; a.mirror = c->mirror.p;
+  a.slots = c->slots.p; a.hb_flag = c->hb_flag.p; a.hb_ene = c->hb_ene.p; a.site_exc = c->site_exc.p;
+  a.elabel = nullptr; a.reuse_hb = 0; a.ebeta = c->beta_global; a.out_energy = c->out_energy.p;
+  a.out_force = c->out_force.p;
+  a.noise = c->noise_nsteps ? c->noise.p : nullptr;
+  a.noise_nsteps = c->noise_nsteps;
+  a.noise_base = c->noise_base;
+  a.unif = c->n_unif ? c->unif.p : nullptr;
+  a.n_unif = c->n_unif;
+  a.nbead_total = c->nbead_total;
+  return a;
+}
+
+int launch_lane(tis_ctx *c, const KArgs &a) {
+  CK(lane_kernel_launch(c->par.precision == TIS_PREC_MIXED, a.only_lane >= 0 ? 1 : a.nlane, c->threads, c->smem,
+                        c->stream, a));
+  return TIS_OK;
+}
+
+int check_lanes(tis_ctx *c) {
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  long long clamps = 0;
+  int code = TIS_OK;
+  for (int i = 0; i < c->nlane; ++i) {
+    if (ls[i].flags & LF_NAN) code = fail(c, TIS_E_NAN, "non-finite force in lane " + std::to_string(i + 1));
+    if (ls[i].flags & LF_OVERFLOW) code = fail(c, TIS_E_LIST_OVERFLOW, "hbond site list overflow");
+    if (ls[i].flags & (LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED))
+      code = fail(c, TIS_E_NOISE_EXHAUSTED, "injected noise or uniforms exhausted");
+    clamps += ls[i].nclamp - c->clamp_seen[i];
+    c->clamp_seen[i] = ls[i].nclamp;
+  }
+  if (code < 0) return code;
+  return (int)std::min<long long>(clamps, 0x7fffffff);
+}
+
+}  // namespace
+
+extern "C" int tis_neighbor(tis_ctx *c, int32_t irep) {
+  if (!c || irep == 0 || irep > c->nlane || irep < -1) return TIS_E_ARG;
+  KArgs a = make_args(c, KM_NEIGHBOR, 0, irep > 0 ? irep - 1 : -1);
+  int rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  return check_lanes(c);
+}
+
+namespace {
+int fetch_rows(tis_ctx *c, int lane, std::vector<uint32_t> &rows, std::vector<int> &cnt) {
+  const LaneDesc &L = c->lanes[lane];
+  const int N = c->lane_nmp[lane];
+  const int rl = N > 1 ? N - 1 : 1;
+  rows.resize((size_t)N * rl);
+  cnt.resize(N);
+  CK(cudaMemcpy(rows.data(), c->nbr.p + L.nbr0, rows.size() * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(cnt.data(), c->rowcnt.p + L.rowcnt0, cnt.size() * 4, cudaMemcpyDeviceToHost));
+  return TIS_OK;
+}
+}  // namespace
+
+extern "C" int tis_get_exv_list(tis_ctx *c, int32_t irep, int32_t *iexv2mp, int32_t cap, int32_t *n) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  std::vector<uint32_t> rows;
+  std::vector<int> cnt;
+  int rc = fetch_rows(c, irep - 1, rows, cnt);
+  if (rc < 0) return rc;
+  const int N = c->lane_nmp[irep - 1], rl = N > 1 ? N - 1 : 1;
+  const bool peri = c->par.i_periodic == 1;
+  int k = 0;
+  for (int i = 0; i < N; ++i)
+    for (int e = 0; e < cnt[i]; ++e) {
+      uint32_t ent = rows[(size_t)i * rl + e];
+      int j = ent & 0xFFFF;
+      if (j <= i || !(ent & (1u << 16))) continue;
+      if (k < cap && iexv2mp) {
+        iexv2mp[3 * k] = i + 1;
+        iexv2mp[3 * k + 1] = j + 1;
+        iexv2mp[3 * k + 2] = peri ? (int)(ent >> 18) : 1;
+      }
+      ++k;
+    }
+  if (n) *n = k;
+  return k > cap ? TIS_E_LIST_OVERFLOW : TIS_OK;
+}
+
+extern "C" int tis_get_ele_list(tis_ctx *c, int32_t irep, int32_t *iele2mp, double *coef_ele, int32_t cap, int32_t *n) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  std::vector<uint32_t> rows;
+  std::vector<int> cnt;
+  int rc = fetch_rows(c, irep - 1, rows, cnt);
+  if (rc < 0) return rc;
+  const int lane = irep - 1;
+  const int N = c->lane_nmp[lane], rl = N > 1 ? N - 1 : 1;
+  const bool peri = c->par.i_periodic == 1;
+  std::vector<double> q(N);
+  const TopDesc &T = c->tops[c->lanes[lane].top];
+  CK(cudaMemcpy(q.data(), c->b_charge.p + T.bead0, N * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<LaneState> ls(1);
+  CK(cudaMemcpy(ls.data(), c->d_lstate.p + lane, sizeof(LaneState), cudaMemcpyDeviceToHost));
+  double coefT = 0.0;
+  CK(cudaMemcpy(&coefT, c->lab_coef.p + ls[0].label, sizeof(double), cudaMemcpyDeviceToHost));
+  int k = 0;
+  for (int i = 0; i < N; ++i)
+    for (int e = 0; e < cnt[i]; ++e) {
+      uint32_t ent = rows[(size_t)i * rl + e];
+      int j = ent & 0xFFFF;
+      if (j <= i || !(ent & (1u << 17))) continue;
+      if (k < cap) {
+        if (iele2mp) {
+          iele2mp[4 * k] = i + 1;
+          iele2mp[4 * k + 1] = j + 1;
+          iele2mp[4 * k + 2] = peri ? (int)(ent >> 18) : 1;
+          iele2mp[4 * k + 3] = 0;
+        }
+        if (coef_ele) coef_ele[k] = q[i] * q[j] * coefT;
+      }
+      ++k;
+    }
+  if (n) *n = k;
+  return k > cap ? TIS_E_LIST_OVERFLOW : TIS_OK;
+}
+
+extern "C" int tis_get_hb_list(tis_ctx *c, int32_t irep, int32_t *ineigh2hb, int32_t cap, int32_t *n) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  const LaneDesc &L = c->lanes[irep - 1];
+  const TopDesc &T = c->tops[L.top];
+  std::vector<uint8_t> f(std::max(T.nhb, 1));
+  if (T.nhb) CK(cudaMemcpy(f.data(), c->hb_flag.p + L.hb0, T.nhb, cudaMemcpyDeviceToHost));
+  int k = 0;
+  for (int h = 0; h < T.nhb; ++h)
+    if (f[h] & 1) {
+      if (k < cap && ineigh2hb) ineigh2hb[k] = h + 1;
+      ++k;
+    }
+  if (n) *n = k;
+  return k > cap ? TIS_E_LIST_OVERFLOW : TIS_OK;
+}
+
+extern "C" int tis_force_sumup(tis_ctx *c, int32_t irep, double *force_mp) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  KArgs a = make_args(c, KM_FORCE, 0, irep - 1);
+  int rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  c->hb_energy_valid = true;
+  const LaneDesc &L = c->lanes[irep - 1];
+  if (force_mp)
+    CK(cudaMemcpyAsync(force_mp, c->out_force.p + 3 * (size_t)L.state0, 3 * (size_t)c->lane_nmp[irep - 1] * 8,
+                       cudaMemcpyDeviceToHost, c->stream));
+  return check_lanes(c);
+}
+
+namespace {
+int run_energy(tis_ctx *c, int only_lane, const int *labels, bool reuse, double beta, std::vector<double> &E,
+               const double *beta_lane = nullptr) {
+  KArgs a = make_args(c, 0, 0, only_lane);
+  if (labels) {
+    CK(cudaMemcpyAsync(c->elabel.p, labels, c->nlane * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    a.elabel = c->elabel.p;
+  }
+  if (beta_lane) {
+    CK(cudaMemcpyAsync(c->ebeta.p, beta_lane, c->nlane * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    a.ebeta_lane = c->ebeta.p;
+  }
+  a.reuse_hb = reuse ? 1 : 0;
+  a.ebeta = beta;
+  CK(energy_kernel_launch(only_lane >= 0 ? 1 : c->nlane, c->stream, a));
+  E.resize((size_t)c->nlane * N_ETYPE);
+  CK(cudaMemcpyAsync(E.data(), c->out_energy.p, E.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return TIS_OK;
+}
+}  // namespace
+
+extern "C" int tis_energy_sumup(tis_ctx *c, int32_t irep, double *energy) {
+  if (!c || irep < 1 || irep > c->nlane || !energy) return TIS_E_ARG;
+  std::vector<double> E;
+  int rc = run_energy(c, irep - 1, nullptr, c->hb_energy_valid, c->beta_global, E);
+  if (rc < 0) return rc;
+  std::memcpy(energy, &E[(size_t)(irep - 1) * N_ETYPE], N_ETYPE * sizeof(double));
+  return check_lanes(c);
+}
+
+extern "C" int tis_time_integral_pre(tis_ctx *c) {
+  if (!c) return TIS_E_ARG;
+  KArgs a = make_args(c, KM_PRE, 0, -1);
+  int rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  c->noise_base += 1;
+  c->hb_energy_valid = true;
+  return check_lanes(c);
+}
+
+extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
+  if (!c || nsteps < 0 || nsteps > 0x7fffffff) return TIS_E_ARG;
+  if (nsteps == 0) return TIS_OK;
+  KArgs a = make_args(c, KM_STEP, (int)nsteps, -1);
+  CK(cudaEventRecord(c->ev0, c->stream));
+  int rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  c->noise_base += (int)nsteps;
+  c->hb_energy_valid = true;
+  return check_lanes(c);
+}
+
+// energy_allrep.F90:123-260 + simu_replica_exchange.F90:87-300 +
+// time_integral_post.F90:293-349 (labels refresh rlan_const(1) and the
+// electrostatic / stack parameters: the kernels read them by label).
+extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_accept) {
+  if (!c) return TIS_E_ARG;
+  if (c->ntop != 1) return fail(c, TIS_E_UNSUPPORTED, "replica exchange needs one topology");
+  const int n = c->nlane;
+  auto pair_of = [&](int l) -> int {   // 1-based labels, exchange_pair_tb (one dimension)
+    if (c->idx_pair == 1) { if (l % 2 == 1) return (l + 1 <= n) ? l + 1 : 0; return l - 1; }
+    if (l == 1) return 0;
+    if (l % 2 == 0) return (l + 1 <= n) ? l + 1 : 0;
+    return l - 1;
+  };
+  std::vector<double> E_own, E_opp;
+  int rc = run_energy(c, -1, nullptr, c->hb_energy_valid, c->beta_global, E_own);
+  if (rc < 0) return rc;
+  std::vector<int> opp(n, -1);
+  for (int r = 0; r < n; ++r) {
+    int lo = pair_of(c->rep2lab[r] + 1);
+    opp[r] = (lo == 0) ? -1 : lo - 1;
+  }
+  // partner energies: recomputed hbonds, beta of the partner label
+  // (energy_allrep.F90:134,209-216); lanes without a partner are skipped.
+  {
+    std::vector<int> lab(n, -1);
+    std::vector<double> beta(n, c->beta_global);
+    for (int r = 0; r < n; ++r)
+      if (opp[r] >= 0) { lab[r] = opp[r]; beta[r] = 1.0e0 / (c->lab_T[opp[r]] * BOLTZ_KCAL_MOL); }
+    rc = run_energy(c, -1, lab.data(), false, c->beta_global, E_opp, beta.data());
+    if (rc < 0) return rc;
+    for (int r = 0; r < n; ++r)
+      if (opp[r] < 0) for (int k = 0; k < N_ETYPE; ++k) E_opp[(size_t)r * N_ETYPE + k] = 0.0;
+  }
+  c->hb_energy_valid = false;
+  int nrand = 0, nacc = 0;
+  std::vector<double> scale(n, 0.0);
+  std::vector<double> ubuf;
+  if (!u) {
+    ubuf.resize((n + 1) / 2);
+    for (auto &x : ubuf) {
+      unsigned long long ctr = c->rex_counter++;
+      U4 o = philox4x32(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x52454D44u, 0u}, (uint32_t)c->par.seed, (uint32_t)(c->par.seed >> 32));
+      x = u01_open0(o.x) - 2.3283064365386963e-10;   // [0, 1)
+    }
+    u = ubuf.data();
+  }
+  for (int li = 1; li <= n; ++li) {
+    int lj = pair_of(li);
+    if (lj < li) continue;
+    nrand++;
+    int ri = c->lab2rep[li - 1], rj = c->lab2rep[lj - 1];
+    double tm = c->lab_T[li - 1], tn = c->lab_T[lj - 1];
+    double pim = E_own[(size_t)ri * N_ETYPE], pin = E_opp[(size_t)ri * N_ETYPE];
+    double pjn = E_own[(size_t)rj * N_ETYPE], pjm = E_opp[(size_t)rj * N_ETYPE];
+    double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / BOLTZ_KCAL_MOL;
+    bool acc = delta < 0.0e0 || u[nrand - 1] <= std::exp(-delta);
+    if (acc) {
+      c->rep2lab[ri] = lj - 1; c->rep2lab[rj] = li - 1;
+      c->lab2rep[li - 1] = rj; c->lab2rep[lj - 1] = ri;
+      double sf = std::sqrt(tn / tm);
+      scale[ri] = sf;
+      scale[rj] = -sf;
+      nacc++;
+    }
+  }
+  c->idx_pair = (c->idx_pair == 2) ? 1 : c->idx_pair + 1;
+  // simu_para2: beta_hbond15 of the last replica's label
+  c->beta_global = 1.0e0 / (c->lab_T[c->rep2lab[n - 1]] * BOLTZ_KCAL_MOL);
+  CK(cudaMemcpyAsync(c->scale.p, scale.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(scale_velo_launch(n, c->stream, c->velo.p, c->d_lanes.p, c->d_tops.p, c->scale.p));
+  std::vector<LaneState> ls(n);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, n * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int r = 0; r < n; ++r) ls[r].label = c->rep2lab[r];
+  CK(cudaMemcpyAsync(c->d_lstate.p, ls.data(), n * sizeof(LaneState), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (n_accept) *n_accept = nacc;
+  return TIS_OK;
+}
+
+extern "C" int tis_get_labels(tis_ctx *c, int32_t *rep2lab) {
+  if (!c || !rep2lab) return TIS_E_ARG;
+  for (int r = 0; r < c->nlane; ++r) rep2lab[r] = c->rep2lab[r] + 1;
+  return TIS_OK;
+}
+
+extern "C" int tis_status(tis_ctx *c, tis_status_t *st) {
+  if (!c || !st) return TIS_E_ARG;
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpy(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost));
+  std::memset(st, 0, sizeof(*st));
+  st->step = ls[0].istep;
+  for (int i = 0; i < c->nlane; ++i) {
+    st->n_rebuild += ls[i].nrebuild;
+    st->n_clamp += ls[i].nclamp;
+    st->list_overflow |= (ls[i].flags & LF_OVERFLOW) ? 1 : 0;
+    st->nan_seen |= (ls[i].flags & LF_NAN) ? 1 : 0;
+    st->exv_pairs_max = std::max(st->exv_pairs_max, ls[i].nexv);
+    st->ele_pairs_max = std::max(st->ele_pairs_max, ls[i].nele);
+  }
+  st->wait_timeout = c->wait_timeout;
+  st->not_spd = c->not_spd;
+  st->last_error = c->last_error;
+  return TIS_OK;
+}
+
+extern "C" double tis_last_step_ms(tis_ctx *c) { return c ? c->last_ms : -1.0; }
+
+extern "C" int tis_timer(tis_ctx *c, int32_t op, double *ms) {
+  if (!c) return TIS_E_ARG;
+  if (!c->tev0) { CK(cudaEventCreate(&c->tev0)); CK(cudaEventCreate(&c->tev1)); }
+  if (op == 0) { CK(cudaEventRecord(c->tev0, c->stream)); return TIS_OK; }
+  if (op != 1 || !ms) return TIS_E_ARG;
+  CK(cudaEventRecord(c->tev1, c->stream));
+  CK(cudaEventSynchronize(c->tev1));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, c->tev0, c->tev1));
+  *ms = f;
+  return TIS_OK;
+}
+
+extern "C" const char *tis_last_error(const tis_ctx *c) { return c ? c->err.c_str() : "null context"; }

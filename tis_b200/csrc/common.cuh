@@ -1,0 +1,183 @@
+// common.cuh -- device-side data layout shared by the lane kernels and the
+// host API of libtis_b200.so.
+//
+// A *lane* is one system replica (one CTA of the persistent kernel).  Lanes
+// point at a *topology* (interaction tables shared by the replicas of one
+// chain) and at a *label* (temperature-dependent parameters; labels are
+// swapped between lanes by replica exchange).  All per-bead state is FP64,
+// Fortran order (xyz fastest): x[3*(state0 + i) + d].
+#pragma once
+#include <cstdint>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#endif
+
+namespace tis {
+
+constexpr int MAX_THREADS = 512;
+constexpr int N_ETYPE = 25;   // E_TYPE%MAX
+
+// per-topology descriptor (offsets into the concatenated topology arrays)
+struct TopDesc {
+  int nmp, nunit;
+  int bead0;        // per-bead topology arrays
+  int unit0;        // lunit2mp / iclass_unit (2 ints per unit) and rneigh2 (nunit^2 doubles at rn0)
+  int rn0;
+  int bd0, nbd;
+  int ba0, nba;
+  int st0, nst;
+  int hb0, nhb;
+  int site0, nsite;
+  int sitehb0;      // CSR of hbonds per site: site_ptr[site0 + s] .. (+1), entries at sitehb0
+  int inc0;         // incidence CSR: inc_ptr[inc0 + i] (nmp + 1 entries)
+  int nslot;        // 2 nbd + 3 nba + 7 nst + 6 nhb
+  int slot_ba, slot_st, slot_hb;   // slot bases inside a lane (bonds start at 0)
+  int nlabel;       // labels that belong to this topology
+};
+
+// per-lane descriptor
+struct LaneDesc {
+  int top;
+  int state0;       // bead offset of this lane's state
+  int nbr0;         // row slabs: nmp rows x (nmp - 1) entries (uint32)
+  int rowcnt0;      // nmp ints
+  int mask0;        // 2 masks x nmp x words (uint32), words = ceil(nmp / 32)
+  long long mirror0;// periodic: nmp x nmp bytes (canonical pair mirror index)
+  int slot0;        // slots x 3 values
+  int hb0;          // hb flags / status / energies (nhb each)
+  int site0;        // per-lane hbond-site excess counters (nsite ints)
+  int unif0;        // injected uniform stream (n_uniform per lane)
+};
+
+// Mutable per-lane scalar state, kept in global memory between launches.
+struct LaneState {
+  long long istep;
+  long long nrebuild;
+  long long nclamp;
+  int label;          // global label index
+  int unif_pos;
+  int flags;          // bit 0 list overflow, 1 nan, 2 uniforms exhausted, 3 noise exhausted
+  int nexv, nele;     // half-list sizes at the last rebuild
+  int need_rebuild;
+};
+
+enum LaneFlags { LF_OVERFLOW = 1, LF_NAN = 2, LF_UNIF_EXHAUSTED = 4, LF_NOISE_EXHAUSTED = 8 };
+
+enum KMode {
+  KM_NEIGHBOR = 1,     // rebuild lists (wrap pxyz if periodic)
+  KM_FORCE = 2,        // force_sumup -> out_force
+  KM_PRE = 3,          // time_integral_pre: lists, force, a(0)
+  KM_STEP = 4,         // nsteps of time_integral
+};
+
+// Kernel arguments (all device pointers).
+struct KArgs {
+  // sizes
+  int nlane;
+  int nsteps;
+  int mode;
+  int only_lane;       // -1: every lane
+  int group;           // threads per bead in the gather pass (power of two <= 32)
+  // constants
+  int periodic;
+  double psize[3], psizeh[3];
+  double neigh_margin;
+  int n_step_neighbor;
+  double exv_dist, exv_dist_PS, exv_adjust;
+  int nsep[3];         // P, S, B
+  int i_ele;           // 0 none, 1 DH
+  double cutoff_ele;
+  double hb_cutoff_dist;
+  double max_abscos;   // MAX_ANG_ABSCOS_HBOND15 == MAX_DIH_ABSCOS_HBOND15
+  double tstep, tstep2, tsteph;
+  double beta_hbond15; // global quirk value (used when hb_beta_global)
+  int hb_beta_global;
+  unsigned long long seed;
+  // descriptors
+  const TopDesc *tops;
+  const LaneDesc *lanes;
+  LaneState *lstate;
+  // topology arrays
+  const int8_t *b_type;    // MPTYPE
+  const int8_t *b_class;   // CLASS of the bead's unit
+  const int16_t *b_unit;   // unit index (local)
+  const double *b_rcmass, *b_fric, *b_radius, *b_eps, *b_charge;
+  const int *u_lunit;      // (first, last) 0-based per unit
+  const int *u_class;
+  const double *rneigh2;   // per topology nunit x nunit
+  const int *bd_idx; const double *bd_nat, *bd_coef;
+  const int *ba_idx; const double *ba_nat, *ba_coef;
+  const int *st_idx; const double *st_nat, *st_coef;
+  const int *hb_idx; const double *hb_nat, *hb_coef; const int *hb_site; const double *hb_nd2;
+  const int *site_val; const int *site_ptr; const int *site_hb;
+  const int *inc_ptr; const int *inc_slot;
+  // labels (temperature-dependent parameters)
+  const double *lab_T, *lab_coef, *lab_cdist, *lab_beta, *lab_rele2;
+  const int *lab_u0off; const double *lab_u0;   // stack U0(T) per label
+  const int *lab_c1off; const double *lab_c1;   // rlan_const(1) per label and bead
+  const double *b_c2, *b_c3, *b_c4;             // rlan_const(2..4) per bead
+  // state
+  double *xyz, *pxyz, *velo, *accel, *dxyz;
+  // lists and scratch
+  uint32_t *nbr; int *rowcnt; uint32_t *mask; uint8_t *mirror;
+  void *slots;             // float or double triplets
+  uint8_t *hb_flag;        // bit0 in neighbour list, bit1 status
+  double *hb_ene;
+  int *site_exc;
+  // energy evaluation (energy_kernel)
+  const int *elabel;       // per lane label override (-1: own label)
+  int reuse_hb;            // 1: sum the hbond energies of the last force pass (flg_hb_energy)
+  double ebeta;            // beta_hbond15 for a recomputed hbond pruning
+  const double *ebeta_lane;// per lane beta (overrides ebeta when set)
+  double *out_energy;      // (N_ETYPE) per lane
+  const double *b_cmass;
+  int i_DH_cutoff_type;
+  // io
+  double *out_force;       // (3, nmp) per lane at state0
+  const double *noise;     // injected: (3, nbead_total, noise_nsteps)
+  int noise_nsteps;
+  int noise_base;          // noise step consumed by the first step of this launch
+  const double *unif;      // injected uniforms per lane
+  int n_unif;
+  int nbead_total;
+};
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11): 10 rounds of the 4x32 S-box with the published
+// multipliers and Weyl key increments.
+struct U4 { uint32_t x, y, z, w; };
+
+__host__ __device__ inline void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {
+  uint64_t p = (uint64_t)a * (uint64_t)b;
+  hi = (uint32_t)(p >> 32);
+  lo = (uint32_t)p;
+}
+
+__host__ __device__ inline U4 philox4x32(U4 ctr, uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0, lo0, hi1, lo1;
+    mulhilo32(M0, ctr.x, hi0, lo0);
+    mulhilo32(M1, ctr.z, hi1, lo1);
+    U4 o;
+    o.x = hi1 ^ ctr.y ^ k0;
+    o.y = lo1;
+    o.z = hi0 ^ ctr.w ^ k1;
+    o.w = lo0;
+    ctr = o;
+    k0 += W0;
+    k1 += W1;
+  }
+  return ctr;
+}
+
+// uniform in (0, 1]: (u + 1) * 2^-32
+__host__ __device__ inline double u01_open0(uint32_t u) { return ((double)u + 1.0) * 2.3283064365386963e-10; }
+__host__ __device__ inline float u01f_open0(uint32_t u) { return ((float)(u >> 8) + 1.0f) * 5.9604645e-08f; }
+
+} // namespace tis

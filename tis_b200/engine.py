@@ -1,0 +1,181 @@
+"""Python mirror of the C-ABI (include/tis_b200.h) over ctypes.
+
+``Engine`` owns one ``tis_ctx``: a batch of replicas (lanes) of one or more
+topologies on cuda:0.  Method names follow the reference routines they
+replace (neighbor, force_sumup, energy_sumup, time_integral_pre,
+time_integral, replica exchange).  Every call goes through the in-tree
+``libtis_b200.so``; a missing library raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .abi import (ETYPE_MAX, Params, Status, Topology, load_library, make_params,
+                  make_topology, ptr_f64, ptr_i32)
+
+
+class TisError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tis error {code}: {msg}")
+        self.code = code
+
+
+class Engine:
+    def __init__(self, systems, par: dict, tempk, nrep=None):
+        """systems: list of topology dicts (tis_b200.synth); nrep[k] replicas of
+        systems[k] (default 1 each) with temperatures tempk (one per lane)."""
+        self.L = load_library()
+        if isinstance(systems, dict):
+            systems = [systems]
+        self.systems = list(systems)
+        if nrep is None:
+            nrep = [1] * len(self.systems) if len(self.systems) > 1 else [len(tempk)]
+        self.nrep = list(int(n) for n in nrep)
+        self.tempk = np.ascontiguousarray(np.asarray(tempk, dtype=np.float64))
+        assert sum(self.nrep) == len(self.tempk)
+        self._keep = []
+        tops = (Topology * len(self.systems))()
+        for k, s in enumerate(self.systems):
+            t, keep = make_topology(s)
+            tops[k] = t
+            self._keep.append(keep)
+        self._tops = tops
+        self._par = make_params(**par)
+        self.par = dict(par)
+        nr = np.ascontiguousarray(np.asarray(self.nrep, dtype=np.int32))
+        self._nr = nr
+        h = C.c_void_p()
+        rc = self.L.tis_init_batch(len(self.systems), tops, C.byref(self._par), ptr_i32(nr), ptr_f64(self.tempk),
+                                   C.byref(h))
+        if rc != 0 or not h.value:
+            raise TisError(rc, "tis_init_batch failed")
+        self.h = h
+        self.nlane = self.L.tis_nrep(self.h)
+        self.lane_nmp = [self.L.tis_nmp(self.h, i + 1) for i in range(self.nlane)]
+        self.nbead = int(sum(self.lane_nmp))
+        self.offsets = np.concatenate([[0], np.cumsum(self.lane_nmp)]).astype(int)
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.L.tis_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc < 0:
+            msg = self.L.tis_last_error(self.h)
+            raise TisError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    # state: arrays of shape (nbead_total, 3) with lanes concatenated
+    def set_state(self, xyz, velo=None, accel=None):
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(self.nbead, 3)
+        v = None if velo is None else np.ascontiguousarray(velo, dtype=np.float64).reshape(self.nbead, 3)
+        a = None if accel is None else np.ascontiguousarray(accel, dtype=np.float64).reshape(self.nbead, 3)
+        self._check(self.L.tis_set_state(self.h, ptr_f64(x), None if v is None else ptr_f64(v),
+                                         None if a is None else ptr_f64(a)), "set_state")
+
+    def get_state(self):
+        x, v, a = (np.zeros((self.nbead, 3)) for _ in range(3))
+        self._check(self.L.tis_get_state(self.h, ptr_f64(x), ptr_f64(v), ptr_f64(a)), "get_state")
+        return x, v, a
+
+    def get_pxyz(self):
+        p = np.zeros((self.nbead, 3))
+        self._check(self.L.tis_get_pxyz(self.h, ptr_f64(p)), "get_pxyz")
+        return p
+
+    def set_noise(self, noise=None, uniforms=None):
+        if noise is not None:
+            n = np.ascontiguousarray(noise, dtype=np.float64)
+            nsteps = n.shape[0]
+            np_ = ptr_f64(n)
+        else:
+            nsteps, np_ = 0, None
+        if uniforms is not None:
+            u = np.ascontiguousarray(uniforms, dtype=np.float64)
+            nu = u.shape[-1]
+            up = ptr_f64(u)
+        else:
+            nu, up = 0, None
+        self._keep_noise = (noise, uniforms)
+        self._check(self.L.tis_set_noise(self.h, np_, nsteps, up, nu), "set_noise")
+
+    def neighbor(self, irep=-1):
+        return self._check(self.L.tis_neighbor(self.h, irep), "neighbor")
+
+    def exv_list(self, irep=1):
+        n = C.c_int32(0)
+        self.L.tis_get_exv_list(self.h, irep, None, 0, C.byref(n))
+        out = np.zeros((max(n.value, 1), 3), dtype=np.int32)
+        self._check(self.L.tis_get_exv_list(self.h, irep, ptr_i32(out), n.value, C.byref(n)), "exv_list")
+        return out[:n.value]
+
+    def ele_list(self, irep=1):
+        n = C.c_int32(0)
+        self.L.tis_get_ele_list(self.h, irep, None, None, 0, C.byref(n))
+        out = np.zeros((max(n.value, 1), 4), dtype=np.int32)
+        coef = np.zeros(max(n.value, 1))
+        self._check(self.L.tis_get_ele_list(self.h, irep, ptr_i32(out), ptr_f64(coef), n.value, C.byref(n)), "ele_list")
+        return out[:n.value], coef[:n.value]
+
+    def hb_list(self, irep=1):
+        n = C.c_int32(0)
+        self.L.tis_get_hb_list(self.h, irep, None, 0, C.byref(n))
+        out = np.zeros(max(n.value, 1), dtype=np.int32)
+        self._check(self.L.tis_get_hb_list(self.h, irep, ptr_i32(out), n.value, C.byref(n)), "hb_list")
+        return out[:n.value]
+
+    def force(self, irep=1):
+        f = np.zeros((self.lane_nmp[irep - 1], 3))
+        rc = self._check(self.L.tis_force_sumup(self.h, irep, ptr_f64(f)), "force_sumup")
+        return f, rc
+
+    def energy(self, irep=1):
+        e = np.zeros(ETYPE_MAX)
+        self._check(self.L.tis_energy_sumup(self.h, irep, ptr_f64(e)), "energy_sumup")
+        return e
+
+    def time_integral_pre(self):
+        return self._check(self.L.tis_time_integral_pre(self.h), "time_integral_pre")
+
+    def step(self, n):
+        return self._check(self.L.tis_step(self.h, int(n)), "step")
+
+    def last_step_ms(self):
+        return self.L.tis_last_step_ms(self.h)
+
+    def timer_start(self):
+        self._check(self.L.tis_timer(self.h, 0, None), "timer")
+
+    def timer_stop(self) -> float:
+        ms = C.c_double(0.0)
+        self._check(self.L.tis_timer(self.h, 1, C.byref(ms)), "timer")
+        return ms.value
+
+    def replica_exchange(self, u=None):
+        na = C.c_int32(0)
+        up = None
+        if u is not None:
+            uu = np.ascontiguousarray(u, dtype=np.float64)
+            up = ptr_f64(uu)
+        self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na)), "replica_exchange")
+        return na.value
+
+    def labels(self):
+        out = np.zeros(self.nlane, dtype=np.int32)
+        self._check(self.L.tis_get_labels(self.h, ptr_i32(out)), "labels")
+        return out
+
+    def status(self):
+        st = Status()
+        self._check(self.L.tis_status(self.h, C.byref(st)), "status")
+        return {k: getattr(st, k) for k, _ in Status._fields_}
