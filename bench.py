@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--workload", default="c3", choices=["c3", "c4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--period", type=int, default=PERIOD, help="MD steps per bench step (exchange period)")
+    ap.add_argument("--quick", action="store_true",
+                    help="device timing only (no CPU leg, e2e or plain path): small profiling runs")
     return ap.parse_args()
 
 
@@ -199,8 +202,11 @@ def run_reference(args, rank, world):
 
 def run_ours(args, rank, world, local_rank):
     import numpy as np
-    pool = None
     cpu_line = None
+    period_len = args.period
+    if args.quick:
+        args.no_cpu_baseline = True
+        args.no_plain = True
     if rank == 0 and not args.no_cpu_baseline:
         # CPU leg first, in spawned processes, before this process touches the GPU
         import multiprocessing as mp
@@ -232,7 +238,7 @@ def run_ours(args, rank, world, local_rank):
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
 
     def period():
-        eng.step(PERIOD)
+        eng.step(period_len)
         if remd:
             eng.replica_exchange()
 
@@ -263,7 +269,7 @@ def run_ours(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    rs = nlane * PERIOD * args.steps * world
+    rs = nlane * period_len * args.steps * world
     value = rs / (total_ms * 1e-3)
 
     # e2e: host buffers through the C-ABI, copies inside the timed region
@@ -271,7 +277,7 @@ def run_ours(args, rank, world, local_rank):
     x, v, a = eng.get_state()
     xh.numpy()[:] = x; vh.numpy()[:] = v; ah.numpy()[:] = a
     e2e_ms = []
-    for _ in range(args.steps):
+    for _ in range(0 if args.quick else args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         eng.timer_start()
@@ -280,8 +286,8 @@ def run_ours(args, rank, world, local_rank):
         xo, vo, ao = eng.get_state()
         e2e_ms.append(eng.timer_stop())
         xh.numpy()[:] = xo; vh.numpy()[:] = vo; ah.numpy()[:] = ao
-    e2e_total = sum(e2e_ms)
-    if dist:
+    e2e_total = sum(e2e_ms) if e2e_ms else float("nan")
+    if dist and e2e_ms:
         t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
@@ -308,14 +314,14 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0:
         peak, src = peaks()
         kern_ms = statistics.mean(kern)
-        achieved = bytes_per_rs * nlane * PERIOD / (kern_ms * 1e-3) / 1e9
+        achieved = bytes_per_rs * nlane * period_len / (kern_ms * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 forces, f64 accumulation and state",
             "data": "synthetic (seeded random-walk DT15 chains, reference parameter tables)",
             "config": {"workload": desc, "replicas_per_gpu": nlane, "beads_per_replica": int(systems[0]["nmp"]),
-                       "md_steps_per_step": PERIOD, "l2": "flushed between timed steps (256 MiB write)",
+                       "md_steps_per_step": period_len, "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"replicas only, {nlane} lanes per GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,

@@ -20,8 +20,9 @@
 #include "common.cuh"
 
 namespace tis {
-size_t smem_bytes_host(int N, bool periodic, bool skin, int real_size, int nunit);
+size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_set_smem(bool mixed, int bytes);
+size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
 cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
@@ -96,17 +97,17 @@ struct tis_ctx {
   DBuf<LaneState> d_lstate;
   DBuf<int8_t> b_type, b_class;
   DBuf<int16_t> b_unit;
-  DBuf<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4;
+  DBuf<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4, b_screen;
   DBuf<int> u_lunit, u_class;
   DBuf<double> rneigh2;
-  DBuf<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot;
+  DBuf<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   DBuf<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   DBuf<double> lab_Td, lab_coef, lab_cdist, lab_beta, lab_rele2, lab_u0, lab_c1;
   DBuf<int> lab_u0off, lab_c1off, elabel;
   DBuf<double> xyz, pxyz, velo, accel, dxyz, out_force, out_energy, scale, ebeta;
   unsigned long long rex_counter = 0;
-  DBuf<uint32_t> nbr, mask;
-  DBuf<int> rowcnt, site_exc;
+  DBuf<uint32_t> mask;
+  DBuf<int> site_exc;
   DBuf<uint8_t> mirror, hb_flag;
   DBuf<double> hb_ene;
   DBuf<unsigned char> slots;
@@ -157,7 +158,16 @@ void append(std::vector<T> &dst, const T *src, size_t n) {
   if (n) dst.insert(dst.end(), src, src + n);
 }
 
-int choose_threads(int maxN) { return maxN <= 96 ? 128 : (maxN <= 200 ? 256 : 512); }
+int choose_threads(int maxN, bool mixed) {
+  const char *env = std::getenv("TIS_THREADS");
+  if (env) {
+    int t = std::atoi(env);
+    if (t >= 64 && t <= (mixed ? 1024 : 512) && t % 32 == 0) return t;
+  }
+  if (maxN <= 96) return 128;
+  if (maxN <= 160) return 256;
+  return 512;
+}
 
 int choose_group(int threads, int maxN) {
   const char *env = std::getenv("TIS_GROUP");
@@ -188,10 +198,10 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   // ---- topology tables
   std::vector<int8_t> b_type, b_class;
   std::vector<int16_t> b_unit;
-  std::vector<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4;
+  std::vector<double> b_rcmass, b_cmass, b_fric, b_radius, b_eps, b_charge, b_c2, b_c3, b_c4, b_screen;
   std::vector<int> u_lunit, u_class;
   std::vector<double> rneigh2;
-  std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot;
+  std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   std::vector<double> st_hsTm_all;
   int maxN = 0;
@@ -228,6 +238,13 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     }
     std::vector<double> q(t.nmp, 0.0);
     for (int i = 0; i < t.ncharge; ++i) q[t.icharge2mp[i] - 1] = t.coef_charge[i];
+    // charged beads in icharge order (neighbor_list_ele.F90:126,138 skip |q| < ZERO_JUDGE)
+    d.q0 = (int)q_bead.size();
+    for (int i = 0; i < t.ncharge; ++i) {
+      if (i > 0 && t.icharge2mp[i] <= t.icharge2mp[i - 1]) { tis_destroy(c); return TIS_E_ARG; }
+      if (std::fabs(t.coef_charge[i]) >= 1.0e-6) q_bead.push_back(t.icharge2mp[i] - 1);
+    }
+    d.nq = (int)q_bead.size() - d.q0;
     for (int i = 0; i < t.nmp; ++i) {
       b_type.push_back((int8_t)t.imp2type[i]);
       b_class.push_back((int8_t)t.iclass_unit[imp2unit[i]]);
@@ -245,6 +262,24 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       b_c2.push_back(u1 * u2);
       b_c3.push_back((0.5e0 * p.tstep) * u1);
       b_c4.push_back(p.tstep * u1);
+    }
+    // exv screen radius: the largest contact distance dij the bead can have
+    // (force_exv_dt15.F90:220-228): RNA-RNA pairs use exv_dist / exv_dist_PS,
+    // every other pair the sum of the two radii
+    {
+      double rmax_all = 0.0, rmax_non_rna = 0.0;
+      for (int i = 0; i < t.nmp; ++i) {
+        rmax_all = std::max(rmax_all, t.exv_radius[i]);
+        if (t.iclass_unit[imp2unit[i]] != TIS_CLASS_RNA) rmax_non_rna = std::max(rmax_non_rna, t.exv_radius[i]);
+      }
+      for (int i = 0; i < t.nmp; ++i) {
+        double sc;
+        if (t.iclass_unit[imp2unit[i]] == TIS_CLASS_RNA)
+          sc = std::max(std::max(p.exv_dist, p.exv_dist_PS), rmax_non_rna > 0 ? t.exv_radius[i] + rmax_non_rna : 0.0);
+        else
+          sc = t.exv_radius[i] + rmax_all;
+        b_screen.push_back(sc);
+      }
     }
     // mloop_neigh_dist.F90:28-149
     for (int u = 0; u < t.nunit; ++u)
@@ -308,12 +343,14 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     for (int b = 0; b < t.nhb; ++b)
       for (int q2 = 0; q2 < 6; ++q2) inc[t.idtrna_hb2mp[6 * b + q2] - 1].push_back(d.slot_hb + 6 * b + q2);
     int ip = (int)inc_slot.size();
+    const int ip0 = ip;
     for (int i = 0; i < t.nmp; ++i) {
       inc_ptr.push_back(ip);
       for (int sl : inc[i]) inc_slot.push_back(sl);
       ip += (int)inc[i].size();
     }
     inc_ptr.push_back(ip);
+    d.ninc = ip - ip0;
     c->tops.push_back(d);
   }
   // ---- lanes and labels
@@ -330,7 +367,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->label_top.resize(nlane);
   c->rep2lab.resize(nlane);
   c->lab2rep.resize(nlane);
-  size_t nbr_off = 0, rowcnt_off = 0, mask_off = 0, slot_off = 0;
+  size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0;
   int lane = 0;
@@ -365,8 +402,6 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       LaneDesc L{};
       L.top = k;
       L.state0 = state_off;
-      L.nbr0 = (int)nbr_off;
-      L.rowcnt0 = (int)rowcnt_off;
       L.mask0 = (int)mask_off;
       L.mirror0 = mirror_off;
       L.slot0 = (int)slot_off;
@@ -374,8 +409,6 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       L.site0 = site_off;
       L.unif0 = 0;
       state_off += N;
-      nbr_off += (size_t)N * (N > 1 ? N - 1 : 1);
-      rowcnt_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
       if (periodic) mirror_off += (long long)N * N;
       slot_off += d.nslot;
@@ -385,7 +418,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       c->lane_nmp.push_back(N);
     }
   }
-  if (nbr_off > 0x7fffffffULL || mask_off > 0x7fffffffULL || slot_off > 0x7fffffffULL) {
+  if (mask_off > 0x7fffffffULL || slot_off > 0x7fffffffULL) {
     tis_destroy(c);
     return TIS_E_ARG;
   }
@@ -393,11 +426,18 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->lab_T = lab_T;
   // the global beta_hbond15 is the value set for the last replica (simu_set_dtrna.F90:58)
   c->beta_global = lab_beta[nlane - 1];
-  c->threads = choose_threads(maxN);
+  c->threads = choose_threads(maxN, p.precision == TIS_PREC_MIXED);
   c->group = choose_group(c->threads, maxN);
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
   size_t smem = 0;
-  for (auto &d : c->tops) smem = std::max(smem, smem_bytes_host(d.nmp, periodic, skin, real_size, d.nunit));
+  for (auto &d : c->tops) {
+    // the per-lane base layout must fit one CTA's shared memory
+    if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit) + 64 > 227 * 1024) {
+      tis_destroy(c);
+      return TIS_E_UNSUPPORTED;
+    }
+    smem = std::max(smem, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit));
+  }
   c->smem = smem;
 
   // ---- device
@@ -413,7 +453,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->b_type.upload(b_type)); CK(c->b_class.upload(b_class)); CK(c->b_unit.upload(b_unit));
   CK(c->b_rcmass.upload(b_rcmass)); CK(c->b_cmass.upload(b_cmass)); CK(c->b_fric.upload(b_fric));
   CK(c->b_radius.upload(b_radius)); CK(c->b_eps.upload(b_eps)); CK(c->b_charge.upload(b_charge));
-  CK(c->b_c2.upload(b_c2)); CK(c->b_c3.upload(b_c3)); CK(c->b_c4.upload(b_c4));
+  CK(c->b_c2.upload(b_c2)); CK(c->b_c3.upload(b_c3)); CK(c->b_c4.upload(b_c4)); CK(c->b_screen.upload(b_screen));
   CK(c->u_lunit.upload(u_lunit)); CK(c->u_class.upload(u_class)); CK(c->rneigh2.upload(rneigh2));
   CK(c->bd_idx.upload(bd_idx)); CK(c->bd_nat.upload(bd_nat)); CK(c->bd_coef.upload(bd_coef));
   CK(c->ba_idx.upload(ba_idx)); CK(c->ba_nat.upload(ba_nat)); CK(c->ba_coef.upload(ba_coef));
@@ -421,7 +461,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->hb_idx.upload(hb_idx)); CK(c->hb_nat.upload(hb_nat)); CK(c->hb_coef.upload(hb_coef));
   CK(c->hb_site.upload(hb_site)); CK(c->hb_nd2.upload(hb_nd2));
   CK(c->site_val.upload(site_val)); CK(c->site_ptr.upload(site_ptr)); CK(c->site_hb.upload(site_hb));
-  CK(c->inc_ptr.upload(inc_ptr)); CK(c->inc_slot.upload(inc_slot));
+  CK(c->inc_ptr.upload(inc_ptr)); CK(c->inc_slot.upload(inc_slot)); CK(c->q_bead.upload(q_bead));
   CK(c->lab_Td.upload(lab_T)); CK(c->lab_coef.upload(lab_coef)); CK(c->lab_cdist.upload(lab_cdist));
   CK(c->lab_beta.upload(lab_beta)); CK(c->lab_rele2.upload(lab_rele2));
   CK(c->lab_u0off.upload(lab_u0off)); CK(c->lab_u0.upload(lab_u0));
@@ -436,8 +476,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->scale.alloc(nlane));
   CK(c->ebeta.alloc(nlane));
   CK(c->elabel.alloc(nlane));
-  CK(c->nbr.alloc(nbr_off)); CK(c->rowcnt.alloc(rowcnt_off)); CK(c->mask.alloc(mask_off));
-  CK(cudaMemset(c->rowcnt.p, 0, std::max<size_t>(rowcnt_off, 1) * sizeof(int)));
+  CK(c->mask.alloc(mask_off));
+  CK(cudaMemset(c->mask.p, 0, std::max<size_t>(mask_off, 1) * sizeof(uint32_t)));
   CK(c->mirror.alloc(periodic ? (size_t)mirror_off : 1));
   CK(c->slots.alloc(slot_off * 3 * real_size));
   CK(c->hb_flag.alloc(hb_off)); CK(c->hb_ene.alloc(hb_off)); CK(c->site_exc.alloc(site_off));
@@ -460,10 +500,11 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->d_tops.free(); c->d_lanes.free(); c->d_lstate.free();
   c->b_type.free(); c->b_class.free(); c->b_unit.free();
   c->b_rcmass.free(); c->b_cmass.free(); c->b_fric.free(); c->b_radius.free(); c->b_eps.free(); c->b_charge.free();
-  c->b_c2.free(); c->b_c3.free(); c->b_c4.free();
+  c->b_c2.free(); c->b_c3.free(); c->b_c4.free(); c->b_screen.free();
   c->u_lunit.free(); c->u_class.free(); c->rneigh2.free();
   c->bd_idx.free(); c->ba_idx.free(); c->st_idx.free(); c->hb_idx.free(); c->hb_site.free();
   c->site_val.free(); c->site_ptr.free(); c->site_hb.free(); c->inc_ptr.free(); c->inc_slot.free();
+  c->q_bead.free();
   c->bd_nat.free(); c->bd_coef.free(); c->ba_nat.free(); c->ba_coef.free(); c->st_nat.free(); c->st_coef.free();
   c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free();
   c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
@@ -471,7 +512,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->ebeta.free();
   c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
-  c->nbr.free(); c->mask.free(); c->rowcnt.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
+  c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
   c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -563,7 +604,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   for (int d = 0; d < 3; ++d) { a.psize[d] = p.psize[d]; a.psizeh[d] = p.psize[d] / 2.0; }
   a.neigh_margin = p.neigh_margin;
   a.n_step_neighbor = p.n_step_neighbor;
-  a.exv_dist = p.exv_dist; a.exv_dist_PS = p.exv_dist_PS; a.exv_adjust = p.exv_adjust;
+  a.exv_dist = p.exv_dist; a.exv_dist_PS = p.exv_dist_PS; a.exv_adjust = p.exv_adjust; a.exv_inf = p.exv_inf;
   a.nsep[0] = p.n_sep_nlocal_P; a.nsep[1] = p.n_sep_nlocal_S; a.nsep[2] = p.n_sep_nlocal_B;
   a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : 0;
   a.cutoff_ele = p.cutoff_ele;
@@ -577,7 +618,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.tops = c->d_tops.p; a.lanes = c->d_lanes.p; a.lstate = c->d_lstate.p;
   a.b_type = c->b_type.p; a.b_class = c->b_class.p; a.b_unit = c->b_unit.p;
   a.b_rcmass = c->b_rcmass.p; a.b_cmass = c->b_cmass.p; a.b_fric = c->b_fric.p; a.b_radius = c->b_radius.p;
-  a.b_eps = c->b_eps.p; a.b_charge = c->b_charge.p;
+  a.b_eps = c->b_eps.p; a.b_charge = c->b_charge.p; a.b_screen = c->b_screen.p;
   a.u_lunit = c->u_lunit.p; a.u_class = c->u_class.p; a.rneigh2 = c->rneigh2.p;
   a.bd_idx = c->bd_idx.p; a.bd_nat = c->bd_nat.p; a.bd_coef = c->bd_coef.p;
   a.ba_idx = c->ba_idx.p; a.ba_nat = c->ba_nat.p; a.ba_coef = c->ba_coef.p;
@@ -585,13 +626,14 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.hb_idx = c->hb_idx.p; a.hb_nat = c->hb_nat.p; a.hb_coef = c->hb_coef.p; a.hb_site = c->hb_site.p;
   a.hb_nd2 = c->hb_nd2.p;
   a.site_val = c->site_val.p; a.site_ptr = c->site_ptr.p; a.site_hb = c->site_hb.p;
-  a.inc_ptr = c->inc_ptr.p; a.inc_slot = c->inc_slot.p;
+  a.inc_ptr = c->inc_ptr.p; a.inc_slot = c->inc_slot.p; a.q_bead = c->q_bead.p;
   a.lab_T = c->lab_Td.p; a.lab_coef = c->lab_coef.p; a.lab_cdist = c->lab_cdist.p; a.lab_beta = c->lab_beta.p;
   a.lab_rele2 = c->lab_rele2.p; a.lab_u0off = c->lab_u0off.p; a.lab_u0 = c->lab_u0.p;
   a.lab_c1off = c->lab_c1off.p; a.lab_c1 = c->lab_c1.p;
   a.b_c2 = c->b_c2.p; a.b_c3 = c->b_c3.p; a.b_c4 = c->b_c4.p;
   a.xyz = c->xyz.p; a.pxyz = c->pxyz.p; a.velo = c->velo.p; a.accel = c->accel.p; a.dxyz = c->dxyz.p;
-  a.nbr = c->nbr.p; a.rowcnt = c->rowcnt.p; a.mask = c->mask.p; a.mirror = c->mirror.p;
+  a.mask = c->mask.p; a.mirror = c->mirror.p;
+  a.smem_total = (int)c->smem;
   a.slots = c->slots.p; a.hb_flag = c->hb_flag.p; a.hb_ene = c->hb_ene.p; a.site_exc = c->site_exc.p;
   a.elabel = nullptr; a.reuse_hb = 0; a.ebeta = c->beta_global; a.out_energy = c->out_energy.p;
   a.out_force = c->out_force.p;
@@ -639,36 +681,36 @@ extern "C" int tis_neighbor(tis_ctx *c, int32_t irep) {
 }
 
 namespace {
-int fetch_rows(tis_ctx *c, int lane, std::vector<uint32_t> &rows, std::vector<int> &cnt) {
+// Copies the lane's list bit matrices (and mirror indices) back.
+int fetch_masks(tis_ctx *c, int lane, std::vector<uint32_t> &m, std::vector<uint8_t> &mir) {
   const LaneDesc &L = c->lanes[lane];
-  const int N = c->lane_nmp[lane];
-  const int rl = N > 1 ? N - 1 : 1;
-  rows.resize((size_t)N * rl);
-  cnt.resize(N);
-  CK(cudaMemcpy(rows.data(), c->nbr.p + L.nbr0, rows.size() * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(cnt.data(), c->rowcnt.p + L.rowcnt0, cnt.size() * 4, cudaMemcpyDeviceToHost));
+  const int N = c->lane_nmp[lane], W = (N + 31) / 32;
+  m.resize(2 * (size_t)N * W);
+  CK(cudaMemcpy(m.data(), c->mask.p + L.mask0, m.size() * 4, cudaMemcpyDeviceToHost));
+  if (c->par.i_periodic == 1) {
+    mir.resize((size_t)N * N);
+    CK(cudaMemcpy(mir.data(), c->mirror.p + L.mirror0, mir.size(), cudaMemcpyDeviceToHost));
+  }
   return TIS_OK;
 }
 }  // namespace
 
 extern "C" int tis_get_exv_list(tis_ctx *c, int32_t irep, int32_t *iexv2mp, int32_t cap, int32_t *n) {
   if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
-  std::vector<uint32_t> rows;
-  std::vector<int> cnt;
-  int rc = fetch_rows(c, irep - 1, rows, cnt);
+  std::vector<uint32_t> m;
+  std::vector<uint8_t> mir;
+  int rc = fetch_masks(c, irep - 1, m, mir);
   if (rc < 0) return rc;
-  const int N = c->lane_nmp[irep - 1], rl = N > 1 ? N - 1 : 1;
+  const int N = c->lane_nmp[irep - 1], W = (N + 31) / 32;
   const bool peri = c->par.i_periodic == 1;
   int k = 0;
   for (int i = 0; i < N; ++i)
-    for (int e = 0; e < cnt[i]; ++e) {
-      uint32_t ent = rows[(size_t)i * rl + e];
-      int j = ent & 0xFFFF;
-      if (j <= i || !(ent & (1u << 16))) continue;
+    for (int j = i + 1; j < N; ++j) {
+      if (!(m[(size_t)i * W + (j >> 5)] >> (j & 31) & 1u)) continue;
       if (k < cap && iexv2mp) {
         iexv2mp[3 * k] = i + 1;
         iexv2mp[3 * k + 1] = j + 1;
-        iexv2mp[3 * k + 2] = peri ? (int)(ent >> 18) : 1;
+        iexv2mp[3 * k + 2] = peri ? (int)mir[(size_t)i * N + j] : 1;
       }
       ++k;
     }
@@ -678,15 +720,16 @@ extern "C" int tis_get_exv_list(tis_ctx *c, int32_t irep, int32_t *iexv2mp, int3
 
 extern "C" int tis_get_ele_list(tis_ctx *c, int32_t irep, int32_t *iele2mp, double *coef_ele, int32_t cap, int32_t *n) {
   if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
-  std::vector<uint32_t> rows;
-  std::vector<int> cnt;
-  int rc = fetch_rows(c, irep - 1, rows, cnt);
-  if (rc < 0) return rc;
+  std::vector<uint32_t> m;
+  std::vector<uint8_t> mir;
   const int lane = irep - 1;
-  const int N = c->lane_nmp[lane], rl = N > 1 ? N - 1 : 1;
-  const bool peri = c->par.i_periodic == 1;
-  std::vector<double> q(N);
+  int rc = fetch_masks(c, lane, m, mir);
+  if (rc < 0) return rc;
   const TopDesc &T = c->tops[c->lanes[lane].top];
+  const int N = T.nmp, W = (N + 31) / 32;
+  const bool peri = c->par.i_periodic == 1;
+  const uint32_t *mele = m.data() + (size_t)N * W;
+  std::vector<double> q(N);
   CK(cudaMemcpy(q.data(), c->b_charge.p + T.bead0, N * sizeof(double), cudaMemcpyDeviceToHost));
   std::vector<LaneState> ls(1);
   CK(cudaMemcpy(ls.data(), c->d_lstate.p + lane, sizeof(LaneState), cudaMemcpyDeviceToHost));
@@ -694,15 +737,13 @@ extern "C" int tis_get_ele_list(tis_ctx *c, int32_t irep, int32_t *iele2mp, doub
   CK(cudaMemcpy(&coefT, c->lab_coef.p + ls[0].label, sizeof(double), cudaMemcpyDeviceToHost));
   int k = 0;
   for (int i = 0; i < N; ++i)
-    for (int e = 0; e < cnt[i]; ++e) {
-      uint32_t ent = rows[(size_t)i * rl + e];
-      int j = ent & 0xFFFF;
-      if (j <= i || !(ent & (1u << 17))) continue;
+    for (int j = i + 1; j < N; ++j) {
+      if (!(mele[(size_t)i * W + (j >> 5)] >> (j & 31) & 1u)) continue;
       if (k < cap) {
         if (iele2mp) {
           iele2mp[4 * k] = i + 1;
           iele2mp[4 * k + 1] = j + 1;
-          iele2mp[4 * k + 2] = peri ? (int)(ent >> 18) : 1;
+          iele2mp[4 * k + 2] = peri ? (int)mir[(size_t)i * N + j] : 1;
           iele2mp[4 * k + 3] = 0;
         }
         if (coef_ele) coef_ele[k] = q[i] * q[j] * coefT;

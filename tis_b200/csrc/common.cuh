@@ -16,7 +16,7 @@
 
 namespace tis {
 
-constexpr int MAX_THREADS = 512;
+constexpr int MAX_THREADS = 1024;
 constexpr int N_ETYPE = 25;   // E_TYPE%MAX
 
 // per-topology descriptor (offsets into the concatenated topology arrays)
@@ -31,7 +31,9 @@ struct TopDesc {
   int hb0, nhb;
   int site0, nsite;
   int sitehb0;      // CSR of hbonds per site: site_ptr[site0 + s] .. (+1), entries at sitehb0
-  int inc0;         // incidence CSR: inc_ptr[inc0 + i] (nmp + 1 entries)
+  int inc0;         // incidence CSR: inc_ptr[inc0 + i] (nmp + 1 entries), values index inc_slot
+  int ninc;         // incidence entries of this topology
+  int q0, nq;       // charged beads (|q| >= ZERO_JUDGE), bead indices at q_bead[q0 ..], ascending
   int nslot;        // 2 nbd + 3 nba + 7 nst + 6 nhb
   int slot_ba, slot_st, slot_hb;   // slot bases inside a lane (bonds start at 0)
   int nlabel;       // labels that belong to this topology
@@ -41,9 +43,7 @@ struct TopDesc {
 struct LaneDesc {
   int top;
   int state0;       // bead offset of this lane's state
-  int nbr0;         // row slabs: nmp rows x (nmp - 1) entries (uint32)
-  int rowcnt0;      // nmp ints
-  int mask0;        // 2 masks x nmp x words (uint32), words = ceil(nmp / 32)
+  int mask0;        // list bit matrices: exv then ele, nmp rows of ceil(nmp / 32) words
   long long mirror0;// periodic: nmp x nmp bytes (canonical pair mirror index)
   int slot0;        // slots x 3 values
   int hb0;          // hb flags / status / energies (nhb each)
@@ -85,7 +85,7 @@ struct KArgs {
   double psize[3], psizeh[3];
   double neigh_margin;
   int n_step_neighbor;
-  double exv_dist, exv_dist_PS, exv_adjust;
+  double exv_dist, exv_dist_PS, exv_adjust, exv_inf;
   int nsep[3];         // P, S, B
   int i_ele;           // 0 none, 1 DH
   double cutoff_ele;
@@ -104,6 +104,7 @@ struct KArgs {
   const int8_t *b_class;   // CLASS of the bead's unit
   const int16_t *b_unit;   // unit index (local)
   const double *b_rcmass, *b_fric, *b_radius, *b_eps, *b_charge;
+  const double *b_screen;  // largest exv contact distance of the bead with any bead of its topology
   const int *u_lunit;      // (first, last) 0-based per unit
   const int *u_class;
   const double *rneigh2;   // per topology nunit x nunit
@@ -113,6 +114,7 @@ struct KArgs {
   const int *hb_idx; const double *hb_nat, *hb_coef; const int *hb_site; const double *hb_nd2;
   const int *site_val; const int *site_ptr; const int *site_hb;
   const int *inc_ptr; const int *inc_slot;
+  const int *q_bead;
   // labels (temperature-dependent parameters)
   const double *lab_T, *lab_coef, *lab_cdist, *lab_beta, *lab_rele2;
   const int *lab_u0off; const double *lab_u0;   // stack U0(T) per label
@@ -121,7 +123,8 @@ struct KArgs {
   // state
   double *xyz, *pxyz, *velo, *accel, *dxyz;
   // lists and scratch
-  uint32_t *nbr; int *rowcnt; uint32_t *mask; uint8_t *mirror;
+  uint32_t *mask; uint8_t *mirror;
+  int smem_total;          // dynamic shared memory bytes of the launch
   void *slots;             // float or double triplets
   uint8_t *hb_flag;        // bit0 in neighbour list, bit1 status
   double *hb_ene;

@@ -1,0 +1,264 @@
+// energy_kernel.cu -- energy_sumup on the device and the replica-exchange
+// velocity rescale.
+#include "device_common.cuh"
+
+// =====================================================================
+// energy_sumup (src/energy_sumup.F90:11-530) for one lane per CTA, FP64.
+// Terms follow the energy twins: energy_bond, energy_bangle (via
+// util_bondangle), energy_dtrna_stack, energy_dtrna_hbond15, energy_exv_dt15,
+// energy_ele_DH and energy_kinetic.  Sums are reduced in a fixed order.
+// =====================================================================
+namespace tis {
+
+__device__ __forceinline__ double3 gpos(const double *x, int idx) {
+  return make_double3(x[3 * (size_t)idx], x[3 * (size_t)idx + 1], x[3 * (size_t)idx + 2]);
+}
+__device__ __forceinline__ double3 sub3(double3 a, double3 b) { return make_double3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ double dot3(double3 a, double3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ double3 cross3(double3 a, double3 b) {
+  return make_double3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double wrapd(double d) {
+  const double PI = 3.14159265358979323846;
+  if (d > PI) d -= 2.0 * PI; else if (d < -PI) d += 2.0 * PI;
+  return d;
+}
+
+enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_N };
+
+__global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
+  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
+  if (lane >= a.nlane) return;
+  const LaneDesc L = a.lanes[lane];
+  const TopDesc T = a.tops[L.top];
+  const int N = T.nmp;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  LaneState &st = a.lstate[lane];
+  const int label = (a.elabel && a.elabel[lane] >= 0) ? a.elabel[lane] : st.label;
+  const double *X = a.xyz + 3 * (size_t)L.state0;
+  const double *P = a.pxyz + 3 * (size_t)L.state0;
+  const double *V = a.velo + 3 * (size_t)L.state0;
+  __shared__ double red[ES_N][8];
+  __shared__ int excess_flag;
+  double es[ES_N];
+  for (int k = 0; k < ES_N; ++k) es[k] = 0.0;
+  if (tid == 0) excess_flag = 0;
+  int *exc = a.site_exc + L.site0;
+  uint8_t *hbf = a.hb_flag + L.hb0;
+  double *hbe = a.hb_ene + L.hb0;
+  if (!a.reuse_hb) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+  __syncthreads();
+  // kinetic
+  for (int i = tid; i < N; i += nth) {
+    double3 v = gpos(V, i);
+    es[ES_VELO] += 0.5 * a.b_cmass[T.bead0 + i] * (v.x * v.x + v.y * v.y + v.z * v.z);
+  }
+  for (int k = tid; k < T.nbd; k += nth) {
+    const int *m = a.bd_idx + 2 * (size_t)(T.bd0 + k);
+    double3 v = sub3(gpos(X, m[1]), gpos(X, m[0]));
+    double dd = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) - a.bd_nat[T.bd0 + k];
+    es[ES_BOND] += a.bd_coef[T.bd0 + k] * (dd * dd);
+  }
+  for (int k = tid; k < T.nba; k += nth) {
+    const int *m = a.ba_idx + 3 * (size_t)(T.ba0 + k);
+    double3 v21 = sub3(gpos(X, m[1]), gpos(X, m[0])), v32 = sub3(gpos(X, m[2]), gpos(X, m[1]));
+    double c11 = dot3(v21, v21), c22 = dot3(v32, v32), c21 = dot3(v32, v21);
+    double co = -c21 / sqrt(c11 * c22);
+    if (co > 1.0) co = 1.0; else if (co < -1.0) co = -1.0;
+    double dba = acos(co) - a.ba_nat[T.ba0 + k];
+    es[ES_ANGLE] += a.ba_coef[T.ba0 + k] * (dba * dba);
+  }
+  const double *u0 = a.lab_u0 + a.lab_u0off[label];
+  for (int k = tid; k < T.nst; k += nth) {
+    const int *m = a.st_idx + 7 * (size_t)(T.st0 + k);
+    const double *nat = a.st_nat + 3 * (size_t)(T.st0 + k);
+    const double *cf = a.st_coef + 3 * (size_t)(T.st0 + k);
+    double3 v21 = sub3(gpos(X, m[1]), gpos(X, m[0])), v34 = sub3(gpos(X, m[2]), gpos(X, m[3]));
+    double3 v54 = sub3(gpos(X, m[4]), gpos(X, m[3])), v56 = sub3(gpos(X, m[4]), gpos(X, m[5]));
+    double3 v76 = sub3(gpos(X, m[6]), gpos(X, m[5]));
+    double ediv = 1.0;
+    double dd = sqrt(dot3(v21, v21)) - nat[0];
+    ediv += cf[0] * dd * dd;
+    double3 mm = cross3(v34, v54), nn = cross3(v54, v56);
+    double d = wrapd(atan2(dot3(v34, nn) * sqrt(dot3(v54, v54)), dot3(mm, nn)) - nat[1]);
+    ediv += cf[1] * d * d;
+    mm = cross3(v76, v56);
+    nn = make_double3(-nn.x, -nn.y, -nn.z);
+    d = wrapd(atan2(dot3(v76, nn) * sqrt(dot3(v56, v56)), dot3(mm, nn)) - nat[2]);
+    ediv += cf[2] * d * d;
+    es[ES_STACK] += u0[k] / ediv;
+  }
+  // non-bonded pairs j > i from the global copy of the list bit matrices
+  const int W = (N + 31) >> 5;
+  const uint32_t *mexv = a.mask + L.mask0, *mele = mexv + (size_t)N * W;
+  const uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
+  const double cdist = a.lab_cdist[label], coefT = a.lab_coef[label];
+  const double cut2 = (a.i_DH_cutoff_type == 0) ? (a.cutoff_ele * cdist) * (a.cutoff_ele * cdist)
+                                                : a.cutoff_ele * a.cutoff_ele;
+  const double rcd = 1.0 / cdist;
+  auto shifted = [&](int i, int j) {   // j > i: canonical orientation
+    double3 w = sub3(gpos(P, j), gpos(P, i));
+    if (mir) {
+      const int im = (int)mir[(size_t)i * N + j] - 1;
+      const int m0 = im / 9, m1 = (im / 3) % 3, m2 = im % 3;
+      if (m0 != 2) w.x += (m0 == 0 ? -a.psize[0] : a.psize[0]);
+      if (m1 != 2) w.y += (m1 == 0 ? -a.psize[1] : a.psize[1]);
+      if (m2 != 2) w.z += (m2 == 0 ? -a.psize[2] : a.psize[2]);
+    }
+    return w;
+  };
+  for (int i = tid; i < N; i += nth) {
+    const int ti = a.b_type[T.bead0 + i], ci = a.b_class[T.bead0 + i];
+    const bool qi = fabs(a.b_charge[T.bead0 + i]) >= 1.0e-6;
+    for (int w = (i + 1) >> 5; w < W; ++w) {
+      uint32_t me = mexv[(size_t)i * W + w], ml = (a.i_ele == 1 && qi) ? mele[(size_t)i * W + w] : 0u;
+      if (w == ((i + 1) >> 5)) {   // keep bits j > i only
+        const uint32_t keep = ((i + 1) & 31) ? ~((1u << ((i + 1) & 31)) - 1u) : 0xffffffffu;
+        me &= keep; ml &= keep;
+      }
+      while (me) {
+        const int j = (w << 5) + __ffs(me) - 1;
+        me &= me - 1;
+        const double3 v = shifted(i, j);
+        const int tj = a.b_type[T.bead0 + j], cj = a.b_class[T.bead0 + j];
+        double dij;
+        if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = a.exv_dist_PS;
+        else if (ci == 2 && cj == 2) dij = a.exv_dist;
+        else dij = a.b_radius[T.bead0 + i] + a.b_radius[T.bead0 + j];
+        double dist = sqrt(dot3(v, v));
+        if (dist <= dij) {
+          dist = dist + a.exv_adjust - dij;
+          double ene;
+          if (dist > a.exv_inf) {
+            double ro = a.exv_adjust / dist, ro2 = ro * ro, ro6 = ro2 * ro2 * ro2;
+            ene = a.b_eps[T.bead0 + i] * a.b_eps[T.bead0 + j] * (ro6 * ro6 - 2 * ro6 + 1.0);
+          } else {
+            ene = 1.0e10;   // HIGH_ENERGY
+          }
+          es[ES_EXV] += ene;
+        }
+      }
+      while (ml) {
+        const int j = (w << 5) + __ffs(ml) - 1;
+        ml &= ml - 1;
+        const double3 v = shifted(i, j);
+        const double r2 = dot3(v, v);
+        if (r2 <= cut2) {
+          const double dist1 = sqrt(r2);
+          const double ce = a.b_charge[T.bead0 + i] * a.b_charge[T.bead0 + j] * coefT;
+          es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
+        }
+      }
+    }
+  }
+  // hydrogen bonds (energy_dtrna_hbond15.F90)
+  if (!a.reuse_hb) {
+    for (int h = tid; h < T.nhb; h += nth) {
+      uint8_t f = hbf[h] & 1;
+      hbe[h] = 0.0;
+      if (f) {
+        const int *m = a.hb_idx + 6 * (size_t)(T.hb0 + h);
+        const double *nat = a.hb_nat + 6 * (size_t)(T.hb0 + h);
+        const double *cf = a.hb_coef + 7 * (size_t)(T.hb0 + h);
+        auto dv = [&](int p, int q) {
+          double3 u = sub3(gpos(a.periodic ? P : X, m[p]), gpos(a.periodic ? P : X, m[q]));
+          if (a.periodic) { pb1(u.x, a.psize[0], a.psizeh[0]); pb1(u.y, a.psize[1], a.psizeh[1]); pb1(u.z, a.psize[2], a.psizeh[2]); }
+          return u;
+        };
+        double3 v12 = dv(0, 1);
+        double a12 = sqrt(dot3(v12, v12));
+        double d = a12 - nat[0];
+        if (fabs(d) <= a.hb_cutoff_dist) {
+          f |= 2;
+          const int *sites = a.hb_site + 6 * (size_t)(T.hb0 + h);
+          for (int q = 0; q < 6; ++q)
+            if (sites[q] >= 0) {
+              int old = atomicAdd(&exc[sites[q]], 1);
+              if (old + 1 > a.site_val[T.site0 + sites[q]]) excess_flag = 1;
+            }
+          double ex = -cf[1] * d * d;
+          double3 v13 = dv(0, 2), v53 = dv(4, 2), v42 = dv(3, 1), v46 = dv(3, 5);
+          double a13 = sqrt(dot3(v13, v13)), a42 = sqrt(dot3(v42, v42));
+          double d1213 = dot3(v13, v12), d1242 = dot3(v12, v42);
+          d = acos(d1213 / (a13 * a12)) - nat[1];
+          ex -= cf[2] * d * d;
+          d = acos(d1242 / (a12 * a42)) - nat[2];
+          ex -= cf[3] * d * d;
+          double3 c4212 = cross3(v42, v12), c1213 = cross3(v12, v13);
+          d = wrapd(atan2(dot3(v42, c1213) * a12, dot3(c4212, c1213)) - nat[3]);
+          ex -= cf[4] * d * d;
+          double3 mm = cross3(v53, v13), n = make_double3(-c1213.x, -c1213.y, -c1213.z);
+          d = wrapd(atan2(dot3(v53, n) * a13, dot3(mm, n)) - nat[4]);
+          ex -= cf[5] * d * d;
+          mm = make_double3(-c4212.x, -c4212.y, -c4212.z);
+          n = cross3(v42, v46);
+          d = wrapd(atan2(dot3(v12, n) * a42, dot3(mm, n)) - nat[5]);
+          ex -= cf[6] * d * d;
+          hbe[h] = cf[0] * exp(ex);
+        }
+      }
+      hbf[h] = f;
+    }
+    __syncthreads();
+    if (excess_flag && tid == 0)
+      prune_hbonds<double>(a, lane, L, T, st.istep, a.ebeta_lane ? a.ebeta_lane[lane] : a.ebeta, false);
+    __syncthreads();
+  }
+  for (int h = tid; h < T.nhb; h += nth)
+    if ((hbf[h] & 3) == 3) es[ES_HB] += hbe[h];
+  // deterministic block reduction: warp butterfly, then warps in order
+  for (int k = 0; k < ES_N; ++k)
+    for (int o = 16; o > 0; o >>= 1) es[k] += __shfl_xor_sync(0xffffffffu, es[k], o);
+  if ((tid & 31) == 0)
+    for (int k = 0; k < ES_N; ++k) red[k][tid >> 5] = es[k];
+  __syncthreads();
+  if (tid == 0) {
+    double tot[ES_N];
+    for (int k = 0; k < ES_N; ++k) {
+      tot[k] = 0.0;
+      for (int w = 0; w < (nth >> 5); ++w) tot[k] += red[k][w];
+    }
+    double *E = a.out_energy + (size_t)lane * N_ETYPE;
+    for (int k = 0; k < N_ETYPE; ++k) E[k] = 0.0;
+    E[1] = tot[ES_VELO];
+    E[2] = tot[ES_BOND];
+    E[3] = tot[ES_ANGLE];
+    E[7] = tot[ES_ELE];
+    E[15] = tot[ES_STACK];
+    E[16] = tot[ES_HB];
+    E[17] = tot[ES_EXV];
+    double sum = 0.0;
+    for (int k = 2; k < N_ETYPE; ++k) sum += E[k];
+    E[0] = sum;
+  }
+}
+
+// velocity rescale after an accepted temperature swap
+// (simu_replica_exchange.F90:272-300): scale > 0 multiplies, scale < 0
+// divides by -scale, 0 leaves the lane alone.
+__global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const TopDesc *tops, const double *scale, int nlane);
+
+cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a) {
+  energy_kernel<<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
+                              const double *scale) {
+  scale_velo_kernel<<<nlane, 128, 0, st>>>(velo, lanes, tops, scale, nlane);
+  return cudaGetLastError();
+}
+
+__global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const TopDesc *tops, const double *scale, int nlane) {
+  const int lane = blockIdx.x;
+  if (lane >= nlane) return;
+  const double f = scale[lane];
+  if (f == 0.0) return;
+  const LaneDesc L = lanes[lane];
+  const int N = tops[L.top].nmp;
+  double *v = velo + 3 * (size_t)L.state0;
+  if (f > 0.0) for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
+  else for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
+}
+
+} // namespace tis
