@@ -211,6 +211,20 @@ int tis_get_hb_list(tis_ctx *ctx, int32_t irep, int32_t *ineigh2hb, int32_t cap,
 /* force_sumup(force_mp, irep) (src/force_sumup.F90:15-593). */
 int tis_force_sumup(tis_ctx *ctx, int32_t irep, double *force_mp);
 
+/* No counterpart in the reference.  Neighbour lists and forces of replica
+ * irep for caller-owned DEVICE arrays xyz_dev (in) and force_dev (out), each
+ * 3*nmp doubles laid out like xyz_mp, without allocating device memory: all
+ * per-call scratch comes from one fixed 1 MiB array that every GPU loading
+ * the library holds until exit.  Topology, parameters and the replica's
+ * temperature label come from ctx; ctx's own state and lists are untouched.
+ * The first call on each device looks up that array's address (set-up) and
+ * should come before any stream capture.  Replicas whose scratch would not
+ * fit return TIS_E_UNSUPPORTED.  All calls on a GPU share the array: calls
+ * that overlap on the GPU (other threads, other contexts) race.  Runs on
+ * ctx's stream; xyz_dev must be ready when called, force_dev is ready on
+ * return.  Returns like tis_force_sumup. */
+int tis_force_sumup_static(tis_ctx *ctx, int32_t irep, const double *xyz_dev, double *force_dev);
+
 /* energy_sumup(irep, ...) -> energy(E_TYPE%MAX) (src/energy_sumup.F90:11-530). */
 int tis_energy_sumup(tis_ctx *ctx, int32_t irep, double *energy);
 

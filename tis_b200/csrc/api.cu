@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -963,3 +964,127 @@ extern "C" int tis_timer(tis_ctx *c, int32_t op, double *ms) {
 }
 
 extern "C" const char *tis_last_error(const tis_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+// ------------------------------------------------ force without allocation
+// tis_force_sumup_static: neighbour lists + forces of one replica for
+// caller-owned device coordinates, with every per-call buffer (lane
+// descriptor and scalar state, coordinates, list bit matrices, mirror
+// indices, interaction slots, hbond flags/energies, site counters) carved
+// out of one file-scope device array instead of the context's buffers.
+// The array is STATIC_SCRATCH_BYTES long, lives on every GPU that loads the
+// library until process exit, and is shared by all calls on that GPU.
+namespace {
+
+constexpr size_t STATIC_SCRATCH_BYTES = (size_t)1 << 20;   // 1 MiB per GPU
+constexpr int STATIC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) unsigned char g_static_scratch[STATIC_SCRATCH_BYTES];
+
+std::mutex g_static_mu;
+unsigned char *g_static_ptr[STATIC_MAX_DEVICES] = {};
+
+// Set-up, once per device with that device current: the address of the
+// array on the current device.  Runs inside the first call on each device.
+int static_scratch_ptr(tis_ctx *c, unsigned char **out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= STATIC_MAX_DEVICES) return fail(c, TIS_E_UNSUPPORTED, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(c, TIS_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    g_static_ptr[dev] = (unsigned char *)p;
+  }
+  *out = g_static_ptr[dev];
+  return TIS_OK;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+// Byte offsets of the per-call buffers inside the static array.
+struct StaticLayout {
+  size_t lanes, lstate, xyz, pxyz, velo, accel, dxyz, mask, mirror, slots, hb_flag, hb_ene, site_exc, total;
+};
+
+StaticLayout static_layout(const tis_ctx *c, int lane) {
+  const TopDesc &T = c->tops[c->lanes[lane].top];
+  const size_t N = (size_t)T.nmp, W = (N + 31) / 32;
+  const size_t real_size = c->par.precision == TIS_PREC_MIXED ? sizeof(float) : sizeof(double);
+  StaticLayout s{};
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o += align256(std::max<size_t>(bytes, 1)); return at; };
+  s.lanes = take((size_t)c->nlane * sizeof(LaneDesc));
+  s.lstate = take((size_t)c->nlane * sizeof(LaneState));
+  s.xyz = take(3 * N * sizeof(double));
+  s.pxyz = take(3 * N * sizeof(double));
+  s.velo = take(3 * N * sizeof(double));
+  s.accel = take(3 * N * sizeof(double));
+  s.dxyz = take(3 * N * sizeof(double));
+  s.mask = take(2 * N * W * sizeof(uint32_t));
+  s.mirror = take(c->par.i_periodic == 1 ? N * N : 1);
+  s.slots = take((size_t)T.nslot * 3 * real_size);
+  s.hb_flag = take((size_t)T.nhb);
+  s.hb_ene = take((size_t)T.nhb * sizeof(double));
+  s.site_exc = take((size_t)T.nsite * sizeof(int));
+  s.total = o;
+  return s;
+}
+
+}  // namespace
+
+extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xyz_dev, double *force_dev) {
+  if (!c || irep < 1 || irep > c->nlane || !xyz_dev || !force_dev) return TIS_E_ARG;
+  const int lane = irep - 1;
+  const StaticLayout lay = static_layout(c, lane);
+  if (lay.total > STATIC_SCRATCH_BYTES)
+    return fail(c, TIS_E_UNSUPPORTED,
+                "tis_force_sumup_static: replica " + std::to_string(irep) + " needs " + std::to_string(lay.total) +
+                    " bytes of scratch, more than the " + std::to_string(STATIC_SCRATCH_BYTES) +
+                    "-byte static area");
+  unsigned char *base = nullptr;
+  int rc = static_scratch_ptr(c, &base);
+  if (rc < 0) return rc;
+  const size_t N = (size_t)c->lane_nmp[lane];
+  // The array keeps the previous call's contents: start from zeros.
+  CK(cudaMemsetAsync(base, 0, lay.total, c->stream));
+  // this replica's descriptor with every offset rebased onto the static array
+  LaneDesc L = c->lanes[lane];
+  L.state0 = 0; L.mask0 = 0; L.mirror0 = 0; L.slot0 = 0; L.hb0 = 0; L.site0 = 0;
+  CK(cudaMemcpyAsync(base + lay.lanes + lane * sizeof(LaneDesc), &L, sizeof(LaneDesc), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(base + lay.lstate + lane * sizeof(LaneState), c->d_lstate.p + lane, sizeof(LaneState),
+                     cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(base + lay.xyz, xyz_dev, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(base + lay.pxyz, xyz_dev, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  LaneState before{};
+  CK(cudaMemcpyAsync(&before, c->d_lstate.p + lane, sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+
+  KArgs a = make_args(c, KM_NEIGHBOR, 0, lane);
+  a.lanes = (const LaneDesc *)(base + lay.lanes);
+  a.lstate = (LaneState *)(base + lay.lstate);
+  a.xyz = (double *)(base + lay.xyz); a.pxyz = (double *)(base + lay.pxyz);
+  a.velo = (double *)(base + lay.velo); a.accel = (double *)(base + lay.accel); a.dxyz = (double *)(base + lay.dxyz);
+  a.mask = (uint32_t *)(base + lay.mask);
+  a.mirror = (uint8_t *)(base + lay.mirror);
+  a.slots = (decltype(a.slots))(base + lay.slots);
+  a.hb_flag = (uint8_t *)(base + lay.hb_flag);
+  a.hb_ene = (double *)(base + lay.hb_ene);
+  a.site_exc = (int *)(base + lay.site_exc);
+  a.out_force = force_dev;
+  rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  a.mode = KM_FORCE;
+  rc = launch_lane(c, a);
+  if (rc < 0) return rc;
+  LaneState after{};
+  CK(cudaMemcpyAsync(&after, base + lay.lstate + lane * sizeof(LaneState), sizeof(LaneState), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (after.flags & LF_NAN) return fail(c, TIS_E_NAN, "non-finite force in lane " + std::to_string(irep));
+  if (after.flags & LF_OVERFLOW) return fail(c, TIS_E_LIST_OVERFLOW, "hbond site list overflow");
+  if (after.flags & (LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED))
+    return fail(c, TIS_E_NOISE_EXHAUSTED, "injected noise or uniforms exhausted");
+  return (int)std::min<long long>(std::max<long long>(after.nclamp - before.nclamp, 0), 0x7fffffff);
+}
