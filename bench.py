@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--period", type=int, default=PERIOD, help="MD steps per bench step (exchange period)")
+    ap.add_argument("--ref-sample", type=int, default=200,
+                    help="reference arm: MD steps per replica in one timed step")
     ap.add_argument("--quick", action="store_true",
                     help="device timing only (no CPU leg, e2e or plain path): small profiling runs")
     return ap.parse_args()
@@ -159,6 +161,21 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def max_over_ranks(x, dist, device):
+    """The largest value over all ranks (the slowest rank's device time)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, total_ms):
+    """Whole-job rate: units every rank processed / the max-over-ranks time."""
+    return units_per_rank * world / (total_ms * 1e-3)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -178,7 +195,7 @@ def run_reference(args, rank, world):
     import multiprocessing as mp
     systems, par, temps, nrep, desc = workload(args.workload)
     cores = os.cpu_count() or 1
-    sample = 200
+    sample = args.ref_sample
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores) as pool:
         for _ in range(max(args.warmup, 0)):
@@ -254,6 +271,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     clocks = Clocks(local_rank) if rank == 0 else None
     times, kern = [], []
+    launches0 = eng.launch_count()
     for _ in range(args.steps):
         flush.zero_()                       # L2 flush between timed steps (outside the timed region)
         torch.cuda.synchronize()
@@ -262,15 +280,14 @@ def run_ours(args, rank, world, local_rank):
         times.append(eng.timer_stop())
         kern.append(eng.last_step_ms())
     torch.cuda.synchronize()
+    launches = eng.launch_count() - launches0
     ck = clocks.stop() if clocks else None
-    total_ms = sum(times)
+    total_ms = max_over_ranks(sum(times), dist, "cuda")
     if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
         dist.barrier()
-    rs = nlane * period_len * args.steps * world
-    value = rs / (total_ms * 1e-3)
+    rs_rank = nlane * period_len * args.steps
+    rs = rs_rank * world
+    value = aggregate_rate(rs_rank, world, total_ms)
 
     # e2e: host buffers through the C-ABI, copies inside the timed region
     xh, vh, ah = (torch.empty((eng.nbead, 3), dtype=torch.float64).pin_memory() for _ in range(3))
@@ -287,11 +304,9 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms.append(eng.timer_stop())
         xh.numpy()[:] = xo; vh.numpy()[:] = vo; ah.numpy()[:] = ao
     e2e_total = sum(e2e_ms) if e2e_ms else float("nan")
-    if dist and e2e_ms:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = rs / (e2e_total * 1e-3)
+    if e2e_ms:
+        e2e_total = max_over_ranks(e2e_total, dist, "cuda")
+    e2e_value = aggregate_rate(rs_rank, world, e2e_total)
     nbytes = 3 * eng.nbead * 3 * 8
 
     plain = None
@@ -330,7 +345,7 @@ def run_ours(args, rank, world, local_rank):
                          "note": "state stays in shared memory across the 1000-step launch; frac > 1 is on-chip reuse"},
             "cpu_baseline": cpu_line,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
-            "gpu_launches": args.steps * (4 if remd else 1),
+            "gpu_launches": launches,
             "clocks": ck,
             "plain_fp64": plain,
             "status": eng.status(),

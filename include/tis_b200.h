@@ -260,6 +260,10 @@ int tis_timer(tis_ctx *ctx, int32_t op, double *ms);
 /* Human-readable text of the last error on this context. */
 const char *tis_last_error(const tis_ctx *ctx);
 
+/* No counterpart in the reference: number of CUDA kernels this context has
+ * launched so far (lets a caller count the launches of a timed region). */
+int64_t tis_launch_count(const tis_ctx *ctx);
+
 #ifdef __cplusplus
 }
 #endif

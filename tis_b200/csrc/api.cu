@@ -121,6 +121,7 @@ struct tis_ctx {
   int last_error = 0;
   int wait_timeout = 0, not_spd = 0;
   std::vector<long long> clamp_seen;
+  long long launches = 0;            // kernels this context has launched
 };
 
 namespace {
@@ -648,6 +649,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
 }
 
 int launch_lane(tis_ctx *c, const KArgs &a) {
+  ++c->launches;
   CK(lane_kernel_launch(c->par.precision == TIS_PREC_MIXED, a.only_lane >= 0 ? 1 : a.nlane, c->threads, c->smem,
                         c->stream, a));
   return TIS_OK;
@@ -798,6 +800,7 @@ int run_energy(tis_ctx *c, int only_lane, const int *labels, bool reuse, double 
   }
   a.reuse_hb = reuse ? 1 : 0;
   a.ebeta = beta;
+  ++c->launches;
   CK(energy_kernel_launch(only_lane >= 0 ? 1 : c->nlane, c->stream, a));
   E.resize((size_t)c->nlane * N_ETYPE);
   CK(cudaMemcpyAsync(E.data(), c->out_energy.p, E.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -911,6 +914,7 @@ extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_acce
   // simu_para2: beta_hbond15 of the last replica's label
   c->beta_global = 1.0e0 / (c->lab_T[c->rep2lab[n - 1]] * BOLTZ_KCAL_MOL);
   CK(cudaMemcpyAsync(c->scale.p, scale.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  ++c->launches;
   CK(scale_velo_launch(n, c->stream, c->velo.p, c->d_lanes.p, c->d_tops.p, c->scale.p));
   std::vector<LaneState> ls(n);
   CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, n * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
@@ -964,6 +968,8 @@ extern "C" int tis_timer(tis_ctx *c, int32_t op, double *ms) {
 }
 
 extern "C" const char *tis_last_error(const tis_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+extern "C" int64_t tis_launch_count(const tis_ctx *c) { return c ? (int64_t)c->launches : -1; }
 
 // ------------------------------------------------ force without allocation
 // tis_force_sumup_static: neighbour lists + forces of one replica for

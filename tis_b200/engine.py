@@ -170,6 +170,9 @@ class Engine:
         self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na)), "replica_exchange")
         return na.value
 
+    def launch_count(self) -> int:
+        return int(self.L.tis_launch_count(self.h))
+
     def labels(self):
         out = np.zeros(self.nlane, dtype=np.int32)
         self._check(self.L.tis_get_labels(self.h, ptr_i32(out)), "labels")
