@@ -40,7 +40,7 @@ PERIOD = 1000
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c3", "c4"])
@@ -125,10 +125,16 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-i", str(gpu_index), "-lms", "200"], stdout=self.f,
+                                       "-i", str(gpu_index), "-lms", "100"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # wait for the first sample so that the timed region is covered
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 5.0:
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:
@@ -174,6 +180,18 @@ def max_over_ranks(x, dist, device):
 def aggregate_rate(units_per_rank, world, total_ms):
     """Whole-job rate: units every rank processed / the max-over-ranks time."""
     return units_per_rank * world / (total_ms * 1e-3)
+
+
+def profiled_traffic():
+    """DRAM bytes per lane_kernel launch at the bench size, from the committed
+    ncu summary (dram__bytes_read.sum + dram__bytes_write.sum), or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", "lane_kernel_c3_launches.md")
+    try:
+        m = re.search(r"traffic per launch \| ([\d,]+) B", open(path).read())
+        return int(m.group(1).replace(",", "")) if m else None
+    except OSError:
+        return None
 
 
 def peaks():
@@ -339,7 +357,10 @@ def run_ours(args, rank, world, local_rank):
                        "md_steps_per_step": period_len, "l2": "flushed between timed steps (256 MiB write)",
                        "parallelism": f"replicas only, {nlane} lanes per GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": profiled_traffic() if (args.workload == "c3" and period_len == PERIOD) else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
+                                           "(profiles/lane_kernel_c3_launches.md)",
                          "kernel": "lane_kernel<float>", "peak_source": src,
                          "bytes_per_replica_step": bytes_per_rs,
                          "note": "state stays in shared memory across the 1000-step launch; frac > 1 is on-chip reuse"},
