@@ -70,7 +70,19 @@ constexpr int CHMAX = 1024;                    // Debye-Hueckel chunks per lane
 constexpr size_t MASK_SMEM_MAX = 64 * 1024;    // bit matrices kept in shared memory up to this size
 
 enum { MISC_EXCESS = 0, MISC_REBUILD = 1, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,
-       MISC_REBUILT = 6, MISC_UNITS = 8 /* neigh_unit ints start here */ };
+       MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8,
+       MISC_UNITS = 10 /* neigh_unit ints start here */ };
+
+// Excluded-volume near lists: at a recording pass every bead keeps, per
+// thread of its group, the exv-list partners within (screen radius +
+// NEAR_SKIN); later passes visit only those until the lists are stale (a
+// rebuild, or a bead displaced by more than NEAR_DISP_MAX since the
+// recording: two beads then close in by less than NEAR_SKIN - 0.05 A).
+// Visiting a sub-list in ascending j is the same summation as the full
+// screen, so the forces are bitwise the same either way.
+constexpr int NEAR_CAP = 32;                   // entries per bead, split over its group
+constexpr float NEAR_SKIN = 1.0f;
+constexpr float NEAR_DISP_MAX = 0.475f;
 
 template <typename Real>
 struct Smem {
@@ -92,13 +104,16 @@ struct Smem {
   int16_t *unit;            // unit index of each bead
   int8_t *typ, *cls;
   uint32_t *mask;           // exv rows then ele rows, W words each (shared or global)
+  uint16_t *near;           // (N, NEAR_CAP) exv near lists (shared only)
+  uint8_t *near_cnt;        // (N, 8) entries per group thread, 0xFF = overflow
+  float4 *NR4;              // positions at the last near-list recording
   Real *slots;              // shared or global
   const int *inc_slot;      // shared copy or global
   int W;                    // words per bit row
-  bool mask_smem, slots_smem, inc_smem;
+  bool mask_smem, slots_smem, inc_smem, near_on;
 };
 
-struct SmemPlan { size_t base, mask, slots, inc; };
+struct SmemPlan { size_t base, mask, slots, inc, near; };
 
 // Byte layout of one lane (host and device use the same arithmetic).
 __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc, bool periodic, bool skin,
@@ -117,6 +132,7 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc
   p.mask = 8 * (size_t)N * ((N + 31) / 32);
   p.slots = ((3 * (size_t)nslot * real_size) + 15) & ~(size_t)15;
   p.inc = ((4 * (size_t)ninc) + 15) & ~(size_t)15;
+  p.near = 16 * (size_t)N + 2 * (size_t)NEAR_CAP * N + 8 * (size_t)N + 16;
   return p;
 }
 
@@ -178,6 +194,14 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   s.slots_smem = pl.slots <= left;
   if (s.slots_smem) { s.slots = (Real *)u; u += pl.slots; left -= pl.slots; }
   else s.slots = (Real *)a.slots + 3 * (size_t)L.slot0;
+  s.near_on = pl.near <= left;
+  if (s.near_on) {
+    s.NR4 = (float4 *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
+    s.near = (uint16_t *)(s.NR4 + N);
+    s.near_cnt = (uint8_t *)(s.near + (size_t)NEAR_CAP * N);
+  } else {
+    s.NR4 = nullptr; s.near = nullptr; s.near_cnt = nullptr;
+  }
   return s;
 }
 

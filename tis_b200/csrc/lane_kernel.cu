@@ -49,11 +49,16 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
     }
   }
   for (int k = tid; k < 2 * N * W; k += nth) mexv[k] = 0u;
-  if (tid == 0) { s.misc[MISC_NEXV] = 0; s.misc[MISC_NELE] = 0; s.misc[MISC_REBUILT] = 1; }
+  if (tid == 0) {
+    s.misc[MISC_NEXV] = 0; s.misc[MISC_NELE] = 0; s.misc[MISC_REBUILT] = 1;
+    s.misc[MISC_NEAR_BAD] = 1;
+  }
   // unit prescreen (neighbor_pre.F90:174-252), thread 0
   const int nu = T.nunit;
   int *nunit_ok = s.misc + MISC_UNITS;
-  if (tid == 0) {
+  if (tid == 0 && nu == 1) {
+    nunit_ok[0] = 1;
+  } else if (tid == 0) {
     double cm[3 * 32], md[32];
     for (int u = 0; u < nu && u < 32; ++u) {
       int is = a.u_lunit[2 * (T.unit0 + u)], ie = a.u_lunit[2 * (T.unit0 + u) + 1];
@@ -90,15 +95,17 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
   int nexv_l = 0, nele_l = 0;
   PHASE_T0(t_pairs);
   // warp w takes rows i = w, w + nwarp, ...; its lanes take j > i
+  const bool one_unit = nu == 1;
+  const double rn2_00 = s.rn2[0];
   for (int i = warp; i < N - 1; i += nwarp) {
     const int ui = s.unit[i];
     const int ci = s.cls[i];
     const int nsep = (s.typ[i] == 2) ? a.nsep[0] : (s.typ[i] == 4 ? a.nsep[1] : (s.typ[i] == 3 ? a.nsep[2] : -1));
     const double xi = s.PX[i], yi = s.PY[i], zi = s.PZ[i];
-    const bool qi = fabs((double)s.A4[i].w) >= 1.0e-6;
+    const bool qi = a.i_ele != 0 && fabs((double)s.A4[i].w) >= 1.0e-6;
     for (int j = i + 1 + lid; j < N; j += 32) {
-      const int uj = s.unit[j];
-      if (!nunit_ok[ui * nu + uj]) continue;
+      const int uj = one_unit ? 0 : s.unit[j];
+      if (!one_unit && !nunit_ok[ui * nu + uj]) continue;
       double v0 = __dsub_rn(s.PX[j], xi), v1 = __dsub_rn(s.PY[j], yi), v2 = __dsub_rn(s.PZ[j], zi);
       int im = 27;
       if (a.periodic) {
@@ -108,18 +115,19 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
         im = 9 * m0 + 3 * m1 + m2 + 1;
       }
       const double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
-      bool ex = d2 < s.rn2[ui * nu + uj];
+      bool ex = d2 < (one_unit ? rn2_00 : s.rn2[ui * nu + uj]);
       if (ex) {
-        const int cj = s.cls[j];
         if (ui == uj) {
           if (ci == 2 /* RNA */ && j < i + nsep) ex = false;
-        } else if (!((ci == 2 && cj == 2) || (ci == 2 && cj == 4) || (ci == 4 && cj == 2) ||
-                     (ci == 4 && cj == 3) || (ci == 3 && cj == 4))) {
-          ex = false;
+        } else {
+          const int cj = s.cls[j];
+          if (!((ci == 2 && cj == 2) || (ci == 2 && cj == 4) || (ci == 4 && cj == 2) ||
+                (ci == 4 && cj == 3) || (ci == 3 && cj == 4)))
+            ex = false;
         }
       }
       bool el = false;
-      if (a.i_ele != 0 && qi && fabs((double)s.A4[j].w) >= 1.0e-6) el = d2 < rele2;
+      if (qi && fabs((double)s.A4[j].w) >= 1.0e-6) el = d2 < rele2;
       if (ex || el) {
         const uint32_t bj = 1u << (j & 31), bi = 1u << (i & 31);
         if (ex) {
@@ -253,6 +261,10 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const double coefT = a.lab_coef[label];
   const Real rcd = (Real)(1.0 / cdist);
   const Real cut2 = (Real)((a.cutoff_ele * cdist) * (a.cutoff_ele * cdist));
+  // near-list state: read here (after the caller's barrier), rewritten by
+  // thread 0 only after the end-of-phase-1 barrier
+  const bool near_rec = s.near_on && (s.misc[MISC_NEAR_BAD] != 0 ||
+                                      __int_as_float(s.misc[MISC_NEAR_DISP]) > NEAR_DISP_MAX * NEAR_DISP_MAX);
   PHASE_T0(t_p1);
   // warp-uniform schedule: 32-item chunks of one kind, most expensive kinds
   // first, dealt round-robin over the warps (no divergence between kinds)
@@ -347,6 +359,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   }
   __syncthreads();
   PHASE_ADD(3, t_p1);
+  if (tid == 0 && s.near_on) { s.misc[MISC_NEAR_BAD] = 0; s.misc[MISC_NEAR_DISP] = 0; }
   if (s.misc[MISC_EXCESS]) {
     if (tid == 0) {
       const double beta = a.hb_beta_global ? a.beta_hbond15 : a.lab_beta[label];
@@ -371,38 +384,60 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       const V pi = s.A4[i], bi = s.B4[i], li = s.L4[i];
       const int ti = s.typ[i], ci = s.cls[i];
       const Real scr2 = bi.z * bi.z;   // (screen radius)^2, rounding margin included
+      const Real nscr = bi.z + (Real)NEAR_SKIN, nscr2 = nscr * nscr;
       const uint32_t *row = mexv + (size_t)i * W;
-      for (int w = g; w < W; w += GA) {
-        uint32_t m = row[w];
-        while (m) {
-          // force_exv_dt15.F90:204-265: one 16-byte load screens the pair;
-          // pairs inside the screen radius use FP64 coordinate differences
-          const int j = (w << 5) + __ffs(m) - 1;
-          m &= m - 1;
-          const V pj = s.A4[j];
-          Real sx = pj.x - pi.x, sy = pj.y - pi.y, sz = pj.z - pi.z;
-          if (mir) mirror_shift<Real>(a, mir, N, i, j, sx, sy, sz);
-          if (sx * sx + sy * sy + sz * sz > scr2) continue;
-          // hi + lo difference: the FP64 difference to ~1e-12 relative
-          const V lj = s.L4[j];
-          const Real wx = sx + (lj.x - li.x), wy = sy + (lj.y - li.y), wz = sz + (lj.z - li.z);
-          const Real r2 = wx * wx + wy * wy + wz * wz;
-          const int tj = s.typ[j], cj = s.cls[j];
-          const V bj = s.B4[j];
-          Real dij;
-          if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = dist_ps;
-          else if (ci == 2 && cj == 2) dij = dist_rr;
-          else dij = bi.x + bj.x;
-          if (r2 > dij * dij) continue;
-          const Real rinv = rsq<Real>(r2);
-          const Real dist = r2 * rinv;
-          const Real coef = bi.y * bj.y;
-          const Real dr = dist + ra - dij;
-          const Real ro2 = fdiv(ra2, dr * dr);
-          const Real ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro2 * ro4 * ro8;
-          Real f = fabs((Real)12 * coef * (ro14 - ro8) * dr * inv_ra2 * rinv);
-          if (f > (Real)50) { f = 50; ++nclamp; }
-          fx -= (double)(f * wx); fy -= (double)(f * wy); fz -= (double)(f * wz);
+      // force_exv_dt15.F90:204-265 for partner j: one 16-byte load screens
+      // the pair; pairs inside the screen radius use the hi + lo difference
+      // (the FP64 difference to ~1e-12 relative).  rec: record j in lst when
+      // it is within the near radius.
+      auto visit = [&](int j, bool rec, int &cnt, uint16_t *lst, int ncap) {
+        const V pj = s.A4[j];
+        Real sx = pj.x - pi.x, sy = pj.y - pi.y, sz = pj.z - pi.z;
+        if (mir) mirror_shift<Real>(a, mir, N, i, j, sx, sy, sz);
+        const Real d2s = sx * sx + sy * sy + sz * sz;
+        if (rec && d2s <= nscr2) {
+          if (cnt < ncap) lst[cnt] = (uint16_t)j;
+          ++cnt;
+        }
+        if (d2s > scr2) return;
+        const V lj = s.L4[j];
+        const Real wx = sx + (lj.x - li.x), wy = sy + (lj.y - li.y), wz = sz + (lj.z - li.z);
+        const Real r2 = wx * wx + wy * wy + wz * wz;
+        const int tj = s.typ[j], cj = s.cls[j];
+        const V bj = s.B4[j];
+        Real dij;
+        if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = dist_ps;
+        else if (ci == 2 && cj == 2) dij = dist_rr;
+        else dij = bi.x + bj.x;
+        if (r2 > dij * dij) return;
+        const Real rinv = rsq<Real>(r2);
+        const Real dist = r2 * rinv;
+        const Real coef = bi.y * bj.y;
+        const Real dr = dist + ra - dij;
+        const Real ro2 = fdiv(ra2, dr * dr);
+        const Real ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro2 * ro4 * ro8;
+        Real f = fabs((Real)12 * coef * (ro14 - ro8) * dr * inv_ra2 * rinv);
+        if (f > (Real)50) { f = 50; ++nclamp; }
+        fx -= (double)(f * wx); fy -= (double)(f * wy); fz -= (double)(f * wz);
+      };
+      const int ncap = NEAR_CAP / GA;
+      uint16_t *lst = s.near_on ? s.near + (size_t)i * NEAR_CAP + g * ncap : nullptr;
+      const int have = s.near_on ? (int)s.near_cnt[i * 8 + g] : 0xFF;
+      int cnt = 0;
+      if (s.near_on && !near_rec && have != 0xFF) {
+        for (int k = 0; k < have; ++k) visit((int)lst[k], false, cnt, lst, ncap);
+      } else {
+        for (int w = g; w < W; w += GA) {
+          uint32_t m = row[w];
+          while (m) {
+            const int j = (w << 5) + __ffs(m) - 1;
+            m &= m - 1;
+            visit(j, near_rec, cnt, lst, ncap);
+          }
+        }
+        if (near_rec) {
+          s.near_cnt[i * 8 + g] = (uint8_t)(cnt > ncap ? 0xFF : cnt);
+          if (g == 0) s.NR4[i] = make_float4((float)pi.x, (float)pi.y, (float)pi.z, 0.f);
         }
       }
       PHASE_ALL(40, t_e0);
@@ -485,6 +520,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
   __syncthreads();
   for (int k = tid; k < NQ; k += nth) s.qidx[s.qb[k]] = k;
+  if (tid == 0) s.misc[MISC_NEAR_BAD] = 1;
   __syncthreads();
 
   const int label0 = st.label;
@@ -565,6 +601,12 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
         if (skin) { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
         set_pos<Real>(s, i);
+        if (s.near_on) {
+          const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
+                      ez = (float)s.A4[i].z - s.NR4[i].z;
+          const float e2 = ex * ex + ey * ey + ez * ez;
+          if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
+        }
       }
       for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
       if (tid == 0) s.misc[MISC_EXCESS] = 0;
@@ -626,7 +668,7 @@ template __global__ void lane_kernel<float, 1024>(KArgs);
 // matrices + incidence lists + slots, capped at the 227 KB a CTA may use.
 size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit) {
   SmemPlan p = smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit);
-  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + 64;
+  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + p.near + 64;
   return want < 227 * 1024 ? want : 227 * 1024;
 }
 
