@@ -26,6 +26,8 @@ cudaError_t lane_kernel_set_smem(bool mixed, int bytes);
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool forces);
+cudaError_t ewald_energy_launch(cudaStream_t st, const KArgs &a);
 cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
                               const double *scale);
 }  // namespace tis
@@ -122,6 +124,10 @@ struct tis_ctx {
   int wait_timeout = 0, not_spd = 0;
   std::vector<long long> clamp_seen;
   long long launches = 0;            // kernels this context has launched
+  // Ewald
+  int nk = 0, hmax = 0, nqblk = 1, nq_max = 0;
+  DBuf<int8_t> ew_h;
+  DBuf<double> ew_coef, ew_tab, ew_S, f_ext;
 };
 
 namespace {
@@ -182,6 +188,46 @@ int choose_group(int threads, int maxN) {
   return g;
 }
 
+// Reciprocal vectors of mloop_ewld.F90:56-156: every integer h != 0 with
+// |h| <= hmax in (x, y, z) loop order, comb-sorted by |h|^2 with the
+// reference's gap rule, and C(k) = 2 pi / L^3 exp(-k^2 / 4 alpha^2) / k^2
+// for k = 2 pi h / L.
+void ewald_table(double L, double alpha, double hmax, std::vector<int8_t> &hv, std::vector<double> &coef) {
+  const int lmax = (int)std::ceil(hmax);
+  const double hmax2 = hmax * hmax;
+  std::vector<int> hh;
+  std::vector<double> h2;
+  for (int ix = -lmax; ix <= lmax; ++ix)
+    for (int iy = -lmax; iy <= lmax; ++iy)
+      for (int iz = -lmax; iz <= lmax; ++iz) {
+        if (ix == 0 && iy == 0 && iz == 0) continue;
+        const double r2 = (double)ix * ix + (double)iy * iy + (double)iz * iz;
+        if (r2 <= hmax2) { hh.push_back(ix); hh.push_back(iy); hh.push_back(iz); h2.push_back(r2); }
+      }
+  const int n = (int)h2.size();
+  int gap = n;
+  bool swapped = false;
+  while (gap > 1 || swapped) {
+    gap = (gap * 10) / 13;
+    if (gap < 1) gap = 1;
+    else if (gap == 9 || gap == 10) gap = 11;
+    swapped = false;
+    for (int i = 0; i + gap < n; ++i)
+      if (h2[i] > h2[i + gap]) {
+        std::swap(h2[i], h2[i + gap]);
+        for (int d = 0; d < 3; ++d) std::swap(hh[3 * i + d], hh[3 * (i + gap) + d]);
+        swapped = true;
+      }
+  }
+  const double f = 2.0 * F_PI / L;
+  hv.resize(3 * (size_t)n);
+  coef.resize(n);
+  for (int i = 0; i < n; ++i) {
+    for (int d = 0; d < 3; ++d) hv[3 * i + d] = (int8_t)hh[3 * i + d];
+    coef[i] = 2.0 * F_PI / (L * L * L) * std::exp(-(f * f) * h2[i] / (4.0 * alpha * alpha)) / ((f * f) * h2[i]);
+  }
+}
+
 }  // namespace
 
 // --------------------------------------------------------------------- init
@@ -193,7 +239,15 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->par = *par;
   const tis_params &p = *par;
   if (p.i_simulate_type != TIS_SIM_LANGEVIN) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
-  if (p.i_ele == TIS_ELE_EWALD) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+  if (p.i_ele == TIS_ELE_EWALD) {
+    // mloop_ewld.F90 uses psize(1) for a cubic box; the per-charge tables
+    // hold |h| <= 11
+    if (p.i_periodic != 1 || p.psize[0] != p.psize[1] || p.psize[0] != p.psize[2] || !(p.ewld_hmax > 0.0) ||
+        std::ceil(p.ewld_hmax) > 11.0 || !(p.ewld_alpha > 0.0)) {
+      tis_destroy(c);
+      return TIS_E_UNSUPPORTED;
+    }
+  }
   const bool periodic = p.i_periodic == 1;
   const bool skin = p.n_step_neighbor <= 0;
   c->ntop = ntop;
@@ -371,7 +425,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->lab2rep.resize(nlane);
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
-  int hb_off = 0, site_off = 0, state_off = 0;
+  int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
@@ -410,6 +464,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       L.hb0 = hb_off;
       L.site0 = site_off;
       L.unif0 = 0;
+      L.ew0 = ew_off;
+      ew_off += d.nq;
       state_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
       if (periodic) mirror_off += (long long)N * N;
@@ -433,6 +489,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
   size_t smem = 0;
   for (auto &d : c->tops) {
+    // electrostatic row chunks: one per charged bead at least
+    if (p.i_ele != TIS_ELE_NONE && d.nq > CHMAX) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+    c->nq_max = std::max(c->nq_max, d.nq);
     // the per-lane base layout must fit one CTA's shared memory
     if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit) + 64 > 227 * 1024) {
       tis_destroy(c);
@@ -485,6 +544,20 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->hb_flag.alloc(hb_off)); CK(c->hb_ene.alloc(hb_off)); CK(c->site_exc.alloc(site_off));
   CK(cudaMemset(c->hb_flag.p, 0, std::max(hb_off, 1)));
   CK(cudaMemset(c->hb_ene.p, 0, std::max(hb_off, 1) * sizeof(double)));
+  if (p.i_ele == TIS_ELE_EWALD) {
+    std::vector<int8_t> h;
+    std::vector<double> coef;
+    ewald_table(p.psize[0], p.ewld_alpha, p.ewld_hmax, h, coef);
+    c->nk = (int)coef.size();
+    c->hmax = (int)std::ceil(p.ewld_hmax);
+    c->nqblk = std::min(16, std::max(1, (c->nq_max + 63) / 64));
+    CK(c->ew_h.upload(h));
+    CK(c->ew_coef.upload(coef));
+    CK(c->ew_tab.alloc(std::max<size_t>((size_t)ew_off * 3 * (c->hmax + 1) * 2, 1)));
+    CK(c->ew_S.alloc(std::max<size_t>((size_t)nlane * c->nqblk * c->nk * 2, 1)));
+    CK(c->f_ext.alloc(n3));
+    CK(cudaMemset(c->f_ext.p, 0, n3 * 8));
+  }
   c->clamp_seen.assign(nlane, 0);
   *out = c;
   return TIS_OK;
@@ -516,6 +589,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
   c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
+  c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tev0) cudaEventDestroy(c->tev0);
@@ -608,7 +682,16 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_step_neighbor = p.n_step_neighbor;
   a.exv_dist = p.exv_dist; a.exv_dist_PS = p.exv_dist_PS; a.exv_adjust = p.exv_adjust; a.exv_inf = p.exv_inf;
   a.nsep[0] = p.n_sep_nlocal_P; a.nsep[1] = p.n_sep_nlocal_S; a.nsep[2] = p.n_sep_nlocal_B;
-  a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : 0;
+  a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : (p.i_ele == TIS_ELE_EWALD ? 2 : 0);
+  if (p.i_ele == TIS_ELE_EWALD) {
+    a.ewld_alpha = p.ewld_alpha;
+    a.ewld_beta = 2.0 * p.ewld_alpha / std::sqrt(F_PI);
+    a.ewld_self = -p.ewld_alpha / std::sqrt(F_PI);
+    a.nk = c->nk; a.hmax = c->hmax; a.nqblk = c->nqblk;
+    for (int d = 0; d < 3; ++d) a.two_pi_L[d] = 2.0 * F_PI / p.psize[0];
+    a.ew_h = c->ew_h.p; a.ew_coef = c->ew_coef.p; a.ew_tab = c->ew_tab.p; a.ew_S = c->ew_S.p;
+  }
+  a.f_ext = nullptr;
   a.cutoff_ele = p.cutoff_ele;
   a.i_DH_cutoff_type = p.i_DH_cutoff_type;
   a.hb_cutoff_dist = p.hb_cutoff_dist;
@@ -646,6 +729,17 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_unif = c->n_unif;
   a.nbead_total = c->nbead_total;
   return a;
+}
+
+// Ewald reciprocal space for the lanes of `a` (tables, structure factors
+// and, when `forces`, the per-charge forces in f_ext, which the next lane
+// launch adds to each bead's sum).  No-op without Ewald.
+int ewald_recip(tis_ctx *c, KArgs &a, bool forces) {
+  if (c->par.i_ele != TIS_ELE_EWALD) return TIS_OK;
+  c->launches += forces ? 3 : 2;
+  if (forces) a.f_ext = c->f_ext.p;   // written by the force kernel, read by the lane kernel
+  CK(ewald_recip_launch(c->stream, a, c->nq_max, forces));
+  return TIS_OK;
 }
 
 int launch_lane(tis_ctx *c, const KArgs &a) {
@@ -776,7 +870,9 @@ extern "C" int tis_get_hb_list(tis_ctx *c, int32_t irep, int32_t *ineigh2hb, int
 extern "C" int tis_force_sumup(tis_ctx *c, int32_t irep, double *force_mp) {
   if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
   KArgs a = make_args(c, KM_FORCE, 0, irep - 1);
-  int rc = launch_lane(c, a);
+  int rc = ewald_recip(c, a, true);
+  if (rc < 0) return rc;
+  rc = launch_lane(c, a);
   if (rc < 0) return rc;
   c->hb_energy_valid = true;
   const LaneDesc &L = c->lanes[irep - 1];
@@ -802,6 +898,12 @@ int run_energy(tis_ctx *c, int only_lane, const int *labels, bool reuse, double 
   a.ebeta = beta;
   ++c->launches;
   CK(energy_kernel_launch(only_lane >= 0 ? 1 : c->nlane, c->stream, a));
+  if (c->par.i_ele == TIS_ELE_EWALD) {
+    int rc = ewald_recip(c, a, false);
+    if (rc < 0) return rc;
+    ++c->launches;
+    CK(ewald_energy_launch(c->stream, a));
+  }
   E.resize((size_t)c->nlane * N_ETYPE);
   CK(cudaMemcpyAsync(E.data(), c->out_energy.p, E.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -821,7 +923,9 @@ extern "C" int tis_energy_sumup(tis_ctx *c, int32_t irep, double *energy) {
 extern "C" int tis_time_integral_pre(tis_ctx *c) {
   if (!c) return TIS_E_ARG;
   KArgs a = make_args(c, KM_PRE, 0, -1);
-  int rc = launch_lane(c, a);
+  int rc = ewald_recip(c, a, true);
+  if (rc < 0) return rc;
+  rc = launch_lane(c, a);
   if (rc < 0) return rc;
   c->noise_base += 1;
   c->hb_energy_valid = true;
@@ -833,8 +937,24 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
   if (nsteps == 0) return TIS_OK;
   KArgs a = make_args(c, KM_STEP, (int)nsteps, -1);
   CK(cudaEventRecord(c->ev0, c->stream));
-  int rc = launch_lane(c, a);
-  if (rc < 0) return rc;
+  if (c->par.i_ele != TIS_ELE_EWALD) {
+    int rc = launch_lane(c, a);
+    if (rc < 0) return rc;
+  } else {
+    // the reciprocal sum needs every charge's new position: each step is
+    // x update -> reciprocal forces -> forces, v / a update
+    for (int64_t k = 0; k < nsteps; ++k) {
+      KArgs x = make_args(c, KM_XSTEP, 1, -1);
+      int rc = launch_lane(c, x);
+      if (rc < 0) return rc;
+      KArgs v = make_args(c, KM_VSTEP, 1, -1);
+      v.noise_base = c->noise_base + (int)k;
+      rc = ewald_recip(c, v, true);
+      if (rc < 0) return rc;
+      rc = launch_lane(c, v);
+      if (rc < 0) return rc;
+    }
+  }
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0.f;
@@ -1042,6 +1162,8 @@ StaticLayout static_layout(const tis_ctx *c, int lane) {
 
 extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xyz_dev, double *force_dev) {
   if (!c || irep < 1 || irep > c->nlane || !xyz_dev || !force_dev) return TIS_E_ARG;
+  if (c->par.i_ele == TIS_ELE_EWALD)
+    return fail(c, TIS_E_UNSUPPORTED, "tis_force_sumup_static: Ewald needs the context's reciprocal-space buffers");
   const int lane = irep - 1;
   const StaticLayout lay = static_layout(c, lane);
   if (lay.total > STATIC_SCRATCH_BYTES)

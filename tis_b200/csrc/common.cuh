@@ -18,6 +18,7 @@ namespace tis {
 
 constexpr int MAX_THREADS = 1024;
 constexpr int N_ETYPE = 25;   // E_TYPE%MAX
+constexpr int CHMAX = 1024;   // electrostatic row chunks per lane (at least one per charged bead)
 
 // per-topology descriptor (offsets into the concatenated topology arrays)
 struct TopDesc {
@@ -49,6 +50,7 @@ struct LaneDesc {
   int hb0;          // hb flags / status / energies (nhb each)
   int site0;        // per-lane hbond-site excess counters (nsite ints)
   int unif0;        // injected uniform stream (n_uniform per lane)
+  int ew0;          // Ewald: first charge of this lane in the per-lane charge tables
 };
 
 // Mutable per-lane scalar state, kept in global memory between launches.
@@ -70,6 +72,8 @@ enum KMode {
   KM_FORCE = 2,        // force_sumup -> out_force
   KM_PRE = 3,          // time_integral_pre: lists, force, a(0)
   KM_STEP = 4,         // nsteps of time_integral
+  KM_XSTEP = 5,        // first half of one step: trigger, rebuild, x update
+  KM_VSTEP = 6,        // second half of one step: forces (+ f_ext), v / a update
 };
 
 // Kernel arguments (all device pointers).
@@ -87,8 +91,20 @@ struct KArgs {
   int n_step_neighbor;
   double exv_dist, exv_dist_PS, exv_adjust, exv_inf;
   int nsep[3];         // P, S, B
-  int i_ele;           // 0 none, 1 DH
-  double cutoff_ele;
+  int i_ele;           // 0 none, 1 DH, 2 Ewald
+  double cutoff_ele;   // DH: in Debye lengths; Ewald: real-space cutoff in A
+  // Ewald (force_ele_coulomb_ewld.F90, mloop_ewld.F90)
+  double ewld_alpha, ewld_beta;   // alpha, 2 alpha / sqrt(pi)
+  double ewld_self;               // -alpha / sqrt(pi)
+  int nk;                         // reciprocal vectors, all +-h with |h| <= hmax
+  int hmax;                       // ceil(hmax): per-dimension table length - 1
+  int nqblk;                      // charge blocks of the structure-factor partial sums
+  double two_pi_L[3];             // 2 pi / L
+  const int8_t *ew_h;             // (nk, 3) integer h
+  const double *ew_coef;          // (nk) 2 pi / L^3 exp(-k^2 / 4 alpha^2) / k^2
+  double *ew_tab;                 // (q, 3, hmax + 1) of (cos, sin)(2 pi h x / L), per lane's charges
+  double *ew_S;                   // (lane, nqblk, nk, 2) partial sums of q cos, q sin
+  double *f_ext;                  // (3, nbead_total) force added to each bead's sum, or null
   double hb_cutoff_dist;
   double max_abscos;   // MAX_ANG_ABSCOS_HBOND15 == MAX_DIH_ABSCOS_HBOND15
   double tstep, tstep2, tsteph;

@@ -66,7 +66,6 @@ template <> struct V4<double> { typedef double4 T; };
 // matrices (exv, ele): bit j of row i is set when the pair (min, max) is in
 // the reference's list.  The matrices, bonded slots and incidence lists live
 // in shared memory when they fit; otherwise they are used in global memory.
-constexpr int CHMAX = 1024;                    // Debye-Hueckel chunks per lane
 constexpr size_t MASK_SMEM_MAX = 64 * 1024;    // bit matrices kept in shared memory up to this size
 
 enum { MISC_EXCESS = 0, MISC_REBUILD = 1, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,

@@ -93,8 +93,10 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const uint32_t *mexv = a.mask + L.mask0, *mele = mexv + (size_t)N * W;
   const uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
   const double cdist = a.lab_cdist[label], coefT = a.lab_coef[label];
-  const double cut2 = (a.i_DH_cutoff_type == 0) ? (a.cutoff_ele * cdist) * (a.cutoff_ele * cdist)
-                                                : a.cutoff_ele * a.cutoff_ele;
+  // DH: energy_ele_DH.F90:33 scales the cutoff only for i_DH_cutoff_type 0;
+  // Ewald: real-space cutoff in A (energy_ele_coulomb_ewld.F90:137)
+  const double cut2 = (a.i_ele == 1 && a.i_DH_cutoff_type == 0) ? (a.cutoff_ele * cdist) * (a.cutoff_ele * cdist)
+                                                                : a.cutoff_ele * a.cutoff_ele;
   const double rcd = 1.0 / cdist;
   auto shifted = [&](int i, int j) {   // j > i: canonical orientation
     double3 w = sub3(gpos(P, j), gpos(P, i));
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     const int ti = a.b_type[T.bead0 + i], ci = a.b_class[T.bead0 + i];
     const bool qi = fabs(a.b_charge[T.bead0 + i]) >= 1.0e-6;
     for (int w = (i + 1) >> 5; w < W; ++w) {
-      uint32_t me = mexv[(size_t)i * W + w], ml = (a.i_ele == 1 && qi) ? mele[(size_t)i * W + w] : 0u;
+      uint32_t me = mexv[(size_t)i * W + w], ml = (a.i_ele != 0 && qi) ? mele[(size_t)i * W + w] : 0u;
       if (w == ((i + 1) >> 5)) {   // keep bits j > i only
         const uint32_t keep = ((i + 1) & 31) ? ~((1u << ((i + 1) & 31)) - 1u) : 0xffffffffu;
         me &= keep; ml &= keep;
@@ -146,7 +148,8 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
         if (r2 <= cut2) {
           const double dist1 = sqrt(r2);
           const double ce = a.b_charge[T.bead0 + i] * a.b_charge[T.bead0 + j] * coefT;
-          es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
+          if (a.i_ele == 1) es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
+          else es[ES_ELE] += ce * erfc(a.ewld_alpha * dist1) / dist1;
         }
       }
     }

@@ -254,13 +254,18 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // (site counters and MISC_EXCESS were cleared by the caller before its barrier)
   const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd;
   const ChunkGeo cg = chunk_geo(NQ, W);
-  const int nch = (a.i_ele == 1) ? cg.nch : 0;
+  const int nch = (a.i_ele != 0) ? cg.nch : 0;
   const int k_st = nhb, k_ch = k_st + nst, k_ba = k_ch + nch, k_bd = k_ba + nba, total = k_bd + nbd;
   const double *u0 = a.lab_u0 + a.lab_u0off[label];
   const double cdist = a.lab_cdist[label];
   const double coefT = a.lab_coef[label];
   const Real rcd = (Real)(1.0 / cdist);
-  const Real cut2 = (Real)((a.cutoff_ele * cdist) * (a.cutoff_ele * cdist));
+  // DH: the force cutoff is always scaled by the Debye length
+  // (force_ele_DH.F90:44); Ewald: real-space cutoff in A
+  const bool ewald = a.i_ele == 2;
+  const Real cut2 = ewald ? (Real)(a.cutoff_ele * a.cutoff_ele)
+                          : (Real)((a.cutoff_ele * cdist) * (a.cutoff_ele * cdist));
+  const Real ew_a = (Real)a.ewld_alpha, ew_a2 = (Real)(a.ewld_alpha * a.ewld_alpha), ew_b = (Real)a.ewld_beta;
   // near-list state: read here (after the caller's barrier), rewritten by
   // thread 0 only after the end-of-phase-1 barrier
   const bool near_rec = s.near_on && (s.misc[MISC_NEAR_BAD] != 0 ||
@@ -333,12 +338,21 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const Real ra2 = ax * ax + ay * ay + az * az, rb2 = bx * bx + by * by + bz * bz;
             const Real ria = rsq<Real>(ra2), rib = rsq<Real>(rb2);
             const Real da = ra2 * ria, db = rb2 * rib;
-            Real fa = qci * p0.w * ria * ria * (ria + rcd) * exp(-da * rcd);
-            Real fb = qci * p1.w * rib * rib * (rib + rcd) * exp(-db * rcd);
+            Real fa, fb;
+            if (!ewald) {
+              fa = qci * p0.w * ria * ria * (ria + rcd) * exp(-da * rcd);
+              fb = qci * p1.w * rib * rib * (rib + rcd) * exp(-db * rcd);
+            } else {
+              // force_ele_coulomb_ewld.F90:118-137 (real space, no clamp)
+              fa = qci * p0.w * (erfc(ew_a * da) * ria + ew_b * exp(-ew_a2 * ra2)) * ria * ria;
+              fb = qci * p1.w * (erfc(ew_a * db) * rib + ew_b * exp(-ew_a2 * rb2)) * rib * rib;
+            }
             if (!(ra2 <= cut2)) fa = 0;
             if (!(rb2 <= cut2) || !two) fb = 0;
-            if (fa > (Real)50) { fa = 50; ++nclamp; }
-            if (fb > (Real)50) { fb = 50; ++nclamp; }
+            if (!ewald) {
+              if (fa > (Real)50) { fa = 50; ++nclamp; }
+              if (fb > (Real)50) { fb = 50; ++nclamp; }
+            }
             ax_.add(-(fa * ax)); ax_.add(-(fb * bx));
             ay_.add(-(fa * ay)); ay_.add(-(fb * by));
             az_.add(-(fa * az)); az_.add(-(fb * bz));
@@ -465,6 +479,10 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (valid) PHASE_ALL(41, t_e2);
     PHASE_T0(t_e1);
     group_reduce<Real>(fx, fy, fz, GA);
+    if (valid && g == 0 && a.f_ext) {
+      const size_t o = 3 * (size_t)(L.state0 + i);
+      fx += a.f_ext[o]; fy += a.f_ext[o + 1]; fz += a.f_ext[o + 2];
+    }
     if (valid && g == 0) sink(i, fx, fy, fz);
     if (valid && g == 0) PHASE_ALL(42, t_e1);
   }
@@ -547,10 +565,10 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
       s.AX[i] = fx * rc + cc * n0; s.AY[i] = fy * rc + cc * n1; s.AZ[i] = fz * rc + cc * n2;
     });
-  } else {  // KM_STEP
-    for (int step = 0; step < a.nsteps; ++step) {
+  } else {  // KM_STEP, KM_XSTEP, KM_VSTEP
+    // time_integral.F90:57-161: neighbour trigger, rebuild, x update
+    auto first_half = [&](long long istep) {
       PHASE_T0(t_trig);
-      const long long istep = st.istep + 1;
       // neighbour trigger (time_integral.F90:57-110)
       bool rebuild;
       if (!skin) {
@@ -612,8 +630,10 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       if (tid == 0) s.misc[MISC_EXCESS] = 0;
       __syncthreads();
       PHASE_ADD(2, t_xu);
+    };
+    // time_integral.F90:162-183: forces (+ f_ext), v / a update
+    auto second_half = [&](long long istep, int nstep_noise) {
       PHASE_T0(t_fp);
-      const int nstep_noise = a.noise_base + step;
       force_pass<Real>(a, lane, L, T, s, istep, [&](int i, double fx, double fy, double fz) {
         // v / a update (time_integral.F90:169-183)
         double n0, n1, n2;
@@ -630,6 +650,17 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       if (tid == 0) st.istep = istep;
       __syncthreads();
       PHASE_ADD(6, t_fp);
+    };
+    if (a.mode == KM_STEP) {
+      for (int step = 0; step < a.nsteps; ++step) {
+        const long long istep = st.istep + 1;
+        first_half(istep);
+        second_half(istep, a.noise_base + step);
+      }
+    } else if (a.mode == KM_XSTEP) {
+      first_half(st.istep + 1);
+    } else {
+      second_half(st.istep + 1, a.noise_base);
     }
   }
   __syncthreads();
