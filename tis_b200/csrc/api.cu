@@ -107,7 +107,7 @@ struct tis_ctx {
   DBuf<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   DBuf<double> lab_Td, lab_coef, lab_cdist, lab_beta, lab_rele2, lab_u0, lab_c1;
   DBuf<int> lab_u0off, lab_c1off, elabel;
-  DBuf<double> xyz, pxyz, velo, accel, dxyz, out_force, out_energy, scale, ebeta;
+  DBuf<double> xyz, pxyz, velo, accel, dxyz, p0xyz, out_force, out_energy, scale, ebeta;
   unsigned long long rex_counter = 0;
   DBuf<uint32_t> mask;
   DBuf<int> site_exc;
@@ -529,7 +529,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->lab_c1off.upload(lab_c1off)); CK(c->lab_c1.upload(lab_c1));
   size_t n3 = 3 * (size_t)state_off;
   CK(c->xyz.alloc(n3)); CK(c->pxyz.alloc(n3)); CK(c->velo.alloc(n3)); CK(c->accel.alloc(n3));
-  CK(c->dxyz.alloc(n3)); CK(c->out_force.alloc(n3));
+  CK(c->dxyz.alloc(n3)); CK(c->out_force.alloc(n3)); CK(c->p0xyz.alloc(n3));
+  CK(cudaMemset(c->p0xyz.p, 0, n3 * 8));
   CK(cudaMemset(c->xyz.p, 0, n3 * 8)); CK(cudaMemset(c->pxyz.p, 0, n3 * 8));
   CK(cudaMemset(c->velo.p, 0, n3 * 8)); CK(cudaMemset(c->accel.p, 0, n3 * 8));
   CK(cudaMemset(c->dxyz.p, 0, n3 * 8));
@@ -585,7 +586,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
   c->lab_u0.free(); c->lab_c1.free(); c->lab_u0off.free(); c->lab_c1off.free(); c->elabel.free();
   c->ebeta.free();
-  c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free();
+  c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free(); c->p0xyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
   c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
@@ -717,6 +718,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.lab_c1off = c->lab_c1off.p; a.lab_c1 = c->lab_c1.p;
   a.b_c2 = c->b_c2.p; a.b_c3 = c->b_c3.p; a.b_c4 = c->b_c4.p;
   a.xyz = c->xyz.p; a.pxyz = c->pxyz.p; a.velo = c->velo.p; a.accel = c->accel.p; a.dxyz = c->dxyz.p;
+  a.p0xyz = c->p0xyz.p;
   a.mask = c->mask.p; a.mirror = c->mirror.p;
   a.smem_total = (int)c->smem;
   a.slots = c->slots.p; a.hb_flag = c->hb_flag.p; a.hb_ene = c->hb_ene.p; a.site_exc = c->site_exc.p;
@@ -736,7 +738,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
 // launch adds to each bead's sum).  No-op without Ewald.
 int ewald_recip(tis_ctx *c, KArgs &a, bool forces) {
   if (c->par.i_ele != TIS_ELE_EWALD) return TIS_OK;
-  c->launches += forces ? 3 : 2;
+  c->launches += (forces ? 3 : 2) + (c->nqblk > 1 ? 1 : 0);
   if (forces) a.f_ext = c->f_ext.p;   // written by the force kernel, read by the lane kernel
   CK(ewald_recip_launch(c->stream, a, c->nq_max, forces));
   return TIS_OK;
@@ -1131,7 +1133,7 @@ size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 // Byte offsets of the per-call buffers inside the static array.
 struct StaticLayout {
-  size_t lanes, lstate, xyz, pxyz, velo, accel, dxyz, mask, mirror, slots, hb_flag, hb_ene, site_exc, total;
+  size_t lanes, lstate, xyz, pxyz, velo, accel, dxyz, p0xyz, mask, mirror, slots, hb_flag, hb_ene, site_exc, total;
 };
 
 StaticLayout static_layout(const tis_ctx *c, int lane) {
@@ -1148,6 +1150,7 @@ StaticLayout static_layout(const tis_ctx *c, int lane) {
   s.velo = take(3 * N * sizeof(double));
   s.accel = take(3 * N * sizeof(double));
   s.dxyz = take(3 * N * sizeof(double));
+  s.p0xyz = take(c->par.i_periodic == 1 ? 3 * N * sizeof(double) : 1);
   s.mask = take(2 * N * W * sizeof(uint32_t));
   s.mirror = take(c->par.i_periodic == 1 ? N * N : 1);
   s.slots = take((size_t)T.nslot * 3 * real_size);
@@ -1194,6 +1197,7 @@ extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xy
   a.lstate = (LaneState *)(base + lay.lstate);
   a.xyz = (double *)(base + lay.xyz); a.pxyz = (double *)(base + lay.pxyz);
   a.velo = (double *)(base + lay.velo); a.accel = (double *)(base + lay.accel); a.dxyz = (double *)(base + lay.dxyz);
+  a.p0xyz = (double *)(base + lay.p0xyz);
   a.mask = (uint32_t *)(base + lay.mask);
   a.mirror = (uint8_t *)(base + lay.mirror);
   a.slots = (decltype(a.slots))(base + lay.slots);

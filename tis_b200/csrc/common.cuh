@@ -138,6 +138,7 @@ struct KArgs {
   const double *b_c2, *b_c3, *b_c4;             // rlan_const(2..4) per bead
   // state
   double *xyz, *pxyz, *velo, *accel, *dxyz;
+  double *p0xyz;           // periodic: pxyz as wrapped at the last rebuild (fixes each pair's image)
   // lists and scratch
   uint32_t *mask; uint8_t *mirror;
   int smem_total;          // dynamic shared memory bytes of the launch

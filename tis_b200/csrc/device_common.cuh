@@ -90,6 +90,7 @@ struct Smem {
   double *VX, *VY, *VZ;
   double *AX, *AY, *AZ;
   double *DX, *DY, *DZ;     // dxyz_mp (skin rule only)
+  double *QX, *QY, *QZ;     // periodic: pxyz wrapped at the last rebuild
   double *red;              // 64 doubles of reduction scratch
   double *ch_part;          // (3 * CHMAX) partial Debye-Hueckel force of each chunk
   double *rn2;              // rneighbordist2_unit (nunit x nunit)
@@ -118,7 +119,7 @@ struct SmemPlan { size_t base, mask, slots, inc, near; };
 __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc, bool periodic, bool skin,
                                               int real_size, int nunit) {
   size_t nd = 9 * (size_t)N + 64 + 3 * (size_t)CHMAX + (size_t)nunit * nunit + 2;
-  if (periodic) nd += 3 * (size_t)N;
+  if (periodic) nd += 6 * (size_t)N;
   if (skin) nd += 3 * (size_t)N;
   size_t b = nd * 8;
   b += 12 * (size_t)N * real_size;                  // A4, B4, L4
@@ -162,8 +163,13 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   s.X = d; s.Y = d + N; s.Z = d + 2 * N; d += 3 * N;
   s.VX = d; s.VY = d + N; s.VZ = d + 2 * N; d += 3 * N;
   s.AX = d; s.AY = d + N; s.AZ = d + 2 * N; d += 3 * N;
-  if (periodic) { s.PX = d; s.PY = d + N; s.PZ = d + 2 * N; d += 3 * N; }
-  else { s.PX = s.X; s.PY = s.Y; s.PZ = s.Z; }
+  if (periodic) {
+    s.PX = d; s.PY = d + N; s.PZ = d + 2 * N; d += 3 * N;
+    s.QX = d; s.QY = d + N; s.QZ = d + 2 * N; d += 3 * N;
+  } else {
+    s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
+    s.QX = s.QY = s.QZ = nullptr;
+  }
   if (skin) { s.DX = d; s.DY = d + N; s.DZ = d + 2 * N; d += 3 * N; }
   else { s.DX = s.DY = s.DZ = nullptr; }
   s.red = d; d += 64;

@@ -11,8 +11,9 @@
 //   ewald_tab_kernel    per charge: 3 (hmax + 1) sincos
 //   ewald_sk_kernel     per k and charge block: partial S_c(k) = sum q cos,
 //                       S_s(k) = sum q sin (charges in ascending order)
+//   ewald_sk_sum_kernel S(k) = the charge-block partials summed in block order
 //   ewald_force_kernel  per charge (one warp): F = sum_k coef 2 C(k)
-//                       q (sin S_c - cos S_s) k, partial S summed in block order
+//                       q (sin S_c - cos S_s) k
 //   ewald_energy_kernel per lane: coef (sum_k C(k) (S_c^2 + S_s^2) + self)
 //
 // All sums run in a fixed order, so the results do not depend on scheduling.
@@ -95,7 +96,27 @@ __global__ void __launch_bounds__(EW_SK_THREADS) ewald_sk_kernel(KArgs a) {
   }
 }
 
-// grid (ceil(nq / 8), nlane), 256 threads: one warp per charge
+// grid (ceil(nk / 256), nlane): S(k) = sum of the charge-block partials in
+// block order, stored in block 0's slot
+__global__ void __launch_bounds__(256) ewald_sk_sum_kernel(KArgs a) {
+  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.y;
+  if (lane >= a.nlane) return;
+  const int k = blockIdx.x * 256 + threadIdx.x;
+  if (k >= a.nk) return;
+  double *S = a.ew_S + (size_t)lane * a.nqblk * a.nk * 2;
+  double sc = S[2 * (size_t)k], ss = S[2 * (size_t)k + 1];
+  for (int b = 1; b < a.nqblk; ++b) {
+    sc += S[((size_t)b * a.nk + k) * 2];
+    ss += S[((size_t)b * a.nk + k) * 2 + 1];
+  }
+  S[2 * (size_t)k] = sc;
+  S[2 * (size_t)k + 1] = ss;
+}
+
+constexpr int EW_F_KCHUNK = 512;     // k vectors staged in shared memory at a time
+
+// grid (ceil(nq / 8), nlane), 256 threads: one warp per charge; the CTA
+// stages (S_c, S_s, C(k), h) of EW_F_KCHUNK vectors at a time for its 8 warps
 __global__ void __launch_bounds__(256) ewald_force_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.y;
   if (lane >= a.nlane) return;
@@ -104,33 +125,45 @@ __global__ void __launch_bounds__(256) ewald_force_kernel(KArgs a) {
   const int H = a.hmax + 1;
   const int warp = threadIdx.x >> 5, lid = threadIdx.x & 31;
   const int kq = blockIdx.x * 8 + warp;
-  if (kq >= T.nq) return;
-  const int bead = a.q_bead[T.q0 + kq];
-  const double q = a.b_charge[T.bead0 + bead];
+  const bool qv = kq < T.nq;
+  const int bead = qv ? a.q_bead[T.q0 + kq] : 0;
+  const double q = qv ? a.b_charge[T.bead0 + bead] : 0.0;
   const double coefT = a.lab_coef[a.lstate[lane].label];
-  const double2 *t = (const double2 *)a.ew_tab + (size_t)(L.ew0 + kq) * 3 * H;
+  const double2 *t = (const double2 *)a.ew_tab + (size_t)(L.ew0 + (qv ? kq : 0)) * 3 * H;
   const double *S = a.ew_S + (size_t)lane * a.nqblk * a.nk * 2;
+  __shared__ double2 sS[EW_F_KCHUNK];
+  __shared__ double sC[EW_F_KCHUNK];
+  __shared__ char4 sH[EW_F_KCHUNK];
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  for (int k = lid; k < a.nk; k += 32) {
-    const int hx = a.ew_h[3 * k], hy = a.ew_h[3 * k + 1], hz = a.ew_h[3 * k + 2];
-    const double2 e = cmul(cmul(tab_get(t, hx), tab_get(t + H, hy)), tab_get(t + 2 * H, hz));
-    double sc = 0.0, ss = 0.0;
-    for (int b = 0; b < a.nqblk; ++b) {
-      sc += S[((size_t)b * a.nk + k) * 2];
-      ss += S[((size_t)b * a.nk + k) * 2 + 1];
+  for (int k0 = 0; k0 < a.nk; k0 += EW_F_KCHUNK) {
+    const int nkc = min(EW_F_KCHUNK, a.nk - k0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < nkc; e += blockDim.x) {
+      const int k = k0 + e;
+      sS[e] = make_double2(S[2 * (size_t)k], S[2 * (size_t)k + 1]);
+      sC[e] = a.ew_coef[k];
+      sH[e] = make_char4(a.ew_h[3 * k], a.ew_h[3 * k + 1], a.ew_h[3 * k + 2], 0);
     }
-    // qs * scos - qc * ssin (force_ele_coulomb_ewld.F90:74-80)
-    const double dv = coefT * 2.0 * a.ew_coef[k] * (q * e.y * sc - q * e.x * ss);
-    fx += dv * (a.two_pi_L[0] * hx);
-    fy += dv * (a.two_pi_L[1] * hy);
-    fz += dv * (a.two_pi_L[2] * hz);
+    __syncthreads();
+    if (qv) {
+      for (int e = lid; e < nkc; e += 32) {
+        const char4 h = sH[e];
+        const double2 ex = cmul(cmul(tab_get(t, h.x), tab_get(t + H, h.y)), tab_get(t + 2 * H, h.z));
+        const double2 sk = sS[e];
+        // qs * scos - qc * ssin (force_ele_coulomb_ewld.F90:74-80)
+        const double dv = coefT * 2.0 * sC[e] * (q * ex.y * sk.x - q * ex.x * sk.y);
+        fx += dv * (a.two_pi_L[0] * h.x);
+        fy += dv * (a.two_pi_L[1] * h.y);
+        fz += dv * (a.two_pi_L[2] * h.z);
+      }
+    }
   }
   for (int o = 16; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
     fy += __shfl_xor_sync(0xffffffffu, fy, o);
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
-  if (lid == 0) {
+  if (qv && lid == 0) {
     double *f = a.f_ext + 3 * (size_t)(L.state0 + bead);
     f[0] = fx; f[1] = fy; f[2] = fz;
   }
@@ -147,11 +180,7 @@ __global__ void __launch_bounds__(256) ewald_energy_kernel(KArgs a) {
   const double *S = a.ew_S + (size_t)lane * a.nqblk * a.nk * 2;
   double ef = 0.0, qq = 0.0;
   for (int k = threadIdx.x; k < a.nk; k += blockDim.x) {
-    double sc = 0.0, ss = 0.0;
-    for (int b = 0; b < a.nqblk; ++b) {
-      sc += S[((size_t)b * a.nk + k) * 2];
-      ss += S[((size_t)b * a.nk + k) * 2 + 1];
-    }
+    const double sc = S[2 * (size_t)k], ss = S[2 * (size_t)k + 1];
     ef += a.ew_coef[k] * (sc * sc + ss * ss);
   }
   for (int kq = threadIdx.x; kq < T.nq; kq += blockDim.x) {
@@ -182,6 +211,7 @@ cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool
   const int nl = a.only_lane >= 0 ? 1 : a.nlane;
   ewald_tab_kernel<<<dim3((nq_max + 127) / 128, nl), 128, 0, st>>>(a);
   ewald_sk_kernel<<<dim3((a.nk + EW_SK_THREADS - 1) / EW_SK_THREADS, a.nqblk, nl), EW_SK_THREADS, 0, st>>>(a);
+  if (a.nqblk > 1) ewald_sk_sum_kernel<<<dim3((a.nk + 255) / 256, nl), 256, 0, st>>>(a);
   if (forces) ewald_force_kernel<<<dim3((nq_max + 7) / 8, nl), 256, 0, st>>>(a);
   return cudaGetLastError();
 }

@@ -45,6 +45,7 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
       s.PX[i] = wrap1(s.PX[i], a.psize[0]);
       s.PY[i] = wrap1(s.PY[i], a.psize[1]);
       s.PZ[i] = wrap1(s.PZ[i], a.psize[2]);
+      s.QX[i] = s.PX[i]; s.QY[i] = s.PY[i]; s.QZ[i] = s.PZ[i];
       set_pos<Real>(s, i);
     }
   }
@@ -198,18 +199,20 @@ __device__ __forceinline__ int pow2_floor_clamp(int x, int hi) {
   return g;
 }
 
-// periodic image of the pair fixed at the last rebuild: d_mirror(:, imirror)
-// of the canonical (min, max) orientation, negated for the reverse one
-template <typename T>
-__device__ __forceinline__ void mirror_shift(const KArgs &a, const uint8_t *mir, int N, int i, int j,
-                                             T &w0, T &w1, T &w2) {
+// Periodic image of the pair fixed at the last rebuild (d_mirror(:, imirror)
+// of the canonical (min, max) orientation, negated for the reverse one),
+// recomputed from the positions wrapped at that rebuild with the same
+// rounded FP64 operations as the list build: the same image as its mirror
+// table, without a global-memory lookup.
+template <typename T, typename S>
+__device__ __forceinline__ void mirror_shift(const KArgs &a, const S &s, int i, int j, T &w0, T &w1, T &w2) {
   const int lo = i < j ? i : j, hi = i < j ? j : i;
-  const int im = (int)mir[(size_t)lo * N + hi] - 1;
   const T sg = (j > i) ? (T)1 : (T)-1;
-  const int m0 = im / 9, m1 = (im / 3) % 3, m2 = im % 3;
-  if (m0 != 2) w0 += sg * (T)(m0 == 0 ? -a.psize[0] : a.psize[0]);
-  if (m1 != 2) w1 += sg * (T)(m1 == 0 ? -a.psize[1] : a.psize[1]);
-  if (m2 != 2) w2 += sg * (T)(m2 == 0 ? -a.psize[2] : a.psize[2]);
+  const double v0 = __dsub_rn(s.QX[hi], s.QX[lo]), v1 = __dsub_rn(s.QY[hi], s.QY[lo]),
+               v2 = __dsub_rn(s.QZ[hi], s.QZ[lo]);
+  if (v0 > a.psizeh[0]) w0 -= sg * (T)a.psize[0]; else if (v0 < -a.psizeh[0]) w0 += sg * (T)a.psize[0];
+  if (v1 > a.psizeh[1]) w1 -= sg * (T)a.psize[1]; else if (v1 < -a.psizeh[1]) w1 += sg * (T)a.psize[1];
+  if (v2 > a.psizeh[2]) w2 -= sg * (T)a.psize[2]; else if (v2 < -a.psizeh[2]) w2 += sg * (T)a.psize[2];
 }
 
 template <typename Real> __device__ __forceinline__ Real rsq(Real x);
@@ -334,7 +337,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const V p0 = s.A4[j0], p1 = s.A4[j1];
             Real ax = p0.x - pi.x, ay = p0.y - pi.y, az = p0.z - pi.z;
             Real bx = p1.x - pi.x, by = p1.y - pi.y, bz = p1.z - pi.z;
-            if (mir) { mirror_shift<Real>(a, mir, N, i, j0, ax, ay, az); mirror_shift<Real>(a, mir, N, i, j1, bx, by, bz); }
+            if (mir) { mirror_shift<Real>(a, s, i, j0, ax, ay, az); mirror_shift<Real>(a, s, i, j1, bx, by, bz); }
             const Real ra2 = ax * ax + ay * ay + az * az, rb2 = bx * bx + by * by + bz * bz;
             const Real ria = rsq<Real>(ra2), rib = rsq<Real>(rb2);
             const Real da = ra2 * ria, db = rb2 * rib;
@@ -407,7 +410,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       auto visit = [&](int j, bool rec, int &cnt, uint16_t *lst, int ncap) {
         const V pj = s.A4[j];
         Real sx = pj.x - pi.x, sy = pj.y - pi.y, sz = pj.z - pi.z;
-        if (mir) mirror_shift<Real>(a, mir, N, i, j, sx, sy, sz);
+        if (mir) mirror_shift<Real>(a, s, i, j, sx, sy, sz);
         const Real d2s = sx * sx + sy * sy + sz * sz;
         if (rec && d2s <= nscr2) {
           if (cnt < ncap) lst[cnt] = (uint16_t)j;
@@ -510,7 +513,10 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   for (int i = tid; i < N; i += nth) {
     const size_t o = 3 * (size_t)(L.state0 + i);
     s.X[i] = a.xyz[o]; s.Y[i] = a.xyz[o + 1]; s.Z[i] = a.xyz[o + 2];
-    if (a.periodic) { s.PX[i] = a.pxyz[o]; s.PY[i] = a.pxyz[o + 1]; s.PZ[i] = a.pxyz[o + 2]; }
+    if (a.periodic) {
+      s.PX[i] = a.pxyz[o]; s.PY[i] = a.pxyz[o + 1]; s.PZ[i] = a.pxyz[o + 2];
+      s.QX[i] = a.p0xyz[o]; s.QY[i] = a.p0xyz[o + 1]; s.QZ[i] = a.p0xyz[o + 2];
+    }
     s.VX[i] = a.velo[o]; s.VY[i] = a.velo[o + 1]; s.VZ[i] = a.velo[o + 2];
     s.AX[i] = a.accel[o]; s.AY[i] = a.accel[o + 1]; s.AZ[i] = a.accel[o + 2];
     if (skin) { s.DX[i] = a.dxyz[o]; s.DY[i] = a.dxyz[o + 1]; s.DZ[i] = a.dxyz[o + 2]; }
@@ -565,102 +571,96 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
       s.AX[i] = fx * rc + cc * n0; s.AY[i] = fy * rc + cc * n1; s.AZ[i] = fz * rc + cc * n2;
     });
-  } else {  // KM_STEP, KM_XSTEP, KM_VSTEP
-    // time_integral.F90:57-161: neighbour trigger, rebuild, x update
-    auto first_half = [&](long long istep) {
-      PHASE_T0(t_trig);
-      // neighbour trigger (time_integral.F90:57-110)
-      bool rebuild;
-      if (!skin) {
-        rebuild = (istep % a.n_step_neighbor) == 1 || istep == 1;
-      } else {
-        double m1 = 0, m2 = 0;
-        for (int i = tid; i < N; i += nth) {
-          double d2 = s.DX[i] * s.DX[i] + s.DY[i] * s.DY[i] + s.DZ[i] * s.DZ[i];
-          if (d2 > m1) { m2 = m1; m1 = d2; } else if (d2 > m2) m2 = d2;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-          double o1 = __shfl_xor_sync(0xffffffffu, m1, o), o2 = __shfl_xor_sync(0xffffffffu, m2, o);
-          double n1 = fmax(m1, o1), n2 = fmax(fmin(m1, o1), fmax(m2, o2));
-          m1 = n1; m2 = n2;
-        }
-        if ((tid & 31) == 0) { s.red[2 * (tid >> 5)] = m1; s.red[2 * (tid >> 5) + 1] = m2; }
-        __syncthreads();
-        if (tid == 0) {
-          double b1 = 0, b2 = 0;
-          for (int w = 0; w < (nth >> 5); ++w) {
-            double o1 = s.red[2 * w], o2 = s.red[2 * w + 1];
-            double n1 = fmax(b1, o1), n2 = fmax(fmin(b1, o1), fmax(b2, o2));
-            b1 = n1; b2 = n2;
+  } else {  // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step)
+    const int nloop = (a.mode == KM_STEP) ? a.nsteps : 1;
+    for (int step = 0; step < nloop; ++step) {
+      const long long istep = st.istep + 1;
+      if (a.mode != KM_VSTEP) {
+        // time_integral.F90:57-161: neighbour trigger, rebuild, x update
+        PHASE_T0(t_trig);
+        // neighbour trigger (time_integral.F90:57-110)
+        bool rebuild;
+        if (!skin) {
+          rebuild = (istep % a.n_step_neighbor) == 1 || istep == 1;
+        } else {
+          double m1 = 0, m2 = 0;
+          for (int i = tid; i < N; i += nth) {
+            double d2 = s.DX[i] * s.DX[i] + s.DY[i] * s.DY[i] + s.DZ[i] * s.DZ[i];
+            if (d2 > m1) { m2 = m1; m1 = d2; } else if (d2 > m2) m2 = d2;
           }
-          s.misc[MISC_REBUILD] = (sqrt(b1) + sqrt(b2) > a.neigh_margin) ? 1 : 0;
+          for (int o = 16; o > 0; o >>= 1) {
+            double o1 = __shfl_xor_sync(0xffffffffu, m1, o), o2 = __shfl_xor_sync(0xffffffffu, m2, o);
+            double n1 = fmax(m1, o1), n2 = fmax(fmin(m1, o1), fmax(m2, o2));
+            m1 = n1; m2 = n2;
+          }
+          if ((tid & 31) == 0) { s.red[2 * (tid >> 5)] = m1; s.red[2 * (tid >> 5) + 1] = m2; }
+          __syncthreads();
+          if (tid == 0) {
+            double b1 = 0, b2 = 0;
+            for (int w = 0; w < (nth >> 5); ++w) {
+              double o1 = s.red[2 * w], o2 = s.red[2 * w + 1];
+              double n1 = fmax(b1, o1), n2 = fmax(fmin(b1, o1), fmax(b2, o2));
+              b1 = n1; b2 = n2;
+            }
+            s.misc[MISC_REBUILD] = (sqrt(b1) + sqrt(b2) > a.neigh_margin) ? 1 : 0;
+          }
+          __syncthreads();
+          rebuild = s.misc[MISC_REBUILD] != 0;
         }
-        __syncthreads();
-        rebuild = s.misc[MISC_REBUILD] != 0;
-      }
-      PHASE_ADD(0, t_trig);
-      PHASE_T0(t_reb);
-      if (rebuild) {
-        build_lists<Real>(a, lane, L, T, s);
-        // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
-        if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
-        __syncthreads();
-      }
-      PHASE_ADD(1, t_reb);
-      PHASE_T0(t_xu);
-      // x update (time_integral.F90:152-161); clear hbond-site counters
-      for (int i = tid; i < N; i += nth) {
-        const int b = T.bead0 + i;
-        const double c4 = a.b_c4[b];
-        double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
-        double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
-        double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
-        s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
-        if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
-        if (skin) { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
-        set_pos<Real>(s, i);
-        if (s.near_on) {
-          const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
-                      ez = (float)s.A4[i].z - s.NR4[i].z;
-          const float e2 = ex * ex + ey * ey + ez * ez;
-          if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
+        PHASE_ADD(0, t_trig);
+        PHASE_T0(t_reb);
+        if (rebuild) {
+          build_lists<Real>(a, lane, L, T, s);
+          // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
+          if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
+          __syncthreads();
         }
+        PHASE_ADD(1, t_reb);
+        PHASE_T0(t_xu);
+        // x update (time_integral.F90:152-161); clear hbond-site counters
+        for (int i = tid; i < N; i += nth) {
+          const int b = T.bead0 + i;
+          const double c4 = a.b_c4[b];
+          double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
+          double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
+          double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
+          s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
+          if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
+          if (skin) { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
+          set_pos<Real>(s, i);
+          if (s.near_on) {
+            const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
+                        ez = (float)s.A4[i].z - s.NR4[i].z;
+            const float e2 = ex * ex + ey * ey + ez * ez;
+            if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
+          }
+        }
+        for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+        if (tid == 0) s.misc[MISC_EXCESS] = 0;
+        __syncthreads();
+        PHASE_ADD(2, t_xu);
       }
-      for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
-      if (tid == 0) s.misc[MISC_EXCESS] = 0;
-      __syncthreads();
-      PHASE_ADD(2, t_xu);
-    };
-    // time_integral.F90:162-183: forces (+ f_ext), v / a update
-    auto second_half = [&](long long istep, int nstep_noise) {
-      PHASE_T0(t_fp);
-      force_pass<Real>(a, lane, L, T, s, istep, [&](int i, double fx, double fy, double fz) {
-        // v / a update (time_integral.F90:169-183)
-        double n0, n1, n2;
-        noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
-        const int b = T.bead0 + i;
-        const double rc = a.b_rcmass[b], cc = c1[i], c2 = a.b_c2[b], c3 = a.b_c3[b];
-        const double ax = fx * rc + cc * n0, ay = fy * rc + cc * n1, az = fz * rc + cc * n2;
-        s.VX[i] = c2 * s.VX[i] + c3 * (s.AX[i] + ax);
-        s.VY[i] = c2 * s.VY[i] + c3 * (s.AY[i] + ay);
-        s.VZ[i] = c2 * s.VZ[i] + c3 * (s.AZ[i] + az);
-        s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
-        if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
-      });
-      if (tid == 0) st.istep = istep;
-      __syncthreads();
-      PHASE_ADD(6, t_fp);
-    };
-    if (a.mode == KM_STEP) {
-      for (int step = 0; step < a.nsteps; ++step) {
-        const long long istep = st.istep + 1;
-        first_half(istep);
-        second_half(istep, a.noise_base + step);
+      if (a.mode != KM_XSTEP) {
+        // time_integral.F90:162-183: forces (+ f_ext), v / a update
+        const int nstep_noise = a.noise_base + step;
+        PHASE_T0(t_fp);
+        force_pass<Real>(a, lane, L, T, s, istep, [&](int i, double fx, double fy, double fz) {
+          // v / a update (time_integral.F90:169-183)
+          double n0, n1, n2;
+          noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
+          const int b = T.bead0 + i;
+          const double rc = a.b_rcmass[b], cc = c1[i], c2 = a.b_c2[b], c3 = a.b_c3[b];
+          const double ax = fx * rc + cc * n0, ay = fy * rc + cc * n1, az = fz * rc + cc * n2;
+          s.VX[i] = c2 * s.VX[i] + c3 * (s.AX[i] + ax);
+          s.VY[i] = c2 * s.VY[i] + c3 * (s.AY[i] + ay);
+          s.VZ[i] = c2 * s.VZ[i] + c3 * (s.AZ[i] + az);
+          s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
+          if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
+        });
+        if (tid == 0) st.istep = istep;
+        __syncthreads();
+        PHASE_ADD(6, t_fp);
       }
-    } else if (a.mode == KM_XSTEP) {
-      first_half(st.istep + 1);
-    } else {
-      second_half(st.istep + 1, a.noise_base);
     }
   }
   __syncthreads();
@@ -673,8 +673,12 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   for (int i = tid; i < N; i += nth) {
     const size_t o = 3 * (size_t)(L.state0 + i);
     a.xyz[o] = s.X[i]; a.xyz[o + 1] = s.Y[i]; a.xyz[o + 2] = s.Z[i];
-    if (a.periodic) { a.pxyz[o] = s.PX[i]; a.pxyz[o + 1] = s.PY[i]; a.pxyz[o + 2] = s.PZ[i]; }
-    else { a.pxyz[o] = s.X[i]; a.pxyz[o + 1] = s.Y[i]; a.pxyz[o + 2] = s.Z[i]; }
+    if (a.periodic) {
+      a.pxyz[o] = s.PX[i]; a.pxyz[o + 1] = s.PY[i]; a.pxyz[o + 2] = s.PZ[i];
+      a.p0xyz[o] = s.QX[i]; a.p0xyz[o + 1] = s.QY[i]; a.p0xyz[o + 2] = s.QZ[i];
+    } else {
+      a.pxyz[o] = s.X[i]; a.pxyz[o + 1] = s.Y[i]; a.pxyz[o + 2] = s.Z[i];
+    }
     a.velo[o] = s.VX[i]; a.velo[o + 1] = s.VY[i]; a.velo[o + 2] = s.VZ[i];
     a.accel[o] = s.AX[i]; a.accel[o + 1] = s.AY[i]; a.accel[o + 2] = s.AZ[i];
     if (skin) { a.dxyz[o] = s.DX[i]; a.dxyz[o + 1] = s.DY[i]; a.dxyz[o + 2] = s.DZ[i]; }
