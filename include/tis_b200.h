@@ -141,6 +141,8 @@ typedef struct tis_params {
   int32_t precision;               /* TIS_PREC_* */
   int32_t hb_beta_global;          /* 1: reference quirk (one beta_hbond15 for all replicas) */
   uint64_t seed;                   /* counter-based noise key */
+  double hi_radius;                /* Brownian-HI: Rotne-Prager bead radius (radius(1) of HI_TENSOR%RPY) */
+  int32_t n_step_hydro;            /* Brownian-HI: refactor D and its Cholesky factor every n steps (reference: 1) */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */

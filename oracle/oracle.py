@@ -60,6 +60,7 @@ def lib():
         L.orc_coulomb_direct.argtypes = [vp, C.c_int, C.c_int]
         L.orc_coulomb_direct.restype = C.c_double
         L.orc_hydro_tensors.argtypes = [vp, C.c_int, C.c_double, f64p, f64p]
+        L.orc_not_spd.argtypes = [vp]
         L.orc_nclamp.argtypes = [vp]
         L.orc_nclamp.restype = C.c_long
         L.orc_boltz_kcal_mol.restype = C.c_double
@@ -205,6 +206,9 @@ class Oracle:
         rc = self.L.orc_hydro_tensors(self.h, irep, rad, ptr_f64(D), None if Lm is None else ptr_f64(Lm))
         # column-major (3N, 3N) buffers: transpose to row-major views
         return D.T.copy(), (None if Lm is None else Lm.T.copy()), rc
+
+    def not_spd(self):
+        return self.L.orc_not_spd(self.h)
 
     def nclamp(self):
         return self.L.orc_nclamp(self.h)

@@ -77,6 +77,8 @@ struct Rep {
   bool unif_exhausted = false;
   long nclamp = 0;
   long nrebuild = 0;
+  std::vector<double> hD, hL;     // Brownian-HI: diffuse_tensor, random_tensor (3N x 3N, column-major)
+  int not_spd = 0;
 };
 
 } // namespace
@@ -937,6 +939,28 @@ double energy_fene(const orc_ctx &c, const Rep &r) {
   }
   return e;
 }
+// energy_wca.F90 (loop body): repulsive and attractive parts
+void energy_wca(const orc_ctx &c, const Rep &r, double &e_rep, double &e_att) {
+  double rcut_off2 = 1.0 / sq(c.par.wca_coef_cutoff);
+  const bool peri = c.par.i_periodic == 1;
+  e_rep = 0.0; e_att = 0.0;
+  for (int i = 0; i < c.nwca; ++i) {
+    int i1 = c.wca2mp[2 * i] - 1, i2 = c.wca2mp[2 * i + 1] - 1;
+    double v21[3];
+    if (!peri) for (int k = 0; k < 3; ++k) v21[k] = r.xyz[3 * i2 + k] - r.xyz[3 * i1 + k];
+    else { for (int k = 0; k < 3; ++k) v21[k] = r.pxyz[3 * i2 + k] - r.pxyz[3 * i1 + k]; pbneighbor(c, v21, nullptr); }
+    double dist2 = dot3(v21, v21);
+    double ro2 = c.wca_nat[i] * c.wca_nat[i] / dist2;
+    if (ro2 < rcut_off2) continue;
+    double ro6 = std::pow(ro2, 6), ro3 = std::pow(ro2, 3);
+    if (ro2 >= 1.0e0) {
+      e_rep += c.coef_wca[i] * (ro6 - 2.0e0 * ro3 + 1.0e0);
+      e_att += -c.coef_wca[c.nwca + i];
+    } else {
+      e_att += c.coef_wca[c.nwca + i] * (ro6 - 2.0e0 * ro3);
+    }
+  }
+}
 // energy_dtrna_stack.F90 (loop body)
 double energy_stack(const orc_ctx &c, const Rep &r) {
   const Label &L = c.lab[r.label - 1];
@@ -1061,6 +1085,7 @@ void energy_sumup(orc_ctx &c, Rep &r, double *E, bool reuse_hb) {
     ek += 0.5 * c.cmass[imp] * (sq(r.velo[3 * imp]) + sq(r.velo[3 * imp + 1]) + sq(r.velo[3 * imp + 2]));
   E[TIS_E_VELO - 1] = ek;
   E[TIS_E_BOND - 1] = energy_bond(c, r) + energy_fene(c, r);   // energy_fene.F90 adds to E_TYPE%BOND
+  if (c.nwca) energy_wca(c, r, E[TIS_E_WCA_REP - 1], E[TIS_E_WCA_ATT - 1]);
   E[TIS_E_BANGLE - 1] = energy_bangle(c, r);
   if (c.nst > 0 || c.nhb > 0) {
     if (r.st_status.size() != (size_t)c.nst) r.st_status.assign(c.nst, 1);
@@ -1381,12 +1406,73 @@ int orc_energy_sumup(orc_ctx *c, int irep, double *energy, int reuse_hb) {
   return 0;
 }
 
-// time_integral_pre.F90:75-180 (Langevin)
+// simu_hydro_tensors.F90:139-182 (HI_TENSOR%RPY, one radius) and 304-324
+// (Cholesky); D and L are (3N, 3N) column-major.  Returns 0 or TIS_E_NOT_SPD.
+int hydro_tensors(const orc_ctx *c, const Rep &r, double rad, double *D, double *Lc) {
+  double tempk = c->lab[r.label - 1].tempk;
+  int N = c->nmp, n = 3 * N;
+  double c6 = BOLTZ_KCAL_MOL * tempk / (6.0e0 * F_PI * c->par.viscosity);
+  double c8 = BOLTZ_KCAL_MOL * tempk / (8.0e0 * F_PI * c->par.viscosity);
+  auto Dm = [&](int i, int j) -> double & { return D[(size_t)j * n + i]; };
+  std::fill(D, D + (size_t)n * n, 0.0);
+  for (int i = 0; i < N; ++i) {
+    int i0 = 3 * i;
+    for (int j = i + 1; j < N; ++j) {
+      int j0 = 3 * j;
+      double rv[3];
+      for (int d = 0; d < 3; ++d) rv[d] = r.xyz[3 * j + d] - r.xyz[3 * i + d];
+      double r_sq = dot3(rv, rv), r_abs = std::sqrt(r_sq);
+      double rad_sq = rad * rad;
+      double pre1 = c8 / r_abs * (1.0 + 2.0 * rad_sq / (3.0 * r_sq));
+      double pre2 = c8 / r_abs * (1.0 - 2.0 * rad_sq / r_sq) / r_sq;
+      for (int ii = 0; ii < 3; ++ii) {
+        Dm(i0 + ii, j0 + ii) = pre1 + pre2 * rv[ii] * rv[ii];
+        for (int jj = ii + 1; jj < 3; ++jj) {
+          Dm(i0 + ii, j0 + jj) = pre2 * rv[ii] * rv[jj];
+          Dm(i0 + jj, j0 + ii) = Dm(i0 + ii, j0 + jj);
+        }
+      }
+    }
+  }
+  // D = D + transpose(D)
+  for (int j = 0; j < n; ++j)
+    for (int i = j + 1; i < n; ++i) {
+      double s = Dm(i, j) + Dm(j, i);
+      Dm(i, j) = s; Dm(j, i) = s;
+    }
+  for (int i = 0; i < n; ++i) Dm(i, i) = c6 / rad;
+  if (!Lc) return 0;
+  auto Lm = [&](int i, int j) -> double & { return Lc[(size_t)j * n + i]; };
+  std::fill(Lc, Lc + (size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double x = Dm(i, i);
+    for (int k = 0; k < i; ++k) x -= Lm(i, k) * Lm(i, k);
+    if (x <= 0.0) return TIS_E_NOT_SPD;
+    x = std::sqrt(x);
+    Lm(i, i) = x;
+    for (int j = i + 1; j < n; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < i; ++k) s += Lm(j, k) * Lm(i, k);
+      Lm(j, i) = (Dm(i, j) - s) / x;
+    }
+  }
+  return 0;
+}
+// time_integral_pre.F90:75-180 (Langevin) and :313-317 (Brownian-HI:
+// velocities zero, rlan_const(1) = tstep / kT, rlan_const(2) = sqrt(2 tstep))
 int orc_time_integral_pre(orc_ctx *c) {
   for (auto &r : c->rep) neighbor(*c, r);
   for (auto &r : c->rep) std::fill(r.dxyz.begin(), r.dxyz.end(), 0.0);
   std::vector<double> rbm;
   take_noise_step(*c, rbm);
+  if (c->par.i_simulate_type == TIS_SIM_BROWNIAN_HI) {
+    for (auto &r : c->rep) {
+      force_sumup(*c, r, r.force.data());
+      std::fill(r.velo.begin(), r.velo.end(), 0.0);
+      std::fill(r.accel.begin(), r.accel.end(), 0.0);
+    }
+    return c->noise_exhausted ? TIS_E_NOISE_EXHAUSTED : 0;
+  }
   size_t n3 = 3 * (size_t)c->nmp;
   for (int i = 0; i < c->nrep; ++i) {
     Rep &r = c->rep[i];
@@ -1428,6 +1514,35 @@ int orc_step(orc_ctx *c, long nsteps) {
       }
     }
     take_noise_step(*c, rbm);
+    if (c->par.i_simulate_type == TIS_SIM_BROWNIAN_HI) {
+      // time_integral.F90:429-457: D and L at the current x (every
+      // n_step_hydro steps), dx = rlan1 D F + rlan2 L xi, then the force
+      const int n = 3 * c->nmp;
+      const int every = c->par.n_step_hydro > 0 ? c->par.n_step_hydro : 1;
+      for (int i = 0; i < c->nrep; ++i) {
+        Rep &r = c->rep[i];
+        r.istep++;
+        const double T = c->lab[r.label - 1].tempk;
+        if ((r.istep - 1) % every == 0) {
+          r.hD.resize((size_t)n * n);
+          r.hL.resize((size_t)n * n);
+          if (hydro_tensors(c, r, c->par.hi_radius, r.hD.data(), r.hL.data()) != 0) r.not_spd = 1;
+        }
+        const double rl1 = c->par.tstep / (BOLTZ_KCAL_MOL * T), rl2 = std::sqrt(2.0e0 * c->par.tstep);
+        const double *xi = &rbm[n3 * i];
+        for (int k = 0; k < n; ++k) {
+          double df = 0.0, dr = 0.0;
+          for (int m = 0; m < n; ++m) df += r.hD[(size_t)k * n + m] * r.force[m];
+          for (int m = 0; m <= k; ++m) dr += r.hL[(size_t)m * n + k] * xi[m];
+          const double dx = rl1 * df + rl2 * dr;
+          r.xyz[k] = r.xyz[k] + dx;
+          r.pxyz[k] = r.pxyz[k] + dx;
+          r.dxyz[k] = r.dxyz[k] + dx;
+        }
+        force_sumup(*c, r, r.force.data());
+      }
+      continue;
+    }
     for (int i = 0; i < c->nrep; ++i) {
       Rep &r = c->rep[i];
       r.istep++;
@@ -1568,58 +1683,14 @@ double orc_coulomb_direct(orc_ctx *c, int irep, int nlat) {
   return L.coef * e;
 }
 
-// simu_hydro_tensors.F90:139-182 (RPY, one radius) and 304-324 (Cholesky);
-// D and L are (3N, 3N) column-major.  Returns 0 or TIS_E_NOT_SPD.
 int orc_hydro_tensors(orc_ctx *c, int irep, double rad, double *D, double *Lc) {
-  const Rep &r = c->rep[irep - 1];
-  double tempk = c->lab[r.label - 1].tempk;
-  int N = c->nmp, n = 3 * N;
-  double c6 = BOLTZ_KCAL_MOL * tempk / (6.0e0 * F_PI * c->par.viscosity);
-  double c8 = BOLTZ_KCAL_MOL * tempk / (8.0e0 * F_PI * c->par.viscosity);
-  auto Dm = [&](int i, int j) -> double & { return D[(size_t)j * n + i]; };
-  std::fill(D, D + (size_t)n * n, 0.0);
-  for (int i = 0; i < N; ++i) {
-    int i0 = 3 * i;
-    for (int j = i + 1; j < N; ++j) {
-      int j0 = 3 * j;
-      double rv[3];
-      for (int d = 0; d < 3; ++d) rv[d] = r.xyz[3 * j + d] - r.xyz[3 * i + d];
-      double r_sq = dot3(rv, rv), r_abs = std::sqrt(r_sq);
-      double rad_sq = rad * rad;
-      double pre1 = c8 / r_abs * (1.0 + 2.0 * rad_sq / (3.0 * r_sq));
-      double pre2 = c8 / r_abs * (1.0 - 2.0 * rad_sq / r_sq) / r_sq;
-      for (int ii = 0; ii < 3; ++ii) {
-        Dm(i0 + ii, j0 + ii) = pre1 + pre2 * rv[ii] * rv[ii];
-        for (int jj = ii + 1; jj < 3; ++jj) {
-          Dm(i0 + ii, j0 + jj) = pre2 * rv[ii] * rv[jj];
-          Dm(i0 + jj, j0 + ii) = Dm(i0 + ii, j0 + jj);
-        }
-      }
-    }
-  }
-  // D = D + transpose(D)
-  for (int j = 0; j < n; ++j)
-    for (int i = j + 1; i < n; ++i) {
-      double s = Dm(i, j) + Dm(j, i);
-      Dm(i, j) = s; Dm(j, i) = s;
-    }
-  for (int i = 0; i < n; ++i) Dm(i, i) = c6 / rad;
-  if (!Lc) return 0;
-  auto Lm = [&](int i, int j) -> double & { return Lc[(size_t)j * n + i]; };
-  std::fill(Lc, Lc + (size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) {
-    double x = Dm(i, i);
-    for (int k = 0; k < i; ++k) x -= Lm(i, k) * Lm(i, k);
-    if (x <= 0.0) return TIS_E_NOT_SPD;
-    x = std::sqrt(x);
-    Lm(i, i) = x;
-    for (int j = i + 1; j < n; ++j) {
-      double s = 0.0;
-      for (int k = 0; k < i; ++k) s += Lm(j, k) * Lm(i, k);
-      Lm(j, i) = (Dm(i, j) - s) / x;
-    }
-  }
-  return 0;
+  return hydro_tensors(c, c->rep[irep - 1], rad, D, Lc);
+}
+
+int orc_not_spd(orc_ctx *c) {
+  int f = 0;
+  for (auto &r : c->rep) f |= r.not_spd;
+  return f;
 }
 
 long orc_nclamp(orc_ctx *c) {

@@ -1,0 +1,101 @@
+"""Brownian dynamics with hydrodynamic interactions (Ermak-McCammon with the
+Rotne-Prager tensor and its Cholesky factor, time_integral.F90:429-457,
+simu_hydro_tensors.F90) on the GPU against the CPU restatement, through the
+C-ABI.  Bead chains with FENE bonds and WCA records for every non-bonded
+pair.  Everything is FP64: forces and energies relative 1e-9, trajectories
+with injected noise 1e-9 A.
+"""
+import numpy as np
+import pytest
+
+from tis_b200 import synth
+from tis_b200.engine import Engine, TisError
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+TIS_E_NOT_SPD = -4
+
+
+def rel_force_err(f, ref):
+    mag = np.linalg.norm(ref, axis=1)
+    den = np.maximum(mag, np.median(mag))
+    return np.max(np.linalg.norm(f - ref, axis=1) / den)
+
+
+def squeezed_chain(n, seed):
+    """A chain pulled together so that some WCA pairs are inside sigma."""
+    s = synth.bead_chain(n, seed)
+    s = dict(s)
+    s["xyz"] = s["xyz"] * 0.85
+    return s
+
+
+@pytest.mark.parametrize("n", [24, 90])
+def test_bdhi_forces_and_energy(tis_lib, n):
+    s = squeezed_chain(n, 7)
+    par = synth.bdhi_params()
+    eng = Engine([s], par, [300.0])
+    orc = Oracle(s, par, [300.0])
+    eng.set_state(s["xyz"])
+    orc.set_state(s["xyz"][None])
+    orc.neighbor()
+    f, _ = eng.force()
+    fr, _ = orc.force()
+    assert np.abs(orc.force_term("wca")).max() > 0.1       # WCA pairs inside sigma
+    assert rel_force_err(f, fr) < 1e-9
+    e = eng.energy()
+    er = orc.energy()
+    for k in (3, 23, 24):   # BOND (FENE), WCA_REP, WCA_ATT
+        assert abs(e[k - 1] - er[k - 1]) <= 1e-9 * max(1.0, abs(er[k - 1])), k
+    eng.close()
+
+
+@pytest.mark.parametrize("every", [1, 3])
+def test_bdhi_trajectory_injected_noise(tis_lib, every):
+    ns = [30, 47, 64]
+    systems = [squeezed_chain(n, 11 + k) for k, n in enumerate(ns)]
+    par = synth.bdhi_params(n_step_hydro=every)
+    nsteps = 7
+    eng = Engine(systems, par, [290.0, 300.0, 310.0], nrep=[1, 1, 1])
+    eng.set_state(np.concatenate([s["xyz"] for s in systems]))
+    rng = np.random.default_rng(5)
+    noise = rng.normal(size=(nsteps + 1, sum(ns), 3))
+    eng.set_noise(noise)
+    assert eng.time_integral_pre() >= 0
+    assert eng.step(nsteps) >= 0
+    x, _, _ = eng.get_state()
+    off = 0
+    for k, (s, T) in enumerate(zip(systems, [290.0, 300.0, 310.0])):
+        orc = Oracle(s, par, [T])
+        orc.set_state(s["xyz"][None])
+        orc.set_noise(noise[:, off:off + s["nmp"]].reshape(nsteps + 1, 1, s["nmp"], 3))
+        assert orc.time_integral_pre() == 0
+        assert orc.step(nsteps) == 0
+        assert not orc.not_spd()
+        xr = orc.get_state()[0].reshape(-1, 3)
+        moved = np.abs(xr - s["xyz"]).max()
+        assert moved > 1e-3
+        assert np.abs(x[off:off + s["nmp"]] - xr).max() < 1e-9, k
+        off += s["nmp"]
+    eng.close()
+
+
+def test_bdhi_reports_non_spd_tensor(tis_lib):
+    s = synth.bead_chain(40, 3)
+    s = dict(s)
+    x = s["xyz"].copy()
+    x[5] = x[20] + np.array([0.05, 0.0, 0.0])   # two beads almost on top of each other
+    s["xyz"] = x
+    par = synth.bdhi_params()
+    orc = Oracle(s, par, [300.0])
+    orc.set_state(x[None])
+    _, _, rc = orc.hydro_tensors(par["hi_radius"])
+    assert rc == TIS_E_NOT_SPD
+    eng = Engine([s], par, [300.0])
+    eng.set_state(x)
+    eng.time_integral_pre()
+    with pytest.raises(TisError) as e:
+        eng.step(1)
+    assert e.value.code == TIS_E_NOT_SPD
+    assert eng.status()["not_spd"] == 1
+    eng.close()

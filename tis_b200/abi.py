@@ -70,6 +70,7 @@ class Params(C.Structure):
         ("i_simulate_type", C.c_int32), ("tstep", C.c_double),
         ("viscosity", C.c_double), ("wca_coef_cutoff", C.c_double),
         ("precision", C.c_int32), ("hb_beta_global", C.c_int32), ("seed", C.c_uint64),
+        ("hi_radius", C.c_double), ("n_step_hydro", C.c_int32),
     ]
 
 

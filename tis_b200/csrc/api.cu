@@ -28,6 +28,10 @@ cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cud
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
 cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool forces);
 cudaError_t ewald_energy_launch(cudaStream_t st, const KArgs &a);
+cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp);
+int bd_refactor_launches(int max_nmp);
+cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp);
+cudaError_t bd_force_launch(cudaStream_t st, const KArgs &a, int max_nmp);
 cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
                               const double *scale);
 }  // namespace tis
@@ -128,6 +132,12 @@ struct tis_ctx {
   int nk = 0, hmax = 0, nqblk = 1, nq_max = 0;
   DBuf<int8_t> ew_h;
   DBuf<double> ew_coef, ew_tab, ew_S, f_ext;
+  // Brownian dynamics with hydrodynamic interactions
+  bool bdhi = false;
+  int max_nmp = 0;
+  long long bd_istep = 0;
+  DBuf<int> fene_idx, wca_idx, bd_ptr, bd_ent, d_not_spd;
+  DBuf<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef, bd_D, bd_L, bd_F, bd_xi;
 };
 
 namespace {
@@ -238,7 +248,17 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   tis_ctx *c = new tis_ctx();
   c->par = *par;
   const tis_params &p = *par;
-  if (p.i_simulate_type != TIS_SIM_LANGEVIN) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+  if (p.i_simulate_type != TIS_SIM_LANGEVIN && p.i_simulate_type != TIS_SIM_BROWNIAN_HI) {
+    tis_destroy(c);
+    return TIS_E_UNSUPPORTED;
+  }
+  c->bdhi = p.i_simulate_type == TIS_SIM_BROWNIAN_HI;
+  // the Brownian-HI path evaluates FENE and WCA records (the C5 bead chains):
+  // no electrostatics, no DT15 or harmonic terms
+  if (c->bdhi && (p.i_ele != TIS_ELE_NONE || !(p.viscosity > 0.0) || !(p.hi_radius > 0.0))) {
+    tis_destroy(c);
+    return TIS_E_UNSUPPORTED;
+  }
   if (p.i_ele == TIS_ELE_EWALD) {
     // mloop_ewld.F90 uses psize(1) for a cubic box; the per-charge tables
     // hold |h| <= 11
@@ -260,6 +280,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   std::vector<double> st_hsTm_all;
+  std::vector<int> fene_idx, wca_idx, bdp, bde;
+  std::vector<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef;
   int maxN = 0;
   for (int k = 0; k < ntop; ++k) {
     const tis_topology &t = tops[k];
@@ -282,6 +304,38 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     d.slot_hb = d.slot_st + 7 * t.nst;
     d.nslot = d.slot_hb + 6 * t.nhb;
     maxN = std::max(maxN, t.nmp);
+    if (c->bdhi && (t.nbd || t.nba || t.nst || t.nhb)) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+    // FENE / WCA records (read_nativeinfo.F90:153-176, 306-332); per bead
+    // incidence lists (record * 2 + kind, FENE records first) for the
+    // Brownian-HI force gather
+    d.fe0 = (int)fene_nat.size(); d.nfe = t.nfene;
+    d.wc0 = (int)wca_nat.size(); d.nwc = t.nwca;
+    d.bp0 = (int)bdp.size(); d.be0 = (int)bde.size();
+    if (c->bdhi) {
+      std::vector<std::vector<int>> per(t.nmp);
+      for (int r = 0; r < t.nfene; ++r) {
+        const int i1 = t.ifene2mp[2 * r] - 1, i2 = t.ifene2mp[2 * r + 1] - 1;
+        if (i1 < 0 || i2 < 0 || i1 >= t.nmp || i2 >= t.nmp || i1 == i2) { tis_destroy(c); return TIS_E_ARG; }
+        fene_idx.push_back(i1); fene_idx.push_back(i2);
+        fene_nat.push_back(t.fene_nat[r]); fene_coef.push_back(t.coef_fene[r]); fene_d2.push_back(t.dist2_fene[r]);
+        per[i1].push_back(2 * (d.fe0 + r)); per[i2].push_back(2 * (d.fe0 + r));
+      }
+      for (int r = 0; r < t.nwca; ++r) {
+        const int i1 = t.iwca2mp[2 * r] - 1, i2 = t.iwca2mp[2 * r + 1] - 1;
+        if (i1 < 0 || i2 < 0 || i1 >= t.nmp || i2 >= t.nmp || i1 == i2) { tis_destroy(c); return TIS_E_ARG; }
+        wca_idx.push_back(i1); wca_idx.push_back(i2);
+        wca_nat.push_back(t.wca_nat[r]);
+        wca_coef.push_back(t.coef_wca[r]); wca_coef.push_back(t.coef_wca[t.nwca + r]);
+        per[i1].push_back(2 * (d.wc0 + r) + 1); per[i2].push_back(2 * (d.wc0 + r) + 1);
+      }
+      int off = 0;
+      for (int i = 0; i < t.nmp; ++i) {
+        bdp.push_back(off);
+        for (int e : per[i]) bde.push_back(e);
+        off += (int)per[i].size();
+      }
+      bdp.push_back(off);
+    }
     // beads
     std::vector<int> imp2unit(t.nmp, 0);
     for (int u = 0; u < t.nunit; ++u) {
@@ -426,6 +480,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
+  long long bd_off = 0;
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
@@ -466,6 +521,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       L.unif0 = 0;
       L.ew0 = ew_off;
       ew_off += d.nq;
+      L.bd0 = bd_off;
+      if (c->bdhi) bd_off += 9LL * N * N;
       state_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
       if (periodic) mirror_off += (long long)N * N;
@@ -492,7 +549,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     // electrostatic row chunks: one per charged bead at least
     if (p.i_ele != TIS_ELE_NONE && d.nq > CHMAX) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
     c->nq_max = std::max(c->nq_max, d.nq);
-    // the per-lane base layout must fit one CTA's shared memory
+    // the per-lane base layout must fit one CTA's shared memory (the
+    // Brownian-HI path does not run the lane kernel)
+    if (c->bdhi) continue;
     if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit) + 64 > 227 * 1024) {
       tis_destroy(c);
       return TIS_E_UNSUPPORTED;
@@ -505,7 +564,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
-  CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem));
+  if (!c->bdhi) CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem));
   CK(c->d_tops.upload(c->tops));
   CK(c->d_lanes.upload(c->lanes));
   std::vector<LaneState> ls(nlane);
@@ -545,6 +604,18 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->hb_flag.alloc(hb_off)); CK(c->hb_ene.alloc(hb_off)); CK(c->site_exc.alloc(site_off));
   CK(cudaMemset(c->hb_flag.p, 0, std::max(hb_off, 1)));
   CK(cudaMemset(c->hb_ene.p, 0, std::max(hb_off, 1) * sizeof(double)));
+  c->max_nmp = maxN;
+  if (c->bdhi) {
+    CK(c->fene_idx.upload(fene_idx)); CK(c->fene_nat.upload(fene_nat)); CK(c->fene_coef.upload(fene_coef));
+    CK(c->fene_d2.upload(fene_d2));
+    CK(c->wca_idx.upload(wca_idx)); CK(c->wca_nat.upload(wca_nat)); CK(c->wca_coef.upload(wca_coef));
+    CK(c->bd_ptr.upload(bdp)); CK(c->bd_ent.upload(bde));
+    CK(c->bd_D.alloc((size_t)bd_off)); CK(c->bd_L.alloc((size_t)bd_off));
+    CK(c->bd_F.alloc(n3)); CK(c->bd_xi.alloc(n3));
+    CK(cudaMemset(c->bd_F.p, 0, n3 * 8));
+    CK(c->d_not_spd.alloc(nlane));
+    CK(cudaMemset(c->d_not_spd.p, 0, nlane * sizeof(int)));
+  }
   if (p.i_ele == TIS_ELE_EWALD) {
     std::vector<int8_t> h;
     std::vector<double> coef;
@@ -591,6 +662,9 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
   c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
+  c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->d_not_spd.free();
+  c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
+  c->bd_D.free(); c->bd_L.free(); c->bd_F.free(); c->bd_xi.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tev0) cudaEventDestroy(c->tev0);
@@ -693,6 +767,15 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
     a.ew_h = c->ew_h.p; a.ew_coef = c->ew_coef.p; a.ew_tab = c->ew_tab.p; a.ew_S = c->ew_S.p;
   }
   a.f_ext = nullptr;
+  a.fene_idx = c->fene_idx.p; a.fene_nat = c->fene_nat.p; a.fene_coef = c->fene_coef.p; a.fene_d2 = c->fene_d2.p;
+  a.wca_idx = c->wca_idx.p; a.wca_nat = c->wca_nat.p; a.wca_coef = c->wca_coef.p;
+  a.wca_rcut2 = 1.0 / (p.wca_coef_cutoff * p.wca_coef_cutoff);
+  a.bd_ptr = c->bd_ptr.p; a.bd_ent = c->bd_ent.p;
+  a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
+  a.not_spd = c->d_not_spd.p;
+  a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
+  a.boltz = BOLTZ_KCAL_MOL; a.pi = F_PI;
+  a.bd_istep = c->bd_istep; a.bd_kpanel = 0;
   a.cutoff_ele = p.cutoff_ele;
   a.i_DH_cutoff_type = p.i_DH_cutoff_type;
   a.hb_cutoff_dist = p.hb_cutoff_dist;
@@ -765,6 +848,16 @@ int check_lanes(tis_ctx *c) {
     clamps += ls[i].nclamp - c->clamp_seen[i];
     c->clamp_seen[i] = ls[i].nclamp;
   }
+  if (c->bdhi) {
+    std::vector<int> ns(c->nlane);
+    CK(cudaMemcpy(ns.data(), c->d_not_spd.p, ns.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < c->nlane; ++i)
+      if (ns[i]) {
+        c->not_spd = 1;
+        code = fail(c, TIS_E_NOT_SPD, "Cholesky factorisation of the diffusion tensor failed in lane " +
+                                          std::to_string(i + 1));
+      }
+  }
   if (code < 0) return code;
   return (int)std::min<long long>(clamps, 0x7fffffff);
 }
@@ -773,6 +866,7 @@ int check_lanes(tis_ctx *c) {
 
 extern "C" int tis_neighbor(tis_ctx *c, int32_t irep) {
   if (!c || irep == 0 || irep > c->nlane || irep < -1) return TIS_E_ARG;
+  if (c->bdhi) return TIS_OK;   // no pair-list terms on the Brownian-HI path
   KArgs a = make_args(c, KM_NEIGHBOR, 0, irep > 0 ? irep - 1 : -1);
   int rc = launch_lane(c, a);
   if (rc < 0) return rc;
@@ -871,6 +965,16 @@ extern "C" int tis_get_hb_list(tis_ctx *c, int32_t irep, int32_t *ineigh2hb, int
 
 extern "C" int tis_force_sumup(tis_ctx *c, int32_t irep, double *force_mp) {
   if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  if (c->bdhi) {
+    KArgs a = make_args(c, 0, 0, -1);
+    ++c->launches;
+    CK(bd_force_launch(c->stream, a, c->max_nmp));
+    const LaneDesc &L = c->lanes[irep - 1];
+    if (force_mp)
+      CK(cudaMemcpyAsync(force_mp, c->bd_F.p + 3 * (size_t)L.state0, 3 * (size_t)c->lane_nmp[irep - 1] * 8,
+                         cudaMemcpyDeviceToHost, c->stream));
+    return check_lanes(c);
+  }
   KArgs a = make_args(c, KM_FORCE, 0, irep - 1);
   int rc = ewald_recip(c, a, true);
   if (rc < 0) return rc;
@@ -924,6 +1028,18 @@ extern "C" int tis_energy_sumup(tis_ctx *c, int32_t irep, double *energy) {
 
 extern "C" int tis_time_integral_pre(tis_ctx *c) {
   if (!c) return TIS_E_ARG;
+  if (c->bdhi) {
+    // time_integral_pre.F90:313-317: velocities zero; forces at x0
+    const size_t n3 = 3 * (size_t)c->nbead_total;
+    CK(cudaMemsetAsync(c->velo.p, 0, n3 * 8, c->stream));
+    CK(cudaMemsetAsync(c->accel.p, 0, n3 * 8, c->stream));
+    CK(cudaMemsetAsync(c->dxyz.p, 0, n3 * 8, c->stream));
+    KArgs a = make_args(c, 0, 0, -1);
+    ++c->launches;
+    CK(bd_force_launch(c->stream, a, c->max_nmp));
+    c->noise_base += 1;
+    return check_lanes(c);
+  }
   KArgs a = make_args(c, KM_PRE, 0, -1);
   int rc = ewald_recip(c, a, true);
   if (rc < 0) return rc;
@@ -939,7 +1055,23 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
   if (nsteps == 0) return TIS_OK;
   KArgs a = make_args(c, KM_STEP, (int)nsteps, -1);
   CK(cudaEventRecord(c->ev0, c->stream));
-  if (c->par.i_ele != TIS_ELE_EWALD) {
+  if (c->bdhi) {
+    // time_integral.F90:429-457, all lanes together
+    const int every = c->par.n_step_hydro > 0 ? c->par.n_step_hydro : 1;
+    for (int64_t k = 0; k < nsteps; ++k) {
+      const long long istep = c->bd_istep + 1;
+      KArgs b = make_args(c, 0, 0, -1);
+      b.bd_istep = istep;
+      b.noise_base = c->noise_base + (int)k;
+      if ((istep - 1) % every == 0) {
+        c->launches += bd_refactor_launches(c->max_nmp);
+        CK(bd_refactor_launch(c->stream, b, c->max_nmp));
+      }
+      c->launches += 3;
+      CK(bd_step_launch(c->stream, b, c->max_nmp));
+      c->bd_istep = istep;
+    }
+  } else if (c->par.i_ele != TIS_ELE_EWALD) {
     int rc = launch_lane(c, a);
     if (rc < 0) return rc;
   } else {

@@ -35,6 +35,9 @@ struct TopDesc {
   int inc0;         // incidence CSR: inc_ptr[inc0 + i] (nmp + 1 entries), values index inc_slot
   int ninc;         // incidence entries of this topology
   int q0, nq;       // charged beads (|q| >= ZERO_JUDGE), bead indices at q_bead[q0 ..], ascending
+  int fe0, nfe;     // FENE records
+  int wc0, nwc;     // WCA records
+  int bp0, be0;     // Brownian-HI force incidence: bd_ptr[bp0 .. bp0 + nmp], entries from bd_ent[be0]
   int nslot;        // 2 nbd + 3 nba + 7 nst + 6 nhb
   int slot_ba, slot_st, slot_hb;   // slot bases inside a lane (bonds start at 0)
   int nlabel;       // labels that belong to this topology
@@ -51,6 +54,7 @@ struct LaneDesc {
   int site0;        // per-lane hbond-site excess counters (nsite ints)
   int unif0;        // injected uniform stream (n_uniform per lane)
   int ew0;          // Ewald: first charge of this lane in the per-lane charge tables
+  long long bd0;    // Brownian-HI: first element of this lane's (3N)^2 diffusion / Cholesky matrices
 };
 
 // Mutable per-lane scalar state, kept in global memory between launches.
@@ -105,6 +109,19 @@ struct KArgs {
   double *ew_tab;                 // (q, 3, hmax + 1) of (cos, sin)(2 pi h x / L), per lane's charges
   double *ew_S;                   // (lane, nqblk, nk, 2) partial sums of q cos, q sin
   double *f_ext;                  // (3, nbead_total) force added to each bead's sum, or null
+  // Brownian dynamics with hydrodynamic interactions (time_integral.F90:429-457)
+  const int *fene_idx; const double *fene_nat, *fene_coef, *fene_d2;   // force_fene.F90
+  const int *wca_idx; const double *wca_nat, *wca_coef;                 // force_wca.F90 (coef: rep, att)
+  double wca_rcut2;                // 1 / cutoff_wca^2
+  const int *bd_ptr;               // per bead: range of its records in bd_ent
+  const int *bd_ent;               // record id * 2 + kind (0 FENE, 1 WCA)
+  double *bd_D, *bd_L;             // per lane (3N x 3N, row-major): diffusion tensor, its Cholesky factor
+  double *bd_F, *bd_xi;            // per lane (3N): force, Gaussian noise of the step
+  int *not_spd;                    // per lane: a Cholesky pivot was <= 0
+  double hi_radius, viscosity;
+  double boltz, pi;                // BOLTZ_KCAL_MOL and F_PI of const_physical.F90
+  long long bd_istep;              // step being taken (1-based)
+  int bd_kpanel;                   // Cholesky panel of this launch
   double hb_cutoff_dist;
   double max_abscos;   // MAX_ANG_ABSCOS_HBOND15 == MAX_DIH_ABSCOS_HBOND15
   double tstep, tstep2, tsteph;

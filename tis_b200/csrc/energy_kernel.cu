@@ -24,7 +24,7 @@ __device__ __forceinline__ double wrapd(double d) {
   return d;
 }
 
-enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_N };
+enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_N };
 
 __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
@@ -58,6 +58,26 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     double3 v = sub3(gpos(X, m[1]), gpos(X, m[0]));
     double dd = sqrt(v.x * v.x + v.y * v.y + v.z * v.z) - a.bd_nat[T.bd0 + k];
     es[ES_BOND] += a.bd_coef[T.bd0 + k] * (dd * dd);
+  }
+  // energy_fene.F90 (added to E_TYPE%BOND) and energy_wca.F90
+  for (int k = tid; k < T.nfe; k += nth) {
+    const int r = T.fe0 + k;
+    double3 v = sub3(gpos(X, a.fene_idx[2 * r + 1]), gpos(X, a.fene_idx[2 * r]));
+    const double dd = sqrt(dot3(v, v)) - a.fene_nat[r];
+    es[ES_BOND] += -0.5 * a.fene_coef[r] * a.fene_d2[r] * log(1.0 - dd * dd / a.fene_d2[r]);
+  }
+  for (int k = tid; k < T.nwc; k += nth) {
+    const int r = T.wc0 + k;
+    double3 v = sub3(gpos(X, a.wca_idx[2 * r + 1]), gpos(X, a.wca_idx[2 * r]));
+    const double ro2 = a.wca_nat[r] * a.wca_nat[r] / dot3(v, v);
+    if (ro2 < a.wca_rcut2) continue;
+    const double ro3 = ro2 * ro2 * ro2, ro6 = ro3 * ro3;
+    if (ro2 >= 1.0) {
+      es[ES_WREP] += a.wca_coef[2 * (size_t)r] * (ro6 - 2.0 * ro3 + 1.0);
+      es[ES_WATT] += -a.wca_coef[2 * (size_t)r + 1];
+    } else {
+      es[ES_WATT] += a.wca_coef[2 * (size_t)r + 1] * (ro6 - 2.0 * ro3);
+    }
   }
   for (int k = tid; k < T.nba; k += nth) {
     const int *m = a.ba_idx + 3 * (size_t)(T.ba0 + k);
@@ -230,6 +250,8 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     E[15] = tot[ES_STACK];
     E[16] = tot[ES_HB];
     E[17] = tot[ES_EXV];
+    E[22] = tot[ES_WREP];
+    E[23] = tot[ES_WATT];
     double sum = 0.0;
     for (int k = 2; k < N_ETYPE; ++k) sum += E[k];
     E[0] = sum;

@@ -28,7 +28,7 @@ import math
 
 import numpy as np
 
-from .abi import (CLASS_ION, CLASS_RNA, MP_ION_CA2, MP_ION_CL, MP_ION_K, MP_ION_MG,
+from .abi import (CLASS_ION, CLASS_LIG, CLASS_RNA, MP_ION_CA2, MP_ION_CL, MP_ION_K, MP_ION_MG,
                   MP_ION_NA, MP_RNA_BASE, MP_RNA_PHOS, MP_RNA_SUGAR)
 
 DEG = math.pi / 180.0
@@ -385,7 +385,7 @@ def dt15_params(**over):
              i_ele=1, i_diele=1, diele_water=78.0, ionic_strength=0.15, cutoff_ele=20.0,
              i_DH_cutoff_type=0, ewld_alpha=0.05, ewld_hmax=10.0,
              i_simulate_type=1, tstep=0.05, viscosity=0.0, wca_coef_cutoff=1.0,
-             precision=0, hb_beta_global=1, seed=12345)
+             precision=0, hb_beta_global=1, seed=12345, hi_radius=2.0, n_step_hydro=1)
     p.update(over)
     return p
 
@@ -412,6 +412,63 @@ def workload_c2(seed: int = 2):
     par = dt15_params(i_periodic=1, psize=(box, box, box), i_ele=2, cutoff_ele=20.0,
                       ewld_alpha=0.05, ewld_hmax=10.0, ionic_strength=0.150 + 3 * 0.005, precision=1)
     return [s], par, [300.0]
+
+
+def bead_chain(n: int, seed: int, bond: float = 3.8, sigma: float = 4.0, min_dist: float = 4.2,
+               k_fene: float = 20.0, r2_fene: float = 2.0, eps_wca: float = 1.0, mass: float = 100.0):
+    """Brownian-HI bead chain: one LIG-class unit of n beads (no DT15 terms:
+    zero excluded-volume radius), FENE bonds between consecutive beads
+    (fene_nat = bond, coef_fene = k_fene, dist2_fene = r2_fene, the column
+    meaning of read_nativeinfo.F90:153-176) and a WCA record for every
+    non-bonded pair j >= i + 2 (wca_nat = sigma, coef_wca = (eps, eps):
+    read_nativeinfo.F90:306-332).  Coordinates: seeded self-avoiding walk."""
+    rng = np.random.default_rng(seed)
+    kinds = ["S"] * n
+    parents = [0] + list(range(n - 1))
+    lengths = [0.0] + list(bond + rng.uniform(-0.05, 0.05, n - 1))
+    X = _walk(kinds, parents, lengths, rng, min_dist=min_dist, persist=0.3)
+    X = X - X.mean(axis=0)
+    ii, jj = np.triu_indices(n, k=2)
+    nw = len(ii)
+    return dict(
+        nmp=n, nunit=1, lunit2mp=np.array([[1, n]], dtype=np.int32),
+        iclass_unit=np.array([CLASS_LIG], dtype=np.int32),
+        imp2type=np.full(n, MP_RNA_SUGAR, dtype=np.int32),
+        cmass=np.full(n, mass), fric=np.full(n, 0.5),
+        exv_radius=np.zeros(n), exv_epsilon=np.zeros(n),
+        ncharge=0, icharge2mp=np.zeros(0, dtype=np.int32), coef_charge=np.zeros(0),
+        nbd=0, nba=0, nst=0, nhb=0, nhbsite=0,
+        nfene=n - 1,
+        ifene2mp=np.stack([np.arange(1, n), np.arange(2, n + 1)], axis=1).astype(np.int32),
+        fene_nat=np.full(n - 1, bond), coef_fene=np.full(n - 1, k_fene), dist2_fene=np.full(n - 1, r2_fene),
+        nwca=nw,
+        iwca2mp=np.stack([ii + 1, jj + 1], axis=1).astype(np.int32),
+        wca_nat=np.full(nw, sigma),
+        coef_wca=np.stack([np.full(nw, eps_wca), np.full(nw, eps_wca)], axis=0),
+        xyz=X,
+    )
+
+
+def bdhi_params(**over):
+    """Brownian dynamics with hydrodynamic interactions (i_simulate_type 6,
+    HI_TENSOR%RPY): water viscosity 1e-3 Pa s in the internal units of
+    setp_mass_fric.F90:67 (x sqrt(1e3 JOUL2KCAL) N_AVO 1e-20 = 2.944), RPY
+    radius 2 A, dt 0.01, no electrostatics, WCA cut at sigma."""
+    visc = 1.0e-3 * np.sqrt(1.0e3 / 4184.0) * 6.022140857e23 * 1.0e-20
+    p = dt15_params(i_simulate_type=6, i_ele=0, tstep=0.01, viscosity=visc, hi_radius=2.0,
+                    n_step_hydro=1, wca_coef_cutoff=1.0, n_step_neighbor=10)
+    p.update(over)
+    return p
+
+
+def workload_c5(seed: int = 5, nchain: int = 32):
+    """Brownian-HI batch: nchain bead chains, N uniform in 100..1000, FENE
+    bonds, WCA between all non-bonded pairs, RPY radius 2 A, dt 0.01, D and
+    its Cholesky factor refreshed every 10 steps, 300 K."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(100, 1001, size=nchain)
+    systems = [bead_chain(int(n), seed * 1000 + k) for k, n in enumerate(ns)]
+    return systems, bdhi_params(n_step_hydro=10), [300.0] * nchain
 
 
 def temperature_ladder(n=64, tlo=280.0, thi=400.0):
