@@ -43,10 +43,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c3", "c4"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c4", "c2", "c5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--period", type=int, default=PERIOD, help="MD steps per bench step (exchange period)")
+    ap.add_argument("--period", type=int, default=None, help="MD steps per bench step (C3: exchange period)")
     ap.add_argument("--ref-sample", type=int, default=200,
                     help="reference arm: MD steps per replica in one timed step")
     ap.add_argument("--quick", action="store_true",
@@ -62,12 +62,27 @@ def workload(name):
         desc = ("C3: 64-replica temperature REMD of a 76-nt DT15 chain (227 beads), 20 random stem "
                 "hbond pairs, Debye-Hueckel 100 mM, ladder 280-400 K, Langevin dt 0.05 tau, "
                 "friction 0.5/tau, rebuild every 10 steps, exchange every 1000 steps")
-    else:
+    elif name == "c4":
         systems, par, temps = synth.workload_c4()
         nrep = [1] * len(systems)
         desc = ("C4: 256 independent DT15 chains, lengths log-uniform 20-400 nt, 30% of residues in "
                 "hbond pairs, Debye-Hueckel 150 mM, 300 K, Langevin dt 0.05 tau, rebuild every 10 steps")
+    elif name == "c2":
+        systems, par, temps = synth.workload_c2()
+        nrep = [1]
+        desc = ("C2: 51-nt DT15 chain + 590 ions (Mg 5 mM, K 150 mM, Cl to neutrality) in a 150 A periodic "
+                "box, Ewald alpha 0.05, r_c 20 A, |h| <= 10 (4168 k), FP32 forces, 300 K")
+    else:
+        systems, par, temps = synth.workload_c5()
+        nrep = [1] * len(systems)
+        desc = ("C5: 32 bead chains, N uniform 100-1000, FENE bonds, WCA between all non-bonded pairs, "
+                "Brownian dynamics with the Rotne-Prager tensor (radius 2 A) and its Cholesky factor "
+                "refreshed every 10 steps, dt 0.01, FP64")
     return systems, par, temps, nrep, desc
+
+
+# MD steps per bench step, by workload (C3: one exchange period)
+PERIODS = {"c3": PERIOD, "c4": PERIOD, "c2": 100, "c5": 10}
 
 
 def algorithmic_bytes(systems, nrep, exv_pairs, ele_pairs):
@@ -83,6 +98,17 @@ def algorithmic_bytes(systems, nrep, exv_pairs, ele_pairs):
                       + 84 * s["nst"] + 128 * s["nhb"])
             lane += 1
     return total / lane
+
+
+def bdhi_bytes(systems, every):
+    """Bytes per chain-step of the Brownian-HI path: the two matrix-vector
+    products read D (n^2) and the lower half of L (n(n+1)/2) in FP64, n = 3N;
+    the tensor refresh writes D and tril(D) (2 n^2) every `every` steps."""
+    tot = 0.0
+    for s in systems:
+        n = 3 * s["nmp"]
+        tot += 8.0 * (n * n + n * (n + 1) / 2) + 16.0 * n * n / every
+    return tot / len(systems)
 
 
 # ------------------------------------------------------------------ CPU leg
@@ -238,7 +264,9 @@ def run_reference(args, rank, world):
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     cpu_line = None
-    period_len = args.period
+    period_len = args.period or PERIODS[args.workload]
+    if args.workload != "c3":
+        args.no_plain = True
     if args.quick:
         args.no_cpu_baseline = True
         args.no_plain = True
@@ -247,7 +275,7 @@ def run_ours(args, rank, world, local_rank):
         import multiprocessing as mp
         systems, par, temps, nrep, _ = workload(args.workload)
         cores = os.cpu_count() or 1
-        sample = 1000
+        sample = {"c3": 1000, "c4": 1000, "c2": 20, "c5": 10}[args.workload]
         with mp.get_context("spawn").Pool(cores) as pool:
             v = cpu_run(systems, par, temps, nrep, sample, cores, pool)
         cpu_line = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
@@ -280,10 +308,13 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         period()
     nlane = eng.nlane
-    # pair counts for the algorithmic bytes
-    exv = [len(eng.exv_list(i + 1)) for i in range(nlane)]
-    ele = [len(eng.ele_list(i + 1)[0]) for i in range(nlane)]
-    bytes_per_rs = algorithmic_bytes(systems, nrep, exv, ele)
+    if args.workload == "c5":
+        bytes_per_rs = bdhi_bytes(systems, par["n_step_hydro"])
+    else:
+        # pair counts for the algorithmic bytes
+        exv = [len(eng.exv_list(i + 1)) for i in range(nlane)]
+        ele = [len(eng.ele_list(i + 1)[0]) for i in range(nlane)]
+        bytes_per_rs = algorithmic_bytes(systems, nrep, exv, ele)
 
     if dist:
         dist.barrier()
@@ -361,7 +392,8 @@ def run_ours(args, rank, world, local_rank):
                          "traffic": profiled_traffic() if (args.workload == "c3" and period_len == PERIOD) else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
                                            "(profiles/lane_kernel_c3_launches.md)",
-                         "kernel": "lane_kernel<float>", "peak_source": src,
+                         "kernel": ("bd_update_kernel + Cholesky refresh" if args.workload == "c5"
+                                    else "lane_kernel<float>"), "peak_source": src,
                          "bytes_per_replica_step": bytes_per_rs,
                          "note": "state stays in shared memory across the 1000-step launch; frac > 1 is on-chip reuse"},
             "cpu_baseline": cpu_line,
