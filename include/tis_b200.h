@@ -157,6 +157,7 @@ typedef struct tis_status_t {
   int32_t last_error;              /* last TIS_E_* returned */
   int32_t exv_pairs_max;           /* largest exv half list among replicas */
   int32_t ele_pairs_max;           /* largest ele half list among replicas */
+  int32_t ctas_per_lane;           /* CTAs (one cluster) that tis_step gives each replica: 1 or 2 */
 } tis_status_t;
 
 typedef struct tis_ctx tis_ctx;

@@ -79,7 +79,7 @@ class Status(C.Structure):
         ("step", C.c_int64), ("n_rebuild", C.c_int64), ("n_clamp", C.c_int64),
         ("list_overflow", C.c_int32), ("nan_seen", C.c_int32), ("wait_timeout", C.c_int32),
         ("not_spd", C.c_int32), ("last_error", C.c_int32),
-        ("exv_pairs_max", C.c_int32), ("ele_pairs_max", C.c_int32),
+        ("exv_pairs_max", C.c_int32), ("ele_pairs_max", C.c_int32), ("ctas_per_lane", C.c_int32),
     ]
 
 

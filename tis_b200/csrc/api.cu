@@ -21,8 +21,10 @@
 #include "common.cuh"
 
 namespace tis {
-size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
-cudaError_t lane_kernel_set_smem(bool mixed, int bytes);
+size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
+                       bool dbuf);
+cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2);
+cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, const KArgs &a);
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
@@ -128,6 +130,8 @@ struct tis_ctx {
   int wait_timeout = 0, not_spd = 0;
   std::vector<long long> clamp_seen;
   long long launches = 0;            // kernels this context has launched
+  bool pair = false;                 // tis_step runs two CTAs (a cluster) per lane
+  size_t smem2 = 0;
   // Ewald
   int nk = 0, hmax = 0, nqblk = 1, nq_max = 0;
   DBuf<int8_t> ew_h;
@@ -544,7 +548,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->threads = choose_threads(maxN, p.precision == TIS_PREC_MIXED);
   c->group = choose_group(c->threads, maxN);
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
-  size_t smem = 0;
+  size_t smem = 0, smem2 = 0;
+  int minN = 1 << 30;
   for (auto &d : c->tops) {
     // electrostatic row chunks: one per charged bead at least
     if (p.i_ele != TIS_ELE_NONE && d.nq > CHMAX) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
@@ -556,15 +561,30 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       tis_destroy(c);
       return TIS_E_UNSUPPORTED;
     }
-    smem = std::max(smem, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit));
+    smem = std::max(smem, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, false));
+    smem2 = std::max(smem2, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, true));
+    minN = std::min(minN, d.nmp);
   }
   c->smem = smem;
+  // two CTAs per lane (a cluster) when the lanes fill at most half of the
+  // SMs: mixed precision, no periodic box, fixed rebuild cadence, DH or no
+  // electrostatics; TIS_CLUSTER=0 turns it off
+  {
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const char *env = std::getenv("TIS_CLUSTER");
+    const bool allow = !(env && env[0] == '0');
+    c->pair = allow && !c->bdhi && p.precision == TIS_PREC_MIXED && !periodic && !skin &&
+              p.i_ele != TIS_ELE_EWALD && minN >= 64 && nsm > 0 && 2 * nlane <= nsm && smem2 <= 227 * 1024;
+    c->smem2 = c->pair ? smem2 : 0;
+  }
 
   // ---- device
   CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
-  if (!c->bdhi) CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem));
+  if (!c->bdhi) CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem, (int)c->smem2));
   CK(c->d_tops.upload(c->tops));
   CK(c->d_lanes.upload(c->lanes));
   std::vector<LaneState> ls(nlane);
@@ -813,6 +833,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.unif = c->n_unif ? c->unif.p : nullptr;
   a.n_unif = c->n_unif;
   a.nbead_total = c->nbead_total;
+  a.noise_in_sweep = 0;
   return a;
 }
 
@@ -1055,7 +1076,14 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
   if (nsteps == 0) return TIS_OK;
   KArgs a = make_args(c, KM_STEP, (int)nsteps, -1);
   CK(cudaEventRecord(c->ev0, c->stream));
-  if (c->bdhi) {
+  if (c->pair) {
+    a.smem_total = (int)c->smem2;
+    // the two-CTA sweep has idle warps: the sink's noise is drawn there
+    const char *env = std::getenv("TIS_NOISE_SWEEP");
+    a.noise_in_sweep = (env && env[0] == '0') ? 0 : 1;
+    ++c->launches;
+    CK(lane_kernel_launch_pair(c->nlane, c->smem2, c->stream, a));
+  } else if (c->bdhi) {
     // time_integral.F90:429-457, all lanes together
     const int every = c->par.n_step_hydro > 0 ? c->par.n_step_hydro : 1;
     for (int64_t k = 0; k < nsteps; ++k) {
@@ -1200,6 +1228,7 @@ extern "C" int tis_status(tis_ctx *c, tis_status_t *st) {
     st->exv_pairs_max = std::max(st->exv_pairs_max, ls[i].nexv);
     st->ele_pairs_max = std::max(st->ele_pairs_max, ls[i].nele);
   }
+  st->ctas_per_lane = c->pair ? 2 : 1;
   st->wait_timeout = c->wait_timeout;
   st->not_spd = c->not_spd;
   st->last_error = c->last_error;

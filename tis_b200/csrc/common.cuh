@@ -179,6 +179,7 @@ struct KArgs {
   const double *unif;      // injected uniforms per lane
   int n_unif;
   int nbead_total;
+  int noise_in_sweep;      // 1: the sink's noise is drawn in the bonded sweep (kept in shared memory)
 };
 
 // ---------------------------------------------------------------- Philox

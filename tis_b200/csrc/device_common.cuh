@@ -91,12 +91,14 @@ struct Smem {
   double *AX, *AY, *AZ;
   double *DX, *DY, *DZ;     // dxyz_mp (skin rule only)
   double *QX, *QY, *QZ;     // periodic: pxyz wrapped at the last rebuild
+  double *XN, *YN, *ZN;     // two-CTA lanes: next-step positions (double buffer)
   double *red;              // 64 doubles of reduction scratch
   double *ch_part;          // (3 * CHMAX) partial Debye-Hueckel force of each chunk
   double *rn2;              // rneighbordist2_unit (nunit x nunit)
   typename V4<Real>::T *A4; // (px, py, pz, q) rounded to Real
   typename V4<Real>::T *B4; // (exv radius, exv sqrt(eps), exv screen radius, 0)
   typename V4<Real>::T *L4; // (px, py, pz) - A4 rounded to Real: hi + lo carries pxyz to ~2^-48
+  typename V4<Real>::T *A4N, *L4N;   // two-CTA lanes: next-step A4, L4
   int *qb;                  // charged bead indices (nq)
   int *qidx;                // charge row of each bead (-1: uncharged)
   int *inc_ptr;             // (N + 1), relative to the lane's incidence entries
@@ -110,19 +112,23 @@ struct Smem {
   Real *slots;              // shared or global
   const int *inc_slot;      // shared copy or global
   int W;                    // words per bit row
-  bool mask_smem, slots_smem, inc_smem, near_on;
+  double *C1, *C2, *C3, *C4, *RC;   // rlan_const(1..4) and 1/m of each bead (cst_on)
+  double *NX, *NY, *NZ;              // this step's Gaussian noise, drawn in the bonded sweep (cst_on)
+  bool mask_smem, slots_smem, inc_smem, near_on, cst_on;
 };
 
-struct SmemPlan { size_t base, mask, slots, inc, near; };
+struct SmemPlan { size_t base, mask, slots, inc, near, cst; };
 
 // Byte layout of one lane (host and device use the same arithmetic).
 __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc, bool periodic, bool skin,
-                                              int real_size, int nunit) {
+                                              int real_size, int nunit, bool dbuf = false) {
   size_t nd = 9 * (size_t)N + 64 + 3 * (size_t)CHMAX + (size_t)nunit * nunit + 2;
   if (periodic) nd += 6 * (size_t)N;
   if (skin) nd += 3 * (size_t)N;
+  if (dbuf) nd += 3 * (size_t)N;
   size_t b = nd * 8;
   b += 12 * (size_t)N * real_size;                  // A4, B4, L4
+  if (dbuf) b += 8 * (size_t)N * real_size;         // A4N, L4N
   b = (b + 15) & ~(size_t)15;
   b += 4 * ((size_t)nq + N + (N + 1) + MISC_UNITS + (size_t)nunit * nunit + 8);
   b += 4 * (size_t)N;                               // unit, typ, cls
@@ -133,6 +139,7 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc
   p.slots = ((3 * (size_t)nslot * real_size) + 15) & ~(size_t)15;
   p.inc = ((4 * (size_t)ninc) + 15) & ~(size_t)15;
   p.near = 16 * (size_t)N + 2 * (size_t)NEAR_CAP * N + 8 * (size_t)N + 16;
+  p.cst = 8 * 8 * (size_t)N + 16;
   return p;
 }
 
@@ -155,10 +162,10 @@ __device__ __forceinline__ void two_sum_add(float &hi, float &lo, float x) {
 
 template <typename Real>
 __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, const LaneDesc &L, const TopDesc &T,
-                            bool periodic, bool skin) {
+                            bool periodic, bool skin, bool dbuf = false) {
   const int N = T.nmp;
   Smem<Real> s;
-  SmemPlan pl = smem_plan(N, T.nq, T.nslot, T.ninc, periodic, skin, (int)sizeof(Real), T.nunit);
+  SmemPlan pl = smem_plan(N, T.nq, T.nslot, T.ninc, periodic, skin, (int)sizeof(Real), T.nunit, dbuf);
   double *d = (double *)base;
   s.X = d; s.Y = d + N; s.Z = d + 2 * N; d += 3 * N;
   s.VX = d; s.VY = d + N; s.VZ = d + 2 * N; d += 3 * N;
@@ -172,12 +179,16 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   }
   if (skin) { s.DX = d; s.DY = d + N; s.DZ = d + 2 * N; d += 3 * N; }
   else { s.DX = s.DY = s.DZ = nullptr; }
+  if (dbuf) { s.XN = d; s.YN = d + N; s.ZN = d + 2 * N; d += 3 * N; }
+  else { s.XN = s.YN = s.ZN = nullptr; }
   s.red = d; d += 64;
   s.ch_part = d; d += 3 * CHMAX;
   s.rn2 = d; d += T.nunit * T.nunit;
   typedef typename V4<Real>::T V;
   V *v4 = (V *)(((uintptr_t)d + 15) & ~(uintptr_t)15);
   s.A4 = v4; s.B4 = v4 + N; s.L4 = v4 + 2 * N; v4 += 3 * N;
+  if (dbuf) { s.A4N = v4; s.L4N = v4 + N; v4 += 2 * N; }
+  else { s.A4N = s.L4N = nullptr; }
   int *ip = (int *)(((uintptr_t)v4 + 15) & ~(uintptr_t)15);
   s.qb = ip; ip += T.nq;
   s.qidx = ip; ip += N;
@@ -204,8 +215,18 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
     s.NR4 = (float4 *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
     s.near = (uint16_t *)(s.NR4 + N);
     s.near_cnt = (uint8_t *)(s.near + (size_t)NEAR_CAP * N);
+    u = (unsigned char *)(s.near_cnt + 8 * (size_t)N);
+    left = (size_t)total > (size_t)(u - base) ? (size_t)total - (size_t)(u - base) : 0;
   } else {
     s.NR4 = nullptr; s.near = nullptr; s.near_cnt = nullptr;
+  }
+  s.cst_on = pl.cst <= left;
+  if (s.cst_on) {
+    double *c = (double *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
+    s.C1 = c; s.C2 = c + N; s.C3 = c + 2 * N; s.C4 = c + 3 * N; s.RC = c + 4 * N;
+    s.NX = c + 5 * N; s.NY = c + 6 * N; s.NZ = c + 7 * N;
+  } else {
+    s.C1 = s.C2 = s.C3 = s.C4 = s.RC = s.NX = s.NY = s.NZ = nullptr;
   }
   return s;
 }
@@ -249,9 +270,18 @@ __device__ __forceinline__ double lane_uniform(const KArgs &a, int lane, const L
 }
 
 // ------------------------------------------------------------ bonded terms
+// Destination of the bonded slots: the slot of a bead goes to `loc`, or to
+// `peer` when the bead belongs to the other CTA of a two-CTA lane (beads
+// outside [lo, hi)).  peer == nullptr: one CTA per lane, everything local.
+struct SlotDst {
+  void *loc, *peer;
+  int lo, hi;
+};
+
 template <typename Real>
-__device__ __forceinline__ void put_slot(void *slots, size_t k, Real fx, Real fy, Real fz) {
-  Real *p = (Real *)slots + 3 * k;
+__device__ __forceinline__ void put_slot(const SlotDst &d, size_t k, int bead, Real fx, Real fy, Real fz) {
+  void *base = (d.peer && (bead < d.lo || bead >= d.hi)) ? d.peer : d.loc;
+  Real *p = (Real *)base + 3 * k;
   p[0] = fx; p[1] = fy; p[2] = fz;
 }
 
@@ -272,26 +302,27 @@ template <typename Real> __device__ __forceinline__ Real wrap_pi(Real d) {
 
 // force_bond.F90:41-56
 template <typename Real>
-__device__ void term_bond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, void *slots, int k) {
+__device__ void term_bond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
   const int *m = a.bd_idx + 2 * (size_t)(T.bd0 + k);
   R3<Real> v = dvec(s, m[0], m[1]);
   Real dist = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
   Real dd = dist - (Real)a.bd_nat[T.bd0 + k];
   Real f = (Real)a.bd_coef[T.bd0 + k] * ((Real)-2.0 * fdiv(dd, dist));
-  put_slot<Real>(slots, 2 * k, -f * v.x, -f * v.y, -f * v.z);
-  put_slot<Real>(slots, 2 * k + 1, f * v.x, f * v.y, f * v.z);
+  put_slot<Real>(slots, 2 * k, m[0], -f * v.x, -f * v.y, -f * v.z);
+  put_slot<Real>(slots, 2 * k + 1, m[1], f * v.x, f * v.y, f * v.z);
 }
 
 // force_bangle.F90:103-147
 template <typename Real>
-__device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s, void *slots, int k) {
+__device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
   const size_t sb = T.slot_ba + 3 * (size_t)k;
   const Real cf = (Real)a.ba_coef[T.ba0 + k];
+  const int *m = a.ba_idx + 3 * (size_t)(T.ba0 + k);
   if (cf < (Real)1.0e-6) {
-    put_slot<Real>(slots, sb, 0, 0, 0); put_slot<Real>(slots, sb + 1, 0, 0, 0); put_slot<Real>(slots, sb + 2, 0, 0, 0);
+    put_slot<Real>(slots, sb, m[0], 0, 0, 0); put_slot<Real>(slots, sb + 1, m[1], 0, 0, 0);
+    put_slot<Real>(slots, sb + 2, m[2], 0, 0, 0);
     return;
   }
-  const int *m = a.ba_idx + 3 * (size_t)(T.ba0 + k);
   R3<Real> v21 = dvec(s, m[0], m[1]), v32 = dvec(s, m[1], m[2]);
   Real c11 = dot(v21, v21), c22 = dot(v32, v32), c21 = dot(v32, v21);
   Real co = -c21 * frsq(c11 * c22);
@@ -303,14 +334,14 @@ __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   Real a1 = fdiv(c21, c11), a2 = fdiv(c21, c22);
   R3<Real> f21{f * (v21.x * a1 - v32.x), f * (v21.y * a1 - v32.y), f * (v21.z * a1 - v32.z)};
   R3<Real> f32{f * (v32.x * a2 - v21.x), f * (v32.y * a2 - v21.y), f * (v32.z * a2 - v21.z)};
-  put_slot<Real>(slots, sb, -f21.x, -f21.y, -f21.z);
-  put_slot<Real>(slots, sb + 1, f21.x - f32.x, f21.y - f32.y, f21.z - f32.z);
-  put_slot<Real>(slots, sb + 2, f32.x, f32.y, f32.z);
+  put_slot<Real>(slots, sb, m[0], -f21.x, -f21.y, -f21.z);
+  put_slot<Real>(slots, sb + 1, m[1], f21.x - f32.x, f21.y - f32.y, f21.z - f32.z);
+  put_slot<Real>(slots, sb + 2, m[2], f32.x, f32.y, f32.z);
 }
 
 // force_dtrna_stack.F90:54-165
 template <typename Real>
-__device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, void *slots, int k, double u0) {
+__device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, double u0) {
   const int *m = a.st_idx + 7 * (size_t)(T.st0 + k);
   const double *nat = a.st_nat + 3 * (size_t)(T.st0 + k);
   const double *cf = a.st_coef + 3 * (size_t)(T.st0 + k);
@@ -367,13 +398,13 @@ __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   const Real pre = (Real)(u0 / ((double)ediv * (double)ediv));
   const size_t sb = T.slot_st + 7 * (size_t)k;
 #pragma unroll
-  for (int p = 0; p < 7; ++p) put_slot<Real>(slots, sb + p, pre * fr[p][0], pre * fr[p][1], pre * fr[p][2]);
+  for (int p = 0; p < 7; ++p) put_slot<Real>(slots, sb + p, m[p], pre * fr[p][0], pre * fr[p][1], pre * fr[p][2]);
 }
 
 // force_dtrna_hbond15.F90:91-353 (one hbond of the neighbour list).
 // Returns the energy; active = |d| <= hb_cutoff_dist.
 template <typename Real>
-__device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, void *slots, int k, bool &active) {
+__device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, bool &active) {
   const int *m = a.hb_idx + 6 * (size_t)(T.hb0 + k);
   const double *nat = a.hb_nat + 6 * (size_t)(T.hb0 + k);
   const double *cf = a.hb_coef + 7 * (size_t)(T.hb0 + k);
@@ -497,7 +528,7 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
   const double ene = (double)e;
   const size_t sb = T.slot_hb + 6 * (size_t)k;
 #pragma unroll
-  for (int p = 0; p < 6; ++p) put_slot<Real>(slots, sb + p, e * fo[p][0], e * fo[p][1], e * fo[p][2]);
+  for (int p = 0; p < 6; ++p) put_slot<Real>(slots, sb + p, m[p], e * fo[p][0], e * fo[p][1], e * fo[p][2]);
   return ene;
 }
 

@@ -21,9 +21,28 @@
 // sums with a fixed xor-butterfly, so results do not depend on scheduling.
 // Neighbour pair sets are bit-exact with the reference: the FP64 distance
 // test uses explicitly rounded operations in the Fortran order.
+#include <cooperative_groups.h>
+
 #include "device_common.cuh"
 
 namespace tis {
+
+namespace cg = cooperative_groups;
+
+// Split of one lane over the CTAs of its cluster: this CTA owns beads
+// [lo, hi) (their x / v / a updates, list rows, near lists, force sums).
+// nrank == 1: one CTA per lane, owns every bead.
+struct Clu {
+  int rank, nrank;
+  int lo, hi;
+  int kq_lo, kq_hi;   // charged rows (electrostatic chunks) of the own beads
+};
+
+// the same shared-memory object in the other CTA of a two-CTA cluster
+template <typename T>
+__device__ __forceinline__ T *peer_ptr(T *p, const Clu &cu) {
+  return cg::this_cluster().map_shared_rank(p, cu.rank ^ 1);
+}
 
 // ------------------------------------------------------------ list build
 // neighbor_list.F90:49-90 + neighbor_assign.F90:481-559 (the EXV_DT15 type
@@ -31,8 +50,9 @@ namespace tis {
 // unordered pair is tested once and sets its bit in both rows of the exv
 // and/or ele matrix.  Periodic systems also record the mirror index of the
 // canonical (min, max) orientation (neighbor_assign.F90:742-770).
-template <typename Real>
-__device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s) {
+template <typename Real, int CL>
+__device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
+                            const Clu &cu) {
   const int N = T.nmp, W = s.W;
   const int tid = threadIdx.x, nth = blockDim.x;
   const int warp = tid >> 5, lid = tid & 31, nwarp = nth >> 5;
@@ -49,7 +69,17 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
       set_pos<Real>(s, i);
     }
   }
-  for (int k = tid; k < 2 * N * W; k += nth) mexv[k] = 0u;
+  if (CL == 1) {
+    for (int k = tid; k < 2 * N * W; k += nth) mexv[k] = 0u;
+  } else {
+    // own rows only: the other CTA writes its own rows (and, with a global
+    // matrix, nothing else) before the barrier below
+    const int nw = (cu.hi - cu.lo) * W;
+    for (int k = tid; k < nw; k += nth) {
+      mexv[(size_t)cu.lo * W + k] = 0u;
+      mele[(size_t)cu.lo * W + k] = 0u;
+    }
+  }
   if (tid == 0) {
     s.misc[MISC_NEXV] = 0; s.misc[MISC_NELE] = 0; s.misc[MISC_REBUILT] = 1;
     s.misc[MISC_NEAR_BAD] = 1;
@@ -94,11 +124,20 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
   const double rele2 = (a.i_ele != 0) ? a.lab_rele2[st.label] : -1.0;
   uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
   int nexv_l = 0, nele_l = 0;
+  // two CTAs: every row must be cleared before either CTA sets bits in it
+  uint32_t *pexv = mexv, *pele = mele;
+  if (CL == 2) {
+    cg::this_cluster().sync();
+    if (s.mask_smem) { pexv = peer_ptr(mexv, cu); pele = peer_ptr(mele, cu); }
+  }
   PHASE_T0(t_pairs);
-  // warp w takes rows i = w, w + nwarp, ...; its lanes take j > i
+  // warp w takes rows i = w, w + nwarp, ...; its lanes take j > i (two CTAs:
+  // CTA r takes the rows of parity r and sets each bit in the copy of the
+  // row's owner)
   const bool one_unit = nu == 1;
   const double rn2_00 = s.rn2[0];
-  for (int i = warp; i < N - 1; i += nwarp) {
+  const int rstep = nwarp * CL;
+  for (int i = warp * CL + cu.rank; i < N - 1; i += rstep) {
     const int ui = s.unit[i];
     const int ci = s.cls[i];
     const int nsep = (s.typ[i] == 2) ? a.nsep[0] : (s.typ[i] == 4 ? a.nsep[1] : (s.typ[i] == 3 ? a.nsep[2] : -1));
@@ -131,14 +170,16 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
       if (qi && fabs((double)s.A4[j].w) >= 1.0e-6) el = d2 < rele2;
       if (ex || el) {
         const uint32_t bj = 1u << (j & 31), bi = 1u << (i & 31);
+        const bool own_i = CL == 1 || (i >= cu.lo && i < cu.hi);
+        const bool own_j = CL == 1 || (j >= cu.lo && j < cu.hi);
         if (ex) {
-          atomicOr(&mexv[(size_t)i * W + (j >> 5)], bj);
-          atomicOr(&mexv[(size_t)j * W + (i >> 5)], bi);
+          atomicOr(&(own_i ? mexv : pexv)[(size_t)i * W + (j >> 5)], bj);
+          atomicOr(&(own_j ? mexv : pexv)[(size_t)j * W + (i >> 5)], bi);
           ++nexv_l;
         }
         if (el) {
-          atomicOr(&mele[(size_t)i * W + (j >> 5)], bj);
-          atomicOr(&mele[(size_t)j * W + (i >> 5)], bi);
+          atomicOr(&(own_i ? mele : pele)[(size_t)i * W + (j >> 5)], bj);
+          atomicOr(&(own_j ? mele : pele)[(size_t)j * W + (i >> 5)], bi);
           ++nele_l;
         }
         if (mir) mir[(size_t)i * N + j] = (uint8_t)im;
@@ -148,9 +189,10 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
   if (nexv_l) atomicAdd(&s.misc[MISC_NEXV], nexv_l);
   if (nele_l) atomicAdd(&s.misc[MISC_NELE], nele_l);
   PHASE_ADD(7, t_pairs);
-  // hbond neighbour flags (neighbor_list_hb.F90:335-354)
+  // hbond neighbour flags (neighbor_list_hb.F90:335-354); two CTAs: the
+  // first one, which evaluates every hbond
   uint8_t *hbf = a.hb_flag + L.hb0;
-  for (int h = tid; h < T.nhb; h += nth) {
+  for (int h = tid; h < (cu.rank == 0 ? T.nhb : 0); h += nth) {
     const int *m = a.hb_idx + 6 * (size_t)(T.hb0 + h);
     double v0, v1, v2;
     v0 = __dsub_rn(s.PX[m[0]], s.PX[m[1]]);
@@ -160,11 +202,17 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
     double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
     hbf[h] = (d2 < a.hb_nd2[T.hb0 + h]) ? 1 : 0;
   }
-  __syncthreads();
-  if (tid == 0) {
+  if (CL == 1) {
+    __syncthreads();
+  } else {
+    cg::this_cluster().sync();   // every bit of the own rows is in
+  }
+  if (tid == 0 && cu.rank == 0) {
+    int ne = s.misc[MISC_NEXV], nl = s.misc[MISC_NELE];
+    if (CL == 2) { ne += peer_ptr(s.misc, cu)[MISC_NEXV]; nl += peer_ptr(s.misc, cu)[MISC_NELE]; }
     st.nrebuild++;
-    st.nexv = s.misc[MISC_NEXV];
-    st.nele = s.misc[MISC_NELE];
+    st.nexv = ne;
+    st.nele = nl;
   }
 }
 
@@ -239,15 +287,18 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
 // thread into ch_part), angles, bonds.  Phase 2 gives each bead a group of GA
 // threads that sums its exv pairs, its bonded slots and its Debye-Hueckel
 // chunk partials; the group's owner thread hands the FP64 total to `sink`.
-template <typename Real, typename Sink>
+template <typename Real, int CL, typename Sink>
 __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
-                           long long istep, Sink sink) {
+                           long long istep, const Clu &cu, int noise_step, Sink sink) {
   typedef typename V4<Real>::T V;
   const int N = T.nmp, NQ = T.nq, W = s.W;
   const int tid = threadIdx.x, nth = blockDim.x;
   LaneState &st = a.lstate[lane];
   const int label = st.label;
-  Real *slots = s.slots;
+  // slots of beads owned by the other CTA go to its copy (one global array
+  // when the slots do not fit shared memory)
+  const SlotDst slots{s.slots, (CL == 2 && s.slots_smem) ? (void *)peer_ptr(s.slots, cu) : nullptr, cu.lo, cu.hi};
+  const Real *my_slots = s.slots;
   uint8_t *hbf = a.hb_flag + L.hb0;
   double *hbe = a.hb_ene + L.hb0;
   int *exc = a.site_exc + L.site0;
@@ -256,8 +307,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   int nclamp = 0;
   // (site counters and MISC_EXCESS were cleared by the caller before its barrier)
   const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd;
-  const ChunkGeo cg = chunk_geo(NQ, W);
-  const int nch = (a.i_ele != 0) ? cg.nch : 0;
+  const ChunkGeo geo = chunk_geo(NQ, W);
+  const int nch = (a.i_ele != 0) ? geo.nch : 0;
   const int k_st = nhb, k_ch = k_st + nst, k_ba = k_ch + nch, k_bd = k_ba + nba, total = k_bd + nbd;
   const double *u0 = a.lab_u0 + a.lab_u0off[label];
   const double cdist = a.lab_cdist[label];
@@ -277,16 +328,32 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // warp-uniform schedule: 32-item chunks of one kind, most expensive kinds
   // first, dealt round-robin over the warps (no divergence between kinds)
   const int nwarp = nth >> 5, warp = tid >> 5, lid = tid & 31;
-  const int c_st = (nhb + 31) >> 5, c_ch = c_st + ((nst + 31) >> 5), c_ba = c_ch + ((nch + 31) >> 5);
-  const int c_bd = c_ba + ((nba + 31) >> 5), c_end = c_bd + ((nbd + 31) >> 5);
+  // items of this CTA, [x0, x1) per kind: all of them for one CTA per lane;
+  // with two CTAs every hbond goes to the first one (the valence pruning that
+  // may follow is serial), the rows of the own charged beads, and halves of
+  // the stacks, angles and bonds
+  int hb_0 = 0, hb_1 = nhb, st_0 = 0, st_1 = nst, ch_0 = 0, ch_1 = nch, ba_0 = 0, ba_1 = nba, bd_0 = 0, bd_1 = nbd;
+  if (CL == 2) {
+    if (cu.rank == 1) hb_1 = 0;
+    st_0 = cu.rank ? nst / 2 : 0; st_1 = cu.rank ? nst : nst / 2;
+    ba_0 = cu.rank ? nba / 2 : 0; ba_1 = cu.rank ? nba : nba / 2;
+    bd_0 = cu.rank ? nbd / 2 : 0; bd_1 = cu.rank ? nbd : nbd / 2;
+    ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
+  }
+  const int c_st = (hb_1 - hb_0 + 31) >> 5, c_ch = c_st + ((st_1 - st_0 + 31) >> 5);
+  const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
+  const int c_bd = c_ba + ((ba_1 - ba_0 + 31) >> 5), c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
+  // the sink's Gaussian noise of the own beads, drawn here where warps have slack
+  const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
+  const int c_end = c_nz + ((n_nz + 31) >> 5);
   (void)k_st; (void)k_ch; (void)k_ba; (void)k_bd; (void)total;
   for (int c = warp; c < c_end; c += nwarp) {
     PHASE_T0(t_item);
     int kind;
     if (c < c_st) {
       kind = 0;
-      const int h = (c << 5) + lid;
-      if (h < nhb) {
+      const int h = hb_0 + (c << 5) + lid;
+      if (h < hb_1) {
         uint8_t f = hbf[h] & 1;
         if (f) {
           bool act;
@@ -300,7 +367,10 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
               int sid = sites[q];
               if (sid >= 0) {
                 int old = atomicAdd(&exc[sid], 1);
-                if (old + 1 > a.site_val[T.site0 + sid]) s.misc[MISC_EXCESS] = 1;
+                if (old + 1 > a.site_val[T.site0 + sid]) {
+                  s.misc[MISC_EXCESS] = 1;
+                  if (CL == 2) peer_ptr(s.misc, cu)[MISC_EXCESS] = 1;
+                }
               }
             }
           }
@@ -311,22 +381,22 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       }
     } else if (c < c_ch) {
       kind = 1;
-      const int k = ((c - c_st) << 5) + lid;
-      if (k < nst) term_stack<Real>(a, T, s, slots, k, u0[k]);
+      const int k = st_0 + ((c - c_st) << 5) + lid;
+      if (k < st_1) term_stack<Real>(a, T, s, slots, k, u0[k]);
     } else if (c < c_ba) {
       kind = 2;
-      const int cc = ((c - c_ch) << 5) + lid;
-      if (cc < nch) {
+      const int cc = ch_0 + ((c - c_ch) << 5) + lid;
+      if (cc < ch_1) {
         // force_ele_DH.F90:72-117 over a word range of one charged bead's
         // ele row; two pairs in flight per iteration
-        const int kq = cc / cg.cpr, part = cc - kq * cg.cpr;
+        const int kq = cc / geo.cpr, part = cc - kq * geo.cpr;
         const int i = s.qb[kq];
         const V pi = s.A4[i];
         const Real qci = (Real)((double)pi.w * coefT);
         const uint32_t *row = mele + (size_t)i * W;
-        const int w1 = min(W, (part + 1) * cg.gw);
+        const int w1 = min(W, (part + 1) * geo.gw);
         Acc<Real> ax_, ay_, az_;
-        for (int w = part * cg.gw; w < w1; ++w) {
+        for (int w = part * geo.gw; w < w1; ++w) {
           uint32_t m = row[w];
           while (m) {
             const int j0 = (w << 5) + __ffs(m) - 1;
@@ -365,35 +435,48 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       }
     } else if (c < c_bd) {
       kind = 3;
-      const int k = ((c - c_ba) << 5) + lid;
-      if (k < nba) term_angle<Real>(a, T, s, slots, k);
+      const int k = ba_0 + ((c - c_ba) << 5) + lid;
+      if (k < ba_1) term_angle<Real>(a, T, s, slots, k);
+    } else if (c < c_nz) {
+      kind = 4;
+      const int k = bd_0 + ((c - c_bd) << 5) + lid;
+      if (k < bd_1) term_bond<Real>(a, T, s, slots, k);
     } else {
       kind = 4;
-      const int k = ((c - c_bd) << 5) + lid;
-      if (k < nbd) term_bond<Real>(a, T, s, slots, k);
+      const int i = cu.lo + ((c - c_nz) << 5) + lid;
+      if (i < cu.hi) {
+        double n0, n1, n2;
+        noise3(a, lane, L.state0 + i, istep, noise_step, n0, n1, n2);
+        s.NX[i] = n0; s.NY[i] = n1; s.NZ[i] = n2;
+      }
     }
     PHASE_ALL(32 + kind, t_item);
   }
-  __syncthreads();
   PHASE_ADD(3, t_p1);
+  PHASE_T0(t_b2);
+  if (CL == 1) __syncthreads(); else cg::this_cluster().sync();
+  PHASE_ADD(9, t_b2);
   if (tid == 0 && s.near_on) { s.misc[MISC_NEAR_BAD] = 0; s.misc[MISC_NEAR_DISP] = 0; }
+  // both CTAs hold the same flag (the first one sets it in both), so both
+  // take the same barriers
   if (s.misc[MISC_EXCESS]) {
-    if (tid == 0) {
+    if (tid == 0 && cu.rank == 0) {
       const double beta = a.hb_beta_global ? a.beta_hbond15 : a.lab_beta[label];
       prune_hbonds<Real>(a, lane, L, T, istep, beta, true);
     }
-    __syncthreads();
+    if (CL == 1) __syncthreads(); else cg::this_cluster().sync();
   }
   PHASE_T0(t_p2);
   // ---- phase 2: exv pairs + bonded slots + Debye-Hueckel chunk partials
-  const int GA = pow2_floor_clamp(nth / N, 8);
+  const int nown = cu.hi - cu.lo;
+  const int GA = pow2_floor_clamp(nth / nown, 8);
   const int g = tid & (GA - 1), grp = tid / GA, ngrp = nth / GA;
   const Real ra = (Real)a.exv_adjust, ra2 = ra * ra, inv_ra2 = (Real)(1.0 / (a.exv_adjust * a.exv_adjust));
   const Real dist_ps = (Real)a.exv_dist_PS, dist_rr = (Real)a.exv_dist;
-  const int iters = (N + ngrp - 1) / ngrp;
+  const int iters = (nown + ngrp - 1) / ngrp;
   for (int it = 0; it < iters; ++it) {
-    const int i = grp + it * ngrp;
-    const bool valid = i < N;
+    const int i = cu.lo + grp + it * ngrp;
+    const bool valid = i < cu.hi;
     double fx = 0, fy = 0, fz = 0;
     PHASE_T0(t_e0);
     PHASE_T0(t_e2);
@@ -469,12 +552,12 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
           const int h = (sid - T.slot_hb) / 6;
           if (!(hbf[h] & 2)) continue;
         }
-        fx += (double)slots[3 * (size_t)sid]; fy += (double)slots[3 * (size_t)sid + 1];
-        fz += (double)slots[3 * (size_t)sid + 2];
+        fx += (double)my_slots[3 * (size_t)sid]; fy += (double)my_slots[3 * (size_t)sid + 1];
+        fz += (double)my_slots[3 * (size_t)sid + 2];
       }
       const int kq = s.qidx[i];
       if (nch > 0 && kq >= 0) {
-        for (int c = kq * cg.cpr + g; c < (kq + 1) * cg.cpr; c += GA) {
+        for (int c = kq * geo.cpr + g; c < (kq + 1) * geo.cpr; c += GA) {
           fx += s.ch_part[3 * c]; fy += s.ch_part[3 * c + 1]; fz += s.ch_part[3 * c + 2];
         }
       }
@@ -497,18 +580,34 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
 }
 
 // ------------------------------------------------------------ the kernel
-template <typename Real, int NT>
+// CL = 1: one CTA per lane.  CL = 2 (mixed precision, KM_STEP, no periodic
+// box, fixed rebuild cadence): a cluster of two CTAs per lane; CTA r owns
+// half of the beads (x / v / a updates, list rows, force sums) and half of
+// the bonded items; new positions go to both CTAs' double-buffered copies
+// through distributed shared memory.  Per step: one cluster barrier after
+// the x update, one after the bonded sweep (two more at a rebuild, one more
+// after a valence pruning).  Every branch that decides a cluster barrier is
+// uniform over both CTAs.
+template <typename Real, int NT, int CL>
 __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
-  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
+  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)(blockIdx.x / CL);
   if (lane >= a.nlane) return;
+  if (CL == 2 && a.mode != KM_STEP) return;
   const LaneDesc L = a.lanes[lane];
   const TopDesc T = a.tops[L.top];
   const int N = T.nmp, NQ = T.nq;
   const int tid = threadIdx.x, nth = blockDim.x;
   const bool skin = a.n_step_neighbor <= 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  Smem<Real> s = carve<Real>(smem_raw, a.smem_total, a, L, T, a.periodic != 0, skin);
+  Smem<Real> s = carve<Real>(smem_raw, a.smem_total, a, L, T, a.periodic != 0, skin, CL == 2);
   LaneState &st = a.lstate[lane];
+  Clu cu;
+  cu.nrank = CL;
+  cu.rank = (CL == 2) ? (int)cg::this_cluster().block_rank() : 0;
+  cu.lo = (CL == 2 && cu.rank == 1) ? (N + 1) / 2 : 0;
+  cu.hi = (CL == 2 && cu.rank == 0) ? (N + 1) / 2 : N;
+  cu.kq_lo = 0; cu.kq_hi = NQ;
+  const long long istep0 = st.istep;   // two CTAs: written only after the final cluster barrier
   // ---- load state, per-bead parameters, incidence lists, list bit matrices
   for (int i = tid; i < N; i += nth) {
     const size_t o = 3 * (size_t)(L.state0 + i);
@@ -546,28 +645,116 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   for (int k = tid; k < NQ; k += nth) s.qidx[s.qb[k]] = k;
   if (tid == 0) s.misc[MISC_NEAR_BAD] = 1;
   __syncthreads();
+  if (CL == 2) {
+    // charged rows of the own beads (q_bead ascends in bead index)
+    int ql = 0, qh = 0;
+    for (int k = 0; k < NQ; ++k) { ql += s.qb[k] < cu.lo; qh += s.qb[k] < cu.hi; }
+    cu.kq_lo = ql; cu.kq_hi = qh;
+  }
 
   const int label0 = st.label;
   const double *c1 = a.lab_c1 + a.lab_c1off[label0];
   const int gb0 = L.state0;
+  if (s.cst_on) {
+    for (int i = tid; i < N; i += nth) {
+      const int b = T.bead0 + i;
+      s.C1[i] = c1[i]; s.C2[i] = a.b_c2[b]; s.C3[i] = a.b_c3[b]; s.C4[i] = a.b_c4[b]; s.RC[i] = a.b_rcmass[b];
+    }
+    __syncthreads();
+  }
+  // time_integral.F90:169-183: v / a update of bead i from its force
+  auto vstep = [&](long long istep, int nstep_noise) {
+    return [&, istep, nstep_noise](int i, double fx, double fy, double fz) {
+      double n0, n1, n2, rc, cc, c2, c3;
+      if (s.cst_on) {
+        if (a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }   // drawn in the bonded sweep
+        else noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
+        rc = s.RC[i]; cc = s.C1[i]; c2 = s.C2[i]; c3 = s.C3[i];
+      } else {
+        noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
+        const int b = T.bead0 + i;
+        rc = a.b_rcmass[b]; cc = c1[i]; c2 = a.b_c2[b]; c3 = a.b_c3[b];
+      }
+      const double ax = fx * rc + cc * n0, ay = fy * rc + cc * n1, az = fz * rc + cc * n2;
+      s.VX[i] = c2 * s.VX[i] + c3 * (s.AX[i] + ax);
+      s.VY[i] = c2 * s.VY[i] + c3 * (s.AY[i] + ay);
+      s.VZ[i] = c2 * s.VZ[i] + c3 * (s.AZ[i] + az);
+      s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
+      if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
+    };
+  };
 
-  if (a.mode == KM_NEIGHBOR) {
-    build_lists<Real>(a, lane, L, T, s);
+  if constexpr (CL == 2) {
+    typedef typename V4<Real>::T V;
+    cg::this_cluster().sync();   // both CTAs are running before any distributed access
+    double *pXN = peer_ptr(s.XN, cu), *pYN = peer_ptr(s.YN, cu), *pZN = peer_ptr(s.ZN, cu);
+    V *pA4N = peer_ptr(s.A4N, cu), *pL4N = peer_ptr(s.L4N, cu);
+    for (int step = 0; step < a.nsteps; ++step) {
+      const long long istep = istep0 + step + 1;
+      // time_integral.F90:94 fixed cadence (the two-CTA path has no skin rule)
+      PHASE_T0(t_reb);
+      if ((istep % a.n_step_neighbor) == 1 || istep == 1) build_lists<Real, 2>(a, lane, L, T, s, cu);
+      PHASE_ADD(1, t_reb);
+      PHASE_T0(t_xu);
+      // swap in the double buffers after both CTAs wrote them; the other
+      // CTA's copy of the own beads is written through distributed memory
+      for (int i = cu.lo + tid; i < cu.hi; i += nth) {
+        const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
+        const double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
+        const double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
+        const double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
+        const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
+        s.XN[i] = nx; s.YN[i] = ny; s.ZN[i] = nz;
+        pXN[i] = nx; pYN[i] = ny; pZN[i] = nz;
+        V av = s.A4[i], lv;
+        av.x = (Real)nx; av.y = (Real)ny; av.z = (Real)nz;
+        lv.x = (Real)(nx - (double)av.x); lv.y = (Real)(ny - (double)av.y); lv.z = (Real)(nz - (double)av.z);
+        lv.w = (Real)0;
+        s.A4N[i] = av; s.L4N[i] = lv;
+        pA4N[i] = av; pL4N[i] = lv;
+        if (s.near_on) {
+          const float ex = (float)av.x - s.NR4[i].x, ey = (float)av.y - s.NR4[i].y, ez = (float)av.z - s.NR4[i].z;
+          const float e2 = ex * ex + ey * ey + ez * ez;
+          if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
+        }
+      }
+      if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+      if (tid == 0) s.misc[MISC_EXCESS] = 0;
+      PHASE_ADD(2, t_xu);
+      PHASE_T0(t_b1);
+      cg::this_cluster().sync();
+      PHASE_ADD(8, t_b1);
+      { double *t; t = s.X; s.X = s.XN; s.XN = t; t = s.Y; s.Y = s.YN; s.YN = t; t = s.Z; s.Z = s.ZN; s.ZN = t; }
+      s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
+      { V *t; t = s.A4; s.A4 = s.A4N; s.A4N = t; t = s.L4; s.L4 = s.L4N; s.L4N = t; }
+      pXN = peer_ptr(s.XN, cu); pYN = peer_ptr(s.YN, cu); pZN = peer_ptr(s.ZN, cu);
+      pA4N = peer_ptr(s.A4N, cu); pL4N = peer_ptr(s.L4N, cu);
+      PHASE_T0(t_fp);
+      force_pass<Real, 2>(a, lane, L, T, s, istep, cu, a.noise_base + step, vstep(istep, a.noise_base + step));
+      // the next x update reads v / a and the near-list positions that
+      // other threads of this CTA wrote in the force pass
+      __syncthreads();
+      PHASE_ADD(6, t_fp);
+    }
+    cg::this_cluster().sync();   // no distributed shared-memory access after this
+  } else if (a.mode == KM_NEIGHBOR) {
+    build_lists<Real, 1>(a, lane, L, T, s, cu);
   } else if (a.mode == KM_FORCE) {
     double *out = a.out_force;
-    force_pass<Real>(a, lane, L, T, s, st.istep, [&](int i, double fx, double fy, double fz) {
+    force_pass<Real, 1>(a, lane, L, T, s, st.istep, cu, -1, [&](int i, double fx, double fy, double fz) {
       const size_t o = 3 * (size_t)(L.state0 + i);
       out[o] = fx; out[o + 1] = fy; out[o + 2] = fz;
     });
   } else if (a.mode == KM_PRE) {
-    build_lists<Real>(a, lane, L, T, s);
+    build_lists<Real, 1>(a, lane, L, T, s, cu);
     // dxyz_mp = 0 (time_integral_pre.F90:79)
     if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
     __syncthreads();
     const long long is = st.istep;
-    force_pass<Real>(a, lane, L, T, s, is, [&](int i, double fx, double fy, double fz) {
+    force_pass<Real, 1>(a, lane, L, T, s, is, cu, a.noise_base, [&](int i, double fx, double fy, double fz) {
       double n0, n1, n2;
-      noise3(a, lane, gb0 + i, is, a.noise_base, n0, n1, n2);
+      if (s.cst_on && a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }
+      else noise3(a, lane, gb0 + i, is, a.noise_base, n0, n1, n2);
       const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
       s.AX[i] = fx * rc + cc * n0; s.AY[i] = fy * rc + cc * n1; s.AZ[i] = fz * rc + cc * n2;
     });
@@ -610,7 +797,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         PHASE_ADD(0, t_trig);
         PHASE_T0(t_reb);
         if (rebuild) {
-          build_lists<Real>(a, lane, L, T, s);
+          build_lists<Real, 1>(a, lane, L, T, s, cu);
           // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
           if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
           __syncthreads();
@@ -619,8 +806,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         PHASE_T0(t_xu);
         // x update (time_integral.F90:152-161); clear hbond-site counters
         for (int i = tid; i < N; i += nth) {
-          const int b = T.bead0 + i;
-          const double c4 = a.b_c4[b];
+          const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
           double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
           double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
           double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
@@ -644,19 +830,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         // time_integral.F90:162-183: forces (+ f_ext), v / a update
         const int nstep_noise = a.noise_base + step;
         PHASE_T0(t_fp);
-        force_pass<Real>(a, lane, L, T, s, istep, [&](int i, double fx, double fy, double fz) {
-          // v / a update (time_integral.F90:169-183)
-          double n0, n1, n2;
-          noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
-          const int b = T.bead0 + i;
-          const double rc = a.b_rcmass[b], cc = c1[i], c2 = a.b_c2[b], c3 = a.b_c3[b];
-          const double ax = fx * rc + cc * n0, ay = fy * rc + cc * n1, az = fz * rc + cc * n2;
-          s.VX[i] = c2 * s.VX[i] + c3 * (s.AX[i] + ax);
-          s.VY[i] = c2 * s.VY[i] + c3 * (s.AY[i] + ay);
-          s.VZ[i] = c2 * s.VZ[i] + c3 * (s.AZ[i] + az);
-          s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
-          if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
-        });
+        force_pass<Real, 1>(a, lane, L, T, s, istep, cu, nstep_noise, vstep(istep, nstep_noise));
         if (tid == 0) st.istep = istep;
         __syncthreads();
         PHASE_ADD(6, t_fp);
@@ -667,10 +841,19 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   // the global copy of the bit matrices is read by the energy kernel and the list exports
   if (s.misc[MISC_REBUILT] && s.mask_smem) {
     uint32_t *gm = a.mask + L.mask0;
-    for (int k = tid; k < 2 * N * s.W; k += nth) gm[k] = s.mask[k];
+    if (CL == 1) {
+      for (int k = tid; k < 2 * N * s.W; k += nth) gm[k] = s.mask[k];
+    } else {   // own rows of both matrices
+      const int nw = (cu.hi - cu.lo) * s.W;
+      for (int k = tid; k < nw; k += nth) {
+        const size_t o = (size_t)cu.lo * s.W + k;
+        gm[o] = s.mask[o];
+        gm[(size_t)N * s.W + o] = s.mask[(size_t)N * s.W + o];
+      }
+    }
   }
   // write back
-  for (int i = tid; i < N; i += nth) {
+  for (int i = cu.lo + tid; i < cu.hi; i += nth) {
     const size_t o = 3 * (size_t)(L.state0 + i);
     a.xyz[o] = s.X[i]; a.xyz[o + 1] = s.Y[i]; a.xyz[o + 2] = s.Z[i];
     if (a.periodic) {
@@ -684,8 +867,14 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     if (skin) { a.dxyz[o] = s.DX[i]; a.dxyz[o + 1] = s.DY[i]; a.dxyz[o + 2] = s.DZ[i]; }
   }
   if (tid == 0) {
-    st.nclamp += s.misc[MISC_CLAMP];
-    if (s.misc[MISC_NAN]) st.flags |= LF_NAN;
+    if (CL == 1) {
+      st.nclamp += s.misc[MISC_CLAMP];
+      if (s.misc[MISC_NAN]) st.flags |= LF_NAN;
+    } else {
+      if (s.misc[MISC_CLAMP]) atomicAdd((unsigned long long *)&st.nclamp, (unsigned long long)s.misc[MISC_CLAMP]);
+      if (s.misc[MISC_NAN]) atomicOr(&st.flags, LF_NAN);
+      if (cu.rank == 0) st.istep = istep0 + a.nsteps;
+    }
   }
 }
 
@@ -695,15 +884,17 @@ extern "C" int tis_phase_read(unsigned long long *out) {
 }
 #endif
 
-template __global__ void lane_kernel<double, 512>(KArgs);
-template __global__ void lane_kernel<float, 512>(KArgs);
-template __global__ void lane_kernel<float, 1024>(KArgs);
+template __global__ void lane_kernel<double, 512, 1>(KArgs);
+template __global__ void lane_kernel<float, 512, 1>(KArgs);
+template __global__ void lane_kernel<float, 1024, 1>(KArgs);
+template __global__ void lane_kernel<float, 512, 2>(KArgs);
 
 // Dynamic shared memory to request for a topology: base layout + bit
 // matrices + incidence lists + slots, capped at the 227 KB a CTA may use.
-size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit) {
-  SmemPlan p = smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit);
-  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + p.near + 64;
+size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
+                       bool dbuf) {
+  SmemPlan p = smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit, dbuf);
+  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + p.near + p.cst + 64;
   return want < 227 * 1024 ? want : 227 * 1024;
 }
 
@@ -711,22 +902,43 @@ size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool sk
   return smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit).base;
 }
 
-cudaError_t lane_kernel_set_smem(bool mixed, int bytes) {
+cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2) {
   cudaError_t e;
   if (mixed) {
-    e = cudaFuncSetAttribute(lane_kernel<float, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    e = cudaFuncSetAttribute(lane_kernel<float, 512, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(lane_kernel<float, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    e = cudaFuncSetAttribute(lane_kernel<float, 1024, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    if (bytes2 > 0)
+      return cudaFuncSetAttribute(lane_kernel<float, 512, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes2);
+    return cudaSuccess;
   }
-  return cudaFuncSetAttribute(lane_kernel<double, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  return cudaFuncSetAttribute(lane_kernel<double, 512, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 // block: threads per CTA (mixed: up to 1024, FP64: up to 512)
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a) {
-  if (mixed && block > 512) lane_kernel<float, 1024><<<grid, block, smem, st>>>(a);
-  else if (mixed) lane_kernel<float, 512><<<grid, block, smem, st>>>(a);
-  else lane_kernel<double, 512><<<grid, block, smem, st>>>(a);
+  if (mixed && block > 512) lane_kernel<float, 1024, 1><<<grid, block, smem, st>>>(a);
+  else if (mixed) lane_kernel<float, 512, 1><<<grid, block, smem, st>>>(a);
+  else lane_kernel<double, 512, 1><<<grid, block, smem, st>>>(a);
   return cudaGetLastError();
+}
+
+// Two CTAs per lane (clusters of 2): nlane lanes, 512 threads, KM_STEP only.
+cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, const KArgs &a) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * nlane, 1, 1);
+  cfg.blockDim = dim3(512, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, lane_kernel<float, 512, 2>, a);
 }
 
 } // namespace tis
