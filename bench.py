@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--period", type=int, default=None, help="MD steps per bench step (C3: exchange period)")
+    ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
+                    help="override the workload's arithmetic (0 FP64, 1 mixed)")
     ap.add_argument("--ref-sample", type=int, default=200,
                     help="reference arm: MD steps per replica in one timed step")
     ap.add_argument("--quick", action="store_true",
@@ -293,6 +295,8 @@ def run_ours(args, rank, world, local_rank):
 
     systems, par, temps, nrep, desc = workload(args.workload)
     par = dict(par, seed=1234 + rank)
+    if args.precision is not None:
+        par["precision"] = args.precision
     eng = Engine(systems, par, temps, nrep=nrep)
     x0 = np.vstack([np.tile(s["xyz"], (r, 1)) for s, r in zip(systems, nrep)])
     eng.set_state(x0)

@@ -263,6 +263,12 @@ int tis_timer(tis_ctx *ctx, int32_t op, double *ms);
 /* Human-readable text of the last error on this context. */
 const char *tis_last_error(const tis_ctx *ctx);
 
+/* Brownian-HI: diffuse_tensor and random_tensor of replica irep as the last
+ * refresh left them (simu_hydro_tensors.F90:17-352; var_simu arrays), each
+ * (3 nmp, 3 nmp) column-major; random_tensor is the lower Cholesky factor.
+ * Either pointer may be NULL. */
+int tis_get_hydro_tensors(tis_ctx *ctx, int32_t irep, double *diffuse, double *random);
+
 /* No counterpart in the reference: number of CUDA kernels this context has
  * launched so far (lets a caller count the launches of a timed region). */
 int64_t tis_launch_count(const tis_ctx *ctx);

@@ -99,3 +99,53 @@ def test_bdhi_reports_non_spd_tensor(tis_lib):
     assert e.value.code == TIS_E_NOT_SPD
     assert eng.status()["not_spd"] == 1
     eng.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-5)])
+def test_bdhi_cholesky_factor(tis_lib, precision, tol):
+    """The refreshed diffusion tensor and its Cholesky factor against the
+    restatement; precision 1 runs the trailing updates on the tensor cores
+    (3xTF32 split, FP32 accumulation), precision 0 in FP64."""
+    s = squeezed_chain(150, 9)           # 3N = 450: 8 tiles of 64, the last one partial
+    par = synth.bdhi_params(precision=precision)
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(np.zeros((2, s["nmp"], 3)))
+    eng.time_integral_pre()
+    x0 = s["xyz"].copy()
+    assert eng.step(1) >= 0              # refreshes D and L at the initial coordinates
+    D, L = eng.hydro_tensors()
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(x0[None])
+    Dr, Lr, rc = orc.hydro_tensors(par["hi_radius"])
+    assert rc == 0
+    assert np.abs(D - Dr).max() <= 1e-12 * np.abs(Dr).max()
+    assert np.abs(np.triu(L, 1)).max() == 0.0
+    assert np.abs(L - Lr).max() <= tol * np.abs(Lr).max()
+    cov = np.linalg.norm(L @ L.T - Dr) / np.linalg.norm(Dr)
+    assert cov <= tol
+    eng.close()
+
+
+def test_bdhi_tensor_core_trajectory(tis_lib):
+    """Mixed precision (tensor-core factor) trajectory against the FP64
+    restatement with the same injected noise."""
+    s = squeezed_chain(70, 13)
+    par = synth.bdhi_params(precision=1, n_step_hydro=2)
+    nsteps = 6
+    noise = np.random.default_rng(8).normal(size=(nsteps + 1, s["nmp"], 3))
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(noise)
+    eng.time_integral_pre()
+    assert eng.step(nsteps) >= 0
+    x = eng.get_state()[0]
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(s["xyz"][None])
+    orc.set_noise(noise.reshape(nsteps + 1, 1, s["nmp"], 3))
+    orc.time_integral_pre()
+    orc.step(nsteps)
+    xr = orc.get_state()[0].reshape(-1, 3)
+    assert np.abs(xr - s["xyz"]).max() > 1e-3
+    assert np.abs(x - xr).max() < 1e-6
+    eng.close()

@@ -796,6 +796,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
   a.boltz = BOLTZ_KCAL_MOL; a.pi = F_PI;
   a.bd_istep = c->bd_istep; a.bd_kpanel = 0;
+  a.bd_tc = (c->bdhi && p.precision == TIS_PREC_MIXED) ? 1 : 0;
   a.cutoff_ele = p.cutoff_ele;
   a.i_DH_cutoff_type = p.i_DH_cutoff_type;
   a.hb_cutoff_dist = p.hb_cutoff_dist;
@@ -872,12 +873,17 @@ int check_lanes(tis_ctx *c) {
   if (c->bdhi) {
     std::vector<int> ns(c->nlane);
     CK(cudaMemcpy(ns.data(), c->d_not_spd.p, ns.size() * sizeof(int), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < c->nlane; ++i)
-      if (ns[i]) {
+    for (int i = 0; i < c->nlane; ++i) {
+      if (ns[i] & 1) {
         c->not_spd = 1;
         code = fail(c, TIS_E_NOT_SPD, "Cholesky factorisation of the diffusion tensor failed in lane " +
                                           std::to_string(i + 1));
       }
+      if (ns[i] & 2) {
+        c->wait_timeout = 1;
+        code = fail(c, TIS_E_TIMEOUT, "tensor-core update of the Cholesky factor did not complete");
+      }
+    }
   }
   if (code < 0) return code;
   return (int)std::min<long long>(clamps, 0x7fffffff);
@@ -1253,6 +1259,24 @@ extern "C" int tis_timer(tis_ctx *c, int32_t op, double *ms) {
 extern "C" const char *tis_last_error(const tis_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
 extern "C" int64_t tis_launch_count(const tis_ctx *c) { return c ? (int64_t)c->launches : -1; }
+
+extern "C" int tis_get_hydro_tensors(tis_ctx *c, int32_t irep, double *diffuse, double *random) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  if (!c->bdhi) return fail(c, TIS_E_UNSUPPORTED, "no hydrodynamic tensors: not a Brownian-HI context");
+  const LaneDesc &L = c->lanes[irep - 1];
+  const size_t n = 3 * (size_t)c->lane_nmp[irep - 1];
+  std::vector<double> buf(n * n);
+  // device storage is row-major; the reference arrays are column-major
+  for (int which = 0; which < 2; ++which) {
+    double *out = which == 0 ? diffuse : random;
+    if (!out) continue;
+    CK(cudaMemcpy(buf.data(), (which == 0 ? c->bd_D.p : c->bd_L.p) + L.bd0, n * n * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < n; ++r)
+      for (size_t col = 0; col < n; ++col) out[col * n + r] = buf[r * n + col];
+  }
+  return TIS_OK;
+}
 
 // ------------------------------------------------ force without allocation
 // tis_force_sumup_static: neighbour lists + forces of one replica for

@@ -76,7 +76,8 @@ __device__ __forceinline__ int lane_tiles(const KArgs &a, const LaneDesc &L, int
   return (n + CT - 1) / CT;
 }
 
-// grid nlane, 256 threads: factor the diagonal tile of panel k in place
+// grid nlane, 256 threads (16 x 16): factor the diagonal tile of panel k in
+// place; thread (ty, tx) owns rows ty + 16 a and columns tx + 16 b of the tile
 __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
   const int lane = blockIdx.x;
   if (lane >= a.nlane) return;
@@ -88,12 +89,15 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
   double *Lm = a.bd_L + L.bd0;
   __shared__ double A[CT * CTP];
   __shared__ int bad;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   if (tid == 0) bad = 0;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, c = e - i * nb;
-    A[i * CTP + c] = Lm[(size_t)(r0 + i) * n + r0 + c];
-  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = ty + 16 * u, c = tx + 16 * v;
+      A[i * CTP + c] = (i < nb && c < nb) ? Lm[(size_t)(r0 + i) * n + r0 + c] : (i == c ? 1.0 : 0.0);
+    }
   __syncthreads();
   for (int j = 0; j < nb; ++j) {
     if (tid == 0) {
@@ -102,26 +106,35 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
       A[j * CTP + j] = sqrt(d);
     }
     __syncthreads();
-    const double piv = A[j * CTP + j];
-    for (int i = j + 1 + tid; i < nb; i += blockDim.x) A[i * CTP + j] /= piv;
+    if (tid < CT && tid > j) A[tid * CTP + j] /= A[j * CTP + j];
     __syncthreads();
-    const int m = nb - j - 1;
-    for (int e = tid; e < m * m; e += blockDim.x) {
-      const int i = j + 1 + e / m, c = j + 1 + e % m;
-      if (c <= i) A[i * CTP + c] -= A[i * CTP + j] * A[c * CTP + j];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = ty + 16 * u;
+      if (i <= j) continue;
+      const double lij = A[i * CTP + j];
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int c = tx + 16 * v;
+        if (c > j && c <= i) A[i * CTP + c] -= lij * A[c * CTP + j];
+      }
     }
     __syncthreads();
   }
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e / nb, c = e - i * nb;
-    Lm[(size_t)(r0 + i) * n + r0 + c] = (c <= i) ? A[i * CTP + c] : 0.0;
-  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = ty + 16 * u, c = tx + 16 * v;
+      if (i < nb && c < nb) Lm[(size_t)(r0 + i) * n + r0 + c] = (c <= i) ? A[i * CTP + c] : 0.0;
+    }
   if (tid == 0 && bad) atomicOr(&a.not_spd[lane], 1);
 }
 
-// grid (tiles - 1, nlane), 64 threads: tile row i = k + 1 + blockIdx.x of
-// panel k: solve X L_kk^T = A_ik by forward substitution, one row per thread
-__global__ void __launch_bounds__(CT) chol_panel_kernel(KArgs a) {
+// grid (tiles - 1, nlane), 256 threads: tile row i = k + 1 + blockIdx.x of
+// panel k: solve X L_kk^T = A_ik by forward substitution; four threads per
+// row split each dot product (fixed order: strided partials, butterfly)
+__global__ void __launch_bounds__(256) chol_panel_kernel(KArgs a) {
   const int lane = blockIdx.y;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
@@ -134,29 +147,27 @@ __global__ void __launch_bounds__(CT) chol_panel_kernel(KArgs a) {
   double *Lm = a.bd_L + L.bd0;
   extern __shared__ double shp[];
   double *Lk = shp, *X = shp + CT * CTP;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += CT) {
-    const int i = e / nb, c = e - i * nb;
-    Lk[i * CTP + c] = Lm[(size_t)(r0 + i) * n + r0 + c];
-  }
-  for (int e = tid; e < mb * nb; e += CT) {
-    const int i = e / nb, c = e - i * nb;
-    X[i * CTP + c] = Lm[(size_t)(i0 + i) * n + r0 + c];
+  const int tid = threadIdx.x, tx = tid & 63, ty = tid >> 6;   // 4 rows of 64 per pass
+#pragma unroll 4
+  for (int i = ty; i < CT; i += 4) {
+    Lk[i * CTP + tx] = (i < nb && tx < nb) ? Lm[(size_t)(r0 + i) * n + r0 + tx] : (i == tx ? 1.0 : 0.0);
+    X[i * CTP + tx] = (i < mb && tx < nb) ? Lm[(size_t)(i0 + i) * n + r0 + tx] : 0.0;
   }
   __syncthreads();
-  if (tid < mb) {
-    double *x = X + tid * CTP;
-    for (int c = 0; c < nb; ++c) {
-      double s = x[c];
-      for (int m = 0; m < c; ++m) s -= x[m] * Lk[c * CTP + m];
-      x[c] = s / Lk[c * CTP + c];
-    }
+  const int row = tid >> 2, part = tid & 3;
+  double *x = X + row * CTP;
+  for (int c = 0; c < CT; ++c) {
+    double p = 0.0;
+    for (int m = part; m < c; m += 4) p += x[m] * Lk[c * CTP + m];
+    p += __shfl_xor_sync(0xffffffffu, p, 1);
+    p += __shfl_xor_sync(0xffffffffu, p, 2);
+    if (part == 0) x[c] = (x[c] - p) / Lk[c * CTP + c];
+    __syncwarp();
   }
   __syncthreads();
-  for (int e = tid; e < mb * nb; e += CT) {
-    const int i = e / nb, c = e - i * nb;
-    Lm[(size_t)(i0 + i) * n + r0 + c] = X[i * CTP + c];
-  }
+#pragma unroll 4
+  for (int i = ty; i < mb; i += 4)
+    if (tx < nb) Lm[(size_t)(i0 + i) * n + r0 + tx] = X[i * CTP + tx];
 }
 
 // grid (pairs, nlane), 256 threads: trailing tile (ti, tj), k < tj <= ti:
@@ -214,6 +225,176 @@ __global__ void __launch_bounds__(256) chol_update_kernel(KArgs a) {
       Lm[(size_t)(i0 + r) * n + j0 + c] -= acc[u][v];
     }
   }
+}
+
+// ------------------------------------------------------------ tensor cores
+// Trailing update on the 5th-generation tensor cores (mixed precision):
+// A_ij -= L_ik L_jk^T for a 128 x 64 output block (row tiles ti, ti + 1 of
+// panel k, column tile tj) per CTA.  Each FP64 operand x is split into TF32
+// parts x = hi + lo (hi keeps the top 10 mantissa bits), and the product is
+// hi.hi + hi.lo + lo.hi (the lo.lo term is below FP32 rounding), accumulated
+// in FP32 in tensor memory by 24 tcgen05.mma (M = 128, N = 64, K = 8) issued
+// by one thread.  Diagonal tiles and panel solves stay in FP64.
+//
+// Shared-memory operands use the canonical K-major layout without swizzle:
+// 8-row x 16-byte core matrices, rows 16 B apart, 8-row groups SBO = 128 B
+// apart, 4-element K chunks LBO apart (A: 16 groups -> 2048 B; B: 8 -> 1024 B).
+constexpr int TC_M = 128, TC_N = 64, TC_K = 64;
+constexpr int TC_SMEM = 2 * TC_M * TC_K * 4 + 2 * TC_N * TC_K * 4;   // A hi/lo, B hi/lo (FP32)
+constexpr uint32_t TC_WAIT_MAX = 1u << 24;                           // polls of the completion barrier
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// UMMA shared-memory descriptor: start >> 4 [0,14), LBO >> 4 [16,30),
+// SBO >> 4 [32,46), version 1 [46,48), no swizzle (layout type 0 [61,64))
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// byte offset of element (r, k) in a K-major, no-swizzle tile of `rows` rows
+__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int rows) {
+  return (uint32_t)(((k >> 2) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ void tf32_split(double x, float &hi, float &lo) {
+  const float xf = (float)x;
+  hi = __uint_as_float((__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u);
+  lo = xf - hi;
+}
+
+// grid (ceil(m_max / 2) * m_max, nlane), 128 threads (4 warps; warp w owns
+// TMEM lanes / output rows 32 w .. 32 w + 31)
+__global__ void __launch_bounds__(128) chol_update_tc_kernel(KArgs a, int m_max) {
+  const int lane = blockIdx.y;
+  if (lane >= a.nlane) return;
+  const LaneDesc L = a.lanes[lane];
+  int n;
+  const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
+  const int m = T - k - 1;
+  const int R = blockIdx.x / m_max, tjr = blockIdx.x - R * m_max;
+  if (m <= 0 || 2 * R >= m || tjr >= m || tjr > 2 * R + 1) return;   // uniform over the CTA
+  const int ti0 = k + 1 + 2 * R, tj = k + 1 + tjr;
+  const int r0 = k * CT, nb = min(CT, n - r0);
+  const int j0 = tj * CT, mj = min(CT, n - j0);
+  double *Lm = a.bd_L + L.bd0;
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  unsigned char *base = (unsigned char *)(((uintptr_t)tsm + 1023) & ~(uintptr_t)1023);
+  unsigned char *Ahi = base, *Alo = base + TC_M * TC_K * 4;
+  unsigned char *Bhi = Alo + TC_M * TC_K * 4, *Blo = Bhi + TC_N * TC_K * 4;
+  __shared__ uint32_t tmem_slot;
+  __shared__ __align__(8) uint64_t mbar;
+  const int tid = threadIdx.x, warp = tid >> 5, lid = tid & 31;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TC_N));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  // operands: rows of tile ti0 then ti0 + 1 (zero past the matrix), columns
+  // of panel k; each pass of the block reads 4 rows x 64 columns (coalesced),
+  // all loads of a thread in flight before the conversions
+  {
+    const int kk = tid & 63, rq = tid >> 6;   // 0..1 with 128 threads
+    double va[TC_M / 2], vb[TC_N / 2];
+#pragma unroll
+    for (int u = 0; u < TC_M / 2; ++u) {
+      const int r = rq + 2 * u;
+      const int grow = (ti0 + (r >> 6)) * CT + (r & 63);
+      va[u] = (grow < n && kk < nb) ? Lm[(size_t)grow * n + r0 + kk] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < TC_N / 2; ++u) {
+      const int r = rq + 2 * u;
+      vb[u] = (r < mj && kk < nb) ? Lm[(size_t)(j0 + r) * n + r0 + kk] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < TC_M / 2; ++u) {
+      float hi, lo;
+      tf32_split(va[u], hi, lo);
+      const uint32_t o = kmajor_off(rq + 2 * u, kk, TC_M);
+      *(float *)(Ahi + o) = hi;
+      *(float *)(Alo + o) = lo;
+    }
+#pragma unroll
+    for (int u = 0; u < TC_N / 2; ++u) {
+      float hi, lo;
+      tf32_split(vb[u], hi, lo);
+      const uint32_t o = kmajor_off(rq + 2 * u, kk, TC_N);
+      *(float *)(Bhi + o) = hi;
+      *(float *)(Blo + o) = lo;
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t taddr = tmem_slot;
+  if (tid == 0) {
+    // kind::tf32, D F32 [4,6) = 1, A TF32 [7,10) = 2, B TF32 [10,13) = 2,
+    // both K-major, N >> 3 at [17,23), M >> 4 at [24,29)
+    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                           ((uint32_t)(TC_M >> 4) << 24);
+    const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo), b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
+    for (int s = 0; s < TC_K / 8; ++s) {
+      for (int p = 0; p < 3; ++p) {
+        const uint32_t sa = (p == 2 ? a_lo : a_hi) + (uint32_t)s * 2u * (TC_M / 8) * 128u;
+        const uint32_t sb = (p == 1 ? b_lo : b_hi) + (uint32_t)s * 2u * (TC_N / 8) * 128u;
+        const uint64_t da = umma_desc(sa, (TC_M / 8) * 128, 128);
+        const uint64_t db = umma_desc(sb, (TC_N / 8) * 128, 128);
+        const uint32_t acc = (s | p) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(taddr), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(&mbar))
+                 : "memory");
+  }
+  // bounded wait for the products
+  uint32_t done = 0;
+  for (uint32_t it = 0; it < TC_WAIT_MAX && !done; ++it) {
+    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                 : "=r"(done)
+                 : "r"(smem_u32(&mbar)), "r"(0u)
+                 : "memory");
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // TMEM lane = output row (32 per warp), column = output column: stage the
+  // FP32 products in shared memory (the operands are no longer read), then
+  // subtract them from the FP64 tiles with coalesced row accesses
+  float *stage = (float *)Ahi;   // (TC_M, TC_N + 1), within A hi + A lo
+  const int row = warp * 32 + lid;
+  for (int c = 0; c < TC_N / 8; ++c) {
+    uint32_t v[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 8)));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; ++q) stage[row * (TC_N + 1) + c * 8 + q] = __uint_as_float(v[q]);
+  }
+  __syncthreads();
+  if (done) {
+    const int col = tid & 63, rq = tid >> 6;
+    for (int u = 0; u < TC_M / 2; ++u) {
+      const int r = rq + 2 * u;
+      const int trow = ti0 + (r >> 6);
+      const int grow = trow * CT + (r & 63);
+      if (grow < n && col < mj && trow >= tj)
+        Lm[(size_t)grow * n + j0 + col] -= (double)stage[r * (TC_N + 1) + col];
+    }
+  }
+  if (tid == 0 && !done) atomicOr(&a.not_spd[lane], 2);   // the tensor-core wait gave up
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TC_N));
 }
 
 // ------------------------------------------------------------ step
@@ -322,6 +503,8 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
   e = cudaFuncSetAttribute(chol_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            2 * CT * CTP * (int)sizeof(double));
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(chol_update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM + 1024);
+  if (e != cudaSuccess) return e;
   const long long nn = (long long)max_nmp * max_nmp;
   rpy_kernel<<<dim3((unsigned)((nn + 255) / 256), a.nlane), 256, 0, st>>>(a);
   const int T = (3 * max_nmp + CT - 1) / CT;
@@ -329,9 +512,12 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
     a.bd_kpanel = k;
     chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
     if (k + 1 < T) {
-      chol_panel_kernel<<<dim3(T - k - 1, a.nlane), CT, 2 * CT * CTP * sizeof(double), st>>>(a);
+      chol_panel_kernel<<<dim3(T - k - 1, a.nlane), 256, 2 * CT * CTP * sizeof(double), st>>>(a);
       const int m = T - k - 1;
-      chol_update_kernel<<<dim3(m * (m + 1) / 2, a.nlane), 256, 2 * CT * CT * sizeof(double), st>>>(a);
+      if (a.bd_tc)
+        chol_update_tc_kernel<<<dim3(((m + 1) / 2) * m, a.nlane), 128, TC_SMEM + 1024, st>>>(a, m);
+      else
+        chol_update_kernel<<<dim3(m * (m + 1) / 2, a.nlane), 256, 2 * CT * CT * sizeof(double), st>>>(a);
     }
   }
   return cudaGetLastError();

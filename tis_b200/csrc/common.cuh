@@ -122,6 +122,7 @@ struct KArgs {
   double boltz, pi;                // BOLTZ_KCAL_MOL and F_PI of const_physical.F90
   long long bd_istep;              // step being taken (1-based)
   int bd_kpanel;                   // Cholesky panel of this launch
+  int bd_tc;                       // 1: trailing updates on the tensor cores (3xTF32 split, FP32 accumulation)
   double hb_cutoff_dist;
   double max_abscos;   // MAX_ANG_ABSCOS_HBOND15 == MAX_DIH_ABSCOS_HBOND15
   double tstep, tstep2, tsteph;

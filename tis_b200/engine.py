@@ -170,6 +170,15 @@ class Engine:
         self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na)), "replica_exchange")
         return na.value
 
+    def hydro_tensors(self, irep=1):
+        """(D, L) of the last Brownian-HI refresh, row-major (3N, 3N) arrays."""
+        n = 3 * self.lane_nmp[irep - 1]
+        D = np.zeros((n, n))
+        Lm = np.zeros((n, n))
+        self._check(self.L.tis_get_hydro_tensors(self.h, irep, ptr_f64(D), ptr_f64(Lm)), "hydro_tensors")
+        # column-major buffers: transpose to row-major views
+        return D.T.copy(), Lm.T.copy()
+
     def launch_count(self) -> int:
         return int(self.L.tis_launch_count(self.h))
 
