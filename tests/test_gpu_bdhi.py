@@ -127,6 +127,28 @@ def test_bdhi_cholesky_factor(tis_lib, precision, tol):
     eng.close()
 
 
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, 1e-5)])
+def test_bdhi_cholesky_many_lanes(tis_lib, precision, tol):
+    """A batch whose panel launches hold more CTAs than the GPU runs at once
+    (24 lanes, 3N up to 1800), so CTAs of one launch run in several waves:
+    every lane's factor against an FP64 factorisation of its own D."""
+    rng = np.random.default_rng(17)
+    ns = [int(v) for v in rng.integers(120, 601, size=24)]
+    systems = [synth.bead_chain(n, 300 + k) for k, n in enumerate(ns)]
+    par = synth.bdhi_params(precision=precision)
+    eng = Engine(systems, par, [300.0] * len(ns), nrep=[1] * len(ns))
+    eng.set_state(np.vstack([s["xyz"] for s in systems]))
+    eng.time_integral_pre()
+    assert eng.step(1) >= 0
+    for irep in range(1, len(ns) + 1):
+        D, L = eng.hydro_tensors(irep)
+        Lr = np.linalg.cholesky(D)
+        assert np.abs(np.triu(L, 1)).max() == 0.0
+        err = np.abs(L - Lr).max() / np.abs(Lr).max()
+        assert err <= tol, (irep, ns[irep - 1], err)
+    eng.close()
+
+
 def test_bdhi_tensor_core_trajectory(tis_lib):
     """Mixed precision (tensor-core factor) trajectory against the FP64
     restatement with the same injected noise."""

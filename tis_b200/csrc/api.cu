@@ -32,6 +32,7 @@ cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool
 cudaError_t ewald_energy_launch(cudaStream_t st, const KArgs &a);
 cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp);
 int bd_refactor_launches(int max_nmp);
+long long bd_plane_floats(int nmp);
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp);
 cudaError_t bd_force_launch(cudaStream_t st, const KArgs &a, int max_nmp);
 cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
@@ -142,6 +143,8 @@ struct tis_ctx {
   long long bd_istep = 0;
   DBuf<int> fene_idx, wca_idx, bd_ptr, bd_ent, d_not_spd;
   DBuf<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef, bd_D, bd_L, bd_F, bd_xi;
+  DBuf<float> bd_P;
+  DBuf<double> bd_W;
 };
 
 namespace {
@@ -484,7 +487,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
-  long long bd_off = 0;
+  long long bd_off = 0, bdp_off = 0;
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
@@ -526,7 +529,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       L.ew0 = ew_off;
       ew_off += d.nq;
       L.bd0 = bd_off;
+      L.bdp0 = bdp_off;
       if (c->bdhi) bd_off += 9LL * N * N;
+      if (c->bdhi && p.precision == TIS_PREC_MIXED) bdp_off += bd_plane_floats(N);
       state_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
       if (periodic) mirror_off += (long long)N * N;
@@ -631,6 +636,11 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     CK(c->wca_idx.upload(wca_idx)); CK(c->wca_nat.upload(wca_nat)); CK(c->wca_coef.upload(wca_coef));
     CK(c->bd_ptr.upload(bdp)); CK(c->bd_ent.upload(bde));
     CK(c->bd_D.alloc((size_t)bd_off)); CK(c->bd_L.alloc((size_t)bd_off));
+    CK(c->bd_W.alloc((size_t)nlane * 64 * 64));
+    if (bdp_off) {
+      CK(c->bd_P.alloc((size_t)bdp_off));
+      CK(cudaMemset(c->bd_P.p, 0, (size_t)bdp_off * sizeof(float)));   // tile T of each lane stays zero
+    }
     CK(c->bd_F.alloc(n3)); CK(c->bd_xi.alloc(n3));
     CK(cudaMemset(c->bd_F.p, 0, n3 * 8));
     CK(c->d_not_spd.alloc(nlane));
@@ -684,7 +694,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
   c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
-  c->bd_D.free(); c->bd_L.free(); c->bd_F.free(); c->bd_xi.free();
+  c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tev0) cudaEventDestroy(c->tev0);
@@ -791,7 +801,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.wca_idx = c->wca_idx.p; a.wca_nat = c->wca_nat.p; a.wca_coef = c->wca_coef.p;
   a.wca_rcut2 = 1.0 / (p.wca_coef_cutoff * p.wca_coef_cutoff);
   a.bd_ptr = c->bd_ptr.p; a.bd_ent = c->bd_ent.p;
-  a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
+  a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_P = c->bd_P.p; a.bd_W = c->bd_W.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
   a.not_spd = c->d_not_spd.p;
   a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
   a.boltz = BOLTZ_KCAL_MOL; a.pi = F_PI;

@@ -1,13 +1,16 @@
 // bdhi_kernel.cu -- Brownian dynamics with hydrodynamic interactions
 // (Ermak-McCammon, i_simulate_type = BROWNIAN_HI), batched over lanes of
-// different sizes, FP64.
+// different sizes, FP64 (precision 1: Cholesky trailing updates on the
+// tensor cores in split TF32).
 //
 // One step of time_integral.F90:429-457 for every lane:
 //   [every n_step_hydro steps] D = RPY tensor at x (simu_hydro_tensors.F90:
 //       139-182, HI_TENSOR%RPY), L = Cholesky factor of D (:304-324):
-//       rpy_kernel, then per 64-wide panel k: chol_diag_kernel (factor the
-//       diagonal tile), chol_panel_kernel (L_ik = A_ik L_kk^-T below it),
-//       chol_update_kernel (A_ij -= L_ik L_jk^T for the trailing tiles)
+//       rpy_kernel, chol_diag_kernel (L_00), then per 64-wide panel k:
+//       chol_panel_kernel (L_ik = A_ik L_kk^-T below the diagonal tile),
+//       chol_update_kernel or chol_update_tc_kernel (A_ij -= L_ik L_jk^T for
+//       the trailing tiles, FP64 or tensor cores; the CTA that finishes tile
+//       (k + 1, k + 1) factors it for the next panel)
 //   bd_noise_kernel     xi (counter-based or injected r_boxmuller)
 //   bd_update_kernel    dx_k = tstep/kT (D F)_k + sqrt(2 tstep) (L xi)_k,
 //                       x += dx (one warp per row, HBM-bound matrix-vector)
@@ -76,64 +79,167 @@ __device__ __forceinline__ int lane_tiles(const KArgs &a, const LaneDesc &L, int
   return (n + CT - 1) / CT;
 }
 
-// grid nlane, 256 threads (16 x 16): factor the diagonal tile of panel k in
-// place; thread (ty, tx) owns rows ty + 16 a and columns tx + 16 b of the tile
+// TF32 split of an FP64 value: hi keeps the top 10 mantissa bits of the
+// FP32 rounding (round half up in magnitude), lo = the FP32 rest
+__device__ __forceinline__ void tf32_split(double x, float &hi, float &lo) {
+  const float xf = (float)x;
+  hi = __uint_as_float((__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u);
+  lo = xf - hi;
+}
+
+// Panel operand planes for the tensor cores: per lane, (T + 1) tiles of
+// 64 rows x 64 panel columns of TF32 hi parts, then as many of lo parts
+// (tile T stays zero: the partner of an odd last row tile).  Inside a tile
+// the layout is the K-major, no-swizzle canonical UMMA layout with 8-row
+// groups outermost: float offset of (r, c) = (r / 8) 512 + (c / 4) 32 +
+// (r % 8) 4 + c % 4, so consecutive row tiles form one operand of 128 rows.
+constexpr int PT = CT * CT;   // floats per plane tile
+// shared memory of the FP64 tile kernels: a padded tile and an unpadded one
+constexpr int U64_SMEM = (CT * CTP + CT * CT) * (int)sizeof(double);
+
+// Factor diagonal tile td of a lane and invert its factor with the 256
+// threads of the calling group (tid 0..255; sync() is the group's barrier),
+// in registers: thread (ty, tx) = (tid / 16, tid % 16) owns rows ty + 16 u
+// and columns tx + 16 v of the tile A (identity beyond the matrix) and of E,
+// which starts as the identity.  Gaussian elimination of [A | E] without
+// pivoting, one barrier per column j: with p_j = A_jj and m_ij = A_ij / p_j,
+//   A_ic -= m_ij A_cj (j < c <= i, the lower part by symmetry),
+//   E_ic -= m_ij E_jc (c <= j),
+// the owners of column j + 1 of A and of row j + 1 of E publish them in
+// double-buffered shared vectors.  Then A = Lt P Lt^T with Lt unit lower,
+// E = Lt^-1, so L = Lt P^1/2 (L_ic = A_ic / sqrt(p_c), L_ii = sqrt(p_i)) and
+// L^-1 = P^-1/2 E.  A pivot <= 0 is replaced by 1 (no NaN spreads) and
+// flags the lane.  Stores L_tt (zero above the diagonal) and, when a panel
+// follows, U_tt = L_tt^-T into the lane's inverse slot, through the shared
+// stage S (CT x CTP doubles); vec holds 4 CT + CT doubles.
+template <typename Sync>
+__device__ void factor_diag_tile(const KArgs &a, int lane, double *Lm, int n, int td, double *S, double *vec,
+                                 int tid, Sync sync) {
+  const int r0 = td * CT, nb = min(CT, n - r0);
+  const int tx = tid & 15, ty = tid >> 4;
+  double *col = vec, *erow = vec + 2 * CT, *piv = vec + 4 * CT;
+  double av[4][4], ev[4][4];
+  sync();   // the group's stores to the tile are visible; earlier users of S and vec are done
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = ty + 16 * u, c = tx + 16 * v;
+      av[u][v] = (i < nb && c < nb) ? Lm[(size_t)(r0 + i) * n + r0 + c] : (i == c ? 1.0 : 0.0);
+      ev[u][v] = (i == c) ? 1.0 : 0.0;
+    }
+  if (tx == 0) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) col[ty + 16 * u] = av[u][0];
+  }
+  if (ty == 0) {
+#pragma unroll
+    for (int v = 0; v < 4; ++v) erow[tx + 16 * v] = ev[0][v];
+  }
+  int bad = 0;
+  for (int j = 0; j < nb; ++j) {
+    sync();
+    const int q = (j & 1) * CT;
+    double p = col[q + j];
+    if (!(p > 0.0)) {
+      p = 1.0;
+      bad = 1;
+    }
+    if (tid == 0) piv[j] = p;
+    const double ip = 1.0 / p;
+    double ac[4], er[4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      ac[v] = col[q + tx + 16 * v];
+      er[v] = erow[q + tx + 16 * v];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = ty + 16 * u;
+      if (i <= j) continue;
+      const double mlt = col[q + i] * ip;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int c = tx + 16 * v;
+        if (c > j && c <= i) av[u][v] -= mlt * ac[v];
+        if (c <= j) ev[u][v] -= mlt * er[v];
+      }
+    }
+    const int jn = j + 1, qn = CT - q;
+    if (jn < nb) {
+      // register selects (an indexed read would put the arrays in local memory)
+      const int sel = jn >> 4;
+      if (tx == (jn & 15)) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          double x = av[u][0];
+          x = sel == 1 ? av[u][1] : x;
+          x = sel == 2 ? av[u][2] : x;
+          x = sel == 3 ? av[u][3] : x;
+          col[qn + ty + 16 * u] = x;
+        }
+      }
+      if (ty == (jn & 15)) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          double x = ev[0][v];
+          x = sel == 1 ? ev[1][v] : x;
+          x = sel == 2 ? ev[2][v] : x;
+          x = sel == 3 ? ev[3][v] : x;
+          erow[qn + tx + 16 * v] = x;
+        }
+      }
+    }
+  }
+  sync();
+  if (tid < nb) piv[tid] = sqrt(piv[tid]);
+  sync();
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = ty + 16 * u, c = tx + 16 * v;
+      if (i < nb && c < nb)
+        Lm[(size_t)(r0 + i) * n + r0 + c] = (c < i) ? av[u][v] / piv[c] : (c == i ? piv[c] : 0.0);
+    }
+  if (tid == 0 && bad) atomicOr(&a.not_spd[lane], 1);
+  if (r0 + CT < n) {   // a panel of rows below follows (then nb = CT)
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int i = ty + 16 * u, c = tx + 16 * v;
+        S[c * CTP + i] = (c <= i) ? ev[u][v] / piv[i] : 0.0;   // U[c][i] = W[i][c]
+      }
+    sync();
+    double *w = a.bd_W + (size_t)lane * CT * CT;
+    for (int e = tid; e < CT * CT; e += 256) w[e] = S[(e >> 6) * CTP + (e & 63)];
+  }
+}
+
+struct BlockSync {
+  __device__ void operator()() const { __syncthreads(); }
+};
+
+// grid nlane, 256 threads: the first diagonal tile of every lane.  The
+// diagonal tile of panel k + 1 is factored by the trailing update of panel k
+// (the CTA that finishes it), so only panel 0 needs this launch.
 __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
   const int lane = blockIdx.x;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
   int n;
-  const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
-  if (k >= T) return;
-  const int r0 = k * CT, nb = min(CT, n - r0);
-  double *Lm = a.bd_L + L.bd0;
-  __shared__ double A[CT * CTP];
-  __shared__ int bad;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  if (tid == 0) bad = 0;
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = ty + 16 * u, c = tx + 16 * v;
-      A[i * CTP + c] = (i < nb && c < nb) ? Lm[(size_t)(r0 + i) * n + r0 + c] : (i == c ? 1.0 : 0.0);
-    }
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
-    if (tid == 0) {
-      double d = A[j * CTP + j];
-      if (!(d > 0.0)) { bad = 1; d = 1.0; }
-      A[j * CTP + j] = sqrt(d);
-    }
-    __syncthreads();
-    if (tid < CT && tid > j) A[tid * CTP + j] /= A[j * CTP + j];
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = ty + 16 * u;
-      if (i <= j) continue;
-      const double lij = A[i * CTP + j];
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int c = tx + 16 * v;
-        if (c > j && c <= i) A[i * CTP + c] -= lij * A[c * CTP + j];
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = ty + 16 * u, c = tx + 16 * v;
-      if (i < nb && c < nb) Lm[(size_t)(r0 + i) * n + r0 + c] = (c <= i) ? A[i * CTP + c] : 0.0;
-    }
-  if (tid == 0 && bad) atomicOr(&a.not_spd[lane], 1);
+  lane_tiles(a, L, n);
+  __shared__ double S[CT * CTP], vec[5 * CT];
+  factor_diag_tile(a, lane, a.bd_L + L.bd0, n, 0, S, vec, threadIdx.x, BlockSync{});
 }
 
-// grid (tiles - 1, nlane), 256 threads: tile row i = k + 1 + blockIdx.x of
-// panel k: solve X L_kk^T = A_ik by forward substitution; four threads per
-// row split each dot product (fixed order: strided partials, butterfly)
+// grid (T - k - 1, nlane), 256 threads: row tile ti = k + 1 + blockIdx.x of
+// the panel below the factored diagonal tile: X = A_ik L_kk^-T as a 64 x 64
+// x 64 FP64 product with the stored transposed inverse U_kk (thread (ty, tx)
+// owns rows ty + 16 u, columns tx + 16 v; sums over m in increasing order),
+// stored in FP64 and, for the tensor-core update, split into TF32 hi / lo
+// in the panel planes.  Loads and stores are row-contiguous.
 __global__ void __launch_bounds__(256) chol_panel_kernel(KArgs a) {
   const int lane = blockIdx.y;
   if (lane >= a.nlane) return;
@@ -141,45 +247,76 @@ __global__ void __launch_bounds__(256) chol_panel_kernel(KArgs a) {
   int n;
   const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
   const int ti = k + 1 + blockIdx.x;
-  if (ti >= T) return;
-  const int r0 = k * CT, nb = min(CT, n - r0);
-  const int i0 = ti * CT, mb = min(CT, n - i0);
+  if (ti >= T) return;   // rows below the diagonal tile: the panel is full (64 columns)
+  const int r0 = k * CT, i0 = ti * CT, mi = min(CT, n - i0);
   double *Lm = a.bd_L + L.bd0;
-  extern __shared__ double shp[];
-  double *Lk = shp, *X = shp + CT * CTP;
-  const int tid = threadIdx.x, tx = tid & 63, ty = tid >> 6;   // 4 rows of 64 per pass
+  extern __shared__ double dsm[];   // U64_SMEM
+  double *As = dsm, *Us = As + CT * CTP;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const double *w = a.bd_W + (size_t)lane * CT * CT;
 #pragma unroll 4
-  for (int i = ty; i < CT; i += 4) {
-    Lk[i * CTP + tx] = (i < nb && tx < nb) ? Lm[(size_t)(r0 + i) * n + r0 + tx] : (i == tx ? 1.0 : 0.0);
-    X[i * CTP + tx] = (i < mb && tx < nb) ? Lm[(size_t)(i0 + i) * n + r0 + tx] : 0.0;
+  for (int e = tid; e < CT * CT; e += 256) {
+    const int r = e >> 6, c = e & 63;
+    As[r * CTP + c] = (r < mi) ? Lm[(size_t)(i0 + r) * n + r0 + c] : 0.0;
+    Us[e] = w[e];
   }
   __syncthreads();
-  const int row = tid >> 2, part = tid & 3;
-  double *x = X + row * CTP;
-  for (int c = 0; c < CT; ++c) {
-    double p = 0.0;
-    for (int m = part; m < c; m += 4) p += x[m] * Lk[c * CTP + m];
-    p += __shfl_xor_sync(0xffffffffu, p, 1);
-    p += __shfl_xor_sync(0xffffffffu, p, 2);
-    if (part == 0) x[c] = (x[c] - p) / Lk[c * CTP + c];
-    __syncwarp();
+  double acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+#pragma unroll 4
+  for (int m = 0; m < CT; ++m) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) av[u] = As[(ty + 16 * u) * CTP + m];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) bv[v] = Us[m * CT + tx + 16 * v];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] += av[u] * bv[v];
   }
   __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) As[(ty + 16 * u) * CTP + tx + 16 * v] = acc[u][v];
+  __syncthreads();
 #pragma unroll 4
-  for (int i = ty; i < mb; i += 4)
-    if (tx < nb) Lm[(size_t)(i0 + i) * n + r0 + tx] = X[i * CTP + tx];
+  for (int e = tid; e < CT * CT; e += 256) {
+    const int r = e >> 6, c = e & 63;
+    if (r < mi) Lm[(size_t)(i0 + r) * n + r0 + c] = As[r * CTP + c];
+  }
+  if (a.bd_tc) {
+    float *ph = a.bd_P + L.bdp0 + (size_t)ti * PT, *pl = ph + (size_t)(T + 1) * PT;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q, r = e & 63, g = e >> 6;
+      const double *x = As + r * CTP + 4 * g;
+      float4 h, l;
+      tf32_split(x[0], h.x, l.x);
+      tf32_split(x[1], h.y, l.y);
+      tf32_split(x[2], h.z, l.z);
+      tf32_split(x[3], h.w, l.w);
+      const int o = (r >> 3) * 512 + g * 32 + (r & 7) * 4;
+      *(float4 *)(ph + o) = h;
+      *(float4 *)(pl + o) = l;
+    }
+  }
 }
 
-// grid (pairs, nlane), 256 threads: trailing tile (ti, tj), k < tj <= ti:
+// grid (nlane, pairs), 256 threads: trailing tile (ti, tj), k < tj <= ti:
 // A_ij -= L_ik L_jk^T, a 64x64x64 FP64 product (4x4 outputs per thread)
 __global__ void __launch_bounds__(256) chol_update_kernel(KArgs a) {
-  const int lane = blockIdx.y;
+  const int lane = blockIdx.x;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
   int n;
   const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
   const int m = T - k - 1;
-  const int p = blockIdx.x;
+  const int p = blockIdx.y;
   if (m <= 0 || p >= m * (m + 1) / 2) return;
   int ii = (int)((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
   while (ii * (ii + 1) / 2 > p) --ii;
@@ -225,176 +362,253 @@ __global__ void __launch_bounds__(256) chol_update_kernel(KArgs a) {
       Lm[(size_t)(i0 + r) * n + j0 + c] -= acc[u][v];
     }
   }
+  if (p == 0) {
+    // tile (k + 1, k + 1) is now final: factor it for the next panel
+    __shared__ double vec[5 * CT];
+    factor_diag_tile(a, lane, Lm, n, k + 1, sh, vec, tid, BlockSync{});
+  }
 }
 
 // ------------------------------------------------------------ tensor cores
 // Trailing update on the 5th-generation tensor cores (mixed precision):
-// A_ij -= L_ik L_jk^T for a 128 x 64 output block (row tiles ti, ti + 1 of
-// panel k, column tile tj) per CTA.  Each FP64 operand x is split into TF32
-// parts x = hi + lo (hi keeps the top 10 mantissa bits), and the product is
-// hi.hi + hi.lo + lo.hi (the lo.lo term is below FP32 rounding), accumulated
-// in FP32 in tensor memory by 24 tcgen05.mma (M = 128, N = 64, K = 8) issued
-// by one thread.  Diagonal tiles and panel solves stay in FP64.
+// A_ij -= L_ik L_jk^T with L_ik = hi + lo split into TF32 parts (the panel
+// planes written by chol_factor_kernel), the product taken as
+// hi.hi + hi.lo + lo.hi (lo.lo is below FP32 rounding) and accumulated in
+// FP32 in tensor memory; the FP64 tile subtracts it.  Diagonal tiles and
+// panel solves stay in FP64.
 //
-// Shared-memory operands use the canonical K-major layout without swizzle:
-// 8-row x 16-byte core matrices, rows 16 B apart, 8-row groups SBO = 128 B
-// apart, 4-element K chunks LBO apart (A: 16 groups -> 2048 B; B: 8 -> 1024 B).
-constexpr int TC_M = 128, TC_N = 64, TC_K = 64;
-constexpr int TC_SMEM = 2 * TC_M * TC_K * 4 + 2 * TC_N * TC_K * 4;   // A hi/lo, B hi/lo (FP32)
-constexpr uint32_t TC_WAIT_MAX = 1u << 24;                           // polls of the completion barrier
+// A CTA owns a 128-row block (row tiles ti, ti + 1 of panel k) and up to UG
+// column tiles tj of it, and runs them as a pipeline of warp roles:
+//   warp 0, one thread: bulk copies of the A block (once) and of each B tile
+//     (two shared-memory stages) from the panel planes;
+//   warp 1, one thread: 24 tcgen05.mma (M 128, N 64, K 8) per column tile
+//     into one of two 64-column TMEM accumulators;
+//   warps 2..9: epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows)
+//     and column half (w - 2) / 4, transposes the 32 x 32 block through its
+//     own shared-memory stage and updates the FP64 rows with coalesced
+//     256-byte accesses.
+// Every wait on a barrier is bounded; a wait that gives up flags the lane
+// (not_spd bit 2, reported as a device-wait timeout) after the copies and
+// products in flight are drained.
+constexpr int UG = 8;                                 // column tiles per CTA
+constexpr int U_A = 2 * 2 * CT * CT * 4;              // A hi + lo, 128 rows
+constexpr int U_B = 2 * CT * CT * 4;                  // one B stage, hi + lo
+constexpr int U_STG = 32 * 33 * 4;                    // epilogue transpose stage per warp
+constexpr int U_SMEM = U_A + 2 * U_B + 8 * U_STG;
+constexpr int U_THREADS = 320;
+constexpr uint32_t U_WAIT_NS = 100000;                // suspend hint per poll
+constexpr uint32_t U_WAIT_MAX = 20000;                // polls: about 2 s at most
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // UMMA shared-memory descriptor: start >> 4 [0,14), LBO >> 4 [16,30),
-// SBO >> 4 [32,46), version 1 [46,48), no swizzle (layout type 0 [61,64))
+// SBO >> 4 [32,46), version 1 [46,48), no swizzle (layout type 0 [61,64)).
+// K-major without swizzle: LBO = byte step between the two K-adjacent core
+// matrices of one K = 8 slice, SBO = byte step between 8-row groups.
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// byte offset of element (r, k) in a K-major, no-swizzle tile of `rows` rows
-__device__ __forceinline__ uint32_t kmajor_off(int r, int k, int rows) {
-  return (uint32_t)(((k >> 2) * (rows >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 3) * 4);
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t it = 0; it < U_WAIT_MAX; ++it) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2, %3;\n\t"
+                 "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                 : "=r"(done)
+                 : "r"(bar), "r"(parity), "r"(U_WAIT_NS)
+                 : "memory");
+    if (done) return true;
+  }
+  return false;
 }
 
-__device__ __forceinline__ void tf32_split(double x, float &hi, float &lo) {
-  const float xf = (float)x;
-  hi = __uint_as_float((__float_as_uint(xf) + 0x1000u) & 0xFFFFE000u);
-  lo = xf - hi;
+__device__ __forceinline__ void mbar_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
-// grid (ceil(m_max / 2) * m_max, nlane), 128 threads (4 warps; warp w owns
-// TMEM lanes / output rows 32 w .. 32 w + 31)
-__global__ void __launch_bounds__(128) chol_update_tc_kernel(KArgs a, int m_max) {
-  const int lane = blockIdx.y;
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// grid (nlane, ceil(m / 2) * gmax) with m = T - k - 1 and gmax = ceil(m / UG)
+// for the largest lane (lanes fastest: the CTAs that factor the next
+// diagonal tile start first); U_THREADS threads, one CTA per SM
+__global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, int gmax) {
+  const int lane = blockIdx.x;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
   int n;
   const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
   const int m = T - k - 1;
-  const int R = blockIdx.x / m_max, tjr = blockIdx.x - R * m_max;
-  if (m <= 0 || 2 * R >= m || tjr >= m || tjr > 2 * R + 1) return;   // uniform over the CTA
-  const int ti0 = k + 1 + 2 * R, tj = k + 1 + tjr;
-  const int r0 = k * CT, nb = min(CT, n - r0);
-  const int j0 = tj * CT, mj = min(CT, n - j0);
+  const int R = blockIdx.y / gmax, g = blockIdx.y - R * gmax;
+  if (m <= 0 || 2 * R >= m) return;   // uniform over the CTA
+  const int ncol = min(2 * R + 2, m), c0 = g * UG;
+  if (c0 >= ncol) return;
+  const int nt = min(UG, ncol - c0);
+  const int ti0 = k + 1 + 2 * R, tj0 = k + 1 + c0;
   double *Lm = a.bd_L + L.bd0;
+  const float *ph = a.bd_P + L.bdp0, *pl = ph + (size_t)(T + 1) * PT;
+
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char *base = (unsigned char *)(((uintptr_t)tsm + 1023) & ~(uintptr_t)1023);
-  unsigned char *Ahi = base, *Alo = base + TC_M * TC_K * 4;
-  unsigned char *Bhi = Alo + TC_M * TC_K * 4, *Blo = Bhi + TC_N * TC_K * 4;
+  const uint32_t s_ahi = smem_u32(base), s_alo = s_ahi + U_A / 2;
+  const uint32_t s_b0 = s_ahi + U_A;   // stage s: hi at s_b0 + s U_B, lo 16 KB later
+  __shared__ __align__(8) uint64_t bars[10];   // fullA, fullB0/1, emptyB0/1, tfull0/1, tempty0/1, mdone
   __shared__ uint32_t tmem_slot;
-  __shared__ __align__(8) uint64_t mbar;
+  __shared__ int gaveup;
+  const uint32_t b_fullA = smem_u32(&bars[0]), b_fullB = smem_u32(&bars[1]), b_emptyB = smem_u32(&bars[3]);
+  const uint32_t b_tfull = smem_u32(&bars[5]), b_tempty = smem_u32(&bars[7]), b_mdone = smem_u32(&bars[9]);
   const int tid = threadIdx.x, warp = tid >> 5, lid = tid & 31;
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(TC_N));
+                 "r"(2 * CT));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
-    asm volatile("fence.mbarrier_init.release.cluster;");
+    for (int q = 0; q < 10; ++q) {
+      const uint32_t cnt = (q == 7 || q == 8) ? 8u : 1u;   // tempty: one arrival per epilogue warp
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[q])), "r"(cnt));
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    gaveup = 0;
   }
-  // operands: rows of tile ti0 then ti0 + 1 (zero past the matrix), columns
-  // of panel k; each pass of the block reads 4 rows x 64 columns (coalesced),
-  // all loads of a thread in flight before the conversions
-  {
-    const int kk = tid & 63, rq = tid >> 6;   // 0..1 with 128 threads
-    double va[TC_M / 2], vb[TC_N / 2];
-#pragma unroll
-    for (int u = 0; u < TC_M / 2; ++u) {
-      const int r = rq + 2 * u;
-      const int grow = (ti0 + (r >> 6)) * CT + (r & 63);
-      va[u] = (grow < n && kk < nb) ? Lm[(size_t)grow * n + r0 + kk] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < TC_N / 2; ++u) {
-      const int r = rq + 2 * u;
-      vb[u] = (r < mj && kk < nb) ? Lm[(size_t)(j0 + r) * n + r0 + kk] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < TC_M / 2; ++u) {
-      float hi, lo;
-      tf32_split(va[u], hi, lo);
-      const uint32_t o = kmajor_off(rq + 2 * u, kk, TC_M);
-      *(float *)(Ahi + o) = hi;
-      *(float *)(Alo + o) = lo;
-    }
-#pragma unroll
-    for (int u = 0; u < TC_N / 2; ++u) {
-      float hi, lo;
-      tf32_split(vb[u], hi, lo);
-      const uint32_t o = kmajor_off(rq + 2 * u, kk, TC_N);
-      *(float *)(Bhi + o) = hi;
-      *(float *)(Blo + o) = lo;
-    }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t taddr = tmem_slot;
-  if (tid == 0) {
-    // kind::tf32, D F32 [4,6) = 1, A TF32 [7,10) = 2, B TF32 [10,13) = 2,
-    // both K-major, N >> 3 at [17,23), M >> 4 at [24,29)
-    const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                           ((uint32_t)(TC_M >> 4) << 24);
-    const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo), b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
-    for (int s = 0; s < TC_K / 8; ++s) {
-      for (int p = 0; p < 3; ++p) {
-        const uint32_t sa = (p == 2 ? a_lo : a_hi) + (uint32_t)s * 2u * (TC_M / 8) * 128u;
-        const uint32_t sb = (p == 1 ? b_lo : b_hi) + (uint32_t)s * 2u * (TC_N / 8) * 128u;
-        const uint64_t da = umma_desc(sa, (TC_M / 8) * 128, 128);
-        const uint64_t db = umma_desc(sb, (TC_N / 8) * 128, 128);
-        const uint32_t acc = (s | p) ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-            :: "r"(taddr), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+
+  if (warp == 0) {
+    if (lid == 0) {
+      bool ok = true;
+      int last[2] = {-1, -1};
+      mbar_expect(b_fullA, U_A);
+      bulk_load(s_ahi, ph + (size_t)ti0 * PT, U_A / 2, b_fullA);
+      bulk_load(s_alo, pl + (size_t)ti0 * PT, U_A / 2, b_fullA);
+      for (int t = 0; t < nt; ++t) {
+        const int s = t & 1;
+        if (t >= 2 && !mbar_wait(b_emptyB + 8 * s, ((t >> 1) - 1) & 1)) { ok = false; break; }
+        const uint32_t dst = s_b0 + (uint32_t)s * U_B;
+        mbar_expect(b_fullB + 8 * s, U_B);
+        bulk_load(dst, ph + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
+        bulk_load(dst + U_B / 2, pl + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
+        last[s] = t;
+      }
+      // drain: no copy may still be writing shared memory when the CTA ends
+      ok = mbar_wait(b_fullA, 0) && ok;
+      for (int s = 0; s < 2; ++s)
+        if (last[s] >= 0) ok = mbar_wait(b_fullB + 8 * s, (last[s] >> 1) & 1) && ok;
+      if (!ok) gaveup = 1;
+    }
+  } else if (warp == 1) {
+    if (lid == 0) {
+      // kind::tf32, D F32 [4,6) = 1, A TF32 [7,10) = 2, B TF32 [10,13) = 2,
+      // both K-major, N >> 3 at [17,23), M >> 4 at [24,29)
+      const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(CT >> 3) << 17) |
+                             ((uint32_t)(2 * CT >> 4) << 24);
+      bool ok = mbar_wait(b_fullA, 0);
+      for (int t = 0; t < nt && ok; ++t) {
+        const int s = t & 1;
+        if (!mbar_wait(b_fullB + 8 * s, (t >> 1) & 1)) { ok = false; break; }
+        if (t >= 2 && !mbar_wait(b_tempty + 8 * s, ((t >> 1) - 1) & 1)) { ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t bhi = s_b0 + (uint32_t)s * U_B, blo = bhi + U_B / 2;
+        const uint32_t dacc = taddr + (uint32_t)(s * CT);
+        for (int ks = 0; ks < CT / 8; ++ks) {
+          for (int pp = 0; pp < 3; ++pp) {
+            const uint32_t sa = (pp == 2 ? s_alo : s_ahi) + (uint32_t)ks * 256u;
+            const uint32_t sb = (pp == 1 ? blo : bhi) + (uint32_t)ks * 256u;
+            const uint64_t da = umma_desc(sa, 128, 2048), db = umma_desc(sb, 128, 2048);
+            const uint32_t acc = (ks | pp) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+                :: "r"(dacc), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+          }
+        }
+        umma_commit(b_emptyB + 8 * s);
+        umma_commit(b_tfull + 8 * s);
+      }
+      // every product issued by this thread has landed before TMEM is freed
+      umma_commit(b_mdone);
+      ok = mbar_wait(b_mdone, 0) && ok;
+      if (!ok) gaveup = 1;
+    }
+  } else {
+    const int e = warp - 2, q = warp & 3, h = e >> 2;
+    float *stg = (float *)(base + U_A + 2 * U_B + e * U_STG);
+    uint32_t eok = 1;
+    for (int t = 0; t < nt; ++t) {
+      const int b = t & 1;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(b_tfull + 8 * b, (t >> 1) & 1));
+      if (!ok) {
+        if (lid == 0) gaveup = 1;
+        eok = 0;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t v[32];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+            "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+            "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * CT + h * 32)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lid == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b_tempty + 8 * b) : "memory");
+      // lane = row of the TMEM block: transpose so that a lane owns a column
+#pragma unroll
+      for (int c = 0; c < 32; ++c) stg[lid * 33 + c] = __uint_as_float(v[c]);
+      __syncwarp();
+      const int tj = tj0 + t, col = tj * CT + h * 32 + lid;
+      double old[32];
+#pragma unroll
+      for (int rr = 0; rr < 32; ++rr) {
+        const int rw = q * 32 + rr, trow = ti0 + (rw >> 6), grow = trow * CT + (rw & 63);
+        old[rr] = (grow < n && col < n && trow >= tj) ? Lm[(size_t)grow * n + col] : 0.0;
+      }
+#pragma unroll
+      for (int rr = 0; rr < 32; ++rr) {
+        const int rw = q * 32 + rr, trow = ti0 + (rw >> 6), grow = trow * CT + (rw & 63);
+        if (grow < n && col < n && trow >= tj) Lm[(size_t)grow * n + col] = old[rr] - (double)stg[rr * 33 + lid];
+      }
+      __syncwarp();
+    }
+    if (R == 0 && g == 0) {
+      // tile (k + 1, k + 1), updated above by this CTA, is final: the eight
+      // epilogue warps factor it for the next panel (the operand area is
+      // free: every product has been read out of TMEM)
+      const auto esync = [] { asm volatile("bar.sync 1, 256;" ::: "memory"); };
+      uint32_t all_ok;   // the same on all eight warps
+      asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.and.pred p, 1, 256, q;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n\t}\n"
+                   : "=r"(all_ok)
+                   : "r"(eok)
+                   : "memory");
+      if (all_ok) {
+        double *fs = (double *)base, *fv = fs + CT * CTP;
+        factor_diag_tile(a, lane, Lm, n, k + 1, fs, fv, tid - 64, esync);
       }
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(&mbar))
-                 : "memory");
   }
-  // bounded wait for the products
-  uint32_t done = 0;
-  for (uint32_t it = 0; it < TC_WAIT_MAX && !done; ++it) {
-    asm volatile("{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-                 "selp.b32 %0, 1, 0, P1;\n\t}\n"
-                 : "=r"(done)
-                 : "r"(smem_u32(&mbar)), "r"(0u)
-                 : "memory");
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  // TMEM lane = output row (32 per warp), column = output column: stage the
-  // FP32 products in shared memory (the operands are no longer read), then
-  // subtract them from the FP64 tiles with coalesced row accesses
-  float *stage = (float *)Ahi;   // (TC_M, TC_N + 1), within A hi + A lo
-  const int row = warp * 32 + lid;
-  for (int c = 0; c < TC_N / 8; ++c) {
-    uint32_t v[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
-                 : "r"(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 8)));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int q = 0; q < 8; ++q) stage[row * (TC_N + 1) + c * 8 + q] = __uint_as_float(v[q]);
-  }
-  __syncthreads();
-  if (done) {
-    const int col = tid & 63, rq = tid >> 6;
-    for (int u = 0; u < TC_M / 2; ++u) {
-      const int r = rq + 2 * u;
-      const int trow = ti0 + (r >> 6);
-      const int grow = trow * CT + (r & 63);
-      if (grow < n && col < mj && trow >= tj)
-        Lm[(size_t)grow * n + j0 + col] -= (double)stage[r * (TC_N + 1) + col];
-    }
-  }
-  if (tid == 0 && !done) atomicOr(&a.not_spd[lane], 2);   // the tensor-core wait gave up
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(TC_N));
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(2 * CT));
+  }
+  if (tid == 0 && gaveup) atomicOr(&a.not_spd[lane], 2);   // a tensor-core pipeline wait gave up
 }
 
 // ------------------------------------------------------------ step
@@ -498,26 +712,26 @@ __global__ void __launch_bounds__(256) bd_force_kernel(KArgs a) {
 // ------------------------------------------------------------ launches
 cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
   cudaError_t e = cudaFuncSetAttribute(chol_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       2 * CT * CT * (int)sizeof(double));
+                                       U64_SMEM);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(chol_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           2 * CT * CTP * (int)sizeof(double));
+  e = cudaFuncSetAttribute(chol_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, U64_SMEM);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(chol_update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM + 1024);
+  e = cudaFuncSetAttribute(chol_update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, U_SMEM + 1024);
   if (e != cudaSuccess) return e;
+  if (a.bd_tc && !a.bd_P) return cudaErrorInvalidValue;
   const long long nn = (long long)max_nmp * max_nmp;
   rpy_kernel<<<dim3((unsigned)((nn + 255) / 256), a.nlane), 256, 0, st>>>(a);
+  chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
   const int T = (3 * max_nmp + CT - 1) / CT;
-  for (int k = 0; k < T; ++k) {
+  for (int k = 0; k + 1 < T; ++k) {
     a.bd_kpanel = k;
-    chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
-    if (k + 1 < T) {
-      chol_panel_kernel<<<dim3(T - k - 1, a.nlane), 256, 2 * CT * CTP * sizeof(double), st>>>(a);
-      const int m = T - k - 1;
-      if (a.bd_tc)
-        chol_update_tc_kernel<<<dim3(((m + 1) / 2) * m, a.nlane), 128, TC_SMEM + 1024, st>>>(a, m);
-      else
-        chol_update_kernel<<<dim3(m * (m + 1) / 2, a.nlane), 256, 2 * CT * CT * sizeof(double), st>>>(a);
+    const int m = T - k - 1;
+    chol_panel_kernel<<<dim3(m, a.nlane), 256, U64_SMEM, st>>>(a);
+    if (a.bd_tc) {
+      const int gmax = (m + UG - 1) / UG;
+      chol_update_tc_kernel<<<dim3(a.nlane, ((m + 1) / 2) * gmax), U_THREADS, U_SMEM + 1024, st>>>(a, gmax);
+    } else {
+      chol_update_kernel<<<dim3(a.nlane, m * (m + 1) / 2), 256, U64_SMEM, st>>>(a);
     }
   }
   return cudaGetLastError();
@@ -525,7 +739,13 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
 
 int bd_refactor_launches(int max_nmp) {
   const int T = (3 * max_nmp + CT - 1) / CT;
-  return 1 + T + 2 * (T - 1);
+  return 2 + 2 * (T - 1);
+}
+
+// floats of the panel planes of a lane with N beads (tensor-core update)
+long long bd_plane_floats(int nmp) {
+  const int T = (3 * nmp + CT - 1) / CT;
+  return 2LL * (T + 1) * PT;
 }
 
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp) {

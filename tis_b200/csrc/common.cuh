@@ -55,6 +55,7 @@ struct LaneDesc {
   int unif0;        // injected uniform stream (n_uniform per lane)
   int ew0;          // Ewald: first charge of this lane in the per-lane charge tables
   long long bd0;    // Brownian-HI: first element of this lane's (3N)^2 diffusion / Cholesky matrices
+  long long bdp0;   // Brownian-HI, tensor cores: first float of this lane's TF32 panel planes
 };
 
 // Mutable per-lane scalar state, kept in global memory between launches.
@@ -117,6 +118,8 @@ struct KArgs {
   const int *bd_ent;               // record id * 2 + kind (0 FENE, 1 WCA)
   double *bd_D, *bd_L;             // per lane (3N x 3N, row-major): diffusion tensor, its Cholesky factor
   double *bd_F, *bd_xi;            // per lane (3N): force, Gaussian noise of the step
+  float *bd_P;                     // per lane: TF32 hi / lo planes of the current Cholesky panel
+  double *bd_W;                    // per lane: 64 x 64 transposed inverse of the current diagonal tile
   int *not_spd;                    // per lane: a Cholesky pivot was <= 0
   double hi_radius, viscosity;
   double boltz, pi;                // BOLTZ_KCAL_MOL and F_PI of const_physical.F90
