@@ -105,7 +105,8 @@ def test_bdhi_reports_non_spd_tensor(tis_lib):
 def test_bdhi_cholesky_factor(tis_lib, precision, tol):
     """The refreshed diffusion tensor and its Cholesky factor against the
     restatement; precision 1 runs the trailing updates on the tensor cores
-    (3xTF32 split, FP32 accumulation), precision 0 in FP64."""
+    (3xTF32 split, FP32 accumulation) and keeps D in FP32, precision 0 is
+    FP64 throughout."""
     s = squeezed_chain(150, 9)           # 3N = 450: 8 tiles of 64, the last one partial
     par = synth.bdhi_params(precision=precision)
     eng = Engine([s], par, [300.0])
@@ -119,7 +120,8 @@ def test_bdhi_cholesky_factor(tis_lib, precision, tol):
     orc.set_state(x0[None])
     Dr, Lr, rc = orc.hydro_tensors(par["hi_radius"])
     assert rc == 0
-    assert np.abs(D - Dr).max() <= 1e-12 * np.abs(Dr).max()
+    dtol = 1e-12 if precision == 0 else 1e-7   # precision 1 keeps D in FP32 for the step
+    assert np.abs(D - Dr).max() <= dtol * np.abs(Dr).max()
     assert np.abs(np.triu(L, 1)).max() == 0.0
     assert np.abs(L - Lr).max() <= tol * np.abs(Lr).max()
     cov = np.linalg.norm(L @ L.T - Dr) / np.linalg.norm(Dr)

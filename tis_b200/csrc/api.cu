@@ -9,6 +9,8 @@
 //   setp_periodic.F90:78-113, neighbor_list_ele.F90:73-89.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -30,8 +32,9 @@ cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cud
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
 cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool forces);
 cudaError_t ewald_energy_launch(cudaStream_t st, const KArgs &a);
-cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp);
-int bd_refactor_launches(int max_nmp);
+cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int *items, const int *koff);
+int bd_refactor_launches(int max_nmp, bool tc);
+void bd_update_items(const std::vector<int> &lane_T, std::vector<int> &items, std::vector<int> &koff);
 long long bd_plane_floats(int nmp);
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp);
 cudaError_t bd_force_launch(cudaStream_t st, const KArgs &a, int max_nmp);
@@ -141,9 +144,13 @@ struct tis_ctx {
   bool bdhi = false;
   int max_nmp = 0;
   long long bd_istep = 0;
-  DBuf<int> fene_idx, wca_idx, bd_ptr, bd_ent, d_not_spd;
+  DBuf<int> fene_idx, wca_idx, bd_ptr, d_not_spd;
+  DBuf<int2> bd_ent;
+  DBuf<double> fene_cls, wca_cls;
   DBuf<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef, bd_D, bd_L, bd_F, bd_xi;
-  DBuf<float> bd_P;
+  DBuf<float> bd_P, bd_D32, bd_L32;
+  DBuf<int> bd_items;               // tensor-core update work items, per launch
+  std::vector<int> bd_koff;
   DBuf<double> bd_W;
 };
 
@@ -287,7 +294,10 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   std::vector<double> st_hsTm_all;
-  std::vector<int> fene_idx, wca_idx, bdp, bde;
+  std::vector<int> fene_idx, wca_idx, bdp;
+  std::vector<int2> bde;
+  std::vector<double> fene_cls, wca_cls;
+  std::map<std::array<double, 3>, int> fene_cmap, wca_cmap;
   std::vector<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef;
   int maxN = 0;
   for (int k = 0; k < ntop; ++k) {
@@ -313,19 +323,31 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     maxN = std::max(maxN, t.nmp);
     if (c->bdhi && (t.nbd || t.nba || t.nst || t.nhb)) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
     // FENE / WCA records (read_nativeinfo.F90:153-176, 306-332); per bead
-    // incidence lists (record * 2 + kind, FENE records first) for the
-    // Brownian-HI force gather
+    // incidence lists for the Brownian-HI force gather, FENE records first:
+    // (partner bead, parameter class * 2 + kind), classes = the distinct
+    // parameter triples
     d.fe0 = (int)fene_nat.size(); d.nfe = t.nfene;
     d.wc0 = (int)wca_nat.size(); d.nwc = t.nwca;
     d.bp0 = (int)bdp.size(); d.be0 = (int)bde.size();
     if (c->bdhi) {
-      std::vector<std::vector<int>> per(t.nmp);
+      std::vector<std::vector<int2>> per(t.nmp);
+      auto cls_of = [](std::map<std::array<double, 3>, int> &m, std::vector<double> &tab, double p0, double p1,
+                       double p2) {
+        const std::array<double, 3> key{p0, p1, p2};
+        auto it = m.find(key);
+        if (it != m.end()) return it->second;
+        const int id = (int)m.size();
+        m.emplace(key, id);
+        tab.push_back(p0); tab.push_back(p1); tab.push_back(p2);
+        return id;
+      };
       for (int r = 0; r < t.nfene; ++r) {
         const int i1 = t.ifene2mp[2 * r] - 1, i2 = t.ifene2mp[2 * r + 1] - 1;
         if (i1 < 0 || i2 < 0 || i1 >= t.nmp || i2 >= t.nmp || i1 == i2) { tis_destroy(c); return TIS_E_ARG; }
         fene_idx.push_back(i1); fene_idx.push_back(i2);
         fene_nat.push_back(t.fene_nat[r]); fene_coef.push_back(t.coef_fene[r]); fene_d2.push_back(t.dist2_fene[r]);
-        per[i1].push_back(2 * (d.fe0 + r)); per[i2].push_back(2 * (d.fe0 + r));
+        const int cl = cls_of(fene_cmap, fene_cls, t.fene_nat[r], t.coef_fene[r], t.dist2_fene[r]);
+        per[i1].push_back(make_int2(i2, 2 * cl)); per[i2].push_back(make_int2(i1, 2 * cl));
       }
       for (int r = 0; r < t.nwca; ++r) {
         const int i1 = t.iwca2mp[2 * r] - 1, i2 = t.iwca2mp[2 * r + 1] - 1;
@@ -333,12 +355,13 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
         wca_idx.push_back(i1); wca_idx.push_back(i2);
         wca_nat.push_back(t.wca_nat[r]);
         wca_coef.push_back(t.coef_wca[r]); wca_coef.push_back(t.coef_wca[t.nwca + r]);
-        per[i1].push_back(2 * (d.wc0 + r) + 1); per[i2].push_back(2 * (d.wc0 + r) + 1);
+        const int cl = cls_of(wca_cmap, wca_cls, t.wca_nat[r], t.coef_wca[r], t.coef_wca[t.nwca + r]);
+        per[i1].push_back(make_int2(i2, 2 * cl + 1)); per[i2].push_back(make_int2(i1, 2 * cl + 1));
       }
       int off = 0;
       for (int i = 0; i < t.nmp; ++i) {
         bdp.push_back(off);
-        for (int e : per[i]) bde.push_back(e);
+        for (const int2 &e : per[i]) bde.push_back(e);
         off += (int)per[i].size();
       }
       bdp.push_back(off);
@@ -487,7 +510,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
-  long long bd_off = 0, bdp_off = 0;
+  long long bd_off = 0, bdp_off = 0, bd32_off = 0;
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
@@ -530,8 +553,12 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       ew_off += d.nq;
       L.bd0 = bd_off;
       L.bdp0 = bdp_off;
+      L.bd32 = bd32_off;
       if (c->bdhi) bd_off += 9LL * N * N;
-      if (c->bdhi && p.precision == TIS_PREC_MIXED) bdp_off += bd_plane_floats(N);
+      if (c->bdhi && p.precision == TIS_PREC_MIXED) {
+        bdp_off += bd_plane_floats(N);
+        bd32_off += 3LL * N * ((3LL * N + 3) / 4 * 4);
+      }
       state_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
       if (periodic) mirror_off += (long long)N * N;
@@ -635,7 +662,27 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     CK(c->fene_d2.upload(fene_d2));
     CK(c->wca_idx.upload(wca_idx)); CK(c->wca_nat.upload(wca_nat)); CK(c->wca_coef.upload(wca_coef));
     CK(c->bd_ptr.upload(bdp)); CK(c->bd_ent.upload(bde));
-    CK(c->bd_D.alloc((size_t)bd_off)); CK(c->bd_L.alloc((size_t)bd_off));
+    if (fene_cls.empty()) fene_cls.assign(3, 0.0);
+    if (wca_cls.empty()) wca_cls.assign(3, 0.0);
+    CK(c->fene_cls.upload(fene_cls)); CK(c->wca_cls.upload(wca_cls));
+    if (p.precision == TIS_PREC_MIXED) {
+      std::vector<int> lane_T, items;
+      for (int l = 0; l < nlane; ++l) lane_T.push_back((3 * c->lane_nmp[l] + 63) / 64);
+      if (*std::max_element(lane_T.begin(), lane_T.end()) > 500 || nlane > 32767) {
+        tis_destroy(c);
+        return TIS_E_UNSUPPORTED;   // work items pack the row block in 8 bits, the lane in 15
+      }
+      bd_update_items(lane_T, items, c->bd_koff);
+      if (items.empty()) items.push_back(0);
+      CK(c->bd_items.upload(items));
+      CK(c->bd_D32.alloc((size_t)bd32_off)); CK(c->bd_L32.alloc((size_t)bd32_off));
+      // padding columns and the factor's upper part are never written
+      CK(cudaMemset(c->bd_D32.p, 0, (size_t)bd32_off * sizeof(float)));
+      CK(cudaMemset(c->bd_L32.p, 0, (size_t)bd32_off * sizeof(float)));
+    } else {
+      CK(c->bd_D.alloc((size_t)bd_off));
+    }
+    CK(c->bd_L.alloc((size_t)bd_off));
     CK(c->bd_W.alloc((size_t)nlane * 64 * 64));
     if (bdp_off) {
       CK(c->bd_P.alloc((size_t)bdp_off));
@@ -692,9 +739,9 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
   c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
-  c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->d_not_spd.free();
+  c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
-  c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
+  c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_items.free(); c->bd_D32.free(); c->bd_L32.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tev0) cudaEventDestroy(c->tev0);
@@ -800,8 +847,8 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.fene_idx = c->fene_idx.p; a.fene_nat = c->fene_nat.p; a.fene_coef = c->fene_coef.p; a.fene_d2 = c->fene_d2.p;
   a.wca_idx = c->wca_idx.p; a.wca_nat = c->wca_nat.p; a.wca_coef = c->wca_coef.p;
   a.wca_rcut2 = 1.0 / (p.wca_coef_cutoff * p.wca_coef_cutoff);
-  a.bd_ptr = c->bd_ptr.p; a.bd_ent = c->bd_ent.p;
-  a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_P = c->bd_P.p; a.bd_W = c->bd_W.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
+  a.bd_ptr = c->bd_ptr.p; a.bd_ent = c->bd_ent.p; a.fene_cls = c->fene_cls.p; a.wca_cls = c->wca_cls.p;
+  a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_P = c->bd_P.p; a.bd_D32 = c->bd_D32.p; a.bd_L32 = c->bd_L32.p; a.bd_W = c->bd_W.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
   a.not_spd = c->d_not_spd.p;
   a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
   a.boltz = BOLTZ_KCAL_MOL; a.pi = F_PI;
@@ -1108,8 +1155,8 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
       b.bd_istep = istep;
       b.noise_base = c->noise_base + (int)k;
       if ((istep - 1) % every == 0) {
-        c->launches += bd_refactor_launches(c->max_nmp);
-        CK(bd_refactor_launch(c->stream, b, c->max_nmp));
+        c->launches += bd_refactor_launches(c->max_nmp, b.bd_tc != 0);
+        CK(bd_refactor_launch(c->stream, b, c->max_nmp, c->bd_items.p, c->bd_koff.data()));
       }
       c->launches += 3;
       CK(bd_step_launch(c->stream, b, c->max_nmp));
@@ -1276,14 +1323,26 @@ extern "C" int tis_get_hydro_tensors(tis_ctx *c, int32_t irep, double *diffuse, 
   const LaneDesc &L = c->lanes[irep - 1];
   const size_t n = 3 * (size_t)c->lane_nmp[irep - 1];
   std::vector<double> buf(n * n);
-  // device storage is row-major; the reference arrays are column-major
+  std::vector<float> fbuf;
+  // device storage is row-major; the reference arrays are column-major.
+  // Mixed precision keeps D in FP32 only (rows padded to a multiple of 4);
+  // the factor's upper part is never stored on the device (the reference's
+  // random_tensor holds zeros there).
   for (int which = 0; which < 2; ++which) {
     double *out = which == 0 ? diffuse : random;
     if (!out) continue;
-    CK(cudaMemcpy(buf.data(), (which == 0 ? c->bd_D.p : c->bd_L.p) + L.bd0, n * n * sizeof(double),
-                  cudaMemcpyDeviceToHost));
+    if (which == 0 && c->bd_D32.p) {
+      const size_t ld = (n + 3) / 4 * 4;
+      fbuf.resize(n * ld);
+      CK(cudaMemcpy(fbuf.data(), c->bd_D32.p + L.bd32, n * ld * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t r = 0; r < n; ++r)
+        for (size_t col = 0; col < n; ++col) buf[r * n + col] = fbuf[r * ld + col];
+    } else {
+      CK(cudaMemcpy(buf.data(), (which == 0 ? c->bd_D.p : c->bd_L.p) + L.bd0, n * n * sizeof(double),
+                    cudaMemcpyDeviceToHost));
+    }
     for (size_t r = 0; r < n; ++r)
-      for (size_t col = 0; col < n; ++col) out[col * n + r] = buf[r * n + col];
+      for (size_t col = 0; col < n; ++col) out[col * n + r] = (which == 1 && col > r) ? 0.0 : buf[r * n + col];
   }
   return TIS_OK;
 }

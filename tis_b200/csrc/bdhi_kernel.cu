@@ -24,6 +24,9 @@
 // NaN spreads, and the host reports TIS_E_NOT_SPD.
 #include "device_common.cuh"
 
+#include <algorithm>
+#include <vector>
+
 namespace tis {
 
 constexpr int CT = 64;          // Cholesky tile
@@ -63,12 +66,15 @@ __global__ void __launch_bounds__(256) rpy_kernel(KArgs a) {
     for (int p = 0; p < 3; ++p)
       for (int q = 0; q < 3; ++q) blk[p][q] = (p == q ? pre1 : 0.0) + pre2 * r[p] * r[q];
   }
-  double *D = a.bd_D + L.bd0, *Lm = a.bd_L + L.bd0;
+  // D in FP64 (or FP32, rows padded to 4, for the mixed-precision step),
+  // the lower part of L (its upper part is never read)
+  double *Lm = a.bd_L + L.bd0;
   for (int p = 0; p < 3; ++p) {
     const size_t row = (size_t)(3 * i + p) * n + 3 * j;
     for (int q = 0; q < 3; ++q) {
-      D[row + q] = blk[p][q];
-      Lm[row + q] = (3 * j + q <= 3 * i + p) ? blk[p][q] : 0.0;
+      if (a.bd_tc) a.bd_D32[L.bd32 + (size_t)(3 * i + p) * ((n + 3) & ~3) + 3 * j + q] = (float)blk[p][q];
+      else a.bd_D[L.bd0 + row + q] = blk[p][q];
+      if (3 * j + q <= 3 * i + p) Lm[row + q] = blk[p][q];
     }
   }
 }
@@ -87,7 +93,8 @@ __device__ __forceinline__ void tf32_split(double x, float &hi, float &lo) {
   lo = xf - hi;
 }
 
-// Panel operand planes for the tensor cores: per lane, (T + 1) tiles of
+// Panel operand planes for the tensor cores: per lane and panel parity
+// (two slots: the wide update reads panels k and k + 1), (T + 1) tiles of
 // 64 rows x 64 panel columns of TF32 hi parts, then as many of lo parts
 // (tile T stays zero: the partner of an odd last row tile).  Inside a tile
 // the layout is the K-major, no-swizzle canonical UMMA layout with 8-row
@@ -115,6 +122,7 @@ constexpr int U64_SMEM = (CT * CTP + CT * CT) * (int)sizeof(double);
 template <typename Sync>
 __device__ void factor_diag_tile(const KArgs &a, int lane, double *Lm, int n, int td, double *S, double *vec,
                                  int tid, Sync sync) {
+  const long long L32 = a.lanes[lane].bd32;
   const int r0 = td * CT, nb = min(CT, n - r0);
   const int tx = tid & 15, ty = tid >> 4;
   double *col = vec, *erow = vec + 2 * CT, *piv = vec + 4 * CT;
@@ -199,8 +207,11 @@ __device__ void factor_diag_tile(const KArgs &a, int lane, double *Lm, int n, in
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int i = ty + 16 * u, c = tx + 16 * v;
-      if (i < nb && c < nb)
-        Lm[(size_t)(r0 + i) * n + r0 + c] = (c < i) ? av[u][v] / piv[c] : (c == i ? piv[c] : 0.0);
+      if (i < nb && c < nb) {
+        const double l = (c < i) ? av[u][v] / piv[c] : (c == i ? piv[c] : 0.0);
+        Lm[(size_t)(r0 + i) * n + r0 + c] = l;
+        if (a.bd_tc) a.bd_L32[L32 + (size_t)(r0 + i) * ((n + 3) & ~3) + r0 + c] = (float)l;
+      }
     }
   if (tid == 0 && bad) atomicOr(&a.not_spd[lane], 1);
   if (r0 + CT < n) {   // a panel of rows below follows (then nb = CT)
@@ -287,10 +298,14 @@ __global__ void __launch_bounds__(256) chol_panel_kernel(KArgs a) {
 #pragma unroll 4
   for (int e = tid; e < CT * CT; e += 256) {
     const int r = e >> 6, c = e & 63;
-    if (r < mi) Lm[(size_t)(i0 + r) * n + r0 + c] = As[r * CTP + c];
+    if (r < mi) {
+      Lm[(size_t)(i0 + r) * n + r0 + c] = As[r * CTP + c];
+      if (a.bd_tc) a.bd_L32[L.bd32 + (size_t)(i0 + r) * ((n + 3) & ~3) + r0 + c] = (float)As[r * CTP + c];
+    }
   }
   if (a.bd_tc) {
-    float *ph = a.bd_P + L.bdp0 + (size_t)ti * PT, *pl = ph + (size_t)(T + 1) * PT;
+    float *ph = a.bd_P + L.bdp0 + (size_t)(k & 1) * 2 * (T + 1) * PT + (size_t)ti * PT;
+    float *pl = ph + (size_t)(T + 1) * PT;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int e = tid + 256 * q, r = e & 63, g = e >> 6;
@@ -370,28 +385,36 @@ __global__ void __launch_bounds__(256) chol_update_kernel(KArgs a) {
 }
 
 // ------------------------------------------------------------ tensor cores
-// Trailing update on the 5th-generation tensor cores (mixed precision):
-// A_ij -= L_ik L_jk^T with L_ik = hi + lo split into TF32 parts (the panel
-// planes written by chol_factor_kernel), the product taken as
+// Trailing updates on the 5th-generation tensor cores (mixed precision),
+// two panels at a time.  For the panel pair (k, k + 1):
+//   narrow: A_i,k+1 -= L_ik L_k+1,k^T for the column tile k + 1 (K = 64);
+//   wide:   A_ij -= L_ik L_jk^T + L_i,k+1 L_j,k+1^T for j >= k + 2 (K = 128),
+// so the FP64 trailing matrix is read and written once per two panels.
+// L_ik = hi + lo is split into TF32 parts (the panel planes written by
+// chol_panel_kernel, one slot per panel parity), the product taken as
 // hi.hi + hi.lo + lo.hi (lo.lo is below FP32 rounding) and accumulated in
 // FP32 in tensor memory; the FP64 tile subtracts it.  Diagonal tiles and
 // panel solves stay in FP64.
 //
-// A CTA owns a 128-row block (row tiles ti, ti + 1 of panel k) and up to UG
-// column tiles tj of it, and runs them as a pipeline of warp roles:
-//   warp 0, one thread: bulk copies of the A block (once) and of each B tile
+// A CTA owns a 128-row block (row tiles ti, ti + 1) and up to UG column
+// tiles of it, with one 64-column TMEM accumulator per column tile, and
+// runs them as a pipeline of warp roles:
+//   warp 0, one thread: bulk copies of the A block of each panel (the
+//     second after the first panel's products are done) and of each B tile
 //     (two shared-memory stages) from the panel planes;
 //   warp 1, one thread: 24 tcgen05.mma (M 128, N 64, K 8) per column tile
-//     into one of two 64-column TMEM accumulators;
-//   warps 2..9: epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows)
-//     and column half (w - 2) / 4, transposes the 32 x 32 block through its
-//     own shared-memory stage and updates the FP64 rows with coalesced
-//     256-byte accesses.
-// Every wait on a barrier is bounded; a wait that gives up flags the lane
-// (not_spd bit 2, reported as a device-wait timeout) after the copies and
-// products in flight are drained.
-constexpr int UG = 8;                                 // column tiles per CTA
-constexpr int U_A = 2 * 2 * CT * CT * 4;              // A hi + lo, 128 rows
+//     and panel;
+//   warps 2..9: epilogue, as soon as a tile's last panel is in: warp w
+//     reads TMEM lanes 32 (w % 4) .. + 31 (rows) and column half (w - 2) / 4,
+//     transposes the 32 x 32 block through its own shared-memory stage and
+//     updates the FP64 rows with coalesced 256-byte accesses.
+// The CTA whose first tile is the diagonal tile of the first updated column
+// factors it afterwards (look-ahead for the next panel).  Every wait on a
+// barrier is bounded; a wait that gives up flags the lane (not_spd bit 2,
+// reported as a device-wait timeout) after the copies and products in
+// flight are drained.
+constexpr int UG = 8;                                 // column tiles per CTA (8 x 64 TMEM columns)
+constexpr int U_A = 2 * 2 * CT * CT * 4;              // A hi + lo, 128 rows, one panel
 constexpr int U_B = 2 * CT * CT * 4;                  // one B stage, hi + lo
 constexpr int U_STG = 32 * 33 * 4;                    // epilogue transpose stage per warp
 constexpr int U_SMEM = U_A + 2 * U_B + 8 * U_STG;
@@ -437,45 +460,48 @@ __device__ __forceinline__ void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-// grid (nlane, ceil(m / 2) * gmax) with m = T - k - 1 and gmax = ceil(m / UG)
-// for the largest lane (lanes fastest: the CTAs that factor the next
-// diagonal tile start first); U_THREADS threads, one CTA per SM
-__global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, int gmax) {
-  const int lane = blockIdx.x;
-  if (lane >= a.nlane) return;
+// panel planes of panel kp of a lane: hi, then lo (T + 1 tiles each)
+__device__ __forceinline__ const float *plane_hi(const KArgs &a, const LaneDesc &L, int T, int kp) {
+  return a.bd_P + L.bdp0 + (size_t)(kp & 1) * 2 * (T + 1) * PT;
+}
+
+// One CTA per work item (lane << 16 | R << 8 | g) of the launch (bd_update_items):
+// narrow (nph = 1): column tile k + 1 only, panel k; wide (nph = 2): column
+// tiles >= k + 2, panels k and k + 1.  U_THREADS threads, one CTA per SM.
+__global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, const int *items, int nph) {
+  const int item = items[blockIdx.x];
+  const int lane = item >> 16, R = (item >> 8) & 255, g = item & 255;
   const LaneDesc L = a.lanes[lane];
   int n;
   const int T = lane_tiles(a, L, n), k = a.bd_kpanel;
-  const int m = T - k - 1;
-  const int R = blockIdx.y / gmax, g = blockIdx.y - R * gmax;
-  if (m <= 0 || 2 * R >= m) return;   // uniform over the CTA
-  const int ncol = min(2 * R + 2, m), c0 = g * UG;
+  const int cf = k + nph;   // first updated row and column tile
+  const int m = T - cf;
+  if (m <= 0 || 2 * R >= m) return;   // not produced by the item tables; uniform over the CTA
+  const int ncol = nph == 1 ? 1 : min(2 * R + 2, m), c0 = g * UG;
   if (c0 >= ncol) return;
   const int nt = min(UG, ncol - c0);
-  const int ti0 = k + 1 + 2 * R, tj0 = k + 1 + c0;
+  const int ti0 = cf + 2 * R, tj0 = cf + c0;
   double *Lm = a.bd_L + L.bd0;
-  const float *ph = a.bd_P + L.bdp0, *pl = ph + (size_t)(T + 1) * PT;
 
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char *base = (unsigned char *)(((uintptr_t)tsm + 1023) & ~(uintptr_t)1023);
   const uint32_t s_ahi = smem_u32(base), s_alo = s_ahi + U_A / 2;
   const uint32_t s_b0 = s_ahi + U_A;   // stage s: hi at s_b0 + s U_B, lo 16 KB later
-  __shared__ __align__(8) uint64_t bars[10];   // fullA, fullB0/1, emptyB0/1, tfull0/1, tempty0/1, mdone
+  // fullA, fullB0/1, emptyB0/1, afree, mdone, tfull0..7
+  __shared__ __align__(8) uint64_t bars[7 + UG];
   __shared__ uint32_t tmem_slot;
   __shared__ int gaveup;
   const uint32_t b_fullA = smem_u32(&bars[0]), b_fullB = smem_u32(&bars[1]), b_emptyB = smem_u32(&bars[3]);
-  const uint32_t b_tfull = smem_u32(&bars[5]), b_tempty = smem_u32(&bars[7]), b_mdone = smem_u32(&bars[9]);
+  const uint32_t b_afree = smem_u32(&bars[5]), b_mdone = smem_u32(&bars[6]), b_tfull = smem_u32(&bars[7]);
   const int tid = threadIdx.x, warp = tid >> 5, lid = tid & 31;
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(2 * CT));
+                 "r"(UG * CT));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    for (int q = 0; q < 10; ++q) {
-      const uint32_t cnt = (q == 7 || q == 8) ? 8u : 1u;   // tempty: one arrival per epilogue warp
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[q])), "r"(cnt));
-    }
+    for (int q = 0; q < 7 + UG; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[q])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     gaveup = 0;
   }
@@ -488,20 +514,27 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
     if (lid == 0) {
       bool ok = true;
       int last[2] = {-1, -1};
-      mbar_expect(b_fullA, U_A);
-      bulk_load(s_ahi, ph + (size_t)ti0 * PT, U_A / 2, b_fullA);
-      bulk_load(s_alo, pl + (size_t)ti0 * PT, U_A / 2, b_fullA);
-      for (int t = 0; t < nt; ++t) {
-        const int s = t & 1;
-        if (t >= 2 && !mbar_wait(b_emptyB + 8 * s, ((t >> 1) - 1) & 1)) { ok = false; break; }
-        const uint32_t dst = s_b0 + (uint32_t)s * U_B;
-        mbar_expect(b_fullB + 8 * s, U_B);
-        bulk_load(dst, ph + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
-        bulk_load(dst + U_B / 2, pl + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
-        last[s] = t;
+      for (int p = 0; p < nph && ok; ++p) {
+        const float *ph = plane_hi(a, L, T, k + p), *pl = ph + (size_t)(T + 1) * PT;
+        // the second panel's A block replaces the first once its products are done
+        if (p == 1 && !mbar_wait(b_afree, 0)) { ok = false; break; }
+        mbar_expect(b_fullA, U_A);
+        bulk_load(s_ahi, ph + (size_t)ti0 * PT, U_A / 2, b_fullA);
+        bulk_load(s_alo, pl + (size_t)ti0 * PT, U_A / 2, b_fullA);
+        for (int t = 0; t < nt; ++t) {
+          const int u = p * nt + t, s = u & 1;
+          if (u >= 2 && !mbar_wait(b_emptyB + 8 * s, ((u >> 1) - 1) & 1)) { ok = false; break; }
+          const uint32_t dst = s_b0 + (uint32_t)s * U_B;
+          mbar_expect(b_fullB + 8 * s, U_B);
+          bulk_load(dst, ph + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
+          bulk_load(dst + U_B / 2, pl + (size_t)(tj0 + t) * PT, U_B / 2, b_fullB + 8 * s);
+          last[s] = u;
+        }
       }
       // drain: no copy may still be writing shared memory when the CTA ends
-      ok = mbar_wait(b_fullA, 0) && ok;
+      // (the last A load has phase parity nph - 1; the MMA thread waited
+      // for the earlier one)
+      ok = mbar_wait(b_fullA, (nph - 1) & 1) && ok;
       for (int s = 0; s < 2; ++s)
         if (last[s] >= 0) ok = mbar_wait(b_fullB + 8 * s, (last[s] >> 1) & 1) && ok;
       if (!ok) gaveup = 1;
@@ -512,28 +545,31 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
       // both K-major, N >> 3 at [17,23), M >> 4 at [24,29)
       const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(CT >> 3) << 17) |
                              ((uint32_t)(2 * CT >> 4) << 24);
-      bool ok = mbar_wait(b_fullA, 0);
-      for (int t = 0; t < nt && ok; ++t) {
-        const int s = t & 1;
-        if (!mbar_wait(b_fullB + 8 * s, (t >> 1) & 1)) { ok = false; break; }
-        if (t >= 2 && !mbar_wait(b_tempty + 8 * s, ((t >> 1) - 1) & 1)) { ok = false; break; }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t bhi = s_b0 + (uint32_t)s * U_B, blo = bhi + U_B / 2;
-        const uint32_t dacc = taddr + (uint32_t)(s * CT);
-        for (int ks = 0; ks < CT / 8; ++ks) {
-          for (int pp = 0; pp < 3; ++pp) {
-            const uint32_t sa = (pp == 2 ? s_alo : s_ahi) + (uint32_t)ks * 256u;
-            const uint32_t sb = (pp == 1 ? blo : bhi) + (uint32_t)ks * 256u;
-            const uint64_t da = umma_desc(sa, 128, 2048), db = umma_desc(sb, 128, 2048);
-            const uint32_t acc = (ks | pp) ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
-                :: "r"(dacc), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      bool ok = true;
+      for (int p = 0; p < nph && ok; ++p) {
+        if (!mbar_wait(b_fullA, p & 1)) { ok = false; break; }
+        for (int t = 0; t < nt; ++t) {
+          const int u = p * nt + t, s = u & 1;
+          if (!mbar_wait(b_fullB + 8 * s, (u >> 1) & 1)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t bhi = s_b0 + (uint32_t)s * U_B, blo = bhi + U_B / 2;
+          const uint32_t dacc = taddr + (uint32_t)(t * CT);
+          for (int ks = 0; ks < CT / 8; ++ks) {
+            for (int pp = 0; pp < 3; ++pp) {
+              const uint32_t sa = (pp == 2 ? s_alo : s_ahi) + (uint32_t)ks * 256u;
+              const uint32_t sb = (pp == 1 ? blo : bhi) + (uint32_t)ks * 256u;
+              const uint64_t da = umma_desc(sa, 128, 2048), db = umma_desc(sb, 128, 2048);
+              const uint32_t acc = (p | ks | pp) ? 1u : 0u;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+                  :: "r"(dacc), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            }
           }
+          umma_commit(b_emptyB + 8 * s);
+          if (p == nph - 1) umma_commit(b_tfull + 8 * t);
         }
-        umma_commit(b_emptyB + 8 * s);
-        umma_commit(b_tfull + 8 * s);
+        if (ok && p == 0 && nph > 1) umma_commit(b_afree);
       }
       // every product issued by this thread has landed before TMEM is freed
       umma_commit(b_mdone);
@@ -545,8 +581,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
     float *stg = (float *)(base + U_A + 2 * U_B + e * U_STG);
     uint32_t eok = 1;
     for (int t = 0; t < nt; ++t) {
-      const int b = t & 1;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(b_tfull + 8 * b, (t >> 1) & 1));
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(b_tfull + 8 * t, 0));
       if (!ok) {
         if (lid == 0) gaveup = 1;
         eok = 0;
@@ -562,11 +597,8 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
             "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
             "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
             "=r"(v[30]), "=r"(v[31])
-          : "r"(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * CT + h * 32)));
+          : "r"(taddr + ((uint32_t)(q * 32) << 16) + (uint32_t)(t * CT + h * 32)));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      __syncwarp();
-      if (lid == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(b_tempty + 8 * b) : "memory");
       // lane = row of the TMEM block: transpose so that a lane owns a column
 #pragma unroll
       for (int c = 0; c < 32; ++c) stg[lid * 33 + c] = __uint_as_float(v[c]);
@@ -586,7 +618,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
       __syncwarp();
     }
     if (R == 0 && g == 0) {
-      // tile (k + 1, k + 1), updated above by this CTA, is final: the eight
+      // tile (cf, cf), updated above by this CTA, is final: the eight
       // epilogue warps factor it for the next panel (the operand area is
       // free: every product has been read out of TMEM)
       const auto esync = [] { asm volatile("bar.sync 1, 256;" ::: "memory"); };
@@ -598,7 +630,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
                    : "memory");
       if (all_ok) {
         double *fs = (double *)base, *fv = fs + CT * CTP;
-        factor_diag_tile(a, lane, Lm, n, k + 1, fs, fv, tid - 64, esync);
+        factor_diag_tile(a, lane, Lm, n, cf, fs, fv, tid - 64, esync);
       }
     }
   }
@@ -606,7 +638,7 @@ __global__ void __launch_bounds__(U_THREADS, 1) chol_update_tc_kernel(KArgs a, i
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(2 * CT));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(UG * CT));
   }
   if (tid == 0 && gaveup) atomicOr(&a.not_spd[lane], 2);   // a tensor-core pipeline wait gave up
 }
@@ -627,7 +659,52 @@ __global__ void __launch_bounds__(128) bd_noise_kernel(KArgs a) {
 }
 
 // grid (ceil(maxN * 3 / 8), nlane), 256 threads: one warp per row k of the
-// lane: dx_k = rlan1 sum_c D_kc F_c + rlan2 sum_{c <= k} L_kc xi_c, x += dx
+// lane: dx_k = rlan1 sum_c D_kc F_c + rlan2 sum_{c <= k} L_kc xi_c, x += dx.
+// HBM-bound: the mixed-precision path streams FP32 copies of D and L
+// (products and sums in FP64), the FP64 path the FP64 matrices.
+__device__ __forceinline__ void row_dots64(const double *Drow, const double *Lrow, const double *F,
+                                           const double *xi, int n, int k, int lid, double &df, double &dr) {
+  df = 0.0;
+  dr = 0.0;
+  int c = lid;
+  for (; c + 96 < n; c += 128)
+    df += Drow[c] * F[c] + Drow[c + 32] * F[c + 32] + Drow[c + 64] * F[c + 64] + Drow[c + 96] * F[c + 96];
+  for (; c < n; c += 32) df += Drow[c] * F[c];
+  c = lid;
+  for (; c + 96 <= k; c += 128)
+    dr += Lrow[c] * xi[c] + Lrow[c + 32] * xi[c + 32] + Lrow[c + 64] * xi[c + 64] + Lrow[c + 96] * xi[c + 96];
+  for (; c <= k; c += 32) dr += Lrow[c] * xi[c];
+}
+
+// FP32 rows padded to a multiple of 4 (16-byte aligned): float4 loads for
+// the whole 4-column groups inside the matrix, then the < 4 last columns
+__device__ __forceinline__ void row_dots32(const float *Drow, const float *Lrow, const double *F, const double *xi,
+                                           int n, int k, int lid, double &df, double &dr) {
+  df = 0.0;
+  dr = 0.0;
+  const float4 *D4 = (const float4 *)Drow, *L4 = (const float4 *)Lrow;
+  const int n4 = n >> 2;
+  // L is zero above the diagonal: whole groups up to column k
+  const int k4 = min((k >> 2) + 1, n4);
+  auto dot4 = [](const float4 &m, const double *v) {
+    return (double)m.x * v[0] + (double)m.y * v[1] + (double)m.z * v[2] + (double)m.w * v[3];
+  };
+  int g = lid;
+  for (; g + 96 < n4; g += 128) {   // four loads in flight per lane
+    const float4 d0 = D4[g], d1 = D4[g + 32], d2 = D4[g + 64], d3 = D4[g + 96];
+    df += dot4(d0, F + 4 * g) + dot4(d1, F + 4 * g + 128) + dot4(d2, F + 4 * g + 256) + dot4(d3, F + 4 * g + 384);
+  }
+  for (; g < n4; g += 32) df += dot4(D4[g], F + 4 * g);
+  if (lid < n - 4 * n4) df += (double)Drow[4 * n4 + lid] * F[4 * n4 + lid];
+  g = lid;
+  for (; g + 96 < k4; g += 128) {
+    const float4 l0 = L4[g], l1 = L4[g + 32], l2 = L4[g + 64], l3 = L4[g + 96];
+    dr += dot4(l0, xi + 4 * g) + dot4(l1, xi + 4 * g + 128) + dot4(l2, xi + 4 * g + 256) + dot4(l3, xi + 4 * g + 384);
+  }
+  for (; g < k4; g += 32) dr += dot4(L4[g], xi + 4 * g);
+  if (4 * k4 + lid <= k) dr += (double)Lrow[4 * k4 + lid] * xi[4 * k4 + lid];
+}
+
 __global__ void __launch_bounds__(256) bd_update_kernel(KArgs a) {
   const int lane = blockIdx.y;
   if (lane >= a.nlane) return;
@@ -637,12 +714,15 @@ __global__ void __launch_bounds__(256) bd_update_kernel(KArgs a) {
   const int k = blockIdx.x * 8 + warp;
   if (blockIdx.x == 0 && threadIdx.x == 0) a.lstate[lane].istep = a.bd_istep;
   if (k >= n) return;
-  const double *Drow = a.bd_D + L.bd0 + (size_t)k * n;
-  const double *Lrow = a.bd_L + L.bd0 + (size_t)k * n;
   const double *F = a.bd_F + 3 * (size_t)L.state0, *xi = a.bd_xi + 3 * (size_t)L.state0;
-  double df = 0.0, dr = 0.0;
-  for (int c = lid; c < n; c += 32) df += Drow[c] * F[c];
-  for (int c = lid; c <= k; c += 32) dr += Lrow[c] * xi[c];
+  double df, dr;
+  if (a.bd_tc) {
+    const size_t row = L.bd32 + (size_t)k * ((n + 3) & ~3);
+    row_dots32(a.bd_D32 + row, a.bd_L32 + row, F, xi, n, k, lid, df, dr);
+  } else {
+    const size_t row = L.bd0 + (size_t)k * n;
+    row_dots64(a.bd_D + row, a.bd_L + row, F, xi, n, k, lid, df, dr);
+  }
   for (int o = 16; o > 0; o >>= 1) {
     df += __shfl_xor_sync(0xffffffffu, df, o);
     dr += __shfl_xor_sync(0xffffffffu, dr, o);
@@ -670,31 +750,33 @@ __global__ void __launch_bounds__(256) bd_force_kernel(KArgs a) {
   if (i >= T.nmp) return;
   const double *x = a.xyz + 3 * (size_t)L.state0;
   const int p0 = a.bd_ptr[T.bp0 + i], p1 = a.bd_ptr[T.bp0 + i + 1];
+  const double xi0 = x[3 * i], xi1 = x[3 * i + 1], xi2 = x[3 * i + 2];
   double fx = 0.0, fy = 0.0, fz = 0.0;
   int nclamp = 0;
+  // entry (j, class * 2 + kind): the record's force on i is f (x_i - x_j),
+  // the same numbers as -/+ f (x_i2 - x_i1) in the record's own orientation
   for (int p = p0 + lid; p < p1; p += 32) {
-    const int ent = a.bd_ent[T.be0 + p];
-    const int rec = ent >> 1;
-    const int *idx = (ent & 1) ? a.wca_idx + 2 * (size_t)rec : a.fene_idx + 2 * (size_t)rec;
-    const int i1 = idx[0], i2 = idx[1];
-    const double v0 = x[3 * i2] - x[3 * i1], v1 = x[3 * i2 + 1] - x[3 * i1 + 1], v2 = x[3 * i2 + 2] - x[3 * i1 + 2];
-    double f;   // force on i2 is f * v21, on i1 -f * v21
-    if (!(ent & 1)) {
+    const int2 ent = a.bd_ent[T.be0 + p];
+    const int j = ent.x, cl = ent.y >> 1;
+    const double v0 = xi0 - x[3 * j], v1 = xi1 - x[3 * j + 1], v2 = xi2 - x[3 * j + 2];
+    double f;
+    if (!(ent.y & 1)) {
+      const double *pc = a.fene_cls + 3 * (size_t)cl;   // nat, coef, dist2
       const double dist = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-      const double dd = dist - a.fene_nat[rec];
-      f = -a.fene_coef[rec] * dd / (1.0 - dd * dd / a.fene_d2[rec]) / dist;
+      const double dd = dist - pc[0];
+      f = -pc[1] * dd / (1.0 - dd * dd / pc[2]) / dist;
     } else {
+      const double *pc = a.wca_cls + 3 * (size_t)cl;    // nat, coef rep, coef att
       const double dist2 = v0 * v0 + v1 * v1 + v2 * v2;
-      const double nat2 = a.wca_nat[rec] * a.wca_nat[rec];
+      const double nat2 = pc[0] * pc[0];
       const double ro2 = nat2 / dist2;
       if (ro2 < a.wca_rcut2) continue;
       const double ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro8 * ro4 * ro2;
-      const double coef = (ro2 > 1.0) ? a.wca_coef[2 * (size_t)rec] : a.wca_coef[2 * (size_t)rec + 1];
+      const double coef = (ro2 > 1.0) ? pc[1] : pc[2];
       f = 12.0 * coef / nat2 * (ro14 - ro8);
       if (f > 50.0) { f = 50.0; ++nclamp; }   // DE_MAX
     }
-    const double s = (i == i2) ? f : -f;
-    fx += s * v0; fy += s * v1; fz += s * v2;
+    fx += f * v0; fy += f * v1; fz += f * v2;
   }
   for (int o = 16; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
@@ -710,7 +792,40 @@ __global__ void __launch_bounds__(256) bd_force_kernel(KArgs a) {
 }
 
 // ------------------------------------------------------------ launches
-cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
+// Work items of the tensor-core updates (lane << 16 | R << 8 | g): for the
+// panel pair starting at k (k even) the narrow launch's items are
+// items[koff[k] .. koff[k + 1]) and the wide launch's items[koff[k + 1] ..
+// koff[k + 2]).  Items that factor the next diagonal tile come first, the
+// rest by decreasing tile count.  lane_T = tiles per lane.
+void bd_update_items(const std::vector<int> &lane_T, std::vector<int> &items, std::vector<int> &koff) {
+  int tmax = 0;
+  for (int t : lane_T) tmax = std::max(tmax, t);
+  items.clear();
+  koff.assign(1, 0);
+  for (int k = 0; k < tmax + 1; ++k) {
+    const int nph = (k & 1) ? 2 : 1;   // odd entries: the wide launch of the pair starting at k - 1
+    const int kp = k & ~1;
+    std::vector<std::pair<int, int>> ks;   // (order key, item)
+    for (size_t l = 0; l < lane_T.size(); ++l) {
+      const int m = lane_T[l] - kp - nph;
+      for (int R = 0; 2 * R < m; ++R) {
+        const int ncol = nph == 1 ? 1 : std::min(2 * R + 2, m);
+        for (int g = 0; g * UG < ncol; ++g) {
+          const int nt = std::min(UG, ncol - g * UG);
+          const int first = (R == 0 && g == 0) ? 1 << 20 : 0;   // factors the next diagonal tile
+          ks.push_back({first + nt, (int)(l << 16) | (R << 8) | g});
+        }
+      }
+    }
+    std::stable_sort(ks.begin(), ks.end(), [](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+      return x.first > y.first;
+    });
+    for (auto &e : ks) items.push_back(e.second);
+    koff.push_back((int)items.size());
+  }
+}
+
+cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int *items, const int *koff) {
   cudaError_t e = cudaFuncSetAttribute(chol_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        U64_SMEM);
   if (e != cudaSuccess) return e;
@@ -718,34 +833,49 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp) {
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(chol_update_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, U_SMEM + 1024);
   if (e != cudaSuccess) return e;
-  if (a.bd_tc && !a.bd_P) return cudaErrorInvalidValue;
+  if (a.bd_tc && (!a.bd_P || !items || !koff)) return cudaErrorInvalidValue;
   const long long nn = (long long)max_nmp * max_nmp;
   rpy_kernel<<<dim3((unsigned)((nn + 255) / 256), a.nlane), 256, 0, st>>>(a);
   chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
   const int T = (3 * max_nmp + CT - 1) / CT;
-  for (int k = 0; k + 1 < T; ++k) {
-    a.bd_kpanel = k;
-    const int m = T - k - 1;
-    chol_panel_kernel<<<dim3(m, a.nlane), 256, U64_SMEM, st>>>(a);
-    if (a.bd_tc) {
-      const int gmax = (m + UG - 1) / UG;
-      chol_update_tc_kernel<<<dim3(a.nlane, ((m + 1) / 2) * gmax), U_THREADS, U_SMEM + 1024, st>>>(a, gmax);
-    } else {
+  if (a.bd_tc) {
+    // panel pairs: panel k, narrow update (column k + 1), panel k + 1, wide update
+    for (int k = 0; k + 1 < T; k += 2) {
+      a.bd_kpanel = k;
+      chol_panel_kernel<<<dim3(T - k - 1, a.nlane), 256, U64_SMEM, st>>>(a);
+      int nit = koff[k + 1] - koff[k];
+      if (nit > 0) chol_update_tc_kernel<<<nit, U_THREADS, U_SMEM + 1024, st>>>(a, items + koff[k], 1);
+      if (k + 2 < T) {
+        KArgs b = a;
+        b.bd_kpanel = k + 1;
+        chol_panel_kernel<<<dim3(T - k - 2, a.nlane), 256, U64_SMEM, st>>>(b);
+        nit = koff[k + 2] - koff[k + 1];
+        if (nit > 0) chol_update_tc_kernel<<<nit, U_THREADS, U_SMEM + 1024, st>>>(a, items + koff[k + 1], 2);
+      }
+    }
+  } else {
+    for (int k = 0; k + 1 < T; ++k) {
+      a.bd_kpanel = k;
+      const int m = T - k - 1;
+      chol_panel_kernel<<<dim3(m, a.nlane), 256, U64_SMEM, st>>>(a);
       chol_update_kernel<<<dim3(a.nlane, m * (m + 1) / 2), 256, U64_SMEM, st>>>(a);
     }
   }
   return cudaGetLastError();
 }
 
-int bd_refactor_launches(int max_nmp) {
+int bd_refactor_launches(int max_nmp, bool tc) {
   const int T = (3 * max_nmp + CT - 1) / CT;
-  return 2 + 2 * (T - 1);
+  if (!tc) return 2 + 2 * (T - 1);
+  int nl = 2;
+  for (int k = 0; k + 1 < T; k += 2) nl += (k + 2 < T) ? 4 : 2;
+  return nl;
 }
 
 // floats of the panel planes of a lane with N beads (tensor-core update)
 long long bd_plane_floats(int nmp) {
   const int T = (3 * nmp + CT - 1) / CT;
-  return 2LL * (T + 1) * PT;
+  return 2LL * 2 * (T + 1) * PT;   // two panel slots of hi + lo planes
 }
 
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp) {

@@ -56,6 +56,7 @@ struct LaneDesc {
   int ew0;          // Ewald: first charge of this lane in the per-lane charge tables
   long long bd0;    // Brownian-HI: first element of this lane's (3N)^2 diffusion / Cholesky matrices
   long long bdp0;   // Brownian-HI, tensor cores: first float of this lane's TF32 panel planes
+  long long bd32;   // Brownian-HI, mixed precision: first float of this lane's FP32 D and L (rows padded to 4)
 };
 
 // Mutable per-lane scalar state, kept in global memory between launches.
@@ -115,8 +116,10 @@ struct KArgs {
   const int *wca_idx; const double *wca_nat, *wca_coef;                 // force_wca.F90 (coef: rep, att)
   double wca_rcut2;                // 1 / cutoff_wca^2
   const int *bd_ptr;               // per bead: range of its records in bd_ent
-  const int *bd_ent;               // record id * 2 + kind (0 FENE, 1 WCA)
-  double *bd_D, *bd_L;             // per lane (3N x 3N, row-major): diffusion tensor, its Cholesky factor
+  const int2 *bd_ent;              // (partner bead, parameter class * 2 + kind (0 FENE, 1 WCA))
+  const double *fene_cls, *wca_cls;// parameter classes: FENE (nat, coef, dist2), WCA (nat, coef rep, coef att)
+  double *bd_D, *bd_L;             // per lane (3N x 3N, row-major): diffusion tensor (FP64 path), Cholesky factor
+  float *bd_D32, *bd_L32;          // mixed precision: FP32 D and lower factor read by the step's matrix-vector products
   double *bd_F, *bd_xi;            // per lane (3N): force, Gaussian noise of the step
   float *bd_P;                     // per lane: TF32 hi / lo planes of the current Cholesky panel
   double *bd_W;                    // per lane: 64 x 64 transposed inverse of the current diagonal tile
