@@ -105,126 +105,165 @@ constexpr int PT = CT * CT;   // floats per plane tile
 constexpr int U64_SMEM = (CT * CTP + CT * CT) * (int)sizeof(double);
 
 // Factor diagonal tile td of a lane and invert its factor with the 256
-// threads of the calling group (tid 0..255; sync() is the group's barrier),
-// in registers: thread (ty, tx) = (tid / 16, tid % 16) owns rows ty + 16 u
-// and columns tx + 16 v of the tile A (identity beyond the matrix) and of E,
-// which starts as the identity.  Gaussian elimination of [A | E] without
-// pivoting, one barrier per column j: with p_j = A_jj and m_ij = A_ij / p_j,
-//   A_ic -= m_ij A_cj (j < c <= i, the lower part by symmetry),
-//   E_ic -= m_ij E_jc (c <= j),
-// the owners of column j + 1 of A and of row j + 1 of E publish them in
-// double-buffered shared vectors.  Then A = Lt P Lt^T with Lt unit lower,
-// E = Lt^-1, so L = Lt P^1/2 (L_ic = A_ic / sqrt(p_c), L_ii = sqrt(p_i)) and
-// L^-1 = P^-1/2 E.  A pivot <= 0 is replaced by 1 (no NaN spreads) and
-// flags the lane.  Stores L_tt (zero above the diagonal) and, when a panel
-// follows, U_tt = L_tt^-T into the lane's inverse slot, through the shared
-// stage S (CT x CTP doubles); vec holds 4 CT + CT doubles.
+// threads of the calling group (tid 0..255, 8 warps; sync() is the group's
+// barrier).  The tile A (identity beyond the matrix) sits in shared memory S
+// (row stride CTP).  Blocked right-looking Cholesky in the unscaled form
+// A_ic -= A_ij A_cj / p_j (p_j the pivot, L_ij = A_ij / sqrt(p_j)), 16
+// columns per block:
+//   warp 0 factors the block's columns for all rows below in registers (lane
+//     l holds rows 16 b + l and 16 b + l + 32), column values passed by warp
+//     shuffles, one pivot after the other;
+//   all warps apply the block's rank-16 update to the trailing lower part.
+// Then W = L^-1 by forward substitution L W = I, four threads per column of
+// W (rows t, t + 4, ...), the solved element passed by shuffles.
+// A pivot <= 0 is replaced by 1 (no NaN spreads) and flags the lane.  Stores
+// L_tt (zero above the diagonal; FP32 copy for mixed precision) and, when a
+// panel follows, U_tt = L_tt^-T into the lane's inverse slot.  vec holds
+// 4 CT doubles.
 template <typename Sync>
 __device__ void factor_diag_tile(const KArgs &a, int lane, double *Lm, int n, int td, double *S, double *vec,
                                  int tid, Sync sync) {
   const long long L32 = a.lanes[lane].bd32;
   const int r0 = td * CT, nb = min(CT, n - r0);
-  const int tx = tid & 15, ty = tid >> 4;
-  double *col = vec, *erow = vec + 2 * CT, *piv = vec + 4 * CT;
-  double av[4][4], ev[4][4];
+  const int warp = tid >> 5, ln = tid & 31;
+  double *A = S, *piv = vec, *ipv = vec + CT, *rinv = vec + 2 * CT;
   sync();   // the group's stores to the tile are visible; earlier users of S and vec are done
+  {
+    double v[CT * CT / 256];   // all loads in flight before the shared-memory stores
 #pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = ty + 16 * u, c = tx + 16 * v;
-      av[u][v] = (i < nb && c < nb) ? Lm[(size_t)(r0 + i) * n + r0 + c] : (i == c ? 1.0 : 0.0);
-      ev[u][v] = (i == c) ? 1.0 : 0.0;
+    for (int q = 0; q < CT * CT / 256; ++q) {
+      const int e = tid + 256 * q, i = e >> 6, c = e & 63;
+      v[q] = (i < nb && c < nb) ? Lm[(size_t)(r0 + i) * n + r0 + c] : (i == c ? 1.0 : 0.0);
     }
-  if (tx == 0) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) col[ty + 16 * u] = av[u][0];
+    for (int q = 0; q < CT * CT / 256; ++q) {
+      const int e = tid + 256 * q;
+      A[(e >> 6) * CTP + (e & 63)] = v[q];
+    }
   }
-  if (ty == 0) {
-#pragma unroll
-    for (int v = 0; v < 4; ++v) erow[tx + 16 * v] = ev[0][v];
-  }
-  int bad = 0;
-  for (int j = 0; j < nb; ++j) {
+  int bad = 0;   // warp 0
+  for (int b = 0; b < CT / 16; ++b) {
+    const int c0 = 16 * b;
     sync();
-    const int q = (j & 1) * CT;
-    double p = col[q + j];
-    if (!(p > 0.0)) {
-      p = 1.0;
-      bad = 1;
-    }
-    if (tid == 0) piv[j] = p;
-    const double ip = 1.0 / p;
-    double ac[4], er[4];
+    if (warp == 0) {
+      const int ra = c0 + ln, rb = c0 + ln + 32;
+      double pa[16], pb[16];
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      ac[v] = col[q + tx + 16 * v];
-      er[v] = erow[q + tx + 16 * v];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = ty + 16 * u;
-      if (i <= j) continue;
-      const double mlt = col[q + i] * ip;
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int c = tx + 16 * v;
-        if (c > j && c <= i) av[u][v] -= mlt * ac[v];
-        if (c <= j) ev[u][v] -= mlt * er[v];
+      for (int cc = 0; cc < 16; ++cc) {
+        pa[cc] = (ra < CT) ? A[ra * CTP + c0 + cc] : 0.0;
+        pb[cc] = (rb < CT) ? A[rb * CTP + c0 + cc] : 0.0;
       }
-    }
-    const int jn = j + 1, qn = CT - q;
-    if (jn < nb) {
-      // register selects (an indexed read would put the arrays in local memory)
-      const int sel = jn >> 4;
-      if (tx == (jn & 15)) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          double x = av[u][0];
-          x = sel == 1 ? av[u][1] : x;
-          x = sel == 2 ? av[u][2] : x;
-          x = sel == 3 ? av[u][3] : x;
-          col[qn + ty + 16 * u] = x;
+      for (int jj = 0; jj < 16; ++jj) {
+        double p = __shfl_sync(0xffffffffu, pa[jj], jj);   // A_jj: row c0 + jj is lane jj's first row
+        if (!(p > 0.0)) {
+          p = 1.0;
+          bad = 1;
+        }
+        const double ip = 1.0 / p;
+        if (ln == 0) {
+          piv[c0 + jj] = p;
+          ipv[c0 + jj] = ip;
+        }
+        double cv[16];   // A_{c0 + cc, j}, cc > jj
+#pragma unroll
+        for (int cc = jj + 1; cc < 16; ++cc) cv[cc] = __shfl_sync(0xffffffffu, pa[jj], cc);
+        if (ln > jj && ra < CT) {
+          const double m = pa[jj] * ip;
+#pragma unroll
+          for (int cc = jj + 1; cc < 16; ++cc)
+            if (cc <= ln) pa[cc] -= m * cv[cc];
+        }
+        if (rb < CT) {
+          const double m = pb[jj] * ip;
+#pragma unroll
+          for (int cc = jj + 1; cc < 16; ++cc) pb[cc] -= m * cv[cc];
         }
       }
-      if (ty == (jn & 15)) {
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          double x = ev[0][v];
-          x = sel == 1 ? ev[1][v] : x;
-          x = sel == 2 ? ev[2][v] : x;
-          x = sel == 3 ? ev[3][v] : x;
-          erow[qn + tx + 16 * v] = x;
-        }
+      for (int cc = 0; cc < 16; ++cc) {
+        if (ra < CT) A[ra * CTP + c0 + cc] = pa[cc];
+        if (rb < CT) A[rb * CTP + c0 + cc] = pb[cc];
       }
+    }
+    sync();
+    // rank-16 update of the trailing lower part: rows and columns >= c0 + 16;
+    // thread (ty, tx) owns rows t0 + ty + 16 u and columns t0 + tx + 16 v
+    // (u, v < 3), all of them accumulated side by side
+    const int t0 = c0 + 16;
+    if (t0 < CT) {
+      const int tx = tid & 15, ty = tid >> 4;
+      double acc[3][3];
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) acc[u][v] = 0.0;
+#pragma unroll
+      for (int jj = 0; jj < 16; ++jj) {
+        double ai[3], ac[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          const int i = min(t0 + ty + 16 * u, CT - 1), c = min(t0 + tx + 16 * u, CT - 1);
+          ai[u] = A[i * CTP + c0 + jj];
+          ac[u] = A[c * CTP + c0 + jj] * ipv[c0 + jj];
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+#pragma unroll
+          for (int v = 0; v < 3; ++v) acc[u][v] += ai[u] * ac[v];
+      }
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+          const int i = t0 + ty + 16 * u, c = t0 + tx + 16 * v;
+          if (i < CT && c <= i) A[i * CTP + c] -= acc[u][v];
+        }
     }
   }
   sync();
-  if (tid < nb) piv[tid] = sqrt(piv[tid]);
+  if (tid < CT) {
+    const double d = sqrt(piv[tid]);
+    piv[tid] = d;
+    rinv[tid] = 1.0 / d;
+  }
   sync();
 #pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = ty + 16 * u, c = tx + 16 * v;
-      if (i < nb && c < nb) {
-        const double l = (c < i) ? av[u][v] / piv[c] : (c == i ? piv[c] : 0.0);
-        Lm[(size_t)(r0 + i) * n + r0 + c] = l;
-        if (a.bd_tc) a.bd_L32[L32 + (size_t)(r0 + i) * ((n + 3) & ~3) + r0 + c] = (float)l;
-      }
+  for (int q = 0; q < CT * CT / 256; ++q) {
+    const int e = tid + 256 * q, i = e >> 6, c = e & 63;
+    const double l = (c < i) ? A[i * CTP + c] * rinv[c] : (c == i ? piv[c] : 0.0);
+    A[i * CTP + c] = l;
+    if (i < nb && c < nb) {
+      Lm[(size_t)(r0 + i) * n + r0 + c] = l;
+      if (a.bd_tc) a.bd_L32[L32 + (size_t)(r0 + i) * ((n + 3) & ~3) + r0 + c] = (float)l;
     }
+  }
   if (tid == 0 && bad) atomicOr(&a.not_spd[lane], 1);
   if (r0 + CT < n) {   // a panel of rows below follows (then nb = CT)
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        const int i = ty + 16 * u, c = tx + 16 * v;
-        S[c * CTP + i] = (c <= i) ? ev[u][v] / piv[i] : 0.0;   // U[c][i] = W[i][c]
-      }
     sync();
-    double *w = a.bd_W + (size_t)lane * CT * CT;
-    for (int e = tid; e < CT * CT; e += 256) w[e] = S[(e >> 6) * CTP + (e & 63)];
+    // column c of W: thread t of the group of four owns rows t + 4 s
+    const int c = tid >> 2, t = tid & 3, lead = ln & ~3;
+    double w[16];
+#pragma unroll
+    for (int s2 = 0; s2 < 16; ++s2) w[s2] = (t + 4 * s2 == c) ? 1.0 : 0.0;
+#pragma unroll
+    for (int j = 0; j < CT; ++j) {
+      double lj[16];   // column j of L for the rows of this thread, loaded off the chain
+#pragma unroll
+      for (int s2 = (j >> 2); s2 < 16; ++s2) lj[s2] = A[(t + 4 * s2) * CTP + j];
+      double wj = 0.0;
+      if (t == (j & 3)) {
+        w[j >> 2] *= rinv[j];
+        wj = w[j >> 2];
+      }
+      wj = __shfl_sync(0xffffffffu, wj, lead | (j & 3));   // zero while j < c
+#pragma unroll
+      for (int s2 = (j >> 2); s2 < 16; ++s2)
+        if (t + 4 * s2 > j) w[s2] -= lj[s2] * wj;
+    }
+    double *wout = a.bd_W + (size_t)lane * CT * CT + (size_t)c * CT;   // U[c][i] = W[i][c]
+#pragma unroll
+    for (int s2 = 0; s2 < 16; ++s2) wout[t + 4 * s2] = w[s2];
   }
 }
 
@@ -232,9 +271,10 @@ struct BlockSync {
   __device__ void operator()() const { __syncthreads(); }
 };
 
-// grid nlane, 256 threads: the first diagonal tile of every lane.  The
-// diagonal tile of panel k + 1 is factored by the trailing update of panel k
-// (the CTA that finishes it), so only panel 0 needs this launch.
+// grid nlane, 256 threads: the diagonal tile of panel k of every lane.  On
+// the tensor-core path the diagonal tile of a later panel is factored by the
+// update launch that finishes it (the CTA that owns it), so only panel 0
+// needs this launch; the FP64 path launches it for every panel.
 __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
   const int lane = blockIdx.x;
   if (lane >= a.nlane) return;
@@ -242,7 +282,7 @@ __global__ void __launch_bounds__(256) chol_diag_kernel(KArgs a) {
   int n;
   lane_tiles(a, L, n);
   __shared__ double S[CT * CTP], vec[5 * CT];
-  factor_diag_tile(a, lane, a.bd_L + L.bd0, n, 0, S, vec, threadIdx.x, BlockSync{});
+  if (a.bd_kpanel < lane_tiles(a, L, n)) factor_diag_tile(a, lane, a.bd_L + L.bd0, n, a.bd_kpanel, S, vec, threadIdx.x, BlockSync{});
 }
 
 // grid (T - k - 1, nlane), 256 threads: row tile ti = k + 1 + blockIdx.x of
@@ -376,11 +416,6 @@ __global__ void __launch_bounds__(256) chol_update_kernel(KArgs a) {
       if (c >= mj) continue;
       Lm[(size_t)(i0 + r) * n + j0 + c] -= acc[u][v];
     }
-  }
-  if (p == 0) {
-    // tile (k + 1, k + 1) is now final: factor it for the next panel
-    __shared__ double vec[5 * CT];
-    factor_diag_tile(a, lane, Lm, n, k + 1, sh, vec, tid, BlockSync{});
   }
 }
 
@@ -836,6 +871,7 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int 
   if (a.bd_tc && (!a.bd_P || !items || !koff)) return cudaErrorInvalidValue;
   const long long nn = (long long)max_nmp * max_nmp;
   rpy_kernel<<<dim3((unsigned)((nn + 255) / 256), a.nlane), 256, 0, st>>>(a);
+  a.bd_kpanel = 0;
   chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
   const int T = (3 * max_nmp + CT - 1) / CT;
   if (a.bd_tc) {
@@ -857,16 +893,20 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int 
     for (int k = 0; k + 1 < T; ++k) {
       a.bd_kpanel = k;
       const int m = T - k - 1;
+      if (k > 0) chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
       chol_panel_kernel<<<dim3(m, a.nlane), 256, U64_SMEM, st>>>(a);
       chol_update_kernel<<<dim3(a.nlane, m * (m + 1) / 2), 256, U64_SMEM, st>>>(a);
     }
+    // the last diagonal tile
+    a.bd_kpanel = T - 1;
+    if (T > 1) chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
   }
   return cudaGetLastError();
 }
 
 int bd_refactor_launches(int max_nmp, bool tc) {
   const int T = (3 * max_nmp + CT - 1) / CT;
-  if (!tc) return 2 + 2 * (T - 1);
+  if (!tc) return 2 + 3 * (T - 1);
   int nl = 2;
   for (int k = 0; k + 1 < T; k += 2) nl += (k + 2 < T) ? 4 : 2;
   return nl;
