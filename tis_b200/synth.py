@@ -464,11 +464,12 @@ def bdhi_params(**over):
 def workload_c5(seed: int = 5, nchain: int = 32):
     """Brownian-HI batch: nchain bead chains, N uniform in 100..1000, FENE
     bonds, WCA between all non-bonded pairs, RPY radius 2 A, dt 0.01, D and
-    its Cholesky factor refreshed every 10 steps, 300 K."""
+    its Cholesky factor refreshed every 10 steps, 300 K; mixed precision
+    (tensor-core trailing updates, FP32 D and L in the step)."""
     rng = np.random.default_rng(seed)
     ns = rng.integers(100, 1001, size=nchain)
     systems = [bead_chain(int(n), seed * 1000 + k) for k, n in enumerate(ns)]
-    return systems, bdhi_params(n_step_hydro=10), [300.0] * nchain
+    return systems, bdhi_params(n_step_hydro=10, precision=1), [300.0] * nchain
 
 
 def temperature_ladder(n=64, tlo=280.0, thi=400.0):
