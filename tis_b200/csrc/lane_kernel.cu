@@ -217,20 +217,12 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
 }
 
 // ------------------------------------------------------------ force pass
-// Accumulator of a chunk's pair forces: FP64 in the FP64 path, an
-// error-free two-sum FP32 pair (FP64-equivalent for these lengths) in the
-// mixed path; the chunk total enters the bead's FP64 sum.
-template <typename Real> struct Acc;
-template <> struct Acc<double> {
-  double v = 0.0;
-  __device__ __forceinline__ void add(double x) { v += x; }
-  __device__ __forceinline__ double value() const { return v; }
-};
-template <> struct Acc<float> {
-  float hi = 0.f, lo = 0.f;
-  __device__ __forceinline__ void add(float x) { two_sum_add(hi, lo, x); }
-  __device__ __forceinline__ double value() const { return (double)hi + (double)lo; }
-};
+// exp for the Debye-Hueckel factor: FP64 in the FP64 path; the fast
+// single-precision exponential in the mixed path (relative error about
+// |x| 2^-22 for the arguments here, |x| <= 25)
+template <typename Real> __device__ __forceinline__ Real fexp(Real x);
+template <> __device__ __forceinline__ double fexp<double>(double x) { return exp(x); }
+template <> __device__ __forceinline__ float fexp<float>(float x) { return __expf(x); }
 
 template <typename Real>
 __device__ __forceinline__ void group_reduce(double &fx, double &fy, double &fz, int G) {
@@ -281,10 +273,10 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
   return g;
 }
 
-// Phase 1 runs every interaction-level item in one balanced sweep, the most
-// expensive first: hbonds, stacks, Debye-Hueckel chunks (force_ele_DH.F90:
-// 72-117 over a word range of one charged bead's ele row, summed by one
-// thread into ch_part), angles, bonds.  Phase 2 gives each bead a group of GA
+// Phase 1 runs every interaction-level item in one balanced sweep: stacks,
+// Debye-Hueckel chunks (force_ele_DH.F90:72-117 over a word range of one
+// charged bead's ele row, summed by one thread into ch_part), angles,
+// hbonds, bonds.  Phase 2 gives each bead a group of GA
 // threads that sums its exv pairs, its bonded slots and its Debye-Hueckel
 // chunk partials; the group's owner thread hands the FP64 total to `sink`.
 template <typename Real, int CL, typename Sink>
@@ -325,8 +317,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const bool near_rec = s.near_on && (s.misc[MISC_NEAR_BAD] != 0 ||
                                       __int_as_float(s.misc[MISC_NEAR_DISP]) > NEAR_DISP_MAX * NEAR_DISP_MAX);
   PHASE_T0(t_p1);
-  // warp-uniform schedule: 32-item chunks of one kind, most expensive kinds
-  // first, dealt round-robin over the warps (no divergence between kinds)
+  // warp-uniform schedule: 32-item chunks of one kind (no divergence between
+  // kinds), dealt to the warps as below
   const int nwarp = nth >> 5, warp = tid >> 5, lid = tid & 31;
   // items of this CTA, [x0, x1) per kind: all of them for one CTA per lane;
   // with two CTAs every hbond goes to the first one (the valence pruning that
@@ -340,19 +332,26 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     bd_0 = cu.rank ? nbd / 2 : 0; bd_1 = cu.rank ? nbd : nbd / 2;
     ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
   }
-  const int c_st = (hb_1 - hb_0 + 31) >> 5, c_ch = c_st + ((st_1 - st_0 + 31) >> 5);
-  const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
-  const int c_bd = c_ba + ((ba_1 - ba_0 + 31) >> 5), c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
+  // chunk ranges, kinds in decreasing cost per chunk (measured on B200):
+  // stacks, Debye-Hueckel row chunks, angles, hbonds, bonds, then noise
+  const int c_ch = (st_1 - st_0 + 31) >> 5, c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
+  const int c_hb = c_ba + ((ba_1 - ba_0 + 31) >> 5), c_bd = c_hb + ((hb_1 - hb_0 + 31) >> 5);
+  const int c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
   // the sink's Gaussian noise of the own beads, drawn here where warps have slack
   const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
   const int c_end = c_nz + ((n_nz + 31) >> 5);
   (void)k_st; (void)k_ch; (void)k_ba; (void)k_bd; (void)total;
-  for (int c = warp; c < c_end; c += nwarp) {
+  // snake deal: round r gives chunk r nwarp + w to warp w (r even) or to
+  // warp nwarp - 1 - w (r odd), so the costly first chunks and the cheap
+  // last ones even out over the warps
+  for (int r = 0; r * nwarp < c_end; ++r) {
+    const int c = r * nwarp + ((r & 1) ? nwarp - 1 - warp : warp);
+    if (c >= c_end) break;
     PHASE_T0(t_item);
     int kind;
-    if (c < c_st) {
+    if (c >= c_hb && c < c_bd) {
       kind = 0;
-      const int h = hb_0 + (c << 5) + lid;
+      const int h = hb_0 + ((c - c_hb) << 5) + lid;
       if (h < hb_1) {
         uint8_t f = hbf[h] & 1;
         if (f) {
@@ -381,7 +380,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       }
     } else if (c < c_ch) {
       kind = 1;
-      const int k = st_0 + ((c - c_st) << 5) + lid;
+      const int k = st_0 + (c << 5) + lid;
       if (k < st_1) term_stack<Real>(a, T, s, slots, k, u0[k]);
     } else if (c < c_ba) {
       kind = 2;
@@ -395,7 +394,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         const Real qci = (Real)((double)pi.w * coefT);
         const uint32_t *row = mele + (size_t)i * W;
         const int w1 = min(W, (part + 1) * geo.gw);
-        Acc<Real> ax_, ay_, az_;
+        // partial sums over at most a few words of the row, in Real (the
+        // chunk totals enter each bead's FP64 sum)
+        Real axs = 0, ays = 0, azs = 0;
         for (int w = part * geo.gw; w < w1; ++w) {
           uint32_t m = row[w];
           while (m) {
@@ -413,8 +414,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const Real da = ra2 * ria, db = rb2 * rib;
             Real fa, fb;
             if (!ewald) {
-              fa = qci * p0.w * ria * ria * (ria + rcd) * exp(-da * rcd);
-              fb = qci * p1.w * rib * rib * (rib + rcd) * exp(-db * rcd);
+              fa = qci * p0.w * ria * ria * (ria + rcd) * fexp<Real>(-da * rcd);
+              fb = qci * p1.w * rib * rib * (rib + rcd) * fexp<Real>(-db * rcd);
             } else {
               // force_ele_coulomb_ewld.F90:118-137 (real space, no clamp)
               fa = qci * p0.w * (erfc(ew_a * da) * ria + ew_b * exp(-ew_a2 * ra2)) * ria * ria;
@@ -426,14 +427,14 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
               if (fa > (Real)50) { fa = 50; ++nclamp; }
               if (fb > (Real)50) { fb = 50; ++nclamp; }
             }
-            ax_.add(-(fa * ax)); ax_.add(-(fb * bx));
-            ay_.add(-(fa * ay)); ay_.add(-(fb * by));
-            az_.add(-(fa * az)); az_.add(-(fb * bz));
+            axs -= fa * ax + fb * bx;
+            ays -= fa * ay + fb * by;
+            azs -= fa * az + fb * bz;
           }
         }
-        s.ch_part[3 * cc] = ax_.value(); s.ch_part[3 * cc + 1] = ay_.value(); s.ch_part[3 * cc + 2] = az_.value();
+        s.ch_part[3 * cc] = axs; s.ch_part[3 * cc + 1] = ays; s.ch_part[3 * cc + 2] = azs;
       }
-    } else if (c < c_bd) {
+    } else if (c < c_hb) {
       kind = 3;
       const int k = ba_0 + ((c - c_ba) << 5) + lid;
       if (k < ba_1) term_angle<Real>(a, T, s, slots, k);
