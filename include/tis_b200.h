@@ -113,6 +113,13 @@ typedef struct tis_topology {
   const int32_t *iwca2mp;          /* (2, nwca) */
   const double *wca_nat;           /* (nwca) sigma */
   const double *coef_wca;          /* (nwca, 2): repulsive, attractive */
+  int32_t ntst;                    /* DT15 tertiary stacks (tbs-dist/-angl/-dihd records,
+                                      src/read_nativeinfo.F90:624-700, force_dtrna_stack_nlocal.F90) */
+  const int32_t *idtrna_tst2mp;    /* (6, ntst) B1 B2 S1 S2 P1' P2' */
+  const double *dtrna_tst_nat;     /* (6, ntst) dist, 2 angles, 3 dihedrals (rad) */
+  const double *coef_dtrna_tst;    /* (7, ntst) index 0 = U0, 1..6 */
+  const int32_t *idtrna_tst2side;  /* (2, ntst) 1: the secondary stack of B with B - 3, 2: with B + 3 */
+  const int32_t *flg_tst_exclusive;/* (2, ntst) nonzero: within 10 A of native, disables that stack */
 } tis_topology;
 
 /* ---------------------------------------------------------------- params */

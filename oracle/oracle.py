@@ -68,7 +68,8 @@ def lib():
     return _LIB
 
 
-TERMS = {"bond": 0, "angle": 1, "stack": 2, "hbond": 3, "exv": 4, "dh": 5, "ewald": 6, "fene": 7, "wca": 8}
+TERMS = {"bond": 0, "angle": 1, "stack": 2, "hbond": 3, "exv": 4, "dh": 5, "ewald": 6, "fene": 7, "wca": 8,
+         "tstack": 9}
 
 
 class Oracle:

@@ -100,6 +100,9 @@ struct orc_ctx {
   std::vector<std::vector<int>> hb_at_site;   // static per-site hb lists (ascending ihb)
   int nfene = 0; std::vector<int> fene2mp; std::vector<double> fene_nat, coef_fene, dist2_fene;
   int nwca = 0; std::vector<int> wca2mp; std::vector<double> wca_nat, coef_wca;
+  int ntst = 0; std::vector<int> tst2mp; std::vector<double> tst_nat, tst_coef;
+  std::vector<int> tst2st;         // (2, ntst) 0-based secondary stack of each side, -1: none
+  std::vector<char> tst_excl;      // (2, ntst) after mloop_dtrna.F90:74-140
   tis_params par;
   // derived
   std::vector<double> rneighbordist2_unit;   // (nunit, nunit)
@@ -512,6 +515,139 @@ void force_dtrna_stack(const orc_ctx &c, const Rep &r, double *F) {
   }
 }
 
+// force_dtrna_stack_nlocal.F90:60-263 (forces) and energy_dtrna_stack_nlocal.F90
+// (energy, U0 / ediv): sets st_status of the secondary stacks that a
+// tertiary stack within 10 A of its native distance excludes.  F may be null
+// (energy only); returns the tertiary stacking energy.
+double dtrna_stack_nlocal(const orc_ctx &c, Rep &r, double *F) {
+  const bool peri = c.par.i_periodic == 1;
+  const double *X = peri ? r.pxyz.data() : r.xyz.data();
+  r.st_status.assign(c.nst, 1);
+  double etot = 0.0;
+  for (int ist = 0; ist < c.ntst; ++ist) {
+    const int *m = &c.tst2mp[6 * ist];
+    const double *nat = &c.tst_nat[6 * ist];
+    const double *cf = &c.tst_coef[7 * ist];
+    auto dv = [&](int p, int q, double *v) {
+      for (int d = 0; d < 3; ++d) v[d] = X[3 * (m[p] - 1) + d] - X[3 * (m[q] - 1) + d];
+      if (peri) { int im; pbneighbor(c, v, &im); }
+    };
+    double v12[3], v13[3], v53[3], v42[3], v46[3];
+    dv(0, 1, v12);
+    const double d1212 = dot3(v12, v12);
+    const double a12 = std::sqrt(d1212);
+    double d = a12 - nat[0];
+    if (d < 10.0) {
+      for (int sd = 0; sd < 2; ++sd)
+        if (c.tst_excl[2 * ist + sd]) r.st_status[c.tst2st[2 * ist + sd]] = 0;
+    }
+    double ediv = 1.0e0;
+    double fr[6][3] = {{0}};
+    dv(0, 2, v13); dv(4, 2, v53); dv(3, 1, v42); dv(3, 5, v46);
+    const double d1313 = dot3(v13, v13), d4242 = dot3(v42, v42);
+    const double a13 = std::sqrt(d1313), a42 = std::sqrt(d4242);
+    const double d1213 = dot3(v13, v12), d1242 = dot3(v12, v42), d4246 = dot3(v42, v46), d1353 = dot3(v13, v53);
+    const double d1213over1212 = d1213 / d1212, d1213over1313 = d1213 / d1313;
+    const double d1242over1212 = d1242 / d1212, d4246over4242 = d4246 / d4242;
+    const double d1242over4242 = d1242 / d4242, d1353over1313 = d1353 / d1313;
+    double fi[3], fk[3], fl[3];
+    // distance 1=2
+    ediv = ediv + cf[1] * d * d;
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = 2.0e0 * cf[1] * d * v12[q] / a12;
+      fr[0][q] = +fi[q];
+      fr[1][q] = -fi[q];
+    }
+    // angle 3-1=2
+    double cos_theta = d1213 / (a13 * a12);
+    d = std::acos(cos_theta) - nat[1];
+    double pre = 2.0e0 * cf[2] * d / std::sqrt(d1313 * d1212 - d1213 * d1213);
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = pre * (v12[q] - (d1213over1313 * v13[q]));
+      fk[q] = pre * (v13[q] - (d1213over1212 * v12[q]));
+      fr[2][q] = fr[2][q] + fi[q];
+      fr[1][q] = fr[1][q] + fk[q];
+      fr[0][q] = fr[0][q] - fi[q] - fk[q];
+    }
+    ediv = ediv + cf[2] * d * d;
+    // angle 1=2-4
+    cos_theta = d1242 / (a12 * a42);
+    d = std::acos(cos_theta) - nat[2];
+    pre = 2.0e0 * cf[3] * d / std::sqrt(d1212 * d4242 - d1242 * d1242);
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = -pre * (v42[q] - (d1242over1212 * v12[q]));
+      fk[q] = -pre * (v12[q] - (d1242over4242 * v42[q]));
+      fr[0][q] = fr[0][q] + fi[q];
+      fr[3][q] = fr[3][q] + fk[q];
+      fr[1][q] = fr[1][q] - fi[q] - fk[q];
+    }
+    ediv = ediv + cf[3] * d * d;
+    // dihedral 4-2=1=3
+    double c4212[3], c1213[3];
+    cross(v42, v12, c4212);
+    cross(v12, v13, c1213);
+    const double c4212_abs2 = dot3(c4212, c4212), c1213_abs2 = dot3(c1213, c1213);
+    double dih = std::atan2(dot3(v42, c1213) * std::sqrt(d1212), dot3(c4212, c1213));
+    d = wrap_pi(dih - nat[3]);
+    ediv = ediv + cf[4] * d * d;
+    pre = 2.0e0 * cf[4] * d * a12;
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = +pre / c4212_abs2 * c4212[q];
+      fl[q] = -pre / c1213_abs2 * c1213[q];
+    }
+    for (int q = 0; q < 3; ++q) {
+      fr[3][q] = fr[3][q] + fi[q];
+      fr[1][q] = fr[1][q] + (-1.0e0 + d1242over1212) * fi[q] - (d1213over1212) * fl[q];
+      fr[0][q] = fr[0][q] + (-1.0e0 + d1213over1212) * fl[q] - (d1242over1212) * fi[q];
+      fr[2][q] = fr[2][q] + fl[q];
+    }
+    // dihedral 5-3-1=2
+    double mm[3], nn[3];
+    cross(v53, v13, mm);
+    for (int q = 0; q < 3; ++q) nn[q] = -c1213[q];
+    double dmm = dot3(mm, mm), dnn = c1213_abs2;
+    dih = std::atan2(dot3(v53, nn) * a13, dot3(mm, nn));
+    d = wrap_pi(dih - nat[4]);
+    ediv = ediv + cf[5] * d * d;
+    pre = 2.0e0 * cf[5] * d * a13;
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = +pre / dmm * mm[q];
+      fl[q] = -pre / dnn * nn[q];
+    }
+    for (int q = 0; q < 3; ++q) {
+      fr[4][q] = fr[4][q] + fi[q];
+      fr[2][q] = fr[2][q] + (-1.0e0 + d1353over1313) * fi[q] - (d1213over1313) * fl[q];
+      fr[0][q] = fr[0][q] + (-1.0e0 + d1213over1313) * fl[q] - (d1353over1313) * fi[q];
+      fr[1][q] = fr[1][q] + fl[q];
+    }
+    // dihedral 1=2-4-6
+    for (int q = 0; q < 3; ++q) mm[q] = -c4212[q];
+    cross(v42, v46, nn);
+    dmm = c4212_abs2;
+    dnn = dot3(nn, nn);
+    dih = std::atan2(dot3(v12, nn) * a42, dot3(mm, nn));
+    d = wrap_pi(dih - nat[5]);
+    ediv = ediv + cf[6] * d * d;
+    pre = 2.0e0 * cf[6] * d * a42;
+    for (int q = 0; q < 3; ++q) {
+      fi[q] = +pre / dmm * mm[q];
+      fl[q] = -pre / dnn * nn[q];
+    }
+    for (int q = 0; q < 3; ++q) {
+      fr[0][q] = fr[0][q] + fi[q];
+      fr[1][q] = fr[1][q] + (-1.0e0 + d1242over4242) * fi[q] - (d4246over4242) * fl[q];
+      fr[3][q] = fr[3][q] + (-1.0e0 + d4246over4242) * fl[q] - (d1242over4242) * fi[q];
+      fr[5][q] = fr[5][q] + fl[q];
+    }
+    etot += cf[0] / ediv;
+    if (F) {
+      for (int k = 0; k < 6; ++k)
+        for (int q = 0; q < 3; ++q) F[3 * (m[k] - 1) + q] = F[3 * (m[k] - 1) + q] + fr[k][q] * cf[0] / (ediv * ediv);
+    }
+  }
+  return etot;
+}
+
 double draw_uniform(Rep &r) {
   if (r.upos < r.unif.size()) return r.unif[r.upos++];
   r.unif_exhausted = true;
@@ -876,16 +1012,17 @@ void force_wca(const orc_ctx &c, Rep &r, double *F) {
 }
 
 // force_sumup.F90:66-333 (single thread: one buffer, so the thread
-// reduction is the identity).  st_status stays .true. for every stack:
-// there are no tertiary stacks (force_dtrna_stack_nlocal.F90:60).
+// reduction is the identity).
 void force_sumup(orc_ctx &c, Rep &r, double *F) {
   std::fill(F, F + 3 * (size_t)c.nmp, 0.0);
   force_bond(c, r, F);
   force_fene(c, r, F);
   force_bangle(c, r, F);
   force_wca(c, r, F);
-  if (c.nst > 0 || c.nhb > 0) {
+  if (c.nst > 0 || c.nhb > 0 || c.ntst > 0) {
+    // force_sumup.F90:159-179: tertiary stacks first (they set st_status)
     r.st_status.assign(c.nst, 1);
+    if (c.ntst > 0) dtrna_stack_nlocal(c, r, F);
     force_dtrna_stack(c, r, F);
     force_dtrna_hbond15(c, r, F);
   }
@@ -1087,8 +1224,10 @@ void energy_sumup(orc_ctx &c, Rep &r, double *E, bool reuse_hb) {
   E[TIS_E_BOND - 1] = energy_bond(c, r) + energy_fene(c, r);   // energy_fene.F90 adds to E_TYPE%BOND
   if (c.nwca) energy_wca(c, r, E[TIS_E_WCA_REP - 1], E[TIS_E_WCA_ATT - 1]);
   E[TIS_E_BANGLE - 1] = energy_bangle(c, r);
-  if (c.nst > 0 || c.nhb > 0) {
-    if (r.st_status.size() != (size_t)c.nst) r.st_status.assign(c.nst, 1);
+  if (c.nst > 0 || c.nhb > 0 || c.ntst > 0) {
+    // energy_sumup.F90:197-215: the tertiary stacks set st_status first
+    r.st_status.assign(c.nst, 1);
+    if (c.ntst > 0) E[TIS_E_TSTACK_DTRNA - 1] = dtrna_stack_nlocal(c, r, nullptr);
     E[TIS_E_STACK_DTRNA - 1] = energy_stack(c, r);
     E[TIS_E_HBOND_DTRNA - 1] = energy_hbond(c, r, reuse_hb);
   }
@@ -1221,6 +1360,29 @@ orc_ctx *orc_create(const tis_topology *t, const tis_params *p, int nrep, const 
     c->fene_nat.assign(t->fene_nat, t->fene_nat + t->nfene);
     c->coef_fene.assign(t->coef_fene, t->coef_fene + t->nfene);
     c->dist2_fene.assign(t->dist2_fene, t->dist2_fene + t->nfene);
+  }
+  c->ntst = t->ntst;
+  if (t->ntst) {
+    c->tst2mp.assign(t->idtrna_tst2mp, t->idtrna_tst2mp + 6 * t->ntst);
+    c->tst_nat.assign(t->dtrna_tst_nat, t->dtrna_tst_nat + 6 * t->ntst);
+    c->tst_coef.assign(t->coef_dtrna_tst, t->coef_dtrna_tst + 7 * t->ntst);
+    c->tst2st.assign(2 * t->ntst, -1);
+    c->tst_excl.assign(2 * t->ntst, 0);
+    // mloop_dtrna.F90:74-140: side s of a tertiary stack is the secondary
+    // stack between its base B and B - 3 (side 1) or B + 3 (side 2); without
+    // such a stack the side is not exclusive
+    for (int itst = 0; itst < t->ntst; ++itst)
+      for (int sd = 0; sd < 2; ++sd) {
+        const int imp1 = t->idtrna_tst2mp[6 * itst + sd];
+        const int imp2 = (t->idtrna_tst2side[2 * itst + sd] == 1) ? imp1 - 3 : imp1 + 3;
+        int found = -1;
+        for (int ist = 0; ist < t->nst; ++ist) {
+          const int a1 = t->idtrna_st2mp[7 * ist], a2 = t->idtrna_st2mp[7 * ist + 1];
+          if ((imp1 == a1 && imp2 == a2) || (imp1 == a2 && imp2 == a1)) { found = ist; break; }
+        }
+        c->tst2st[2 * itst + sd] = found;
+        c->tst_excl[2 * itst + sd] = (found >= 0 && t->flg_tst_exclusive[2 * itst + sd]) ? 1 : 0;
+      }
   }
   c->nwca = t->nwca;
   if (t->nwca) {
@@ -1381,21 +1543,25 @@ int orc_force_sumup(orc_ctx *c, int irep, double *force) {
   return r.unif_exhausted ? TIS_E_NOISE_EXHAUSTED : 0;
 }
 
-// Single force term for tests: term = 0 bond, 1 angle, 2 stack, 3 hbond,
-// 4 exv, 5 DH, 6 Ewald, 7 fene, 8 wca.
+// Single force term for tests: term = 0 bond, 1 angle, 2 stack, 3 hbond, 4 exv, 5 DH, 6 Ewald, 7 fene, 8 wca, 9 tertiary stack.
 int orc_force_term(orc_ctx *c, int irep, int term, double *force) {
   Rep &r = c->rep[irep - 1];
   std::fill(force, force + 3 * (size_t)c->nmp, 0.0);
   switch (term) {
     case 0: force_bond(*c, r, force); break;
     case 1: force_bangle(*c, r, force); break;
-    case 2: r.st_status.assign(c->nst, 1); force_dtrna_stack(*c, r, force); break;
+    case 2:   // st_status as force_sumup sets it
+      if (c->ntst > 0) dtrna_stack_nlocal(*c, r, nullptr);
+      else r.st_status.assign(c->nst, 1);
+      force_dtrna_stack(*c, r, force);
+      break;
     case 3: force_dtrna_hbond15(*c, r, force); break;
     case 4: force_exv_dt15(*c, r, force); break;
     case 5: force_ele_DH(*c, r, force); break;
     case 6: force_ele_ewald(*c, r, force); break;
     case 7: force_fene(*c, r, force); break;
     case 8: force_wca(*c, r, force); break;
+    case 9: dtrna_stack_nlocal(*c, r, force); break;
     default: return TIS_E_ARG;
   }
   return 0;

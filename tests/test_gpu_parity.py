@@ -49,6 +49,7 @@ def periodic_ions(seed=7):
 
 SYSTEMS = {
     "c1_walk": (c1_system, {}),
+    "hairpin_tertiary": (synth.hairpin_tertiary, {}),
     "hairpin": (hairpin, {}),
     "dense": (dense, {}),
     "periodic_ions": (periodic_ions, dict(i_periodic=1, psize=(40.0, 40.0, 40.0))),
@@ -106,14 +107,14 @@ def test_force_mixed(tis_lib, name):
     assert err < FORCE_TOL_MIXED, err
 
 
-@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense"])
+@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary"])
 def test_energy_fp64(tis_lib, name):
     s, par, eng, orc = make_pair(name, 0)
     eng.neighbor(); orc.neighbor()
     eng.force(); orc.force()
     e = eng.energy()
     er = orc.energy(reuse_hb=True)
-    for k in (1, 3, 4, 8, 16, 17, 18):
+    for k in (1, 3, 4, 8, 16, 17, 18, 19):
         assert abs(e[k - 1] - er[k - 1]) <= 1e-9 * max(1.0, abs(er[k - 1])), (k, e[k - 1], er[k - 1])
 
 

@@ -24,7 +24,7 @@ import pytest
 from tis_b200 import synth
 from oracle.oracle import Oracle, boltz
 
-E_IDX = {"bond": 3, "angle": 4, "stack": 16, "hbond": 17, "exv": 18, "dh": 8}
+E_IDX = {"bond": 3, "angle": 4, "stack": 16, "hbond": 17, "exv": 18, "dh": 8, "tstack": 19}
 
 
 def hairpin():
@@ -43,7 +43,12 @@ def periodic_ions():
     return s, dict(i_periodic=1, psize=(40.0, 40.0, 40.0))
 
 
-FD_SYSTEMS = {"hairpin": hairpin, "dense_noclamp": dense_noclamp, "periodic_ions": periodic_ions}
+def hairpin_tertiary():
+    return synth.hairpin_tertiary(1), {}
+
+
+FD_SYSTEMS = {"hairpin": hairpin, "dense_noclamp": dense_noclamp, "periodic_ions": periodic_ions,
+              "hairpin_tertiary": hairpin_tertiary}
 
 
 def fd_forces(o, x0, h=1e-4):
@@ -98,6 +103,48 @@ def test_fd_systems_exercise_every_term(fd_cache):
     for term in E_IDX:
         assert any(np.abs(v[0][term]).max() > 0.1 for v in fd_cache.values()), term
     assert not fd_cache["dense_noclamp"][2]
+
+
+def test_tertiary_stacks_turn_off_secondary_stacks():
+    """force_dtrna_stack_nlocal.F90:83-92 with mloop_dtrna.F90:74-140: a
+    tertiary stack within 10 A of its native distance turns off the
+    secondary stacks of its exclusive sides; the others stay on."""
+    s = synth.hairpin_tertiary(1)
+    par = synth.dt15_params(ionic_strength=0.15)
+    o = Oracle(s, par, [300.0])
+    o.set_state(s["xyz"][None])
+    o.neighbor()
+    e = o.energy()
+    st = s["idtrna_st2mp"]
+    expect_off = set()
+    for k in range(s["ntst"]):
+        m = s["idtrna_tst2mp"][k]
+        d = np.linalg.norm(s["xyz"][m[0] - 1] - s["xyz"][m[1] - 1]) - s["dtrna_tst_nat"][k, 0]
+        if d >= 10.0:
+            continue
+        for sd in range(2):
+            b = m[sd]
+            b2 = b - 3 if s["idtrna_tst2side"][k, sd] == 1 else b + 3
+            for ist in range(s["nst"]):
+                if {st[ist, 0], st[ist, 1]} == {b, b2} and s["flg_tst_exclusive"][k, sd]:
+                    expect_off.add(ist)
+    assert expect_off
+    # the stack energy equals the sum over the stacks left on
+    s_on = dict(s, ntst=0)
+    o2 = Oracle(s_on, par, [300.0])
+    per = []
+    for ist in range(s["nst"]):
+        keep = dict(s_on, nst=1, idtrna_st2mp=st[ist:ist + 1], dtrna_st_nat=s["dtrna_st_nat"][ist:ist + 1],
+                    coef_dtrna_st=s["coef_dtrna_st"][ist:ist + 1], dtrna_st_hsTm=s["dtrna_st_hsTm"][ist:ist + 1])
+        ok = Oracle(keep, par, [300.0])
+        ok.set_state(s["xyz"][None])
+        ok.neighbor()
+        per.append(ok.energy()[15])
+        ok.close()
+    want = sum(v for ist, v in enumerate(per) if ist not in expect_off)
+    assert abs(e[15] - want) <= 1e-12 * max(1.0, abs(want))
+    assert e[18] < 0.0
+    o.close(); o2.close()
 
 
 def neutral_ion_box():

@@ -53,6 +53,8 @@ class Topology(C.Structure):
         ("nfene", C.c_int32), ("ifene2mp", _i32p), ("fene_nat", _f64p),
         ("coef_fene", _f64p), ("dist2_fene", _f64p),
         ("nwca", C.c_int32), ("iwca2mp", _i32p), ("wca_nat", _f64p), ("coef_wca", _f64p),
+        ("ntst", C.c_int32), ("idtrna_tst2mp", _i32p), ("dtrna_tst_nat", _f64p),
+        ("coef_dtrna_tst", _f64p), ("idtrna_tst2side", _i32p), ("flg_tst_exclusive", _i32p),
     ]
 
 
@@ -106,8 +108,10 @@ _TOPO_ARRAYS = {
     "idtrna_hb2hbsite": np.int32, "nvalence_hbsite": np.int32,
     "ifene2mp": np.int32, "fene_nat": np.float64, "coef_fene": np.float64, "dist2_fene": np.float64,
     "iwca2mp": np.int32, "wca_nat": np.float64, "coef_wca": np.float64,
+    "idtrna_tst2mp": np.int32, "dtrna_tst_nat": np.float64, "coef_dtrna_tst": np.float64,
+    "idtrna_tst2side": np.int32, "flg_tst_exclusive": np.int32,
 }
-_TOPO_COUNTS = ("nmp", "nunit", "ncharge", "nbd", "nba", "nst", "nhb", "nhbsite", "nfene", "nwca")
+_TOPO_COUNTS = ("nmp", "nunit", "ncharge", "nbd", "nba", "nst", "nhb", "nhbsite", "nfene", "nwca", "ntst")
 
 
 def make_topology(sysd: dict):

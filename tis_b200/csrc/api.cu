@@ -114,6 +114,8 @@ struct tis_ctx {
   DBuf<int> u_lunit, u_class;
   DBuf<double> rneigh2;
   DBuf<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
+  DBuf<int> tst_idx, stx_ptr, stx_tst;
+  DBuf<double> tst_nat, tst_coef;
   DBuf<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   DBuf<double> lab_Td, lab_coef, lab_cdist, lab_beta, lab_rele2, lab_u0, lab_c1;
   DBuf<int> lab_u0off, lab_c1off, elabel;
@@ -294,6 +296,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   std::vector<double> st_hsTm_all;
+  std::vector<int> tst_idx, stx_ptr, stx_tst;
+  std::vector<double> tst_nat, tst_coef;
   std::vector<int> fene_idx, wca_idx, bdp;
   std::vector<int2> bde;
   std::vector<double> fene_cls, wca_cls;
@@ -312,16 +316,19 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     d.bd0 = (int)bd_nat.size(); d.nbd = t.nbd;
     d.ba0 = (int)ba_nat.size(); d.nba = t.nba;
     d.st0 = (int)(st_nat.size() / 3); d.nst = t.nst;
+    d.tst0 = (int)(tst_nat.size() / 6); d.ntst = t.ntst;
+    d.stx0 = (int)stx_ptr.size();
     d.hb0 = (int)(hb_nat.size() / 6); d.nhb = t.nhb;
     d.site0 = (int)site_val.size(); d.nsite = t.nhbsite;
     d.sitehb0 = (int)site_hb.size();
     d.inc0 = (int)inc_ptr.size();
     d.slot_ba = 2 * t.nbd;
     d.slot_st = d.slot_ba + 3 * t.nba;
-    d.slot_hb = d.slot_st + 7 * t.nst;
+    d.slot_tst = d.slot_st + 7 * t.nst;
+    d.slot_hb = d.slot_tst + 6 * t.ntst;
     d.nslot = d.slot_hb + 6 * t.nhb;
     maxN = std::max(maxN, t.nmp);
-    if (c->bdhi && (t.nbd || t.nba || t.nst || t.nhb)) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+    if (c->bdhi && (t.nbd || t.nba || t.nst || t.nhb || t.ntst)) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
     // FENE / WCA records (read_nativeinfo.F90:153-176, 306-332); per bead
     // incidence lists for the Brownian-HI force gather, FENE records first:
     // (partner bead, parameter class * 2 + kind), classes = the distinct
@@ -448,6 +455,42 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     append(st_nat, t.dtrna_st_nat, 3 * (size_t)t.nst);
     append(st_coef, t.coef_dtrna_st, 3 * (size_t)t.nst);
     append(st_hsTm_all, t.dtrna_st_hsTm, 3 * (size_t)t.nst);
+    // tertiary stacks; each side's secondary stack (mloop_dtrna.F90:74-140):
+    // the stack of base B with B - 3 (side 1) or B + 3 (side 2), exclusive
+    // only when that stack exists; per secondary stack the list of the
+    // tertiary stacks that can turn it off
+    {
+      std::vector<std::vector<int>> excl(t.nst);
+      for (int i = 0; i < 6 * t.ntst; ++i) {
+        if (t.idtrna_tst2mp[i] < 1 || t.idtrna_tst2mp[i] > t.nmp) { tis_destroy(c); return TIS_E_ARG; }
+        tst_idx.push_back(t.idtrna_tst2mp[i] - 1);
+      }
+      append(tst_nat, t.dtrna_tst_nat, 6 * (size_t)t.ntst);
+      append(tst_coef, t.coef_dtrna_tst, 7 * (size_t)t.ntst);
+      for (int itst = 0; itst < t.ntst; ++itst)
+        for (int sd = 0; sd < 2; ++sd) {
+          const int imp1 = t.idtrna_tst2mp[6 * itst + sd];
+          const int side = t.idtrna_tst2side[2 * itst + sd];
+          if (side != 1 && side != 2) { tis_destroy(c); return TIS_E_ARG; }
+          const int imp2 = side == 1 ? imp1 - 3 : imp1 + 3;
+          for (int ist = 0; ist < t.nst; ++ist) {
+            const int a1 = t.idtrna_st2mp[7 * ist], a2 = t.idtrna_st2mp[7 * ist + 1];
+            if ((imp1 == a1 && imp2 == a2) || (imp1 == a2 && imp2 == a1)) {
+              if (t.flg_tst_exclusive[2 * itst + sd]) excl[ist].push_back(itst);
+              break;
+            }
+          }
+        }
+      if (t.ntst > 0) {
+        int off = (int)stx_tst.size();
+        for (int ist = 0; ist < t.nst; ++ist) {
+          stx_ptr.push_back(off);
+          for (int e : excl[ist]) stx_tst.push_back(e);
+          off += (int)excl[ist].size();
+        }
+        stx_ptr.push_back(off);
+      }
+    }
     for (int i = 0; i < 6 * t.nhb; ++i) hb_idx.push_back(t.idtrna_hb2mp[i] - 1);
     append(hb_nat, t.dtrna_hb_nat, 6 * (size_t)t.nhb);
     append(hb_coef, t.coef_dtrna_hb, 7 * (size_t)t.nhb);
@@ -480,6 +523,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       for (int q2 = 0; q2 < 3; ++q2) inc[t.iba2mp[3 * b + q2] - 1].push_back(d.slot_ba + 3 * b + q2);
     for (int b = 0; b < t.nst; ++b)
       for (int q2 = 0; q2 < 7; ++q2) inc[t.idtrna_st2mp[7 * b + q2] - 1].push_back(d.slot_st + 7 * b + q2);
+    for (int b = 0; b < t.ntst; ++b)
+      for (int q2 = 0; q2 < 6; ++q2) inc[t.idtrna_tst2mp[6 * b + q2] - 1].push_back(d.slot_tst + 6 * b + q2);
     for (int b = 0; b < t.nhb; ++b)
       for (int q2 = 0; q2 < 6; ++q2) inc[t.idtrna_hb2mp[6 * b + q2] - 1].push_back(d.slot_hb + 6 * b + q2);
     int ip = (int)inc_slot.size();
@@ -630,6 +675,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->bd_idx.upload(bd_idx)); CK(c->bd_nat.upload(bd_nat)); CK(c->bd_coef.upload(bd_coef));
   CK(c->ba_idx.upload(ba_idx)); CK(c->ba_nat.upload(ba_nat)); CK(c->ba_coef.upload(ba_coef));
   CK(c->st_idx.upload(st_idx)); CK(c->st_nat.upload(st_nat)); CK(c->st_coef.upload(st_coef));
+  CK(c->tst_idx.upload(tst_idx)); CK(c->tst_nat.upload(tst_nat)); CK(c->tst_coef.upload(tst_coef));
+  CK(c->stx_ptr.upload(stx_ptr)); CK(c->stx_tst.upload(stx_tst));
   CK(c->hb_idx.upload(hb_idx)); CK(c->hb_nat.upload(hb_nat)); CK(c->hb_coef.upload(hb_coef));
   CK(c->hb_site.upload(hb_site)); CK(c->hb_nd2.upload(hb_nd2));
   CK(c->site_val.upload(site_val)); CK(c->site_ptr.upload(site_ptr)); CK(c->site_hb.upload(site_hb));
@@ -727,6 +774,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->b_c2.free(); c->b_c3.free(); c->b_c4.free(); c->b_screen.free();
   c->u_lunit.free(); c->u_class.free(); c->rneigh2.free();
   c->bd_idx.free(); c->ba_idx.free(); c->st_idx.free(); c->hb_idx.free(); c->hb_site.free();
+  c->tst_idx.free(); c->tst_nat.free(); c->tst_coef.free(); c->stx_ptr.free(); c->stx_tst.free();
   c->site_val.free(); c->site_ptr.free(); c->site_hb.free(); c->inc_ptr.free(); c->inc_slot.free();
   c->q_bead.free();
   c->bd_nat.free(); c->bd_coef.free(); c->ba_nat.free(); c->ba_coef.free(); c->st_nat.free(); c->st_coef.free();
@@ -870,6 +918,8 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.bd_idx = c->bd_idx.p; a.bd_nat = c->bd_nat.p; a.bd_coef = c->bd_coef.p;
   a.ba_idx = c->ba_idx.p; a.ba_nat = c->ba_nat.p; a.ba_coef = c->ba_coef.p;
   a.st_idx = c->st_idx.p; a.st_nat = c->st_nat.p; a.st_coef = c->st_coef.p;
+  a.tst_idx = c->tst_idx.p; a.tst_nat = c->tst_nat.p; a.tst_coef = c->tst_coef.p;
+  a.stx_ptr = c->stx_ptr.p; a.stx_tst = c->stx_tst.p;
   a.hb_idx = c->hb_idx.p; a.hb_nat = c->hb_nat.p; a.hb_coef = c->hb_coef.p; a.hb_site = c->hb_site.p;
   a.hb_nd2 = c->hb_nd2.p;
   a.site_val = c->site_val.p; a.site_ptr = c->site_ptr.p; a.site_hb = c->site_hb.p;

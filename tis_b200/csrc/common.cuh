@@ -29,6 +29,8 @@ struct TopDesc {
   int bd0, nbd;
   int ba0, nba;
   int st0, nst;
+  int tst0, ntst;   // tertiary stacks
+  int stx0;         // per secondary stack: stx_ptr[stx0 + k] .. (+1) -> tertiary stacks that can disable it
   int hb0, nhb;
   int site0, nsite;
   int sitehb0;      // CSR of hbonds per site: site_ptr[site0 + s] .. (+1), entries at sitehb0
@@ -38,8 +40,8 @@ struct TopDesc {
   int fe0, nfe;     // FENE records
   int wc0, nwc;     // WCA records
   int bp0, be0;     // Brownian-HI force incidence: bd_ptr[bp0 .. bp0 + nmp], entries from bd_ent[be0]
-  int nslot;        // 2 nbd + 3 nba + 7 nst + 6 nhb
-  int slot_ba, slot_st, slot_hb;   // slot bases inside a lane (bonds start at 0)
+  int nslot;        // 2 nbd + 3 nba + 7 nst + 6 ntst + 6 nhb
+  int slot_ba, slot_st, slot_tst, slot_hb;   // slot bases inside a lane (bonds start at 0)
   int nlabel;       // labels that belong to this topology
 };
 
@@ -151,6 +153,8 @@ struct KArgs {
   const int *bd_idx; const double *bd_nat, *bd_coef;
   const int *ba_idx; const double *ba_nat, *ba_coef;
   const int *st_idx; const double *st_nat, *st_coef;
+  const int *tst_idx; const double *tst_nat, *tst_coef;   // tertiary stacks: 6 beads, 6 natives, U0 + 6 coefs
+  const int *stx_ptr, *stx_tst;    // secondary stack -> exclusive tertiary stacks (topology-local index)
   const int *hb_idx; const double *hb_nat, *hb_coef; const int *hb_site; const double *hb_nd2;
   const int *site_val; const int *site_ptr; const int *site_hb;
   const int *inc_ptr; const int *inc_slot;

@@ -339,10 +339,147 @@ __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   put_slot<Real>(slots, sb + 2, m[2], f32.x, f32.y, f32.z);
 }
 
-// force_dtrna_stack.F90:54-165
+// st_status of secondary stack k (force_dtrna_stack_nlocal.F90:83-92): off
+// when an exclusive tertiary stack of it is within 10 A of its native
+// distance; FP64 in the reference's operation order, so the decision is the
+// reference's
+template <typename Real>
+__device__ __forceinline__ bool stack_excluded(const KArgs &a, const TopDesc &T, const Smem<Real> &s, int k) {
+  if (T.ntst == 0) return false;
+  for (int e = a.stx_ptr[T.stx0 + k]; e < a.stx_ptr[T.stx0 + k + 1]; ++e) {
+    const int t = a.stx_tst[e];
+    const int *m = a.tst_idx + 6 * (size_t)(T.tst0 + t);
+    double v0 = s.PX[m[0]] - s.PX[m[1]], v1 = s.PY[m[0]] - s.PY[m[1]], v2 = s.PZ[m[0]] - s.PZ[m[1]];
+    if (a.periodic) { pb1(v0, a.psize[0], a.psizeh[0]); pb1(v1, a.psize[1], a.psizeh[1]); pb1(v2, a.psize[2], a.psizeh[2]); }
+    const double d = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(v0, v0), __dmul_rn(v1, v1)), __dmul_rn(v2, v2))) -
+                     a.tst_nat[6 * (size_t)(T.tst0 + t)];
+    if (d < 10.0) return true;
+  }
+  return false;
+}
+
+// force_dtrna_stack_nlocal.F90:60-263: tertiary stack k into its six slots
+template <typename Real>
+__device__ void term_tstack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
+  const int *m = a.tst_idx + 6 * (size_t)(T.tst0 + k);
+  const double *nat = a.tst_nat + 6 * (size_t)(T.tst0 + k);
+  const double *cf = a.tst_coef + 7 * (size_t)(T.tst0 + k);
+  auto dv = [&](int p, int q) {   // x_p - x_q (pxyz + minimum image when periodic)
+    double w0 = s.PX[m[p]] - s.PX[m[q]], w1 = s.PY[m[p]] - s.PY[m[q]], w2 = s.PZ[m[p]] - s.PZ[m[q]];
+    if (a.periodic) { pb1(w0, a.psize[0], a.psizeh[0]); pb1(w1, a.psize[1], a.psizeh[1]); pb1(w2, a.psize[2], a.psizeh[2]); }
+    return R3<Real>{(Real)w0, (Real)w1, (Real)w2};
+  };
+  const R3<Real> v12 = dv(0, 1), v13 = dv(0, 2), v53 = dv(4, 2), v42 = dv(3, 1), v46 = dv(3, 5);
+  const Real d1212 = dot(v12, v12), d1313 = dot(v13, v13), d4242 = dot(v42, v42);
+  const Real a12 = sqrt(d1212), a13 = sqrt(d1313), a42 = sqrt(d4242);
+  const Real d1213 = dot(v13, v12), d1242 = dot(v12, v42), d4246 = dot(v42, v46), d1353 = dot(v13, v53);
+  const Real o1213_1212 = fdiv(d1213, d1212), o1213_1313 = fdiv(d1213, d1313);
+  const Real o1242_1212 = fdiv(d1242, d1212), o4246_4242 = fdiv(d4246, d4242);
+  const Real o1242_4242 = fdiv(d1242, d4242), o1353_1313 = fdiv(d1353, d1313);
+  Real fr[6][3];
+  Real ediv = 1;
+  // distance 1=2
+  Real d = a12 - (Real)nat[0];
+  ediv += (Real)cf[1] * d * d;
+  {
+    const Real g = fdiv((Real)2 * (Real)cf[1] * d, a12);
+    fr[0][0] = g * v12.x; fr[0][1] = g * v12.y; fr[0][2] = g * v12.z;
+    fr[1][0] = -fr[0][0]; fr[1][1] = -fr[0][1]; fr[1][2] = -fr[0][2];
+  }
+  const Real v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) { fr[2][q] = 0; fr[3][q] = 0; fr[4][q] = 0; fr[5][q] = 0; }
+  // angle 3-1=2
+  {
+    Real co = fdiv(d1213, a13 * a12);
+    co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
+    d = acos(co) - (Real)nat[1];
+    const Real pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const Real fi = pre * (v12a[q] - o1213_1313 * v13a[q]), fk = pre * (v13a[q] - o1213_1212 * v12a[q]);
+      fr[2][q] += fi; fr[1][q] += fk; fr[0][q] -= fi + fk;
+    }
+    ediv += (Real)cf[2] * d * d;
+  }
+  // angle 1=2-4
+  {
+    Real co = fdiv(d1242, a12 * a42);
+    co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
+    d = acos(co) - (Real)nat[2];
+    const Real pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const Real fi = -pre * (v42a[q] - o1242_1212 * v12a[q]), fk = -pre * (v12a[q] - o1242_4242 * v42a[q]);
+      fr[0][q] += fi; fr[3][q] += fk; fr[1][q] -= fi + fk;
+    }
+    ediv += (Real)cf[3] * d * d;
+  }
+  // dihedral 4-2=1=3
+  const R3<Real> c4212 = crs(v42, v12), c1213 = crs(v12, v13);
+  const Real c4212_2 = dot(c4212, c4212), c1213_2 = dot(c1213, c1213);
+  {
+    d = wrap_pi(atan2(dot(v42, c1213) * a12, dot(c4212, c1213)) - (Real)nat[3]);
+    ediv += (Real)cf[4] * d * d;
+    const Real pre = (Real)2 * (Real)cf[4] * d * a12;
+    const Real gi = fdiv(pre, c4212_2), gl = -fdiv(pre, c1213_2);
+    const Real fi[3] = {gi * c4212.x, gi * c4212.y, gi * c4212.z}, fl[3] = {gl * c1213.x, gl * c1213.y, gl * c1213.z};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      fr[3][q] += fi[q];
+      fr[1][q] += ((Real)-1 + o1242_1212) * fi[q] - o1213_1212 * fl[q];
+      fr[0][q] += ((Real)-1 + o1213_1212) * fl[q] - o1242_1212 * fi[q];
+      fr[2][q] += fl[q];
+    }
+  }
+  // dihedral 5-3-1=2
+  {
+    const R3<Real> mm = crs(v53, v13), nn{-c1213.x, -c1213.y, -c1213.z};
+    d = wrap_pi(atan2(dot(v53, nn) * a13, dot(mm, nn)) - (Real)nat[4]);
+    ediv += (Real)cf[5] * d * d;
+    const Real pre = (Real)2 * (Real)cf[5] * d * a13;
+    const Real gi = fdiv(pre, dot(mm, mm)), gl = -fdiv(pre, c1213_2);
+    const Real fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      fr[4][q] += fi[q];
+      fr[2][q] += ((Real)-1 + o1353_1313) * fi[q] - o1213_1313 * fl[q];
+      fr[0][q] += ((Real)-1 + o1213_1313) * fl[q] - o1353_1313 * fi[q];
+      fr[1][q] += fl[q];
+    }
+  }
+  // dihedral 1=2-4-6
+  {
+    const R3<Real> mm{-c4212.x, -c4212.y, -c4212.z}, nn = crs(v42, v46);
+    d = wrap_pi(atan2(dot(v12, nn) * a42, dot(mm, nn)) - (Real)nat[5]);
+    ediv += (Real)cf[6] * d * d;
+    const Real pre = (Real)2 * (Real)cf[6] * d * a42;
+    const Real gi = fdiv(pre, c4212_2), gl = -fdiv(pre, dot(nn, nn));
+    const Real fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      fr[0][q] += fi[q];
+      fr[1][q] += ((Real)-1 + o1242_4242) * fi[q] - o4246_4242 * fl[q];
+      fr[3][q] += ((Real)-1 + o4246_4242) * fl[q] - o1242_4242 * fi[q];
+      fr[5][q] += fl[q];
+    }
+  }
+  const Real pre = (Real)(cf[0] / ((double)ediv * (double)ediv));
+  const size_t sb = T.slot_tst + 6 * (size_t)k;
+#pragma unroll
+  for (int p = 0; p < 6; ++p) put_slot<Real>(slots, sb + p, m[p], pre * fr[p][0], pre * fr[p][1], pre * fr[p][2]);
+}
+
+// force_dtrna_stack.F90:54-165 (skipped when st_status is off)
 template <typename Real>
 __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, double u0) {
   const int *m = a.st_idx + 7 * (size_t)(T.st0 + k);
+  if (stack_excluded<Real>(a, T, s, k)) {
+    const size_t sb = T.slot_st + 7 * (size_t)k;
+#pragma unroll
+    for (int p = 0; p < 7; ++p) put_slot<Real>(slots, sb + p, m[p], 0, 0, 0);
+    return;
+  }
   const double *nat = a.st_nat + 3 * (size_t)(T.st0 + k);
   const double *cf = a.st_coef + 3 * (size_t)(T.st0 + k);
   R3<Real> v21 = dvec(s, m[0], m[1]);

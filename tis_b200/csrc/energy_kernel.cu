@@ -5,7 +5,8 @@
 // =====================================================================
 // energy_sumup (src/energy_sumup.F90:11-530) for one lane per CTA, FP64.
 // Terms follow the energy twins: energy_bond, energy_bangle (via
-// util_bondangle), energy_dtrna_stack, energy_dtrna_hbond15, energy_exv_dt15,
+// util_bondangle), energy_dtrna_stack, energy_dtrna_stack_nlocal,
+// energy_dtrna_hbond15, energy_exv_dt15,
 // energy_ele_DH and energy_kinetic.  Sums are reduced in a fixed order.
 // =====================================================================
 namespace tis {
@@ -24,7 +25,7 @@ __device__ __forceinline__ double wrapd(double d) {
   return d;
 }
 
-enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_N };
+enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_TST, ES_N };
 
 __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
@@ -88,9 +89,52 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     double dba = acos(co) - a.ba_nat[T.ba0 + k];
     es[ES_ANGLE] += a.ba_coef[T.ba0 + k] * (dba * dba);
   }
+  // energy_dtrna_stack_nlocal.F90:106-232: U0 / ediv of every tertiary stack
+  auto tdv = [&](const int *m, int p, int q) {   // x_p - x_q (pxyz + minimum image when periodic)
+    double3 u = sub3(gpos(a.periodic ? P : X, m[p]), gpos(a.periodic ? P : X, m[q]));
+    if (a.periodic) { pb1(u.x, a.psize[0], a.psizeh[0]); pb1(u.y, a.psize[1], a.psizeh[1]); pb1(u.z, a.psize[2], a.psizeh[2]); }
+    return u;
+  };
+  for (int k = tid; k < T.ntst; k += nth) {
+    const int *m = a.tst_idx + 6 * (size_t)(T.tst0 + k);
+    const double *nat = a.tst_nat + 6 * (size_t)(T.tst0 + k);
+    const double *cf = a.tst_coef + 7 * (size_t)(T.tst0 + k);
+    const double3 v12 = tdv(m, 0, 1), v13 = tdv(m, 0, 2), v53 = tdv(m, 4, 2), v42 = tdv(m, 3, 1), v46 = tdv(m, 3, 5);
+    const double d1212 = dot3(v12, v12), d1313 = dot3(v13, v13), d4242 = dot3(v42, v42);
+    const double a12 = sqrt(d1212), a13 = sqrt(d1313), a42 = sqrt(d4242);
+    double ediv = 1.0;
+    double d = a12 - nat[0];
+    ediv += cf[1] * d * d;
+    d = acos(dot3(v13, v12) / (a13 * a12)) - nat[1];
+    ediv += cf[2] * d * d;
+    d = acos(dot3(v12, v42) / (a12 * a42)) - nat[2];
+    ediv += cf[3] * d * d;
+    const double3 c4212 = cross3(v42, v12), c1213 = cross3(v12, v13);
+    d = wrapd(atan2(dot3(v42, c1213) * sqrt(d1212), dot3(c4212, c1213)) - nat[3]);
+    ediv += cf[4] * d * d;
+    const double3 n1 = make_double3(-c1213.x, -c1213.y, -c1213.z);
+    d = wrapd(atan2(dot3(v53, n1) * a13, dot3(cross3(v53, v13), n1)) - nat[4]);
+    ediv += cf[5] * d * d;
+    const double3 m2 = make_double3(-c4212.x, -c4212.y, -c4212.z), n2 = cross3(v42, v46);
+    d = wrapd(atan2(dot3(v12, n2) * a42, dot3(m2, n2)) - nat[5]);
+    ediv += cf[6] * d * d;
+    es[ES_TST] += cf[0] / ediv;
+  }
   const double *u0 = a.lab_u0 + a.lab_u0off[label];
   for (int k = tid; k < T.nst; k += nth) {
     const int *m = a.st_idx + 7 * (size_t)(T.st0 + k);
+    // st_status (energy_dtrna_stack_nlocal.F90:121-129): an exclusive
+    // tertiary stack within 10 A of its native distance turns the stack off
+    bool off = false;
+    for (int e = (T.ntst ? a.stx_ptr[T.stx0 + k] : 0); e < (T.ntst ? a.stx_ptr[T.stx0 + k + 1] : 0); ++e) {
+      const int t = a.stx_tst[e];
+      const int *mt = a.tst_idx + 6 * (size_t)(T.tst0 + t);
+      const double3 u = tdv(mt, 0, 1);
+      const double dd = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(u.y, u.y)), __dmul_rn(u.z, u.z))) -
+                        a.tst_nat[6 * (size_t)(T.tst0 + t)];
+      if (dd < 10.0) off = true;
+    }
+    if (off) continue;
     const double *nat = a.st_nat + 3 * (size_t)(T.st0 + k);
     const double *cf = a.st_coef + 3 * (size_t)(T.st0 + k);
     double3 v21 = sub3(gpos(X, m[1]), gpos(X, m[0])), v34 = sub3(gpos(X, m[2]), gpos(X, m[3]));
@@ -252,6 +296,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     E[17] = tot[ES_EXV];
     E[22] = tot[ES_WREP];
     E[23] = tot[ES_WATT];
+    E[18] = tot[ES_TST];
     double sum = 0.0;
     for (int k = 2; k < N_ETYPE; ++k) sum += E[k];
     E[0] = sum;

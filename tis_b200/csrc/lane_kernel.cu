@@ -274,7 +274,7 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
 }
 
 // Phase 1 runs every interaction-level item in one balanced sweep: stacks,
-// Debye-Hueckel chunks (force_ele_DH.F90:72-117 over a word range of one
+// tertiary stacks, Debye-Hueckel chunks (force_ele_DH.F90:72-117 over a word range of one
 // charged bead's ele row, summed by one thread into ch_part), angles,
 // hbonds, bonds.  Phase 2 gives each bead a group of GA
 // threads that sums its exv pairs, its bonded slots and its Debye-Hueckel
@@ -298,7 +298,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
   int nclamp = 0;
   // (site counters and MISC_EXCESS were cleared by the caller before its barrier)
-  const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd;
+  const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd, ntst = T.ntst;
   const ChunkGeo geo = chunk_geo(NQ, W);
   const int nch = (a.i_ele != 0) ? geo.nch : 0;
   const int k_st = nhb, k_ch = k_st + nst, k_ba = k_ch + nch, k_bd = k_ba + nba, total = k_bd + nbd;
@@ -325,16 +325,20 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // may follow is serial), the rows of the own charged beads, and halves of
   // the stacks, angles and bonds
   int hb_0 = 0, hb_1 = nhb, st_0 = 0, st_1 = nst, ch_0 = 0, ch_1 = nch, ba_0 = 0, ba_1 = nba, bd_0 = 0, bd_1 = nbd;
+  int ts_0 = 0, ts_1 = ntst;
   if (CL == 2) {
     if (cu.rank == 1) hb_1 = 0;
     st_0 = cu.rank ? nst / 2 : 0; st_1 = cu.rank ? nst : nst / 2;
+    ts_0 = cu.rank ? ntst / 2 : 0; ts_1 = cu.rank ? ntst : ntst / 2;
     ba_0 = cu.rank ? nba / 2 : 0; ba_1 = cu.rank ? nba : nba / 2;
     bd_0 = cu.rank ? nbd / 2 : 0; bd_1 = cu.rank ? nbd : nbd / 2;
     ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
   }
   // chunk ranges, kinds in decreasing cost per chunk (measured on B200):
-  // stacks, Debye-Hueckel row chunks, angles, hbonds, bonds, then noise
-  const int c_ch = (st_1 - st_0 + 31) >> 5, c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
+  // stacks, tertiary stacks, Debye-Hueckel row chunks, angles, hbonds,
+  // bonds, then noise
+  const int c_ts = (st_1 - st_0 + 31) >> 5, c_ch = c_ts + ((ts_1 - ts_0 + 31) >> 5);
+  const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
   const int c_hb = c_ba + ((ba_1 - ba_0 + 31) >> 5), c_bd = c_hb + ((hb_1 - hb_0 + 31) >> 5);
   const int c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
   // the sink's Gaussian noise of the own beads, drawn here where warps have slack
@@ -378,10 +382,14 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         }
         hbf[h] = f;
       }
-    } else if (c < c_ch) {
+    } else if (c < c_ts) {
       kind = 1;
       const int k = st_0 + (c << 5) + lid;
       if (k < st_1) term_stack<Real>(a, T, s, slots, k, u0[k]);
+    } else if (c < c_ch) {
+      kind = 1;
+      const int k = ts_0 + ((c - c_ts) << 5) + lid;
+      if (k < ts_1) term_tstack<Real>(a, T, s, slots, k);
     } else if (c < c_ba) {
       kind = 2;
       const int cc = ch_0 + ((c - c_ch) << 5) + lid;

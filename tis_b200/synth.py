@@ -556,6 +556,63 @@ def hairpin_coords(sysd: dict, stem: int, seed: int = 0, D: float = 15.2, dx: fl
     return sysd
 
 
+def _tst_geometry(x, m):
+    """Distance, 2 angles and 3 dihedrals of one tertiary stack (beads m,
+    0-based B1 B2 S1 S2 P1' P2') as energy_dtrna_stack_nlocal.F90 defines them."""
+    v12, v13, v53, v42, v46 = x[m[0]] - x[m[1]], x[m[0]] - x[m[2]], x[m[4]] - x[m[2]], x[m[3]] - x[m[1]], x[m[3]] - x[m[5]]
+    a12, a13, a42 = (np.linalg.norm(v) for v in (v12, v13, v42))
+    t1 = np.arccos(np.dot(v13, v12) / (a13 * a12))
+    t2 = np.arccos(np.dot(v12, v42) / (a12 * a42))
+    c4212, c1213 = np.cross(v42, v12), np.cross(v12, v13)
+    p0 = np.arctan2(np.dot(v42, c1213) * a12, np.dot(c4212, c1213))
+    n1 = -c1213
+    p1 = np.arctan2(np.dot(v53, n1) * a13, np.dot(np.cross(v53, v13), n1))
+    m2, n2 = -c4212, np.cross(v42, v46)
+    p2 = np.arctan2(np.dot(v12, n2) * a42, np.dot(m2, n2))
+    return np.array([a12, t1, t2, p0, p1, p2])
+
+
+def add_tertiary_stacks(sysd: dict, pairs, sides, exclusive, seed: int = 0, dist_shift=None,
+                        u0: float = -5.0, coef=(5.0, 1.5, 1.5, 0.15, 0.15, 0.15)):
+    """Appends tertiary stacks (tbs-dist/-angl/-dihd records) between the
+    bases of nucleotides (i, j) of a dt15_chain: beads B_i, B_j, S_i, S_j,
+    P_{i+1}, P_{j+1} (read_nativeinfo.F90:666-671).  Natural values are the
+    current geometry plus small seeded offsets; dist_shift[k], when given,
+    is added to record k's natural distance (a large negative shift puts the
+    stack more than 10 A from native, so it excludes nothing).  sides[k] =
+    (side of B_i, side of B_j): 1 = its stack with B - 3, 2 = with B + 3;
+    exclusive[k] = (flag, flag)."""
+    rng = np.random.default_rng(seed)
+    s = dict(sysd)
+    x = np.asarray(s["xyz"], dtype=np.float64)
+    idx, nat = [], []
+    for k, (i, j) in enumerate(pairs):
+        bi, bj = _bead_index(i, "B"), _bead_index(j, "B")
+        m = (bi, bj, bi - 1, bj - 1, bi + 1, bj + 1)
+        g = _tst_geometry(x, [b - 1 for b in m])
+        g = g + rng.uniform(-1.0, 1.0, size=6) * np.array([0.2, 0.05, 0.05, 0.1, 0.1, 0.1])
+        if dist_shift is not None:
+            g[0] += dist_shift[k]
+        idx.append(m)
+        nat.append(g)
+    s["ntst"] = len(pairs)
+    s["idtrna_tst2mp"] = np.array(idx, dtype=np.int32).reshape(-1, 6)
+    s["dtrna_tst_nat"] = np.array(nat).reshape(-1, 6)
+    s["coef_dtrna_tst"] = np.tile(np.array((u0,) + tuple(coef)), (len(pairs), 1))
+    s["idtrna_tst2side"] = np.array(sides, dtype=np.int32).reshape(-1, 2)
+    s["flg_tst_exclusive"] = np.array(exclusive, dtype=np.int32).reshape(-1, 2)
+    return s
+
+
+def hairpin_tertiary(seed: int = 1):
+    """22-nt hairpin with three tertiary stacks across the stem: two within
+    10 A of their native distance (their exclusive sides turn secondary
+    stacks off), one 15 A short of it (excludes nothing)."""
+    s = hairpin_coords(set_friction(dt15_chain(22, seed, stem=6), 0.5), 6, seed=seed)
+    return add_tertiary_stacks(s, [(3, 19), (5, 17), (8, 14)], sides=[(2, 1), (1, 2), (2, 2)],
+                               exclusive=[(1, 1), (1, 0), (1, 1)], seed=seed + 2, dist_shift=[0.0, 0.0, -15.0])
+
+
 def duplicate_hbonds(sysd: dict, seed: int = 0, shift: float = 0.3):
     """Appends a second record for every hydrogen bond (same beads and sites,
     shifted natural values), so every hbond site is over its valence and the
