@@ -324,7 +324,7 @@ def run_ours(args, rank, world, local_rank):
     def period():
         eng.step(period_len)
         if remd:
-            eng.replica_exchange()
+            eng.replica_exchange(count=False)
 
     for _ in range(args.warmup):
         period()

@@ -174,6 +174,29 @@ def test_replica_exchange(tis_lib):
     assert np.abs(v - vr.reshape(-1, 3)).max() < 1e-8
 
 
+def test_replica_exchange_without_host_wait(tis_lib):
+    """Exchanges that do not ask for the accept count stay on the device
+    (counter-based uniforms, no host wait): labels and velocities equal those
+    of the same run that reads the count after every exchange."""
+    nrep = 8
+    temps = synth.temperature_ladder(nrep, 280.0, 400.0)
+    runs = []
+    for count in (True, False):
+        s, par, eng, orc = make_pair("hairpin", 1, nrep=nrep, temps=temps)
+        eng.time_integral_pre()
+        nacc = 0
+        for k in range(6):
+            eng.step(20)
+            r = eng.replica_exchange(count=count)
+            nacc += r or 0
+        x, v, _ = eng.get_state()
+        runs.append((eng.labels(), v, nacc))
+        eng.close()
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert runs[0][2] > 0   # the ladder makes some swaps happen
+
+
 def test_uneven_batch(tis_lib):
     systems = [synth.set_friction(synth.dt15_chain(n, 100 + n, hb_fraction=0.3), 0.5) for n in (9, 23, 41)]
     par = synth.dt15_params(ionic_strength=0.15, precision=1)

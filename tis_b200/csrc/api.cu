@@ -30,6 +30,11 @@ cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, con
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
+                       double *ebeta);
+cudaError_t rex_exchange_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep,
+                                const double *e_own, const double *e_opp, const double *u, double *scale,
+                                double *velo);
 cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool forces);
 cudaError_t ewald_energy_launch(cudaStream_t st, const KArgs &a);
 cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int *items, const int *koff);
@@ -120,6 +125,9 @@ struct tis_ctx {
   DBuf<double> lab_Td, lab_coef, lab_cdist, lab_beta, lab_rele2, lab_u0, lab_c1;
   DBuf<int> lab_u0off, lab_c1off, elabel;
   DBuf<double> xyz, pxyz, velo, accel, dxyz, p0xyz, out_force, out_energy, scale, ebeta;
+  DBuf<double> e_opp, rex_u;         // partner energies and injected uniforms of an exchange
+  DBuf<int> d_rep2lab, d_lab2rep;    // label maps (the device copy is authoritative)
+  DBuf<RexState> rex;
   unsigned long long rex_counter = 0;
   DBuf<uint32_t> mask;
   DBuf<int> site_exc;
@@ -696,6 +704,18 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->scale.alloc(nlane));
   CK(c->ebeta.alloc(nlane));
   CK(c->elabel.alloc(nlane));
+  CK(c->e_opp.alloc((size_t)nlane * N_ETYPE));
+  CK(c->rex_u.alloc((size_t)nlane / 2 + 1));
+  CK(c->d_rep2lab.upload(c->rep2lab));
+  CK(c->d_lab2rep.upload(c->lab2rep));
+  {
+    RexState r0{};
+    r0.beta_global = c->beta_global;
+    r0.counter = 0;
+    r0.idx_pair = 1;
+    r0.nacc = 0;
+    CK(c->rex.upload(std::vector<RexState>{r0}));
+  }
   CK(c->mask.alloc(mask_off));
   CK(cudaMemset(c->mask.p, 0, std::max<size_t>(mask_off, 1) * sizeof(uint32_t)));
   CK(c->mirror.alloc(periodic ? (size_t)mirror_off : 1));
@@ -781,7 +801,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free();
   c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
   c->lab_u0.free(); c->lab_c1.free(); c->lab_u0off.free(); c->lab_c1off.free(); c->elabel.free();
-  c->ebeta.free();
+  c->ebeta.free(); c->e_opp.free(); c->rex_u.free(); c->d_rep2lab.free(); c->d_lab2rep.free(); c->rex.free();
   c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free(); c->p0xyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
@@ -908,6 +928,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.max_abscos = std::cos((double)(0.57f / 180.0f) * F_PI);
   a.tstep = p.tstep; a.tstep2 = 0.5e0 * p.tstep * p.tstep; a.tsteph = 0.5e0 * p.tstep;
   a.beta_hbond15 = c->beta_global;
+  a.rex = c->rex.p;
   a.hb_beta_global = p.hb_beta_global;
   a.seed = p.seed;
   a.tops = c->d_tops.p; a.lanes = c->d_lanes.p; a.lstate = c->d_lstate.p;
@@ -1247,83 +1268,67 @@ extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_acce
   if (!c) return TIS_E_ARG;
   if (c->ntop != 1) return fail(c, TIS_E_UNSUPPORTED, "replica exchange needs one topology");
   const int n = c->nlane;
-  auto pair_of = [&](int l) -> int {   // 1-based labels, exchange_pair_tb (one dimension)
-    if (c->idx_pair == 1) { if (l % 2 == 1) return (l + 1 <= n) ? l + 1 : 0; return l - 1; }
-    if (l == 1) return 0;
-    if (l % 2 == 0) return (l + 1 <= n) ? l + 1 : 0;
-    return l - 1;
-  };
-  std::vector<double> E_own, E_opp;
-  int rc = run_energy(c, -1, nullptr, c->hb_energy_valid, c->beta_global, E_own);
-  if (rc < 0) return rc;
-  std::vector<int> opp(n, -1);
-  for (int r = 0; r < n; ++r) {
-    int lo = pair_of(c->rep2lab[r] + 1);
-    opp[r] = (lo == 0) ? -1 : lo - 1;
-  }
-  // partner energies: recomputed hbonds, beta of the partner label
-  // (energy_allrep.F90:134,209-216); lanes without a partner are skipped.
-  {
-    std::vector<int> lab(n, -1);
-    std::vector<double> beta(n, c->beta_global);
-    for (int r = 0; r < n; ++r)
-      if (opp[r] >= 0) { lab[r] = opp[r]; beta[r] = 1.0e0 / (c->lab_T[opp[r]] * BOLTZ_KCAL_MOL); }
-    rc = run_energy(c, -1, lab.data(), false, c->beta_global, E_opp, beta.data());
+  // own energies (hbond energies of the last force call reused when valid),
+  // then the energies at the partner labels with the partner's beta for the
+  // recomputed hbonds (energy_allrep.F90:134,209-216); lanes without a
+  // partner are not used
+  KArgs a = make_args(c, 0, 0, -1);
+  a.reuse_hb = c->hb_energy_valid ? 1 : 0;
+  a.elabel = nullptr;
+  a.ebeta_lane = nullptr;
+  a.out_energy = c->out_energy.p;
+  ++c->launches;
+  CK(energy_kernel_launch(n, c->stream, a));
+  if (c->par.i_ele == TIS_ELE_EWALD) {
+    int rc = ewald_recip(c, a, false);
     if (rc < 0) return rc;
-    for (int r = 0; r < n; ++r)
-      if (opp[r] < 0) for (int k = 0; k < N_ETYPE; ++k) E_opp[(size_t)r * N_ETYPE + k] = 0.0;
+    ++c->launches;
+    CK(ewald_energy_launch(c->stream, a));
+  }
+  ++c->launches;
+  CK(rex_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->elabel.p, c->ebeta.p));
+  KArgs b = a;
+  b.reuse_hb = 0;
+  b.elabel = c->elabel.p;
+  b.ebeta_lane = c->ebeta.p;
+  b.out_energy = c->e_opp.p;
+  ++c->launches;
+  CK(energy_kernel_launch(n, c->stream, b));
+  if (c->par.i_ele == TIS_ELE_EWALD) {
+    int rc = ewald_recip(c, b, false);
+    if (rc < 0) return rc;
+    ++c->launches;
+    CK(ewald_energy_launch(c->stream, b));
   }
   c->hb_energy_valid = false;
-  int nrand = 0, nacc = 0;
-  std::vector<double> scale(n, 0.0);
-  std::vector<double> ubuf;
-  if (!u) {
-    ubuf.resize((n + 1) / 2);
-    for (auto &x : ubuf) {
-      unsigned long long ctr = c->rex_counter++;
-      U4 o = philox4x32(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x52454D44u, 0u}, (uint32_t)c->par.seed, (uint32_t)(c->par.seed >> 32));
-      x = u01_open0(o.x) - 2.3283064365386963e-10;   // [0, 1)
-    }
-    u = ubuf.data();
-  }
-  for (int li = 1; li <= n; ++li) {
-    int lj = pair_of(li);
-    if (lj < li) continue;
-    nrand++;
-    int ri = c->lab2rep[li - 1], rj = c->lab2rep[lj - 1];
-    double tm = c->lab_T[li - 1], tn = c->lab_T[lj - 1];
-    double pim = E_own[(size_t)ri * N_ETYPE], pin = E_opp[(size_t)ri * N_ETYPE];
-    double pjn = E_own[(size_t)rj * N_ETYPE], pjm = E_opp[(size_t)rj * N_ETYPE];
-    double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / BOLTZ_KCAL_MOL;
-    bool acc = delta < 0.0e0 || u[nrand - 1] <= std::exp(-delta);
-    if (acc) {
-      c->rep2lab[ri] = lj - 1; c->rep2lab[rj] = li - 1;
-      c->lab2rep[li - 1] = rj; c->lab2rep[lj - 1] = ri;
-      double sf = std::sqrt(tn / tm);
-      scale[ri] = sf;
-      scale[rj] = -sf;
-      nacc++;
-    }
-  }
+  // the pair alternation does not depend on the decisions, so the host
+  // knows this exchange's pair count without reading the device state
+  const int npair = (c->idx_pair == 1) ? n / 2 : (n - 1) / 2;
   c->idx_pair = (c->idx_pair == 2) ? 1 : c->idx_pair + 1;
-  // simu_para2: beta_hbond15 of the last replica's label
-  c->beta_global = 1.0e0 / (c->lab_T[c->rep2lab[n - 1]] * BOLTZ_KCAL_MOL);
-  CK(cudaMemcpyAsync(c->scale.p, scale.data(), n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const double *du = nullptr;
+  if (u) {
+    if (npair > 0)
+      CK(cudaMemcpyAsync(c->rex_u.p, u, (size_t)npair * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    du = c->rex_u.p;
+  }
   ++c->launches;
-  CK(scale_velo_launch(n, c->stream, c->velo.p, c->d_lanes.p, c->d_tops.p, c->scale.p));
-  std::vector<LaneState> ls(n);
-  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, n * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  for (int r = 0; r < n; ++r) ls[r].label = c->rep2lab[r];
-  CK(cudaMemcpyAsync(c->d_lstate.p, ls.data(), n * sizeof(LaneState), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  if (n_accept) *n_accept = nacc;
+  CK(rex_exchange_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->out_energy.p, c->e_opp.p, du,
+                         c->scale.p, c->velo.p));
+  if (n_accept) {   // the only host wait of an exchange
+    RexState r;
+    CK(cudaMemcpyAsync(&r, c->rex.p, sizeof(RexState), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *n_accept = r.nacc;
+  }
   return TIS_OK;
 }
 
 extern "C" int tis_get_labels(tis_ctx *c, int32_t *rep2lab) {
   if (!c || !rep2lab) return TIS_E_ARG;
-  for (int r = 0; r < c->nlane; ++r) rep2lab[r] = c->rep2lab[r] + 1;
+  std::vector<int> r(c->nlane);
+  CK(cudaMemcpyAsync(r.data(), c->d_rep2lab.p, r.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < c->nlane; ++k) rep2lab[k] = r[k] + 1;
   return TIS_OK;
 }
 

@@ -134,7 +134,8 @@ struct KArgs {
   double hb_cutoff_dist;
   double max_abscos;   // MAX_ANG_ABSCOS_HBOND15 == MAX_DIH_ABSCOS_HBOND15
   double tstep, tstep2, tsteph;
-  double beta_hbond15; // global quirk value (used when hb_beta_global)
+  double beta_hbond15; // global quirk value (used when hb_beta_global and rex is null)
+  const struct RexState *rex;   // device replica-exchange state (its beta_global overrides beta_hbond15)
   int hb_beta_global;
   unsigned long long seed;
   // descriptors
@@ -197,6 +198,15 @@ struct KArgs {
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
 // easy as 1, 2, 3", SC'11): 10 rounds of the 4x32 S-box with the published
 // multipliers and Weyl key increments.
+// Replica-exchange state kept on the device (simu_replica_exchange.F90,
+// var_replica.F90), so that an exchange needs no host round trip.
+struct RexState {
+  double beta_global;          // beta_hbond15: the last replica's label (simu_set_dtrna.F90:58, simu_para2)
+  unsigned long long counter;  // counter of the exchange's counter-based uniforms
+  int idx_pair;                // odd/even pair alternation (var_replica.F90:134,165-183)
+  int nacc;                    // swaps accepted by the last exchange
+};
+
 struct U4 { uint32_t x, y, z, w; };
 
 __host__ __device__ inline void mulhilo32(uint32_t a, uint32_t b, uint32_t &hi, uint32_t &lo) {

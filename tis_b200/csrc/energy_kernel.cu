@@ -268,7 +268,8 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     }
     __syncthreads();
     if (excess_flag && tid == 0)
-      prune_hbonds<double>(a, lane, L, T, st.istep, a.ebeta_lane ? a.ebeta_lane[lane] : a.ebeta, false);
+      prune_hbonds<double>(a, lane, L, T, st.istep,
+                           a.ebeta_lane ? a.ebeta_lane[lane] : (a.rex ? a.rex->beta_global : a.ebeta), false);
     __syncthreads();
   }
   for (int h = tid; h < T.nhb; h += nth)
@@ -329,6 +330,101 @@ __global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const Top
   double *v = velo + 3 * (size_t)L.state0;
   if (f > 0.0) for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
   else for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
+}
+
+// ----------------------------------------------------------------------
+// Replica exchange on the device (simu_replica_exchange.F90:121-300, one
+// temperature dimension).  rex_prep_kernel: the partner label of every lane
+// for this exchange's odd/even pairing and the partner's beta; the energy
+// kernel then evaluates every lane at its partner label.
+// rex_exchange_kernel (one CTA): thread 0 runs the Metropolis decisions in
+// label order with counter-based uniforms (or injected ones), updates the
+// label maps, the pair alternation and beta_hbond15; then the CTA writes the
+// lanes' labels and rescales the velocities of the swapped lanes.
+
+__device__ __forceinline__ int rex_pair(int l, int n, int idx_pair) {   // 1-based, 0 = no partner
+  if (idx_pair == 1) return (l % 2 == 1) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
+  if (l == 1) return 0;
+  return (l % 2 == 0) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
+}
+
+__global__ void rex_prep_kernel(KArgs a, const int *rep2lab, int *elabel, double *ebeta) {
+  const int lane = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lane >= a.nlane) return;
+  const int lo = rex_pair(rep2lab[lane] + 1, a.nlane, a.rex->idx_pair);
+  elabel[lane] = lo ? lo - 1 : -1;
+  ebeta[lane] = lo ? 1.0e0 / (a.lab_T[lo - 1] * a.boltz) : a.rex->beta_global;
+}
+
+__global__ void __launch_bounds__(256) rex_exchange_kernel(KArgs a, RexState *rex, int *rep2lab, int *lab2rep,
+                                                           const double *e_own, const double *e_opp,
+                                                           const double *u, double *scale, double *velo) {
+  const int n = a.nlane, tid = threadIdx.x;
+  for (int r = tid; r < n; r += blockDim.x) scale[r] = 0.0;
+  __syncthreads();
+  if (tid == 0) {
+    const int ip = rex->idx_pair;
+    int nrand = 0, nacc = 0;
+    unsigned long long ctr = rex->counter;
+    for (int li = 1; li <= n; ++li) {
+      const int lj = rex_pair(li, n, ip);
+      if (lj < li) continue;
+      ++nrand;
+      double uu;
+      if (u) {
+        uu = u[nrand - 1];
+      } else {
+        const U4 o = philox4x32(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x52454D44u, 0u}, (uint32_t)a.seed,
+                                (uint32_t)(a.seed >> 32));
+        ++ctr;
+        uu = u01_open0(o.x) - 2.3283064365386963e-10;   // [0, 1)
+      }
+      const int ri = lab2rep[li - 1], rj = lab2rep[lj - 1];
+      const double tm = a.lab_T[li - 1], tn = a.lab_T[lj - 1];
+      const double pim = e_own[(size_t)ri * N_ETYPE], pin = e_opp[(size_t)ri * N_ETYPE];
+      const double pjn = e_own[(size_t)rj * N_ETYPE], pjm = e_opp[(size_t)rj * N_ETYPE];
+      const double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / a.boltz;
+      if (delta < 0.0e0 || uu <= exp(-delta)) {
+        rep2lab[ri] = lj - 1; rep2lab[rj] = li - 1;
+        lab2rep[li - 1] = rj; lab2rep[lj - 1] = ri;
+        const double sf = sqrt(tn / tm);
+        scale[ri] = sf;
+        scale[rj] = -sf;
+        ++nacc;
+      }
+    }
+    rex->counter = ctr;
+    rex->nacc = nacc;
+    rex->idx_pair = (ip == 2) ? 1 : ip + 1;
+    rex->beta_global = 1.0e0 / (a.lab_T[rep2lab[n - 1]] * a.boltz);
+  }
+  __syncthreads();
+  for (int r = tid; r < n; r += blockDim.x) a.lstate[r].label = rep2lab[r];
+  // time_integral.F90 velocity rescale of a swapped replica (scale > 0
+  // multiplies, scale < 0 divides by -scale)
+  for (int r = 0; r < n; ++r) {
+    const double f = scale[r];
+    if (f == 0.0) continue;
+    const LaneDesc L = a.lanes[r];
+    const int N = a.tops[L.top].nmp;
+    double *v = velo + 3 * (size_t)L.state0;
+    if (f > 0.0) for (int k = tid; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
+    else for (int k = tid; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
+  }
+}
+
+cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
+                       double *ebeta) {
+  rex_prep_kernel<<<(a.nlane + 127) / 128, 128, 0, st>>>(a, rep2lab, elabel, ebeta);
+  (void)lab2rep; (void)rex;
+  return cudaGetLastError();
+}
+
+cudaError_t rex_exchange_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep,
+                                const double *e_own, const double *e_opp, const double *u, double *scale,
+                                double *velo) {
+  rex_exchange_kernel<<<1, 256, 0, st>>>(a, rex, rep2lab, lab2rep, e_own, e_opp, u, scale, velo);
+  return cudaGetLastError();
 }
 
 } // namespace tis

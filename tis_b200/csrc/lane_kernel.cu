@@ -470,7 +470,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // take the same barriers
   if (s.misc[MISC_EXCESS]) {
     if (tid == 0 && cu.rank == 0) {
-      const double beta = a.hb_beta_global ? a.beta_hbond15 : a.lab_beta[label];
+      const double beta = a.hb_beta_global ? (a.rex ? a.rex->beta_global : a.beta_hbond15) : a.lab_beta[label];
       prune_hbonds<Real>(a, lane, L, T, istep, beta, true);
     }
     if (CL == 1) __syncthreads(); else cg::this_cluster().sync();

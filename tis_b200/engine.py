@@ -161,14 +161,17 @@ class Engine:
         self._check(self.L.tis_timer(self.h, 1, C.byref(ms)), "timer")
         return ms.value
 
-    def replica_exchange(self, u=None):
+    def replica_exchange(self, u=None, count=True):
+        """One exchange; returns the number of accepted swaps.  count=False
+        skips that count, so the exchange stays on the device stream with no
+        host wait (returns None)."""
         na = C.c_int32(0)
         up = None
         if u is not None:
             uu = np.ascontiguousarray(u, dtype=np.float64)
             up = ptr_f64(uu)
-        self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na)), "replica_exchange")
-        return na.value
+        self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na) if count else None), "replica_exchange")
+        return na.value if count else None
 
     def hydro_tensors(self, irep=1):
         """(D, L) of the last Brownian-HI refresh, row-major (3N, 3N) arrays."""
