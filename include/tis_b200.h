@@ -51,8 +51,10 @@ enum {
 };
 /* i_simulate_type values used here (src/const_index.F90 SIM). */
 enum { TIS_SIM_LANGEVIN = 1, TIS_SIM_BROWNIAN_HI = 6 };
-/* electrostatics: 0 none, DH = i_function_form 0, EWALD = i_function_form 2 */
-enum { TIS_ELE_NONE = 0, TIS_ELE_DH = 1, TIS_ELE_EWALD = 2 };
+/* electrostatics: 0 none, DH = i_function_form 0, EWALD = i_function_form 2,
+ * COULOMB = i_function_form 1 (plain Coulomb with a cutoff in A,
+ * src/force_ele_coulomb.F90, src/energy_ele_coulomb.F90) */
+enum { TIS_ELE_NONE = 0, TIS_ELE_DH = 1, TIS_ELE_EWALD = 2, TIS_ELE_COULOMB = 3 };
 /* arithmetic of the force terms */
 enum { TIS_PREC_FP64 = 0, TIS_PREC_MIXED = 1 };
 

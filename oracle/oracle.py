@@ -69,7 +69,7 @@ def lib():
 
 
 TERMS = {"bond": 0, "angle": 1, "stack": 2, "hbond": 3, "exv": 4, "dh": 5, "ewald": 6, "fene": 7, "wca": 8,
-         "tstack": 9}
+         "tstack": 9, "coulomb": 10}
 
 
 class Oracle:

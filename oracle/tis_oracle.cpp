@@ -943,6 +943,29 @@ void force_ele_DH(const orc_ctx &c, Rep &r, double *F) {
   }
 }
 
+// force_ele_coulomb.F90:55-82: coef_ele / r^3 along v21 inside the cutoff
+// (A), no DE_MAX clamp
+void force_ele_coulomb(const orc_ctx &c, Rep &r, double *F) {
+  const Label &L = c.lab[r.label - 1];
+  double cutoff2 = sq(c.par.cutoff_ele);
+  size_t nele = r.coef_ele.size();
+  for (size_t e = 0; e < nele; ++e) {
+    int i1 = r.iele2mp[4 * e] - 1, i2 = r.iele2mp[4 * e + 1] - 1, im = r.iele2mp[4 * e + 2] - 1;
+    double v21[3];
+    for (int k = 0; k < 3; ++k) v21[k] = r.pxyz[3 * i2 + k] - r.pxyz[3 * i1 + k] + c.d_mirror[im][k];
+    double dist2 = dot3(v21, v21);
+    if (dist2 > cutoff2) continue;
+    double dist1 = std::sqrt(dist2);
+    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    double dv_dr = ce / (dist1 * dist2);
+    for (int k = 0; k < 3; ++k) {
+      double fk = dv_dr * v21[k];
+      F[3 * i1 + k] = F[3 * i1 + k] - fk;
+      F[3 * i2 + k] = F[3 * i2 + k] + fk;
+    }
+  }
+}
+
 // force_ele_coulomb_ewld.F90:215-313
 void force_ele_ewald(const orc_ctx &c, Rep &r, double *F) {
   const Label &L = c.lab[r.label - 1];
@@ -1029,6 +1052,7 @@ void force_sumup(orc_ctx &c, Rep &r, double *F) {
   force_exv_dt15(c, r, F);
   if (c.par.i_ele == TIS_ELE_DH) force_ele_DH(c, r, F);
   else if (c.par.i_ele == TIS_ELE_EWALD) force_ele_ewald(c, r, F);
+  else if (c.par.i_ele == TIS_ELE_COULOMB) force_ele_coulomb(c, r, F);
 }
 
 // ------------------------------------------------------------- energies
@@ -1169,6 +1193,23 @@ double energy_DH(const orc_ctx &c, const Rep &r) {
   }
   return e;
 }
+// energy_ele_coulomb.F90:31-70: coef_ele (1 / r - 1 / cutoff) inside the cutoff
+double energy_coulomb(const orc_ctx &c, const Rep &r) {
+  const Label &L = c.lab[r.label - 1];
+  double cutoff2 = sq(c.par.cutoff_ele), cut_inv = 1.0e0 / c.par.cutoff_ele, e = 0;
+  size_t nele = r.coef_ele.size();
+  for (size_t k = 0; k < nele; ++k) {
+    int i1 = r.iele2mp[4 * k] - 1, i2 = r.iele2mp[4 * k + 1] - 1, im = r.iele2mp[4 * k + 2] - 1;
+    double v[3];
+    for (int d = 0; d < 3; ++d) v[d] = r.pxyz[3 * i2 + d] - r.pxyz[3 * i1 + d] + c.d_mirror[im][d];
+    double dist2 = dot3(v, v);
+    if (dist2 > cutoff2) continue;
+    double dist1 = std::sqrt(dist2);
+    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    e += ce * (1.0e0 / dist1 - cut_inv);
+  }
+  return e;
+}
 // energy_ele_coulomb_ewld.F90 (Fourier 75-89, real 137, self 212)
 double energy_ewald(const orc_ctx &c, const Rep &r) {
   const Label &L = c.lab[r.label - 1];
@@ -1234,6 +1275,7 @@ void energy_sumup(orc_ctx &c, Rep &r, double *E, bool reuse_hb) {
   E[TIS_E_EXV_DT15 - 1] = energy_exv(c, r);
   if (c.par.i_ele == TIS_ELE_DH) E[TIS_E_ELE - 1] = energy_DH(c, r);
   else if (c.par.i_ele == TIS_ELE_EWALD) E[TIS_E_ELE - 1] = energy_ewald(c, r);
+  else if (c.par.i_ele == TIS_ELE_COULOMB) E[TIS_E_ELE - 1] = energy_coulomb(c, r);
   double tot = 0;
   for (int i = 1; i <= TIS_ETYPE_MAX; ++i) {
     if (i == TIS_E_TOTAL || i == TIS_E_VELO) continue;
@@ -1543,7 +1585,7 @@ int orc_force_sumup(orc_ctx *c, int irep, double *force) {
   return r.unif_exhausted ? TIS_E_NOISE_EXHAUSTED : 0;
 }
 
-// Single force term for tests: term = 0 bond, 1 angle, 2 stack, 3 hbond, 4 exv, 5 DH, 6 Ewald, 7 fene, 8 wca, 9 tertiary stack.
+// Single force term for tests: term = 0 bond, 1 angle, 2 stack, 3 hbond, 4 exv, 5 DH, 6 Ewald, 7 fene, 8 wca, 9 tertiary stack, 10 Coulomb.
 int orc_force_term(orc_ctx *c, int irep, int term, double *force) {
   Rep &r = c->rep[irep - 1];
   std::fill(force, force + 3 * (size_t)c->nmp, 0.0);
@@ -1559,6 +1601,7 @@ int orc_force_term(orc_ctx *c, int irep, int term, double *force) {
     case 4: force_exv_dt15(*c, r, force); break;
     case 5: force_ele_DH(*c, r, force); break;
     case 6: force_ele_ewald(*c, r, force); break;
+    case 10: force_ele_coulomb(*c, r, force); break;
     case 7: force_fene(*c, r, force); break;
     case 8: force_wca(*c, r, force); break;
     case 9: dtrna_stack_nlocal(*c, r, force); break;

@@ -50,6 +50,7 @@ def periodic_ions(seed=7):
 SYSTEMS = {
     "c1_walk": (c1_system, {}),
     "hairpin_tertiary": (synth.hairpin_tertiary, {}),
+    "hairpin_coulomb": (hairpin, dict(i_ele=3, cutoff_ele=60.0)),
     "hairpin": (hairpin, {}),
     "dense": (dense, {}),
     "periodic_ions": (periodic_ions, dict(i_periodic=1, psize=(40.0, 40.0, 40.0))),
@@ -107,7 +108,7 @@ def test_force_mixed(tis_lib, name):
     assert err < FORCE_TOL_MIXED, err
 
 
-@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary"])
+@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary", "hairpin_coulomb"])
 def test_energy_fp64(tis_lib, name):
     s, par, eng, orc = make_pair(name, 0)
     eng.neighbor(); orc.neighbor()

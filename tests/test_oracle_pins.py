@@ -147,6 +147,33 @@ def test_tertiary_stacks_turn_off_secondary_stacks():
     o.close(); o2.close()
 
 
+def test_coulomb_force_is_minus_energy_gradient():
+    """force_ele_coulomb.F90 against the central differences of
+    energy_ele_coulomb.F90 (cutoff 200 A: no pair near it)."""
+    s, _ = hairpin()
+    par = synth.dt15_params(ionic_strength=0.15, i_ele=3, cutoff_ele=200.0)
+    o = Oracle(s, par, [300.0])
+    x0 = s["xyz"].copy()
+    o.set_state(x0[None])
+    o.neighbor()
+    f = o.force_term("coulomb")
+    h = 1e-4
+    g = np.zeros_like(x0)
+    for i in range(x0.shape[0]):
+        for d in range(3):
+            e = []
+            for sgn in (1, -1):
+                xp = x0.copy()
+                xp[i, d] += sgn * h
+                o.set_state(xp[None])
+                o.neighbor()
+                e.append(o.energy()[7])
+            g[i, d] = -(e[0] - e[1]) / (2 * h)
+    assert np.abs(f).max() > 0.1
+    assert np.abs(f - g).max() <= 1e-5 * max(np.abs(f).max(), 1.0)
+    o.close()
+
+
 def neutral_ion_box():
     s = synth.set_friction(synth.dt15_chain(8, 3, stem=0), 0.5)
     return synth.add_ions(s, 40.0, {"Mg": 1, "K": 6, "Cl": 1}, 9, clash=6.0)

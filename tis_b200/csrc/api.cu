@@ -279,6 +279,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->bdhi = p.i_simulate_type == TIS_SIM_BROWNIAN_HI;
   // the Brownian-HI path evaluates FENE and WCA records (the C5 bead chains):
   // no electrostatics, no DT15 or harmonic terms
+  if (p.i_ele < TIS_ELE_NONE || p.i_ele > TIS_ELE_COULOMB) { tis_destroy(c); return TIS_E_ARG; }
   if (c->bdhi && (p.i_ele != TIS_ELE_NONE || !(p.viscosity > 0.0) || !(p.hi_radius > 0.0))) {
     tis_destroy(c);
     return TIS_E_UNSUPPORTED;
@@ -902,7 +903,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_step_neighbor = p.n_step_neighbor;
   a.exv_dist = p.exv_dist; a.exv_dist_PS = p.exv_dist_PS; a.exv_adjust = p.exv_adjust; a.exv_inf = p.exv_inf;
   a.nsep[0] = p.n_sep_nlocal_P; a.nsep[1] = p.n_sep_nlocal_S; a.nsep[2] = p.n_sep_nlocal_B;
-  a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : (p.i_ele == TIS_ELE_EWALD ? 2 : 0);
+  a.i_ele = (p.i_ele == TIS_ELE_DH) ? 1 : (p.i_ele == TIS_ELE_EWALD ? 2 : (p.i_ele == TIS_ELE_COULOMB ? 3 : 0));
   if (p.i_ele == TIS_ELE_EWALD) {
     a.ewld_alpha = p.ewld_alpha;
     a.ewld_beta = 2.0 * p.ewld_alpha / std::sqrt(F_PI);

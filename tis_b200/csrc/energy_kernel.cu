@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
           const double dist1 = sqrt(r2);
           const double ce = a.b_charge[T.bead0 + i] * a.b_charge[T.bead0 + j] * coefT;
           if (a.i_ele == 1) es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
+          else if (a.i_ele == 3) es[ES_ELE] += ce * (1.0e0 / dist1 - 1.0e0 / a.cutoff_ele);   // energy_ele_coulomb.F90:66
           else es[ES_ELE] += ce * erfc(a.ewld_alpha * dist1) / dist1;
         }
       }

@@ -308,9 +308,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const Real rcd = (Real)(1.0 / cdist);
   // DH: the force cutoff is always scaled by the Debye length
   // (force_ele_DH.F90:44); Ewald: real-space cutoff in A
-  const bool ewald = a.i_ele == 2;
-  const Real cut2 = ewald ? (Real)(a.cutoff_ele * a.cutoff_ele)
-                          : (Real)((a.cutoff_ele * cdist) * (a.cutoff_ele * cdist));
+  const bool ewald = a.i_ele == 2, coul = a.i_ele == 3;
+  const Real cut2 = (ewald || coul) ? (Real)(a.cutoff_ele * a.cutoff_ele)
+                                    : (Real)((a.cutoff_ele * cdist) * (a.cutoff_ele * cdist));
   const Real ew_a = (Real)a.ewld_alpha, ew_a2 = (Real)(a.ewld_alpha * a.ewld_alpha), ew_b = (Real)a.ewld_beta;
   // near-list state: read here (after the caller's barrier), rewritten by
   // thread 0 only after the end-of-phase-1 barrier
@@ -421,7 +421,11 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const Real ria = rsq<Real>(ra2), rib = rsq<Real>(rb2);
             const Real da = ra2 * ria, db = rb2 * rib;
             Real fa, fb;
-            if (!ewald) {
+            if (coul) {
+              // force_ele_coulomb.F90:66-71 (no clamp)
+              fa = qci * p0.w * ria * ria * ria;
+              fb = qci * p1.w * rib * rib * rib;
+            } else if (!ewald) {
               fa = qci * p0.w * ria * ria * (ria + rcd) * fexp<Real>(-da * rcd);
               fb = qci * p1.w * rib * rib * (rib + rcd) * fexp<Real>(-db * rcd);
             } else {
@@ -431,7 +435,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             }
             if (!(ra2 <= cut2)) fa = 0;
             if (!(rb2 <= cut2) || !two) fb = 0;
-            if (!ewald) {
+            if (!ewald && !coul) {
               if (fa > (Real)50) { fa = 50; ++nclamp; }
               if (fb > (Real)50) { fb = 50; ++nclamp; }
             }
