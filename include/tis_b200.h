@@ -198,6 +198,17 @@ int tis_set_state(tis_ctx *ctx, const double *xyz, const double *velo, const dou
 int tis_get_state(tis_ctx *ctx, double *xyz, double *velo, double *accel);
 /* Periodic (wrapped) coordinates pxyz_mp_rep. */
 int tis_get_pxyz(tis_ctx *ctx, double *pxyz);
+/* Step counter istep of every replica (var_simu istep; read back by the
+ * restart reader src/read_rst.F90 STEP block): counter-based noise and the
+ * rebuild cadence continue from it. */
+int tis_set_step(tis_ctx *ctx, int64_t istep);
+/* DT15 hbond and stack status of replica irep (var_simu hb_status,
+ * st_status as the restart's DTRNA15 block holds them, src/write_rst.F90:
+ * 104-113): hb_status[ihb] = 1 when hbond ihb was on in the last force
+ * evaluation (in the list, within the cutoff, not pruned); st_status[ist] =
+ * 0 when a tertiary stack excludes stack ist at the current coordinates.
+ * Either pointer may be NULL. */
+int tis_get_dtrna_status(tis_ctx *ctx, int32_t irep, int32_t *hb_status, int32_t *st_status);
 
 /* Parity injection.  noise: r_boxmuller(3, nmp, nrep) for nsteps consecutive
  * steps (step-major); uniforms: for each replica a stream of n_uniform draws

@@ -175,7 +175,7 @@ EXPORTED = [
     "tis_force_sumup", "tis_energy_sumup", "tis_time_integral_pre", "tis_step",
     "tis_replica_exchange", "tis_get_labels", "tis_status", "tis_last_step_ms",
     "tis_last_error", "tis_timer", "tis_force_sumup_static", "tis_launch_count",
-    "tis_get_hydro_tensors",
+    "tis_get_hydro_tensors", "tis_set_step", "tis_get_dtrna_status",
 ]
 
 
@@ -209,5 +209,7 @@ def _declare(lib):
     lib.tis_timer.argtypes = [vp, C.c_int32, _f64p]
     lib.tis_force_sumup_static.argtypes = [vp, C.c_int32, vp, vp]
     lib.tis_get_hydro_tensors.argtypes = [vp, C.c_int32, _f64p, _f64p]
+    lib.tis_set_step.argtypes = [vp, C.c_int64]
+    lib.tis_get_dtrna_status.argtypes = [vp, C.c_int32, _i32p, _i32p]
     lib.tis_launch_count.argtypes = [vp]
     lib.tis_launch_count.restype = C.c_int64

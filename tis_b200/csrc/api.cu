@@ -30,6 +30,7 @@ cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, con
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst, int *out);
 cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
                        double *ebeta);
 cudaError_t rex_exchange_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep,
@@ -847,6 +848,45 @@ extern "C" int tis_get_state(tis_ctx *c, double *xyz, double *velo, double *acce
   if (velo) CK(cudaMemcpyAsync(velo, c->velo.p, n, cudaMemcpyDeviceToHost, c->stream));
   if (accel) CK(cudaMemcpyAsync(accel, c->accel.p, n, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return TIS_OK;
+}
+
+namespace {
+KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane);
+}  // namespace
+
+extern "C" int tis_set_step(tis_ctx *c, int64_t istep) {
+  if (!c || istep < 0) return TIS_E_ARG;
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto &l : ls) l.istep = istep;
+  CK(cudaMemcpyAsync(c->d_lstate.p, ls.data(), ls.size() * sizeof(LaneState), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->bd_istep = istep;
+  return TIS_OK;
+}
+
+extern "C" int tis_get_dtrna_status(tis_ctx *c, int32_t irep, int32_t *hb_status, int32_t *st_status) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  const LaneDesc &L = c->lanes[irep - 1];
+  const TopDesc &T = c->tops[L.top];
+  if (hb_status && T.nhb > 0) {
+    std::vector<uint8_t> f(T.nhb);
+    CK(cudaMemcpyAsync(f.data(), c->hb_flag.p + L.hb0, T.nhb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int h = 0; h < T.nhb; ++h) hb_status[h] = (f[h] & 2) ? 1 : 0;
+  }
+  if (st_status && T.nst > 0) {
+    DBuf<int> out;
+    CK(out.alloc(T.nst));
+    KArgs a = make_args(c, 0, 0, irep - 1);
+    ++c->launches;
+    CK(st_status_launch(c->stream, a, irep - 1, T.nst, out.p));
+    CK(cudaMemcpyAsync(st_status, out.p, T.nst * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out.free();
+  }
   return TIS_OK;
 }
 

@@ -334,6 +334,36 @@ __global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const Top
 }
 
 // ----------------------------------------------------------------------
+// st_status of every secondary stack of one lane (force_dtrna_stack_nlocal.
+// F90:83-92) at the lane's current coordinates, for the restart's DTRNA15
+// block; the same FP64 test as the force pass.
+__global__ void st_status_kernel(KArgs a, int lane, int *out) {
+  const LaneDesc L = a.lanes[lane];
+  const TopDesc T = a.tops[L.top];
+  const double *X = a.xyz + 3 * (size_t)L.state0;
+  const double *P = a.pxyz + 3 * (size_t)L.state0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < T.nst; k += gridDim.x * blockDim.x) {
+    int on = 1;
+    for (int e = (T.ntst ? a.stx_ptr[T.stx0 + k] : 0); e < (T.ntst ? a.stx_ptr[T.stx0 + k + 1] : 0); ++e) {
+      const int t = a.stx_tst[e];
+      const int *m = a.tst_idx + 6 * (size_t)(T.tst0 + t);
+      double3 u = sub3(gpos(a.periodic ? P : X, m[0]), gpos(a.periodic ? P : X, m[1]));
+      if (a.periodic) { pb1(u.x, a.psize[0], a.psizeh[0]); pb1(u.y, a.psize[1], a.psizeh[1]); pb1(u.z, a.psize[2], a.psizeh[2]); }
+      const double d = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(u.x, u.x), __dmul_rn(u.y, u.y)), __dmul_rn(u.z, u.z))) -
+                       a.tst_nat[6 * (size_t)(T.tst0 + t)];
+      if (d < 10.0) on = 0;
+    }
+    out[k] = on;
+  }
+}
+
+cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst, int *out) {
+  if (nst <= 0) return cudaSuccess;
+  st_status_kernel<<<(nst + 127) / 128, 128, 0, st>>>(a, lane, out);
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------
 // Replica exchange on the device (simu_replica_exchange.F90:121-300, one
 // temperature dimension).  rex_prep_kernel: the partner label of every lane
 // for this exchange's odd/even pairing and the partner's beta; the energy

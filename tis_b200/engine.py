@@ -54,6 +54,7 @@ class Engine:
         self.h = h
         self.nlane = self.L.tis_nrep(self.h)
         self.lane_nmp = [self.L.tis_nmp(self.h, i + 1) for i in range(self.nlane)]
+        self.systems_of_lane = [s for s, r in zip(self.systems, self.nrep) for _ in range(r)]
         self.nbead = int(sum(self.lane_nmp))
         self.offsets = np.concatenate([[0], np.cumsum(self.lane_nmp)]).astype(int)
 
@@ -184,6 +185,17 @@ class Engine:
 
     def launch_count(self) -> int:
         return int(self.L.tis_launch_count(self.h))
+
+    def set_step(self, istep: int):
+        self._check(self.L.tis_set_step(self.h, int(istep)), "set_step")
+
+    def dtrna_status(self, irep=1):
+        """(hb_status, st_status) of replica irep as 0/1 int32 arrays."""
+        t = self.systems_of_lane[irep - 1]
+        hb = np.zeros(max(int(t.get("nhb", 0)), 1), dtype=np.int32)
+        st = np.ones(max(int(t.get("nst", 0)), 1), dtype=np.int32)
+        self._check(self.L.tis_get_dtrna_status(self.h, irep, ptr_i32(hb), ptr_i32(st)), "dtrna_status")
+        return hb[:int(t.get("nhb", 0))], st[:int(t.get("nst", 0))]
 
     def labels(self):
         out = np.zeros(self.nlane, dtype=np.int32)
