@@ -122,6 +122,10 @@ typedef struct tis_topology {
   const double *coef_dtrna_tst;    /* (7, ntst) index 0 = U0, 1..6 */
   const int32_t *idtrna_tst2side;  /* (2, ntst) 1: the secondary stack of B with B - 3, 2: with B + 3 */
   const int32_t *flg_tst_exclusive;/* (2, ntst) nonzero: within 10 A of native, disables that stack */
+  const int32_t *flg_hb_tertiary;  /* (nhb) nonzero: hb-dist record typed 'T' (src/read_nativeinfo.F90:
+                                      606-613); its energy goes to TIS_E_THBOND_DTRNA instead of
+                                      TIS_E_HBOND_DTRNA (energy_dtrna_hbond15.F90:135-143).  NULL:
+                                      every hydrogen bond is secondary ('S') */
 } tis_topology;
 
 /* ---------------------------------------------------------------- params */

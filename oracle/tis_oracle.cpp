@@ -96,6 +96,7 @@ struct orc_ctx {
   int nba = 0; std::vector<int> iba2mp; std::vector<double> ba_nat, coef_ba;
   int nst = 0; std::vector<int> st2mp; std::vector<double> st_nat, st_coef, st_hsTm;
   int nhb = 0; std::vector<int> hb2mp; std::vector<double> hb_nat, hb_coef; std::vector<int> hb2site;
+  std::vector<char> hb_tert;        // flg_hb_tertiary (read_nativeinfo.F90:606-613)
   int nhbsite = 0; std::vector<int> nvalence;
   std::vector<std::vector<int>> hb_at_site;   // static per-site hb lists (ascending ihb)
   int nfene = 0; std::vector<int> fene2mp; std::vector<double> fene_nat, coef_fene, dist2_fene;
@@ -1244,15 +1245,20 @@ double energy_ewald(const orc_ctx &c, const Rep &r) {
 }
 // energy_dtrna_hbond15.F90: with flg_hb_energy set the energies of the last
 // force call are summed; otherwise terms and pruning are recomputed.
-double energy_hbond(orc_ctx &c, Rep &r, bool reuse) {
+// Secondary bonds go to HBOND_DTRNA, tertiary ('T') ones to THBOND_DTRNA
+// (energy_dtrna_hbond15.F90:135-143).
+void energy_hbond(orc_ctx &c, Rep &r, bool reuse, double &e_sec, double &e_ter) {
   if (!reuse) {
     hbond15_terms(c, r);
     hbond15_prune(c, r, false);
   }
-  double e = 0;
+  e_sec = 0;
+  e_ter = 0;
   for (int ihb1 : r.ineigh2hb)
-    if (!r.hb_status.empty() && r.hb_status[ihb1 - 1]) e += r.ene_hb[ihb1 - 1];
-  return e;
+    if (!r.hb_status.empty() && r.hb_status[ihb1 - 1]) {
+      if (c.hb_tert[ihb1 - 1]) e_ter += r.ene_hb[ihb1 - 1];
+      else e_sec += r.ene_hb[ihb1 - 1];
+    }
 }
 
 void energy_sumup(orc_ctx &c, Rep &r, double *E, bool reuse_hb) {
@@ -1270,7 +1276,7 @@ void energy_sumup(orc_ctx &c, Rep &r, double *E, bool reuse_hb) {
     r.st_status.assign(c.nst, 1);
     if (c.ntst > 0) E[TIS_E_TSTACK_DTRNA - 1] = dtrna_stack_nlocal(c, r, nullptr);
     E[TIS_E_STACK_DTRNA - 1] = energy_stack(c, r);
-    E[TIS_E_HBOND_DTRNA - 1] = energy_hbond(c, r, reuse_hb);
+    energy_hbond(c, r, reuse_hb, E[TIS_E_HBOND_DTRNA - 1], E[TIS_E_THBOND_DTRNA - 1]);
   }
   E[TIS_E_EXV_DT15 - 1] = energy_exv(c, r);
   if (c.par.i_ele == TIS_ELE_DH) E[TIS_E_ELE - 1] = energy_DH(c, r);
@@ -1386,6 +1392,8 @@ orc_ctx *orc_create(const tis_topology *t, const tis_params *p, int nrep, const 
   c->hb2mp.assign(t->idtrna_hb2mp, t->idtrna_hb2mp + 6 * t->nhb);
   c->hb_nat.assign(t->dtrna_hb_nat, t->dtrna_hb_nat + 6 * t->nhb);
   c->hb_coef.assign(t->coef_dtrna_hb, t->coef_dtrna_hb + 7 * t->nhb);
+  c->hb_tert.assign(t->nhb, 0);
+  for (int ihb = 0; ihb < t->nhb; ++ihb) c->hb_tert[ihb] = (t->flg_hb_tertiary && t->flg_hb_tertiary[ihb]) ? 1 : 0;
   c->hb2site.assign(t->idtrna_hb2hbsite, t->idtrna_hb2hbsite + 6 * t->nhb);
   c->nhbsite = t->nhbsite;
   c->nvalence.assign(t->nvalence_hbsite, t->nvalence_hbsite + t->nhbsite);

@@ -41,6 +41,15 @@ def dense(seed=5, n=30):
     return synth.set_friction(synth.dt15_chain(n, seed, min_dist=2.6, confine=10.0), 0.5)
 
 
+def ninfo_hairpin():
+    """tests/golden/hairpin_tertiary.{cg.pdb,ninfo} read through
+    tis_b200.ninfo: tertiary stacks, 'T' hydrogen bonds, an ion unit."""
+    import os
+    from tis_b200 import ninfo
+    g = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "hairpin_tertiary")
+    return ninfo.load(g + ".cg.pdb", g + ".ninfo", i_fric=0, fric_const=0.5)
+
+
 def periodic_ions(seed=7):
     s = synth.set_friction(synth.dt15_chain(12, seed, stem=3), 0.5)
     s = synth.add_ions(s, 40.0, {"Mg": 2, "K": 12, "Cl": 5}, seed + 1, clash=4.0)
@@ -50,6 +59,7 @@ def periodic_ions(seed=7):
 SYSTEMS = {
     "c1_walk": (c1_system, {}),
     "hairpin_tertiary": (synth.hairpin_tertiary, {}),
+    "ninfo_hairpin": (ninfo_hairpin, {}),
     "hairpin_coulomb": (hairpin, dict(i_ele=3, cutoff_ele=60.0)),
     "hairpin": (hairpin, {}),
     "dense": (dense, {}),
@@ -108,14 +118,17 @@ def test_force_mixed(tis_lib, name):
     assert err < FORCE_TOL_MIXED, err
 
 
-@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary", "hairpin_coulomb"])
+@pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary", "hairpin_coulomb",
+                                  "ninfo_hairpin"])
 def test_energy_fp64(tis_lib, name):
     s, par, eng, orc = make_pair(name, 0)
     eng.neighbor(); orc.neighbor()
     eng.force(); orc.force()
     e = eng.energy()
     er = orc.energy(reuse_hb=True)
-    for k in (1, 3, 4, 8, 16, 17, 18, 19):
+    if name == "ninfo_hairpin":
+        assert er[20 - 1] < 0.0 and er[17 - 1] < 0.0   # both secondary and tertiary bonds formed
+    for k in (1, 3, 4, 8, 16, 17, 18, 19, 20):
         assert abs(e[k - 1] - er[k - 1]) <= 1e-9 * max(1.0, abs(er[k - 1])), (k, e[k - 1], er[k - 1])
 
 

@@ -55,6 +55,7 @@ class Topology(C.Structure):
         ("nwca", C.c_int32), ("iwca2mp", _i32p), ("wca_nat", _f64p), ("coef_wca", _f64p),
         ("ntst", C.c_int32), ("idtrna_tst2mp", _i32p), ("dtrna_tst_nat", _f64p),
         ("coef_dtrna_tst", _f64p), ("idtrna_tst2side", _i32p), ("flg_tst_exclusive", _i32p),
+        ("flg_hb_tertiary", _i32p),
     ]
 
 
@@ -110,7 +111,10 @@ _TOPO_ARRAYS = {
     "iwca2mp": np.int32, "wca_nat": np.float64, "coef_wca": np.float64,
     "idtrna_tst2mp": np.int32, "dtrna_tst_nat": np.float64, "coef_dtrna_tst": np.float64,
     "idtrna_tst2side": np.int32, "flg_tst_exclusive": np.int32,
+    "flg_hb_tertiary": np.int32,
 }
+# Arrays the library accepts as NULL (their absence has a meaning of its own).
+_TOPO_OPTIONAL = ("flg_hb_tertiary",)
 _TOPO_COUNTS = ("nmp", "nunit", "ncharge", "nbd", "nba", "nst", "nhb", "nhbsite", "nfene", "nwca", "ntst")
 
 
@@ -126,6 +130,8 @@ def make_topology(sysd: dict):
         setattr(t, k, int(sysd.get(k, 0)))
     for k, dt in _TOPO_ARRAYS.items():
         a = sysd.get(k)
+        if k in _TOPO_OPTIONAL and a is None:
+            continue
         if a is None or np.size(a) == 0:
             a = np.zeros(1, dtype=dt)
         # record-major (nrec, k) C-order arrays are the Fortran (k, nrec) layout

@@ -133,6 +133,7 @@ struct tis_ctx {
   DBuf<uint32_t> mask;
   DBuf<int> site_exc;
   DBuf<uint8_t> mirror, hb_flag;
+  DBuf<uint8_t> hb_tert;            // (hb) 1: tertiary ('T') hydrogen bond
   DBuf<double> hb_ene;
   DBuf<unsigned char> slots;
   DBuf<double> noise, unif;
@@ -306,6 +307,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<int> bd_idx, ba_idx, st_idx, hb_idx, hb_site, site_val, site_ptr, site_hb, inc_ptr, inc_slot, q_bead;
   std::vector<double> bd_nat, bd_coef, ba_nat, ba_coef, st_nat, st_coef, hb_nat, hb_coef, hb_nd2;
   std::vector<double> st_hsTm_all;
+  std::vector<uint8_t> hb_tert;
+  bool any_tert = false;
   std::vector<int> tst_idx, stx_ptr, stx_tst;
   std::vector<double> tst_nat, tst_coef;
   std::vector<int> fene_idx, wca_idx, bdp;
@@ -505,6 +508,11 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     append(hb_nat, t.dtrna_hb_nat, 6 * (size_t)t.nhb);
     append(hb_coef, t.coef_dtrna_hb, 7 * (size_t)t.nhb);
     for (int i = 0; i < 6 * t.nhb; ++i) hb_site.push_back(t.idtrna_hb2hbsite[i] - 1);
+    for (int h = 0; h < t.nhb; ++h) {   // read_nativeinfo.F90:606-613
+      const uint8_t tt = (t.flg_hb_tertiary && t.flg_hb_tertiary[h]) ? 1 : 0;
+      hb_tert.push_back(tt);
+      any_tert = any_tert || tt;
+    }
     for (int h = 0; h < t.nhb; ++h) {   // mloop_dtrna.F90:151
       double r = t.dtrna_hb_nat[6 * h] + p.hb_cutoff_dist + p.neigh_margin;
       hb_nd2.push_back(r * r);
@@ -689,6 +697,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->stx_ptr.upload(stx_ptr)); CK(c->stx_tst.upload(stx_tst));
   CK(c->hb_idx.upload(hb_idx)); CK(c->hb_nat.upload(hb_nat)); CK(c->hb_coef.upload(hb_coef));
   CK(c->hb_site.upload(hb_site)); CK(c->hb_nd2.upload(hb_nd2));
+  if (any_tert) CK(c->hb_tert.upload(hb_tert));
   CK(c->site_val.upload(site_val)); CK(c->site_ptr.upload(site_ptr)); CK(c->site_hb.upload(site_hb));
   CK(c->inc_ptr.upload(inc_ptr)); CK(c->inc_slot.upload(inc_slot)); CK(c->q_bead.upload(q_bead));
   CK(c->lab_Td.upload(lab_T)); CK(c->lab_coef.upload(lab_coef)); CK(c->lab_cdist.upload(lab_cdist));
@@ -800,7 +809,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->site_val.free(); c->site_ptr.free(); c->site_hb.free(); c->inc_ptr.free(); c->inc_slot.free();
   c->q_bead.free();
   c->bd_nat.free(); c->bd_coef.free(); c->ba_nat.free(); c->ba_coef.free(); c->st_nat.free(); c->st_coef.free();
-  c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free();
+  c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free(); c->hb_tert.free();
   c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
   c->lab_u0.free(); c->lab_c1.free(); c->lab_u0off.free(); c->lab_c1off.free(); c->elabel.free();
   c->ebeta.free(); c->e_opp.free(); c->rex_u.free(); c->d_rep2lab.free(); c->d_lab2rep.free(); c->rex.free();
@@ -983,6 +992,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.tst_idx = c->tst_idx.p; a.tst_nat = c->tst_nat.p; a.tst_coef = c->tst_coef.p;
   a.stx_ptr = c->stx_ptr.p; a.stx_tst = c->stx_tst.p;
   a.hb_idx = c->hb_idx.p; a.hb_nat = c->hb_nat.p; a.hb_coef = c->hb_coef.p; a.hb_site = c->hb_site.p;
+  a.hb_tert = c->hb_tert.p;
   a.hb_nd2 = c->hb_nd2.p;
   a.site_val = c->site_val.p; a.site_ptr = c->site_ptr.p; a.site_hb = c->site_hb.p;
   a.inc_ptr = c->inc_ptr.p; a.inc_slot = c->inc_slot.p; a.q_bead = c->q_bead.p;

@@ -157,6 +157,7 @@ struct KArgs {
   const int *tst_idx; const double *tst_nat, *tst_coef;   // tertiary stacks: 6 beads, 6 natives, U0 + 6 coefs
   const int *stx_ptr, *stx_tst;    // secondary stack -> exclusive tertiary stacks (topology-local index)
   const int *hb_idx; const double *hb_nat, *hb_coef; const int *hb_site; const double *hb_nd2;
+  const uint8_t *hb_tert;            // (hb) 1: tertiary hydrogen bond; null when there are none
   const int *site_val; const int *site_ptr; const int *site_hb;
   const int *inc_ptr; const int *inc_slot;
   const int *q_bead;

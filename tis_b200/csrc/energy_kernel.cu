@@ -25,7 +25,7 @@ __device__ __forceinline__ double wrapd(double d) {
   return d;
 }
 
-enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_TST, ES_N };
+enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_TST, ES_THB, ES_N };
 
 __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
@@ -273,8 +273,9 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
                            a.ebeta_lane ? a.ebeta_lane[lane] : (a.rex ? a.rex->beta_global : a.ebeta), false);
     __syncthreads();
   }
+  // energy_dtrna_hbond15.F90:135-143: tertiary ('T') bonds count separately
   for (int h = tid; h < T.nhb; h += nth)
-    if ((hbf[h] & 3) == 3) es[ES_HB] += hbe[h];
+    if ((hbf[h] & 3) == 3) es[(a.hb_tert && a.hb_tert[T.hb0 + h]) ? ES_THB : ES_HB] += hbe[h];
   // deterministic block reduction: warp butterfly, then warps in order
   for (int k = 0; k < ES_N; ++k)
     for (int o = 16; o > 0; o >>= 1) es[k] += __shfl_xor_sync(0xffffffffu, es[k], o);
@@ -299,6 +300,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     E[22] = tot[ES_WREP];
     E[23] = tot[ES_WATT];
     E[18] = tot[ES_TST];
+    E[19] = tot[ES_THB];
     double sum = 0.0;
     for (int k = 2; k < N_ETYPE; ++k) sum += E[k];
     E[0] = sum;
