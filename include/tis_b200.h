@@ -68,6 +68,7 @@ enum { TIS_PREC_FP64 = 0, TIS_PREC_MIXED = 1 };
 #define TIS_E_NOISE_EXHAUSTED (-6)
 #define TIS_E_UNSUPPORTED (-7)
 #define TIS_E_NAN (-8)
+#define TIS_E_PMF_RANGE (-9)   /* a Mg-P pair came closer than the PMF table's first point (the reference stops: force_ele_DH.F90:90-93) */
 
 /* -------------------------------------------------------------- topology */
 /* One system (unit list + DT15 interaction tables) as read_nativeinfo and
@@ -126,6 +127,8 @@ typedef struct tis_topology {
                                       606-613); its energy goes to TIS_E_THBOND_DTRNA instead of
                                       TIS_E_HBOND_DTRNA (energy_dtrna_hbond15.F90:135-143).  NULL:
                                       every hydrogen bond is secondary ('S') */
+  const int32_t *flg_charge_fixed; /* (ncharge) nonzero: a CHARGE_CHANGE value, kept when i_charge = 1
+                                      (simu_ele_set.F90:152-158).  NULL: none fixed */
 } tis_topology;
 
 /* ---------------------------------------------------------------- params */
@@ -156,6 +159,17 @@ typedef struct tis_params {
   uint64_t seed;                   /* counter-based noise key */
   double hi_radius;                /* Brownian-HI: Rotne-Prager bead radius (radius(1) of HI_TENSOR%RPY) */
   int32_t n_step_hydro;            /* Brownian-HI: refactor D and its Cholesky factor every n steps (reference: 1) */
+  /* DT19 semi-explicit ions (i_dtrna_model = 2019) and Manning phosphate charges */
+  int32_t i_dtrna_model;           /* 2015 (or 0) or 2019: base-base exv contact exv_dist, others the radius sum
+                                      (force_exv_dt15.F90:60-66); no exv between a charged phosphate and an ion
+                                      (neighbor_assign.F90:524-537); Mg-P pairs on the PMF + DH table */
+  int32_t i_charge;                /* 0: topology charges; 1: every phosphate charge not fixed by
+                                      flg_charge_fixed is -Zp of its temperature (simu_ele_set.F90:107-166) */
+  double length_per_unit_P;        /* b, LENGTH_PER_UNIT of P (para/electrostatic.para: 4.38178046) */
+  int32_t pmf_nbin;                /* Mg-P potential of mean force on a uniform grid (setp_pmf.F90:31-105): */
+  double pmf_rmin, pmf_rbin, pmf_rmax; /* first point, spacing, last point read */
+  double pmf_rmerge;               /* pmf_merge: the switch from PMF to DH (simu_ele_set.F90:242-250) */
+  const double *pmf_mg_p;          /* (pmf_nbin) PMF values; NULL when the system has no Mg */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */

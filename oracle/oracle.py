@@ -62,6 +62,10 @@ def lib():
         L.orc_hydro_tensors.argtypes = [vp, C.c_int, C.c_double, f64p, f64p]
         L.orc_not_spd.argtypes = [vp]
         L.orc_nclamp.argtypes = [vp]
+        L.orc_pmf_range.argtypes = [vp]
+        L.orc_pmf_range.restype = C.c_int
+        L.orc_label_pmf.argtypes = [vp, C.c_int, f64p, f64p, f64p, C.c_int]
+        L.orc_label_pmf.restype = C.c_int
         L.orc_nclamp.restype = C.c_long
         L.orc_boltz_kcal_mol.restype = C.c_double
         _LIB = L
@@ -213,6 +217,17 @@ class Oracle:
 
     def nclamp(self):
         return self.L.orc_nclamp(self.h)
+
+    def pmf_range(self):
+        return self.L.orc_pmf_range(self.h)
+
+    def label_pmf(self, label):
+        """(Zp, PMF+DH energy table, force table) of a label."""
+        zp = C.c_double(0.0)
+        n = self.L.orc_label_pmf(self.h, label, C.byref(zp), None, None, 0)
+        e, f = np.zeros(max(n, 1)), np.zeros(max(n, 1))
+        self.L.orc_label_pmf(self.h, label, C.byref(zp), ptr_f64(e), ptr_f64(f), n)
+        return zp.value, e[:n], f[:n]
 
 
 BOLTZ_KCAL_MOL = None

@@ -56,6 +56,8 @@ inline double norm2_3(const double *a) { return std::sqrt(dot3(a, a)); }
 struct Label {           // per temperature label: simu_ele_set / simu_set_dtrna
   double tempk;
   double ek, coef, cdist;
+  double zp = 0.0;             // i_charge = 1: phosphate charge -zp (simu_ele_set.F90:107-166)
+  std::vector<double> pmf_e, pmf_f;   // pmfdh_energy / pmfdh_force (simu_ele_set.F90:231-253)
   std::vector<double> st_u0;   // coef_dtrna_st(0, ist, grep)
 };
 
@@ -77,6 +79,7 @@ struct Rep {
   bool unif_exhausted = false;
   long nclamp = 0;
   long nrebuild = 0;
+  int pmf_range = 0;              // a Mg-P pair below the PMF table's first point
   std::vector<double> hD, hL;     // Brownian-HI: diffuse_tensor, random_tensor (3N x 3N, column-major)
   int not_spd = 0;
 };
@@ -92,6 +95,10 @@ struct orc_ctx {
   std::vector<int> icharge2mp;
   std::vector<int> lmp2charge;
   std::vector<double> coef_charge;
+  std::vector<char> q_kind;        // 1: phosphate whose charge is -Zp of the label (i_charge = 1)
+  int n_mg = 0;                    // num_ion(IONTYPE%MG)
+  bool dt19 = false;               // i_dtrna_model = 2019
+  std::vector<double> pmf;         // inpmf%pmf(:, MG_P)
   int nbd = 0; std::vector<int> ibd2mp; std::vector<double> bd_nat, coef_bd;
   int nba = 0; std::vector<int> iba2mp; std::vector<double> ba_nat, coef_ba;
   int nst = 0; std::vector<int> st2mp; std::vector<double> st_nat, st_coef, st_hsTm;
@@ -142,9 +149,64 @@ void ele_set(const orc_ctx &c, Label &L) {
     ek = MM_A + MM_B * Tc + MM_C * Tc * Tc + MM_D * Tc * Tc * Tc;
   }
   L.ek = ek;
+  // simu_ele_set.F90:107-166: Manning condensation; with Mg in the DT19
+  // model the condensed fraction theta solves the two-ion balance
+  if (c.par.i_charge == 1) {
+    const double lb = ELE * ELE / (4.0e0 * F_PI * EPSI_0 * ek * BOLTZ_J * L.tempk) * 1.0e10;
+    const double b = c.par.length_per_unit_P;
+    if (c.dt19 && c.n_mg > 0) {
+      const double xi = lb / b, b3 = b * b * b;
+      const double conc_Mg = c.n_mg / (N_AVO * 1.0e-27 * c.par.psize[0] * c.par.psize[1] * c.par.psize[2]);
+      const double v1 = 4 * F_PI * b3 * (xi - 1.0e0) * 2;
+      const double v2 = 4 * F_PI * b3 * (xi - 0.5e0) * (2 + 1);
+      const double c1v1 = (N_AVO * 1.0e-27) * c.par.ionic_strength * v1;
+      const double c2v2 = (N_AVO * 1.0e-27) * conc_Mg * v2;
+      const double c1v1_2 = c1v1 * c1v1;
+      const double theta = (-c1v1_2 + std::sqrt(c1v1_2 * c1v1_2 + 8.0e0 * c1v1_2 * c2v2 * (1.0e0 - 1.0e0 / xi))) /
+                           (4.0e0 * c2v2);
+      L.zp = 1.0 - theta;
+    } else {
+      L.zp = b / lb;
+    }
+  }
   L.coef = JOUL2KCAL_MOL * 1.0e10 * (ELE * ELE) / (4.0e0 * F_PI * EPSI_0 * ek);
   L.cdist = 1.0e10 * std::sqrt((1.0e-3 * EPSI_0 * ek * BOLTZ_J) / (2.0 * N_AVO * (ELE * ELE))) *
             std::sqrt(L.tempk / c.par.ionic_strength);
+  // simu_ele_set.F90:231-253: the Mg-P table, PMF switched to DH beyond
+  // pmf_merge; the force of the last point is 0 (the reference never sets it)
+  L.pmf_e.clear(); L.pmf_f.clear();
+  if (c.dt19 && c.n_mg > 0 && !c.pmf.empty()) {
+    const int nb = c.par.pmf_nbin;
+    L.pmf_e.assign(nb, 0.0); L.pmf_f.assign(nb, 0.0);
+    for (int ib = 0; ib < nb; ++ib) {
+      const double r = c.par.pmf_rmin + c.par.pmf_rbin * (double)ib;
+      const double DH = JOUL2KCAL_MOL * 1.0e10 * (ELE * ELE) / (4.0e0 * F_PI * EPSI_0 * ek) * 2.0 * (-L.zp) *
+                        std::exp(-r / L.cdist) / r;
+      const double e_add = (DH - c.pmf[ib]) * std::exp(-(c.par.pmf_rmerge * c.par.pmf_rmerge) / (r * r));
+      L.pmf_e[ib] = c.pmf[ib] + e_add;
+    }
+    const double rbininv = 1.0 / c.par.pmf_rbin;
+    for (int ib = 0; ib + 1 < nb; ++ib) L.pmf_f[ib] = -rbininv * (L.pmf_e[ib + 1] - L.pmf_e[ib]);
+  }
+}
+
+// charge of charge entry ic for label L (coef_charge(ic, grep))
+inline double qch(const orc_ctx &c, const Label &L, int ic) {
+  return c.q_kind[ic] ? -L.zp : c.coef_charge[ic];
+}
+
+bool is_mg_p(const orc_ctx &c, int i1, int i2) {
+  const int t1 = c.imp2type[i1], t2 = c.imp2type[i2];
+  return (t1 == TIS_MP_RNA_PHOS && t2 == TIS_MP_ION_MG) || (t1 == TIS_MP_ION_MG && t2 == TIS_MP_RNA_PHOS);
+}
+
+// force_ele_DH.F90:87-100 / energy_ele_DH.F90:77-95: 0-based bin of a Mg-P
+// distance; below the first point the reference stops, here the pair takes
+// bin 0 and the replica records it
+int pmf_bin(const orc_ctx &c, Rep &r, double dist1) {
+  if (!(dist1 >= c.par.pmf_rmin)) { r.pmf_range = 1; return 0; }
+  int ib = (int)std::floor((dist1 - c.par.pmf_rmin) * (1.0 / c.par.pmf_rbin));
+  return std::min(ib, c.par.pmf_nbin - 1);
 }
 
 // simu_set_dtrna.F90:43-58 (i_temp_independent = 0)
@@ -274,8 +336,15 @@ void neighbor_exv(orc_ctx &c, Rep &r) {
               if (jmp + 1 < imp + 1 + nsep_of(c, imp)) ok = 0;
             }
           } else if (ci == TIS_CLASS_RNA && cj == TIS_CLASS_RNA) ok = 1;
-          else if ((ci == TIS_CLASS_RNA && cj == TIS_CLASS_ION) || (ci == TIS_CLASS_ION && cj == TIS_CLASS_RNA)) ok = 1;
-          else if ((ci == TIS_CLASS_ION && cj == TIS_CLASS_LIG) || (ci == TIS_CLASS_LIG && cj == TIS_CLASS_ION)) ok = 1;
+          else if ((ci == TIS_CLASS_RNA && cj == TIS_CLASS_ION) || (ci == TIS_CLASS_ION && cj == TIS_CLASS_RNA)) {
+            ok = 1;
+            // neighbor_assign.F90:524-537: no exv between a charged phosphate and an ion
+            if (c.dt19) {
+              const Label &L = c.lab[r.label - 1];
+              int pb = (c.imp2type[imp] == TIS_MP_RNA_PHOS) ? imp : (c.imp2type[jmp] == TIS_MP_RNA_PHOS ? jmp : -1);
+              if (pb >= 0 && c.lmp2charge[pb] >= 0 && std::fabs(qch(c, L, c.lmp2charge[pb])) > ZERO_JUDGE) ok = 0;
+            }
+          } else if ((ci == TIS_CLASS_ION && cj == TIS_CLASS_LIG) || (ci == TIS_CLASS_LIG && cj == TIS_CLASS_ION)) ok = 1;
           if (ok) {
             r.iexv2mp.push_back(imp + 1);
             r.iexv2mp.push_back(jmp + 1);
@@ -316,10 +385,10 @@ void neighbor_ele(orc_ctx &c, Rep &r) {
   const bool peri = c.par.i_periodic == 1;
   const double *X = peri ? r.pxyz.data() : r.xyz.data();
   for (int ic = 0; ic < c.ncharge - 1; ++ic) {
-    if (std::fabs(c.coef_charge[ic]) < ZERO_JUDGE) continue;
+    if (std::fabs(qch(c, L, ic)) < ZERO_JUDGE) continue;
     int imp = c.icharge2mp[ic];
     for (int jc = ic + 1; jc < c.ncharge; ++jc) {
-      if (std::fabs(c.coef_charge[jc]) < ZERO_JUDGE) continue;
+      if (std::fabs(qch(c, L, jc)) < ZERO_JUDGE) continue;
       int jmp = c.icharge2mp[jc];
       double v21[3];
       for (int k = 0; k < 3; ++k) v21[k] = X[3 * jmp + k] - X[3 * imp + k];
@@ -330,8 +399,8 @@ void neighbor_ele(orc_ctx &c, Rep &r) {
         r.iele2mp.push_back(imp + 1);
         r.iele2mp.push_back(jmp + 1);
         r.iele2mp.push_back(peri ? imirror : 1);
-        r.iele2mp.push_back(0);
-        r.coef_ele.push_back(c.coef_charge[ic] * c.coef_charge[jc] * L.coef);
+        r.iele2mp.push_back((c.dt19 && is_mg_p(c, imp, jmp)) ? 1 : 0);   // neighbor_list_ele.F90:167-174
+        r.coef_ele.push_back(qch(c, L, ic) * qch(c, L, jc) * L.coef);
       }
     }
   }
@@ -881,9 +950,13 @@ void force_dtrna_hbond15(orc_ctx &c, Rep &r, double *F) {
   }
 }
 
-// force_exv_dt15.F90:204-265 (i_dtrna_model = 2015)
+// force_exv_dt15.F90:60-78
 double exv_dij(const orc_ctx &c, int i1, int i2) {
   int t1 = c.imp2type[i1], t2 = c.imp2type[i2];
+  if (c.dt19) {
+    if (t1 == TIS_MP_RNA_BASE && t2 == TIS_MP_RNA_BASE) return c.par.exv_dist;
+    return c.exv_radius[i1] + c.exv_radius[i2];
+  }
   if (t1 == TIS_MP_RNA_PHOS && t2 == TIS_MP_RNA_SUGAR) return c.par.exv_dist_PS;
   if (t1 == TIS_MP_RNA_SUGAR && t2 == TIS_MP_RNA_PHOS) return c.par.exv_dist_PS;
   if (c.iclass_mp[i1] == TIS_CLASS_RNA && c.iclass_mp[i2] == TIS_CLASS_RNA) return c.par.exv_dist;
@@ -917,7 +990,8 @@ void force_exv_dt15(const orc_ctx &c, Rep &r, double *F) {
   }
 }
 
-// force_ele_DH.F90:42-117 (no PMF pairs)
+// force_ele_DH.F90:42-117; Mg-P pairs of the DT19 model within pmf_rmax
+// take the table force (:87-97)
 void force_ele_DH(const orc_ctx &c, Rep &r, double *F) {
   const Label &L = c.lab[r.label - 1];
   double cutoff2 = sq(c.par.cutoff_ele * L.cdist);
@@ -931,10 +1005,15 @@ void force_ele_DH(const orc_ctx &c, Rep &r, double *F) {
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
     double rdist1 = 1.0 / dist1;
-    // coef_ele(iele) = coef_charge(i) * coef_charge(j) * inele%coef(grep), kept
-    // current for the replica's temperature by simu_para2.F90
-    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
-    double dv = ce * rdist1 * rdist1 * (rdist1 + rcdist) * std::exp(-dist1 * rcdist);
+    double dv;
+    if (r.iele2mp[4 * e + 3] > 0 && !L.pmf_f.empty() && dist1 <= c.par.pmf_rmax) {
+      dv = rdist1 * L.pmf_f[pmf_bin(c, r, dist1)];
+    } else {
+      // coef_ele(iele) = coef_charge(i) * coef_charge(j) * inele%coef(grep), kept
+      // current for the replica's temperature by simu_para2.F90
+      double ce = qch(c, L, c.lmp2charge[i1]) * qch(c, L, c.lmp2charge[i2]) * L.coef;
+      dv = ce * rdist1 * rdist1 * (rdist1 + rcdist) * std::exp(-dist1 * rcdist);
+    }
     if (dv > DE_MAX) { dv = DE_MAX; r.nclamp++; }
     for (int k = 0; k < 3; ++k) {
       double fk = dv * v21[k];
@@ -957,7 +1036,7 @@ void force_ele_coulomb(const orc_ctx &c, Rep &r, double *F) {
     double dist2 = dot3(v21, v21);
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
-    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    double ce = qch(c, L, c.lmp2charge[i1]) * qch(c, L, c.lmp2charge[i2]) * L.coef;
     double dv_dr = ce / (dist1 * dist2);
     for (int k = 0; k < 3; ++k) {
       double fk = dv_dr * v21[k];
@@ -979,7 +1058,7 @@ void force_ele_ewald(const orc_ctx &c, Rep &r, double *F) {
     for (int ic = 0; ic < c.ncharge; ++ic) {
       int imp = c.icharge2mp[ic];
       double dp = dot3(k, &r.pxyz[3 * imp]);
-      double q1 = c.coef_charge[ic];
+      double q1 = qch(c, L, ic);
       qc[ic] = q1 * std::cos(dp);
       qs[ic] = q1 * std::sin(dp);
     }
@@ -1000,7 +1079,7 @@ void force_ele_ewald(const orc_ctx &c, Rep &r, double *F) {
     double dist2 = dot3(v21, v21);
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
-    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    double ce = qch(c, L, c.lmp2charge[i1]) * qch(c, L, c.lmp2charge[i2]) * L.coef;
     double dv = ce * (std::erfc(c.par.ewld_alpha * dist1) / dist1 + beta * std::exp(-alpha2 * dist2)) / dist2;
     for (int k = 0; k < 3; ++k) {
       double fk = dv * v21[k];
@@ -1187,9 +1266,16 @@ double energy_DH(const orc_ctx &c, const Rep &r) {
     double dist2 = dot3(v, v);
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
+    if (r.iele2mp[4 * k + 3] > 0 && !L.pmf_e.empty() && dist1 <= c.par.pmf_rmax) {
+      // energy_ele_DH.F90:77-95: linear between the table points
+      Rep &rw = const_cast<Rep &>(r);
+      const int ib = pmf_bin(c, rw, dist1);
+      e += L.pmf_e[ib] - L.pmf_f[ib] * (dist1 - (c.par.pmf_rmin + (double)ib * c.par.pmf_rbin));
+      continue;
+    }
     // coef_ele is rebuilt with the current label's coef (simu_para2.F90)
     int ic = c.lmp2charge[i1], jc = c.lmp2charge[i2];
-    double ce = c.coef_charge[ic] * c.coef_charge[jc] * L.coef;
+    double ce = qch(c, L, ic) * qch(c, L, jc) * L.coef;
     e += ce / dist1 * std::exp(-dist1 * rcdist);
   }
   return e;
@@ -1206,7 +1292,7 @@ double energy_coulomb(const orc_ctx &c, const Rep &r) {
     double dist2 = dot3(v, v);
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
-    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    double ce = qch(c, L, c.lmp2charge[i1]) * qch(c, L, c.lmp2charge[i2]) * L.coef;
     e += ce * (1.0e0 / dist1 - cut_inv);
   }
   return e;
@@ -1221,8 +1307,8 @@ double energy_ewald(const orc_ctx &c, const Rep &r) {
     for (int ic = 0; ic < c.ncharge; ++ic) {
       int imp = c.icharge2mp[ic];
       double dp = dot3(k, &r.pxyz[3 * imp]);
-      scos += c.coef_charge[ic] * std::cos(dp);
-      ssin += c.coef_charge[ic] * std::sin(dp);
+      scos += qch(c, L, ic) * std::cos(dp);
+      ssin += qch(c, L, ic) * std::sin(dp);
     }
     e_f += c.ewld_f_coef[ig] * (scos * scos + ssin * ssin);
   }
@@ -1235,11 +1321,11 @@ double energy_ewald(const orc_ctx &c, const Rep &r) {
     double dist2 = dot3(v, v);
     if (dist2 > cutoff2) continue;
     double dist1 = std::sqrt(dist2);
-    double ce = c.coef_charge[c.lmp2charge[i1]] * c.coef_charge[c.lmp2charge[i2]] * L.coef;
+    double ce = qch(c, L, c.lmp2charge[i1]) * qch(c, L, c.lmp2charge[i2]) * L.coef;
     e_r += ce * std::erfc(c.par.ewld_alpha * dist1) / dist1;
   }
   double qq = 0;
-  for (int ic = 0; ic < c.ncharge; ++ic) qq += c.coef_charge[ic] * c.coef_charge[ic];
+  for (int ic = 0; ic < c.ncharge; ++ic) qq += qch(c, L, ic) * qch(c, L, ic);
   double e_s = c.ewld_s_coef * qq;
   return L.coef * (e_f + e_s) + e_r;
 }
@@ -1379,6 +1465,15 @@ orc_ctx *orc_create(const tis_topology *t, const tis_params *p, int nrep, const 
   c->lmp2charge.assign(t->nmp, -1);
   for (int i = 0; i < t->ncharge; ++i) { c->icharge2mp[i] = t->icharge2mp[i] - 1; c->lmp2charge[c->icharge2mp[i]] = i; }
   c->coef_charge.assign(t->coef_charge, t->coef_charge + t->ncharge);
+  c->dt19 = p->i_dtrna_model == 2019;
+  c->n_mg = 0;
+  for (int i = 0; i < t->nmp; ++i) c->n_mg += (t->imp2type[i] == TIS_MP_ION_MG) ? 1 : 0;
+  c->q_kind.assign(t->ncharge, 0);
+  for (int i = 0; i < t->ncharge; ++i)   // simu_ele_set.F90:150-166
+    c->q_kind[i] = (p->i_charge == 1 && t->imp2type[t->icharge2mp[i] - 1] == TIS_MP_RNA_PHOS &&
+                    !(t->flg_charge_fixed && t->flg_charge_fixed[i])) ? 1 : 0;
+  if (c->dt19 && c->n_mg > 0 && p->pmf_mg_p && p->pmf_nbin > 1) c->pmf.assign(p->pmf_mg_p, p->pmf_mg_p + p->pmf_nbin);
+  c->par.pmf_mg_p = nullptr;   // borrowed by the caller; the copy above is the ctx's
   c->nbd = t->nbd; c->ibd2mp.assign(t->ibd2mp, t->ibd2mp + 2 * t->nbd);
   c->bd_nat.assign(t->bd_nat, t->bd_nat + t->nbd); c->coef_bd.assign(t->coef_bd, t->coef_bd + t->nbd);
   c->nba = t->nba; c->iba2mp.assign(t->iba2mp, t->iba2mp + 3 * t->nba);
@@ -1914,6 +2009,25 @@ long orc_nclamp(orc_ctx *c) {
   long s = 0;
   for (auto &r : c->rep) s += r.nclamp;
   return s;
+}
+
+int orc_pmf_range(orc_ctx *c) {
+  int f = 0;
+  for (auto &r : c->rep) f |= r.pmf_range;
+  return f;
+}
+
+// Zp of a label and its Mg-P table (energy, force; n entries each).  Returns
+// the table length, 0 when the label has none.
+int orc_label_pmf(orc_ctx *c, int label, double *zp, double *e, double *f, int cap) {
+  const Label &L = c->lab[label - 1];
+  if (zp) *zp = L.zp;
+  const int n = (int)L.pmf_e.size();
+  for (int i = 0; i < std::min(n, cap); ++i) {
+    if (e) e[i] = L.pmf_e[i];
+    if (f) f[i] = L.pmf_f[i];
+  }
+  return n;
 }
 
 double orc_boltz_kcal_mol(void) { return BOLTZ_KCAL_MOL; }

@@ -60,6 +60,9 @@ SYSTEMS = {
     "c1_walk": (c1_system, {}),
     "hairpin_tertiary": (synth.hairpin_tertiary, {}),
     "ninfo_hairpin": (ninfo_hairpin, {}),
+    # DT19 semi-explicit Mg: NHT19 exv rules, Manning charges, Mg-P table
+    "dt19_mg": (synth.dt19_mg_system, dict(_base=synth.dt19_params, i_periodic=1, psize=(80.0, 80.0, 80.0),
+                                           ionic_strength=0.1)),
     "hairpin_coulomb": (hairpin, dict(i_ele=3, cutoff_ele=60.0)),
     "hairpin": (hairpin, {}),
     "dense": (dense, {}),
@@ -70,7 +73,12 @@ SYSTEMS = {
 def make_pair(name, precision, nrep=1, temps=None, **over):
     fn, extra = SYSTEMS[name]
     s = fn()
-    par = synth.dt15_params(ionic_strength=0.15, precision=precision, **extra, **over)
+    extra = dict(extra)
+    base = extra.pop("_base", synth.dt15_params)
+    kw = dict(ionic_strength=0.15, precision=precision)
+    kw.update(extra)
+    kw.update(over)
+    par = base(**kw)
     temps = temps or [300.0] * nrep
     eng = Engine([s], par, temps, nrep=[nrep])
     orc = Oracle(s, par, temps)
@@ -119,7 +127,7 @@ def test_force_mixed(tis_lib, name):
 
 
 @pytest.mark.parametrize("name", ["c1_walk", "hairpin", "dense", "hairpin_tertiary", "hairpin_coulomb",
-                                  "ninfo_hairpin"])
+                                  "ninfo_hairpin", "dt19_mg"])
 def test_energy_fp64(tis_lib, name):
     s, par, eng, orc = make_pair(name, 0)
     eng.neighbor(); orc.neighbor()

@@ -32,6 +32,7 @@ TIS_E_TIMEOUT = -5
 TIS_E_NOISE_EXHAUSTED = -6
 TIS_E_UNSUPPORTED = -7
 TIS_E_NAN = -8
+TIS_E_PMF_RANGE = -9
 
 _i32p = C.POINTER(C.c_int32)
 _f64p = C.POINTER(C.c_double)
@@ -55,7 +56,7 @@ class Topology(C.Structure):
         ("nwca", C.c_int32), ("iwca2mp", _i32p), ("wca_nat", _f64p), ("coef_wca", _f64p),
         ("ntst", C.c_int32), ("idtrna_tst2mp", _i32p), ("dtrna_tst_nat", _f64p),
         ("coef_dtrna_tst", _f64p), ("idtrna_tst2side", _i32p), ("flg_tst_exclusive", _i32p),
-        ("flg_hb_tertiary", _i32p),
+        ("flg_hb_tertiary", _i32p), ("flg_charge_fixed", _i32p),
     ]
 
 
@@ -74,6 +75,9 @@ class Params(C.Structure):
         ("viscosity", C.c_double), ("wca_coef_cutoff", C.c_double),
         ("precision", C.c_int32), ("hb_beta_global", C.c_int32), ("seed", C.c_uint64),
         ("hi_radius", C.c_double), ("n_step_hydro", C.c_int32),
+        ("i_dtrna_model", C.c_int32), ("i_charge", C.c_int32), ("length_per_unit_P", C.c_double),
+        ("pmf_nbin", C.c_int32), ("pmf_rmin", C.c_double), ("pmf_rbin", C.c_double), ("pmf_rmax", C.c_double),
+        ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p),
     ]
 
 
@@ -111,10 +115,10 @@ _TOPO_ARRAYS = {
     "iwca2mp": np.int32, "wca_nat": np.float64, "coef_wca": np.float64,
     "idtrna_tst2mp": np.int32, "dtrna_tst_nat": np.float64, "coef_dtrna_tst": np.float64,
     "idtrna_tst2side": np.int32, "flg_tst_exclusive": np.int32,
-    "flg_hb_tertiary": np.int32,
+    "flg_hb_tertiary": np.int32, "flg_charge_fixed": np.int32,
 }
 # Arrays the library accepts as NULL (their absence has a meaning of its own).
-_TOPO_OPTIONAL = ("flg_hb_tertiary",)
+_TOPO_OPTIONAL = ("flg_hb_tertiary", "flg_charge_fixed")
 _TOPO_COUNTS = ("nmp", "nunit", "ncharge", "nbd", "nba", "nst", "nhb", "nhbsite", "nfene", "nwca", "ntst")
 
 
@@ -142,11 +146,19 @@ def make_topology(sysd: dict):
 
 
 def make_params(**kw) -> Params:
+    """A ``Params`` from keyword values; ``pmf_mg_p`` takes an array, which
+    the returned struct keeps referenced (``p._keep``)."""
     p = Params()
+    p._keep = []
     for k, v in kw.items():
         if k == "psize":
             for i in range(3):
                 p.psize[i] = float(v[i])
+        elif k == "pmf_mg_p":
+            if v is not None:
+                a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))
+                p._keep.append(a)
+                p.pmf_mg_p = a.ctypes.data_as(_f64p)
         else:
             setattr(p, k, v)
     return p

@@ -134,6 +134,8 @@ struct tis_ctx {
   DBuf<int> site_exc;
   DBuf<uint8_t> mirror, hb_flag;
   DBuf<uint8_t> hb_tert;            // (hb) 1: tertiary ('T') hydrogen bond
+  DBuf<uint8_t> b_qkind;            // (bead) 1: phosphate charge -Zp of the label (i_charge = 1)
+  DBuf<double> lab_zp, pmf_e, pmf_f; // per label: Zp; Mg-P table (pmf_nbin per label)
   DBuf<double> hb_ene;
   DBuf<unsigned char> slots;
   DBuf<double> noise, unif;
@@ -195,6 +197,42 @@ void ele_params(const tis_params &p, double tempk, double &ek, double &coef, dou
   coef = JOUL2KCAL_MOL * 1.0e10 * (ELE * ELE) / (4.0e0 * F_PI * EPSI_0 * ek);
   cdist = 1.0e10 * std::sqrt((1.0e-3 * EPSI_0 * ek * BOLTZ_J) / (2.0 * N_AVO * (ELE * ELE))) *
           std::sqrt(tempk / p.ionic_strength);
+}
+
+// simu_ele_set.F90:107-151: Manning condensation on the phosphates.  The
+// DT19 model with Mg balances monovalent and Mg condensation (theta); else
+// Zp = b / l_B.  ek is the dielectric constant at temperature tempk.
+double manning_zp(const tis_params &p, double tempk, double ek, int n_mg, bool dt19) {
+  const double lb = ELE * ELE / (4.0e0 * F_PI * EPSI_0 * ek * BOLTZ_J * tempk) * 1.0e10;
+  const double b = p.length_per_unit_P;
+  if (!(dt19 && n_mg > 0)) return b / lb;
+  const double xi = lb / b, b3 = b * b * b;
+  const double conc_Mg = n_mg / (N_AVO * 1.0e-27 * p.psize[0] * p.psize[1] * p.psize[2]);
+  const double v1 = 4 * F_PI * b3 * (xi - 1.0e0) * 2;
+  const double v2 = 4 * F_PI * b3 * (xi - 0.5e0) * (2 + 1);
+  const double c1v1 = (N_AVO * 1.0e-27) * p.ionic_strength * v1;
+  const double c2v2 = (N_AVO * 1.0e-27) * conc_Mg * v2;
+  const double c1v1_2 = c1v1 * c1v1;
+  const double theta =
+      (-c1v1_2 + std::sqrt(c1v1_2 * c1v1_2 + 8.0e0 * c1v1_2 * c2v2 * (1.0e0 - 1.0e0 / xi))) / (4.0e0 * c2v2);
+  return 1.0 - theta;
+}
+
+// simu_ele_set.F90:231-253: Mg-P energy table = PMF, switched to the DH
+// energy of charges +2 and -Zp below pmf_rmerge, and its finite-difference
+// force; the force of the last point is 0 (the reference never sets it).
+// coef is the DH coefficient of the temperature, cdist the Debye length.
+void pmf_table(const tis_params &p, double coef, double cdist, double zp, double *e, double *f) {
+  const int nb = p.pmf_nbin;
+  for (int ib = 0; ib < nb; ++ib) {
+    const double r = p.pmf_rmin + p.pmf_rbin * (double)ib;
+    const double DH = coef * 2.0 * (-zp) * std::exp(-r / cdist) / r;
+    const double e_add = (DH - p.pmf_mg_p[ib]) * std::exp(-(p.pmf_rmerge * p.pmf_rmerge) / (r * r));
+    e[ib] = p.pmf_mg_p[ib] + e_add;
+  }
+  const double rbininv = 1.0 / p.pmf_rbin;
+  for (int ib = 0; ib + 1 < nb; ++ib) f[ib] = -rbininv * (e[ib + 1] - e[ib]);
+  f[nb - 1] = 0.0;
 }
 
 template <typename T>
@@ -286,6 +324,30 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     tis_destroy(c);
     return TIS_E_UNSUPPORTED;
   }
+  // DT19 semi-explicit ions: its Mg-P table lives in the Debye-Hueckel
+  // routines (force_ele_DH.F90, energy_ele_DH.F90); Manning charges here
+  // feed DH and plain Coulomb
+  const bool dt19 = p.i_dtrna_model == 2019;
+  if (!(p.i_dtrna_model == 0 || p.i_dtrna_model == 2015 || dt19) || (p.i_charge != 0 && p.i_charge != 1) ||
+      (p.i_charge == 1 && !(p.length_per_unit_P > 0.0))) {
+    tis_destroy(c);
+    return TIS_E_ARG;
+  }
+  if ((dt19 && p.i_ele != TIS_ELE_DH) || (p.i_charge == 1 && p.i_ele == TIS_ELE_EWALD) || (dt19 && c->bdhi)) {
+    tis_destroy(c);
+    return TIS_E_UNSUPPORTED;
+  }
+  int n_mg_any = 0;
+  for (int k = 0; k < ntop; ++k)
+    for (int i = 0; i < tops[k].nmp; ++i) n_mg_any += tops[k].imp2type[i] == TIS_MP_ION_MG;
+  // simu_ele_set.F90:231-236: the semi-explicit model with Mg needs i_charge
+  // = 1, the table (setp_pmf.F90) and the box that gives [Mg]
+  if (dt19 && n_mg_any > 0 &&
+      (p.i_charge != 1 || !p.pmf_mg_p || p.pmf_nbin < 2 || !(p.pmf_rbin > 0.0) || !(p.pmf_rmax >= p.pmf_rmin) ||
+       !(p.pmf_rmin > 0.0) || p.i_periodic != 1 || !(p.psize[0] * p.psize[1] * p.psize[2] > 0.0))) {
+    tis_destroy(c);
+    return TIS_E_ARG;
+  }
   if (p.i_ele == TIS_ELE_EWALD) {
     // mloop_ewld.F90 uses psize(1) for a cubic box; the per-charge tables
     // hold |h| <= 11
@@ -309,6 +371,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<double> st_hsTm_all;
   std::vector<uint8_t> hb_tert;
   bool any_tert = false;
+  std::vector<uint8_t> b_qkind;
+  std::vector<int> top_nmg(ntop, 0);
   std::vector<int> tst_idx, stx_ptr, stx_tst;
   std::vector<double> tst_nat, tst_coef;
   std::vector<int> fene_idx, wca_idx, bdp;
@@ -397,12 +461,22 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       u_class.push_back(t.iclass_unit[u]);
     }
     std::vector<double> q(t.nmp, 0.0);
-    for (int i = 0; i < t.ncharge; ++i) q[t.icharge2mp[i] - 1] = t.coef_charge[i];
+    std::vector<uint8_t> qk(t.nmp, 0);
+    for (int i = 0; i < t.ncharge; ++i) {
+      const int b = t.icharge2mp[i] - 1;
+      if (b < 0 || b >= t.nmp) { tis_destroy(c); return TIS_E_ARG; }
+      q[b] = t.coef_charge[i];
+      // simu_ele_set.F90:150-166: with i_charge = 1 every phosphate that no
+      // CHARGE_CHANGE line fixes carries -Zp of its temperature (Zp > 0)
+      if (p.i_charge == 1 && t.imp2type[b] == TIS_MP_RNA_PHOS && !(t.flg_charge_fixed && t.flg_charge_fixed[i]))
+        qk[b] = 1;
+    }
+    for (int i = 0; i < t.nmp; ++i) top_nmg[k] += t.imp2type[i] == TIS_MP_ION_MG;
     // charged beads in icharge order (neighbor_list_ele.F90:126,138 skip |q| < ZERO_JUDGE)
     d.q0 = (int)q_bead.size();
     for (int i = 0; i < t.ncharge; ++i) {
       if (i > 0 && t.icharge2mp[i] <= t.icharge2mp[i - 1]) { tis_destroy(c); return TIS_E_ARG; }
-      if (std::fabs(t.coef_charge[i]) >= 1.0e-6) q_bead.push_back(t.icharge2mp[i] - 1);
+      if (qk[t.icharge2mp[i] - 1] || std::fabs(t.coef_charge[i]) >= 1.0e-6) q_bead.push_back(t.icharge2mp[i] - 1);
     }
     d.nq = (int)q_bead.size() - d.q0;
     for (int i = 0; i < t.nmp; ++i) {
@@ -415,6 +489,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       b_radius.push_back(t.exv_radius[i]);
       b_eps.push_back(t.exv_epsilon[i]);
       b_charge.push_back(q[i]);
+      b_qkind.push_back(qk[i]);
       // time_integral_pre.F90:162-170
       double tfh = 0.5e0 * p.tstep * t.fric[i];
       double u1 = 1.0e0 - tfh;
@@ -434,7 +509,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       }
       for (int i = 0; i < t.nmp; ++i) {
         double sc;
-        if (t.iclass_unit[imp2unit[i]] == TIS_CLASS_RNA)
+        if (dt19)   // force_exv_dt15.F90:60-66: base-base exv_dist, every other pair the radius sum
+          sc = std::max(p.exv_dist, t.exv_radius[i] + rmax_all);
+        else if (t.iclass_unit[imp2unit[i]] == TIS_CLASS_RNA)
           sc = std::max(std::max(p.exv_dist, p.exv_dist_PS), rmax_non_rna > 0 ? t.exv_radius[i] + rmax_non_rna : 0.0);
         else
           sc = t.exv_radius[i] + rmax_all;
@@ -565,6 +642,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->nlane = nlane;
   c->nlabel = nlane;
   std::vector<double> lab_T(nlane), lab_coef(nlane), lab_cdist(nlane), lab_beta(nlane), lab_rele2(nlane);
+  std::vector<double> lab_zp(nlane, 0.0), pmf_e, pmf_f;
+  const bool pmf_on = dt19 && n_mg_any > 0;
+  if (pmf_on) { pmf_e.assign((size_t)nlane * p.pmf_nbin, 0.0); pmf_f.assign((size_t)nlane * p.pmf_nbin, 0.0); }
   std::vector<int> lab_u0off(nlane), lab_c1off(nlane);
   std::vector<double> lab_u0, lab_c1;
   c->label_top.resize(nlane);
@@ -587,6 +667,9 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       lab_T[lane] = T;
       lab_coef[lane] = coef;
       lab_cdist[lane] = cdist;
+      if (p.i_charge == 1) lab_zp[lane] = manning_zp(p, T, ek, top_nmg[k], dt19);
+      if (pmf_on && top_nmg[k] > 0)
+        pmf_table(p, coef, cdist, lab_zp[lane], &pmf_e[(size_t)lane * p.pmf_nbin], &pmf_f[(size_t)lane * p.pmf_nbin]);
       lab_beta[lane] = 1.0e0 / (T * BOLTZ_KCAL_MOL);
       double rr = (p.i_ele == TIS_ELE_DH) ? (p.neigh_margin + p.cutoff_ele * cdist) : (p.neigh_margin + p.cutoff_ele);
       lab_rele2[lane] = rr * rr;
@@ -698,6 +781,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->hb_idx.upload(hb_idx)); CK(c->hb_nat.upload(hb_nat)); CK(c->hb_coef.upload(hb_coef));
   CK(c->hb_site.upload(hb_site)); CK(c->hb_nd2.upload(hb_nd2));
   if (any_tert) CK(c->hb_tert.upload(hb_tert));
+  if (p.i_charge == 1) { CK(c->b_qkind.upload(b_qkind)); CK(c->lab_zp.upload(lab_zp)); }
+  if (pmf_on) { CK(c->pmf_e.upload(pmf_e)); CK(c->pmf_f.upload(pmf_f)); }
   CK(c->site_val.upload(site_val)); CK(c->site_ptr.upload(site_ptr)); CK(c->site_hb.upload(site_hb));
   CK(c->inc_ptr.upload(inc_ptr)); CK(c->inc_slot.upload(inc_slot)); CK(c->q_bead.upload(q_bead));
   CK(c->lab_Td.upload(lab_T)); CK(c->lab_coef.upload(lab_coef)); CK(c->lab_cdist.upload(lab_cdist));
@@ -809,7 +894,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->site_val.free(); c->site_ptr.free(); c->site_hb.free(); c->inc_ptr.free(); c->inc_slot.free();
   c->q_bead.free();
   c->bd_nat.free(); c->bd_coef.free(); c->ba_nat.free(); c->ba_coef.free(); c->st_nat.free(); c->st_coef.free();
-  c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free(); c->hb_tert.free();
+  c->hb_nat.free(); c->hb_coef.free(); c->hb_nd2.free(); c->hb_tert.free(); c->b_qkind.free(); c->lab_zp.free(); c->pmf_e.free(); c->pmf_f.free();
   c->lab_Td.free(); c->lab_coef.free(); c->lab_cdist.free(); c->lab_beta.free(); c->lab_rele2.free();
   c->lab_u0.free(); c->lab_c1.free(); c->lab_u0off.free(); c->lab_c1off.free(); c->elabel.free();
   c->ebeta.free(); c->e_opp.free(); c->rex_u.free(); c->d_rep2lab.free(); c->d_lab2rep.free(); c->rex.free();
@@ -993,6 +1078,11 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.stx_ptr = c->stx_ptr.p; a.stx_tst = c->stx_tst.p;
   a.hb_idx = c->hb_idx.p; a.hb_nat = c->hb_nat.p; a.hb_coef = c->hb_coef.p; a.hb_site = c->hb_site.p;
   a.hb_tert = c->hb_tert.p;
+  a.dt19 = p.i_dtrna_model == 2019;
+  a.b_qkind = c->b_qkind.p; a.lab_zp = c->lab_zp.p;
+  a.pmf_e = c->pmf_e.p; a.pmf_f = c->pmf_f.p;
+  a.pmf_nbin = p.pmf_nbin; a.pmf_rmin = p.pmf_rmin; a.pmf_rbin = p.pmf_rbin; a.pmf_rmax = p.pmf_rmax;
+  a.pmf_rbininv = (p.pmf_rbin > 0.0) ? 1.0 / p.pmf_rbin : 0.0;
   a.hb_nd2 = c->hb_nd2.p;
   a.site_val = c->site_val.p; a.site_ptr = c->site_ptr.p; a.site_hb = c->site_hb.p;
   a.inc_ptr = c->inc_ptr.p; a.inc_slot = c->inc_slot.p; a.q_bead = c->q_bead.p;
@@ -1043,6 +1133,8 @@ int check_lanes(tis_ctx *c) {
   int code = TIS_OK;
   for (int i = 0; i < c->nlane; ++i) {
     if (ls[i].flags & LF_NAN) code = fail(c, TIS_E_NAN, "non-finite force in lane " + std::to_string(i + 1));
+    if (ls[i].flags & LF_PMF)
+      code = fail(c, TIS_E_PMF_RANGE, "Mg-P pair below the PMF table in lane " + std::to_string(i + 1));
     if (ls[i].flags & LF_OVERFLOW) code = fail(c, TIS_E_LIST_OVERFLOW, "hbond site list overflow");
     if (ls[i].flags & (LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED))
       code = fail(c, TIS_E_NOISE_EXHAUSTED, "injected noise or uniforms exhausted");
@@ -1129,11 +1221,22 @@ extern "C" int tis_get_ele_list(tis_ctx *c, int32_t irep, int32_t *iele2mp, doub
   const bool peri = c->par.i_periodic == 1;
   const uint32_t *mele = m.data() + (size_t)N * W;
   std::vector<double> q(N);
+  std::vector<int8_t> typ(N);
   CK(cudaMemcpy(q.data(), c->b_charge.p + T.bead0, N * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(typ.data(), c->b_type.p + T.bead0, N, cudaMemcpyDeviceToHost));
   std::vector<LaneState> ls(1);
   CK(cudaMemcpy(ls.data(), c->d_lstate.p + lane, sizeof(LaneState), cudaMemcpyDeviceToHost));
   double coefT = 0.0;
   CK(cudaMemcpy(&coefT, c->lab_coef.p + ls[0].label, sizeof(double), cudaMemcpyDeviceToHost));
+  if (c->b_qkind.p) {   // i_charge = 1: the label's phosphate charge
+    std::vector<uint8_t> qk(N);
+    double zp = 0.0;
+    CK(cudaMemcpy(qk.data(), c->b_qkind.p + T.bead0, N, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&zp, c->lab_zp.p + ls[0].label, sizeof(double), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < N; ++i)
+      if (qk[i]) q[i] = -zp;
+  }
+  const bool dt19 = c->par.i_dtrna_model == 2019;
   int k = 0;
   for (int i = 0; i < N; ++i)
     for (int j = i + 1; j < N; ++j) {
@@ -1143,7 +1246,9 @@ extern "C" int tis_get_ele_list(tis_ctx *c, int32_t irep, int32_t *iele2mp, doub
           iele2mp[4 * k] = i + 1;
           iele2mp[4 * k + 1] = j + 1;
           iele2mp[4 * k + 2] = peri ? (int)mir[(size_t)i * N + j] : 1;
-          iele2mp[4 * k + 3] = 0;
+          // neighbor_list_ele.F90:167-174: PMFTYPE%MG_P = 1 for Mg-P pairs of the DT19 model
+          iele2mp[4 * k + 3] = (dt19 && ((typ[i] == TIS_MP_RNA_PHOS && typ[j] == TIS_MP_ION_MG) ||
+                                         (typ[i] == TIS_MP_ION_MG && typ[j] == TIS_MP_RNA_PHOS))) ? 1 : 0;
         }
         if (coef_ele) coef_ele[k] = q[i] * q[j] * coefT;
       }
@@ -1575,6 +1680,7 @@ extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xy
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (after.flags & LF_NAN) return fail(c, TIS_E_NAN, "non-finite force in lane " + std::to_string(irep));
+  if (after.flags & LF_PMF) return fail(c, TIS_E_PMF_RANGE, "Mg-P pair below the PMF table in lane " + std::to_string(irep));
   if (after.flags & LF_OVERFLOW) return fail(c, TIS_E_LIST_OVERFLOW, "hbond site list overflow");
   if (after.flags & (LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED))
     return fail(c, TIS_E_NOISE_EXHAUSTED, "injected noise or uniforms exhausted");

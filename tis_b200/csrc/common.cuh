@@ -73,7 +73,7 @@ struct LaneState {
   int need_rebuild;
 };
 
-enum LaneFlags { LF_OVERFLOW = 1, LF_NAN = 2, LF_UNIF_EXHAUSTED = 4, LF_NOISE_EXHAUSTED = 8 };
+enum LaneFlags { LF_OVERFLOW = 1, LF_NAN = 2, LF_UNIF_EXHAUSTED = 4, LF_NOISE_EXHAUSTED = 8, LF_PMF = 16 };
 
 enum KMode {
   KM_NEIGHBOR = 1,     // rebuild lists (wrap pxyz if periodic)
@@ -161,6 +161,13 @@ struct KArgs {
   const int *site_val; const int *site_ptr; const int *site_hb;
   const int *inc_ptr; const int *inc_slot;
   const int *q_bead;
+  // DT19 semi-explicit ions and Manning charges (simu_ele_set.F90:107-253)
+  int dt19;                // i_dtrna_model == 2019
+  const uint8_t *b_qkind;  // per bead 1: the charge is -Zp of the lane's label; null: no such bead
+  const double *lab_zp;    // per label
+  const double *pmf_e, *pmf_f;   // per label, pmf_nbin each: Mg-P energy and force tables; null: none
+  int pmf_nbin;
+  double pmf_rmin, pmf_rbin, pmf_rbininv, pmf_rmax;
   // labels (temperature-dependent parameters)
   const double *lab_T, *lab_coef, *lab_cdist, *lab_beta, *lab_rele2;
   const int *lab_u0off; const double *lab_u0;   // stack U0(T) per label
@@ -194,6 +201,27 @@ struct KArgs {
   int nbead_total;
   int noise_in_sweep;      // 1: the sink's noise is drawn in the bonded sweep (kept in shared memory)
 };
+
+#ifdef __CUDACC__
+// charge of bead b (index into the bead tables) under label lab:
+// coef_charge(icharge, grep) of the reference
+__device__ __forceinline__ double bead_charge(const KArgs &a, int lab, int b) {
+  return (a.b_qkind && a.b_qkind[b]) ? -a.lab_zp[lab] : a.b_charge[b];
+}
+
+// neighbor_list_ele.F90:167-174: Mg-P pairs take the PMF table (DT19)
+__device__ __forceinline__ bool mg_p_pair(int ti, int tj) {
+  return (ti == 2 && tj == 5) || (ti == 5 && tj == 2);
+}
+
+// force_ele_DH.F90:90-94: 0-based table bin of a Mg-P distance.  Below the
+// first point the reference stops; here the pair takes bin 0 and low is set.
+__device__ __forceinline__ int pmf_bin(const KArgs &a, double d, bool &low) {
+  if (!(d >= a.pmf_rmin)) { low = true; return 0; }
+  const int ib = (int)floor((d - a.pmf_rmin) * a.pmf_rbininv);
+  return min(ib, a.pmf_nbin - 1);
+}
+#endif
 
 // ---------------------------------------------------------------- Philox
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as

@@ -69,7 +69,7 @@ template <> struct V4<double> { typedef double4 T; };
 constexpr size_t MASK_SMEM_MAX = 64 * 1024;    // bit matrices kept in shared memory up to this size
 
 enum { MISC_EXCESS = 0, MISC_REBUILD = 1, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,
-       MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8,
+       MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8, MISC_PMF = 9,
        MISC_UNITS = 10 /* neigh_unit ints start here */ };
 
 // Excluded-volume near lists: at a recording pass every bead keeps, per

@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   };
   for (int i = tid; i < N; i += nth) {
     const int ti = a.b_type[T.bead0 + i], ci = a.b_class[T.bead0 + i];
-    const bool qi = fabs(a.b_charge[T.bead0 + i]) >= 1.0e-6;
+    const double q_i = bead_charge(a, label, T.bead0 + i);
+    const bool qi = fabs(q_i) >= 1.0e-6;
     for (int w = (i + 1) >> 5; w < W; ++w) {
       uint32_t me = mexv[(size_t)i * W + w], ml = (a.i_ele != 0 && qi) ? mele[(size_t)i * W + w] : 0u;
       if (w == ((i + 1) >> 5)) {   // keep bits j > i only
@@ -188,7 +189,9 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
         const double3 v = shifted(i, j);
         const int tj = a.b_type[T.bead0 + j], cj = a.b_class[T.bead0 + j];
         double dij;
-        if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = a.exv_dist_PS;
+        if (a.dt19)   // energy_exv_dt15.F90:67-73
+          dij = (ti == 3 && tj == 3) ? a.exv_dist : a.b_radius[T.bead0 + i] + a.b_radius[T.bead0 + j];
+        else if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = a.exv_dist_PS;
         else if (ci == 2 && cj == 2) dij = a.exv_dist;
         else dij = a.b_radius[T.bead0 + i] + a.b_radius[T.bead0 + j];
         double dist = sqrt(dot3(v, v));
@@ -211,7 +214,15 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
         const double r2 = dot3(v, v);
         if (r2 <= cut2) {
           const double dist1 = sqrt(r2);
-          const double ce = a.b_charge[T.bead0 + i] * a.b_charge[T.bead0 + j] * coefT;
+          if (a.pmf_e && mg_p_pair(ti, a.b_type[T.bead0 + j]) && dist1 <= a.pmf_rmax) {
+            // energy_ele_DH.F90:77-95: linear between the table points
+            bool low = false;
+            const int ib = pmf_bin(a, dist1, low);
+            const double *pe = a.pmf_e + (size_t)label * a.pmf_nbin, *pf = a.pmf_f + (size_t)label * a.pmf_nbin;
+            es[ES_ELE] += pe[ib] - pf[ib] * (dist1 - (a.pmf_rmin + (double)ib * a.pmf_rbin));
+            continue;
+          }
+          const double ce = q_i * bead_charge(a, label, T.bead0 + j) * coefT;
           if (a.i_ele == 1) es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
           else if (a.i_ele == 3) es[ES_ELE] += ce * (1.0e0 / dist1 - 1.0e0 / a.cutoff_ele);   // energy_ele_coulomb.F90:66
           else es[ES_ELE] += ce * erfc(a.ewld_alpha * dist1) / dist1;

@@ -164,6 +164,11 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
           if (!((ci == 2 && cj == 2) || (ci == 2 && cj == 4) || (ci == 4 && cj == 2) ||
                 (ci == 4 && cj == 3) || (ci == 3 && cj == 4)))
             ex = false;
+          else if (a.dt19 && ((ci == 2 && cj == 4) || (ci == 4 && cj == 2))) {
+            // neighbor_assign.F90:524-537: no exv between a charged phosphate and an ion
+            const int pb = (s.typ[i] == 2) ? i : ((s.typ[j] == 2) ? j : -1);
+            if (pb >= 0 && fabs((double)s.A4[pb].w) > 1.0e-6) ex = false;
+          }
         }
       }
       bool el = false;
@@ -401,6 +406,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         const V pi = s.A4[i];
         const Real qci = (Real)((double)pi.w * coefT);
         const uint32_t *row = mele + (size_t)i * W;
+        // DT19: Mg-P pairs within pmf_rmax take the table force (force_ele_DH.F90:87-97)
+        const int tq = s.typ[i];
+        const double *pmf_row = (a.pmf_f && (tq == 2 || tq == 5)) ? a.pmf_f + (size_t)label * a.pmf_nbin : nullptr;
         const int w1 = min(W, (part + 1) * geo.gw);
         // partial sums over at most a few words of the row, in Real (the
         // chunk totals enter each bead's FP64 sum)
@@ -428,6 +436,14 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             } else if (!ewald) {
               fa = qci * p0.w * ria * ria * (ria + rcd) * fexp<Real>(-da * rcd);
               fb = qci * p1.w * rib * rib * (rib + rcd) * fexp<Real>(-db * rcd);
+              if (pmf_row) {
+                bool low = false;
+                if (mg_p_pair(tq, s.typ[j0]) && (double)da <= a.pmf_rmax)
+                  fa = (Real)pmf_row[pmf_bin(a, (double)da, low)] * ria;
+                if (two && mg_p_pair(tq, s.typ[j1]) && (double)db <= a.pmf_rmax)
+                  fb = (Real)pmf_row[pmf_bin(a, (double)db, low)] * rib;
+                if (low) s.misc[MISC_PMF] = 1;
+              }
             } else {
               // force_ele_coulomb_ewld.F90:118-137 (real space, no clamp)
               fa = qci * p0.w * (erfc(ew_a * da) * ria + ew_b * exp(-ew_a2 * ra2)) * ria * ria;
@@ -519,7 +535,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         const int tj = s.typ[j], cj = s.cls[j];
         const V bj = s.B4[j];
         Real dij;
-        if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = dist_ps;
+        if (a.dt19) dij = (ti == 3 && tj == 3) ? dist_rr : bi.x + bj.x;   // force_exv_dt15.F90:60-66
+        else if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij = dist_ps;
         else if (ci == 2 && cj == 2) dij = dist_rr;
         else dij = bi.x + bj.x;
         if (r2 > dij * dij) return;
@@ -634,7 +651,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     if (skin) { s.DX[i] = a.dxyz[o]; s.DY[i] = a.dxyz[o + 1]; s.DZ[i] = a.dxyz[o + 2]; }
     const int b = T.bead0 + i;
     set_pos<Real>(s, i);
-    s.A4[i].w = (Real)a.b_charge[b];
+    s.A4[i].w = (Real)bead_charge(a, st.label, b);
     s.B4[i].x = (Real)a.b_radius[b]; s.B4[i].y = (Real)a.b_eps[b];
     s.B4[i].z = (Real)(a.b_screen[b] * (1.0 + 1.0e-4) + 1.0e-3); s.B4[i].w = (Real)0;
     s.typ[i] = a.b_type[b]; s.cls[i] = a.b_class[b];
@@ -883,9 +900,11 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     if (CL == 1) {
       st.nclamp += s.misc[MISC_CLAMP];
       if (s.misc[MISC_NAN]) st.flags |= LF_NAN;
+      if (s.misc[MISC_PMF]) st.flags |= LF_PMF;
     } else {
       if (s.misc[MISC_CLAMP]) atomicAdd((unsigned long long *)&st.nclamp, (unsigned long long)s.misc[MISC_CLAMP]);
       if (s.misc[MISC_NAN]) atomicOr(&st.flags, LF_NAN);
+      if (s.misc[MISC_PMF]) atomicOr(&st.flags, LF_PMF);
       if (cu.rank == 0) st.istep = istep0 + a.nsteps;
     }
   }

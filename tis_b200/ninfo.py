@@ -63,6 +63,12 @@ VISCOSITY_DEFAULT = 0.001  # general.para viscosity [Pa s]
 DT15_EXV = {"P": (2.1, 0.2), "S": (2.9, 0.2), "A": (2.8, 0.2), "G": (3.0, 0.2), "C": (2.7, 0.2),
             "U": (2.7, 0.2), "MG": (0.7926, 0.894700), "CA2": (1.7131, 0.459789),
             "CL": (1.9480, 0.265000), "K": (2.6580, 0.000328), "NA": (1.8680, 0.002770)}
+# para/rna.para:495-507 (NHT19_exv_param, the DT19 model): radius, epsilon.
+# It has no entries for the monovalent ions (the model keeps them implicit).
+NHT19_EXV = {"P": (1.8900, 0.2), "S": (2.6100, 0.2), "A": (2.5200, 0.2), "G": (2.7000, 0.2),
+             "C": (2.4300, 0.2), "U": (2.4300, 0.2), "MG": (2.0000, 0.894700), "CA2": (2.8000, 1.0)}
+# para/electrostatic.para:42 (LENGTH_PER_UNIT of P, the Manning length b)
+LENGTH_PER_UNIT_P = 4.38178046
 # para/electrostatic.para:33-40 (CHARGE_TYPE)
 CHARGE_TYPE = {"P": -1.0, "MG": 2.0, "CA2": 2.0, "K": 1.0, "NA": 1.0, "CL": -1.0}
 # hydrogen-bond sites per bead (setp_dtrna15.F90:40-66) and their valences (:114-161)
@@ -607,6 +613,37 @@ def read_ninfo(sources, st: Structure, all_in_one: bool = True, units=(1, 1), ni
     return ni
 
 
+# -------------------------------------------------------------------- PMF
+def read_pmf(source) -> dict:
+    """The Mg-P potential of mean force file of the DT19 model
+    (setp_pmf.F90:31-105): lines "r V(r)" on a uniform grid.  Returns the
+    tis_params fields pmf_nbin, pmf_rmin, pmf_rbin (second r minus the
+    first), pmf_rmax (the last r read) and pmf_mg_p.  A spacing that departs
+    from the first by more than 1e-4 stops the reference, and raises here."""
+    text = source
+    if isinstance(source, os.PathLike) or (isinstance(source, str) and "\n" not in source and os.path.exists(source)):
+        with open(source) as f:
+            text = f.read()
+    rs, vs = [], []
+    for raw in text.splitlines():
+        tok = _tokens(raw)
+        if not tok:
+            continue
+        if len(tok) < 2:
+            raise NinfoError(f"Error: cannot read a line of PMF file: {raw}")
+        rs.append(_to_real(tok[0], raw)); vs.append(_to_real(tok[1], raw))
+    if len(rs) < 2:
+        raise NinfoError("Error: cannot read the second line of PMF file")
+    rbin = rs[1] - rs[0]
+    for k in range(2, len(rs)):
+        if abs(rs[k] - rs[k - 1] - rbin) > 0.0001:
+            raise NinfoError(f"Error: bin width is not uniform in PMF file (line {k + 1})")
+    if len(rs) > 3000:
+        raise NinfoError("Error: Nbin > MXPMFBIN in setp_pmf")
+    return dict(pmf_nbin=len(rs), pmf_rmin=rs[0], pmf_rbin=rbin, pmf_rmax=rs[-1],
+                pmf_mg_p=np.array(vs, dtype=np.float64))
+
+
 # ------------------------------------------------------------------ set-up
 def _chemical(st: Structure, b: int) -> str:
     """imp2chemicaltype (setp_mass_fric.F90:283-330) for RNA beads and ions."""
@@ -622,16 +659,18 @@ def _chemical(st: Structure, b: int) -> str:
 def build_system(st: Structure, ni: NativeInfo, *, i_mass: int = 1, i_fric: int = 0,
                  fric_const: float = FRIC_CONST_DEFAULT, viscosity: float = VISCOSITY_DEFAULT,
                  i_simulate_type: int = 1, charge_change: dict | None = None,
-                 ele_units=None) -> dict:
+                 ele_units=None, i_dtrna_model: int = 2015) -> dict:
     """The topology dict of ``st`` + ``ni`` (see tis_b200.abi.make_topology).
 
     i_mass 1: masses by chemical type; 0: general.para rmass for every bead
     (setp_mass_fric.F90:40-54).  i_fric 1: Stokes friction
     6 pi eta r (/ m for Langevin) with eta in (Da)(A^-1)(tau^-1)
     (setp_mass_fric.F90:58-113); 0: fric_const.  charge_change maps a
-    1-based bead to its charge (CHARGE_CHANGE lines); ele_units, when given,
-    lists the 1-based units whose beads carry charges (flag_ele), default
-    all units (setp_native_charge.F90:82-112)."""
+    1-based bead to its charge (CHARGE_CHANGE lines; flg_charge_fixed marks
+    them, so that i_charge = 1 keeps them); ele_units, when given, lists the
+    1-based units whose beads carry charges (flag_ele), default all units
+    (setp_native_charge.F90:82-112).  i_dtrna_model 2019 takes the NHT19
+    excluded-volume table (setp_dtrna15.F90:25-28)."""
     n = st.nmp
     chem = [_chemical(st, b) for b in range(n)]
     if i_mass == 1:
@@ -651,23 +690,31 @@ def build_system(st: Structure, ni: NativeInfo, *, i_mass: int = 1, i_fric: int 
             raise NinfoError("i_fric = 1 is set up here for Langevin and Brownian-HI runs")
     elif i_fric != 0:
         raise NinfoError("i_fric must be 0 or 1")
-    exv_radius = np.array([DT15_EXV[c][0] for c in chem])
-    exv_epsilon = np.sqrt(np.array([DT15_EXV[c][1] for c in chem]))
+    if i_dtrna_model == 2019:
+        missing = sorted({c for c in chem if c not in NHT19_EXV})
+        if missing:
+            raise NinfoError(f"the DT19 exv table (NHT19_exv_param) has no entry for {missing}")
+        table = NHT19_EXV
+    elif i_dtrna_model in (0, 2015):
+        table = DT15_EXV
+    else:
+        raise NinfoError("i_dtrna_model must be 2015 or 2019")
+    exv_radius = np.array([table[c][0] for c in chem])
+    exv_epsilon = np.sqrt(np.array([table[c][1] for c in chem]))
 
     # charges in bead order, unit by unit (setp_native_charge.F90:82-112)
     change = dict(charge_change or {})
     units = range(1, st.nunit + 1) if ele_units is None else sorted(ele_units)
-    qb, qv = [], []
+    qb, qv, qfix = [], [], []
     for u in units:
         a, b = st.lunit2mp[u - 1]
         for imp in range(a, b + 1):
             if imp in change:
-                qb.append(imp); qv.append(float(change[imp]))
-            elif st.iclass_unit[u - 1] == CLASS_RNA:
-                if st.imp2type[imp - 1] == MP_RNA_PHOS:
-                    qb.append(imp); qv.append(CHARGE_TYPE["P"])
+                qb.append(imp); qv.append(float(change[imp])); qfix.append(1)
+            elif st.iclass_unit[u - 1] == CLASS_RNA and st.imp2type[imp - 1] == MP_RNA_PHOS:
+                qb.append(imp); qv.append(CHARGE_TYPE["P"]); qfix.append(0)
             elif st.iclass_unit[u - 1] == CLASS_ION:
-                qb.append(imp); qv.append(CHARGE_TYPE[chem[imp - 1]])
+                qb.append(imp); qv.append(CHARGE_TYPE[chem[imp - 1]]); qfix.append(0)
     site_tab, nsite, valence = hbsite_table(st)
 
     def arr(x, dt, k):
@@ -681,6 +728,7 @@ def build_system(st: Structure, ni: NativeInfo, *, i_mass: int = 1, i_fric: int 
         iclass_unit=np.array(st.iclass_unit, dtype=np.int32), imp2type=st.imp2type.astype(np.int32),
         cmass=cmass, fric=fric, exv_radius=exv_radius, exv_epsilon=exv_epsilon,
         ncharge=len(qb), icharge2mp=np.array(qb, dtype=np.int32), coef_charge=np.array(qv),
+        flg_charge_fixed=np.array(qfix, dtype=np.int32),
         nbd=len(ni.ibd2mp), ibd2mp=arr(ni.ibd2mp, np.int32, 2), bd_nat=np.array(ni.bd_nat),
         coef_bd=np.array(ni.coef_bd),
         nba=len(ni.iba2mp), iba2mp=arr(ni.iba2mp, np.int32, 3), ba_nat=np.array(ni.ba_nat),

@@ -628,3 +628,106 @@ def duplicate_hbonds(sysd: dict, seed: int = 0, shift: float = 0.3):
     s["idtrna_hb2hbsite"] = np.vstack([s["idtrna_hb2hbsite"], s["idtrna_hb2hbsite"]])
     s["nhb"] = 2 * nhb
     return s
+
+
+# ----------------------------------------------------- DT19 semi-explicit
+# para/rna.para:495-507 (NHT19_exv_param): radius, epsilon of the DT19 model
+NHT19_EXV = {"P": (1.8900, 0.2), "S": (2.6100, 0.2), "A": (2.5200, 0.2), "G": (2.7000, 0.2),
+             "C": (2.4300, 0.2), "U": (2.4300, 0.2), "Mg": (2.0000, 0.894700)}
+
+
+def mg_p_pmf(seed: int = 0, rmin: float = 1.775, rbin: float = 0.025, nbin: int = 1930):
+    """A seeded synthetic Mg-P potential of mean force on the grid of the
+    reference's RISM table (1.775 A in steps of 0.025 A, 1930 points): a
+    steep repulsive wall, contact and solvent-separated wells and a screened
+    1/r tail, with seeded depths and positions.  It stands in for the RISM
+    table, which is not shipped with this code.  Returns the tis_params
+    fields of tis_b200.ninfo.read_pmf."""
+    rng = np.random.default_rng(seed)
+    r = rmin + rbin * np.arange(nbin)
+    w1, w2 = rng.uniform(0.7, 1.1), rng.uniform(0.8, 1.2)
+    c1, c2 = rng.uniform(2.6, 3.2), rng.uniform(6.0, 7.0)
+    v = (360.0 * np.exp(-(r - rmin) / 0.12) - w1 * np.exp(-((r - c1) / 0.45) ** 2)
+         - w2 * np.exp(-((r - c2) / 1.6) ** 2) - 4.7 / r * (1.0 - np.exp(-r / 3.0)))
+    return dict(pmf_nbin=nbin, pmf_rmin=rmin, pmf_rbin=rbin, pmf_rmax=float(r[-1]), pmf_mg_p=v)
+
+
+def dt19_params(**over):
+    """tis_params of the DT19 model: para/rna.para:423-470 (para_NHT19_rna:
+    n_sep_nlocal P/S 4, exv_inf 0), Manning phosphate charges with
+    LENGTH_PER_UNIT P 4.38178046 (para/electrostatic.para:42), pmf_merge 5 A
+    and the synthetic Mg-P table of mg_p_pmf."""
+    p = dt15_params(n_sep_nlocal_P=4, n_sep_nlocal_S=4, n_sep_nlocal_B=2, exv_inf=0.0,
+                    i_dtrna_model=2019, i_charge=1, length_per_unit_P=4.38178046, pmf_rmerge=5.0)
+    p.update(mg_p_pmf())
+    p.update(over)
+    return p
+
+
+def dt19_mg_system(seed: int = 11, n: int = 16, stem: int = 4, box: float = 80.0, n_near: int = 5, n_far: int = 3):
+    """A DT19 chain in a periodic box with Mg ions: n_near of them 2.4-5.5 A
+    from phosphates (inside the PMF table, some within pmf_merge), one next
+    to a phosphate whose charge is fixed at 0 (a CHARGE_CHANGE line: that
+    pair keeps its excluded volume), n_far elsewhere.  The chain is a
+    self-avoiding walk with 5.2 A between non-bonded beads (the NHT19 radii
+    are larger than the DT15 contact distance); radii and epsilons from the
+    NHT19 table; phosphate charges are replaced by -Zp of each temperature
+    (i_charge = 1)."""
+    rng = np.random.default_rng(seed)
+    s = set_friction(dt15_chain(n, seed, stem=stem, min_dist=5.2), 0.5)
+    kinds = []
+    typ = s["imp2type"]
+    seq = s["seq"]
+    k = 0
+    for b in range(s["nmp"]):
+        if typ[b] == MP_RNA_PHOS:
+            kinds.append("P")
+        elif typ[b] == MP_RNA_SUGAR:
+            kinds.append("S")
+        else:
+            kinds.append(seq[k]); k += 1
+    s["exv_radius"] = np.array([NHT19_EXV[q][0] for q in kinds])
+    s["exv_epsilon"] = np.sqrt(np.array([NHT19_EXV[q][1] for q in kinds]))
+    X = s["xyz"] - s["xyz"].mean(axis=0)
+    phos = [b for b in range(s["nmp"]) if typ[b] == MP_RNA_PHOS]
+    fixed_p = phos[-1]
+    picks = list(rng.choice(phos[:-1], size=n_near, replace=False)) + [fixed_p]
+    ions = []
+    for b in picks:
+        for _ in range(1000):
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
+            # the Mg of the uncharged phosphate sits inside their exv contact distance (3.89 A)
+            cand = X[b] + (rng.uniform(3.4, 3.8) if b == fixed_p else rng.uniform(2.4, 5.5)) * u
+            d_p = np.linalg.norm(X[phos] - cand, axis=1)
+            non_p = [q for q in range(len(X)) if typ[q] != MP_RNA_PHOS]
+            d_o = np.linalg.norm(np.vstack([X[non_p]] + ([np.array(ions)] if ions else [])) - cand, axis=1)
+            if d_p.min() > 2.4 and d_o.min() > 4.7:
+                ions.append(cand)
+                break
+        else:
+            raise RuntimeError("Mg placement failed")
+    while len(ions) < n_near + 1 + n_far:
+        cand = rng.uniform(-box / 2, box / 2, size=3)
+        if np.min(np.linalg.norm(np.vstack([X, np.array(ions)]) - cand, axis=1)) > 12.0:
+            ions.append(cand)
+    nI = len(ions)
+    N0 = s["nmp"]
+    N = N0 + nI
+    s["xyz"] = np.vstack([X, np.array(ions)])
+    s["nmp"] = N
+    s["nunit"] = 2
+    s["lunit2mp"] = np.array([[1, N0], [N0 + 1, N]], dtype=np.int32)
+    s["iclass_unit"] = np.array([CLASS_RNA, CLASS_ION], dtype=np.int32)
+    s["imp2type"] = np.concatenate([typ, np.full(nI, MP_ION_MG, dtype=np.int32)]).astype(np.int32)
+    s["cmass"] = np.concatenate([s["cmass"], np.full(nI, MASS["Mg"])])
+    s["fric"] = np.concatenate([s["fric"], np.full(nI, s["fric"][0])])
+    s["exv_radius"] = np.concatenate([s["exv_radius"], np.full(nI, NHT19_EXV["Mg"][0])])
+    s["exv_epsilon"] = np.concatenate([s["exv_epsilon"], np.full(nI, math.sqrt(NHT19_EXV["Mg"][1]))])
+    q_idx = list(s["icharge2mp"]) + list(range(N0 + 1, N + 1))
+    q_val = [0.0 if b - 1 == fixed_p else v for b, v in zip(s["icharge2mp"], s["coef_charge"])] + [2.0] * nI
+    s["icharge2mp"] = np.array(q_idx, dtype=np.int32)
+    s["coef_charge"] = np.array(q_val)
+    s["flg_charge_fixed"] = np.array([1 if b - 1 == fixed_p else 0 for b in q_idx], dtype=np.int32)
+    s["ncharge"] = len(q_idx)
+    return s
