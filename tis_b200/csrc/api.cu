@@ -24,7 +24,7 @@
 
 namespace tis {
 size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
-                       bool dbuf);
+                       bool dbuf, int nsite);
 cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2);
 cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, const KArgs &a);
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
@@ -739,8 +739,10 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       tis_destroy(c);
       return TIS_E_UNSUPPORTED;
     }
-    smem = std::max(smem, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, false));
-    smem2 = std::max(smem2, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, true));
+    smem = std::max(smem, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, false,
+                                          d.nsite));
+    smem2 = std::max(smem2, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, true,
+                                            d.nsite));
     minN = std::min(minN, d.nmp);
   }
   c->smem = smem;

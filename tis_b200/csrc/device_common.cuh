@@ -114,14 +114,15 @@ struct Smem {
   int W;                    // words per bit row
   double *C1, *C2, *C3, *C4, *RC;   // rlan_const(1..4) and 1/m of each bead (cst_on)
   double *NX, *NY, *NZ;              // this step's Gaussian noise, drawn in the bonded sweep (cst_on)
-  bool mask_smem, slots_smem, inc_smem, near_on, cst_on;
+  int *exc;                 // hbond-site occupancy counters (shared when they fit, else the lane's global copy)
+  bool mask_smem, slots_smem, inc_smem, near_on, cst_on, exc_smem;
 };
 
-struct SmemPlan { size_t base, mask, slots, inc, near, cst; };
+struct SmemPlan { size_t base, mask, slots, inc, near, cst, exc; };
 
 // Byte layout of one lane (host and device use the same arithmetic).
 __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc, bool periodic, bool skin,
-                                              int real_size, int nunit, bool dbuf = false) {
+                                              int real_size, int nunit, bool dbuf = false, int nsite = 0) {
   size_t nd = 9 * (size_t)N + 64 + 3 * (size_t)CHMAX + (size_t)nunit * nunit + 2;
   if (periodic) nd += 6 * (size_t)N;
   if (skin) nd += 3 * (size_t)N;
@@ -140,6 +141,7 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc
   p.inc = ((4 * (size_t)ninc) + 15) & ~(size_t)15;
   p.near = 16 * (size_t)N + 2 * (size_t)NEAR_CAP * N + 8 * (size_t)N + 16;
   p.cst = 8 * 8 * (size_t)N + 16;
+  p.exc = ((4 * (size_t)nsite) + 15) & ~(size_t)15;
   return p;
 }
 
@@ -165,7 +167,7 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
                             bool periodic, bool skin, bool dbuf = false) {
   const int N = T.nmp;
   Smem<Real> s;
-  SmemPlan pl = smem_plan(N, T.nq, T.nslot, T.ninc, periodic, skin, (int)sizeof(Real), T.nunit, dbuf);
+  SmemPlan pl = smem_plan(N, T.nq, T.nslot, T.ninc, periodic, skin, (int)sizeof(Real), T.nunit, dbuf, T.nsite);
   double *d = (double *)base;
   s.X = d; s.Y = d + N; s.Z = d + 2 * N; d += 3 * N;
   s.VX = d; s.VY = d + N; s.VZ = d + 2 * N; d += 3 * N;
@@ -225,9 +227,15 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
     double *c = (double *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
     s.C1 = c; s.C2 = c + N; s.C3 = c + 2 * N; s.C4 = c + 3 * N; s.RC = c + 4 * N;
     s.NX = c + 5 * N; s.NY = c + 6 * N; s.NZ = c + 7 * N;
+    u = (unsigned char *)(c + 8 * (size_t)N);
+    left = (size_t)total > (size_t)(u - base) ? (size_t)total - (size_t)(u - base) : 0;
   } else {
     s.C1 = s.C2 = s.C3 = s.C4 = s.RC = s.NX = s.NY = s.NZ = nullptr;
   }
+  // hbond-site counters: shared atomics instead of returning L2 atomics
+  s.exc_smem = T.nsite > 0 && pl.exc <= left;
+  if (s.exc_smem) s.exc = (int *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
+  else s.exc = a.site_exc + L.site0;
   return s;
 }
 
@@ -672,10 +680,9 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
 // force_dtrna_hbond15.F90:373-509, run by one thread of the lane
 template <typename Real>
 __device__ void prune_hbonds(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, long long istep,
-                             double beta, bool zero_energy) {
+                             double beta, bool zero_energy, int *exc) {
   uint8_t *hbf = a.hb_flag + L.hb0;
   double *ene = a.hb_ene + L.hb0;
-  int *exc = a.site_exc + L.site0;
   const int ns = T.nsite;
   for (int s = 0; s < ns; ++s) exc[s] -= a.site_val[T.site0 + s];
   int draw = 0;

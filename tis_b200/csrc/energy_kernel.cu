@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     __syncthreads();
     if (excess_flag && tid == 0)
       prune_hbonds<double>(a, lane, L, T, st.istep,
-                           a.ebeta_lane ? a.ebeta_lane[lane] : (a.rex ? a.rex->beta_global : a.ebeta), false);
+                           a.ebeta_lane ? a.ebeta_lane[lane] : (a.rex ? a.rex->beta_global : a.ebeta), false, exc);
     __syncthreads();
   }
   // energy_dtrna_hbond15.F90:135-143: tertiary ('T') bonds count separately

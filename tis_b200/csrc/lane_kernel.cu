@@ -298,7 +298,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const Real *my_slots = s.slots;
   uint8_t *hbf = a.hb_flag + L.hb0;
   double *hbe = a.hb_ene + L.hb0;
-  int *exc = a.site_exc + L.site0;
+  int *exc = s.exc;
   const uint32_t *mexv = s.mask, *mele = s.mask + (size_t)N * W;
   const uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
   int nclamp = 0;
@@ -340,11 +340,13 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
   }
   // chunk ranges, kinds in decreasing cost per chunk (measured on B200):
-  // stacks, tertiary stacks, Debye-Hueckel row chunks, angles, hbonds,
-  // bonds, then noise
-  const int c_ts = (st_1 - st_0 + 31) >> 5, c_ch = c_ts + ((ts_1 - ts_0 + 31) >> 5);
+  // hbonds (a formed hbond is the longest serial chain of the phase),
+  // stacks, tertiary stacks, Debye-Hueckel row chunks, angles, bonds, then
+  // noise
+  const int c_st = (hb_1 - hb_0 + 31) >> 5;
+  const int c_ts = c_st + ((st_1 - st_0 + 31) >> 5), c_ch = c_ts + ((ts_1 - ts_0 + 31) >> 5);
   const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
-  const int c_hb = c_ba + ((ba_1 - ba_0 + 31) >> 5), c_bd = c_hb + ((hb_1 - hb_0 + 31) >> 5);
+  const int c_bd = c_ba + ((ba_1 - ba_0 + 31) >> 5);
   const int c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
   // the sink's Gaussian noise of the own beads, drawn here where warps have slack
   const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
@@ -358,9 +360,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (c >= c_end) break;
     PHASE_T0(t_item);
     int kind;
-    if (c >= c_hb && c < c_bd) {
+    if (c < c_st) {
       kind = 0;
-      const int h = hb_0 + ((c - c_hb) << 5) + lid;
+      const int h = hb_0 + (c << 5) + lid;
       if (h < hb_1) {
         uint8_t f = hbf[h] & 1;
         if (f) {
@@ -389,7 +391,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       }
     } else if (c < c_ts) {
       kind = 1;
-      const int k = st_0 + (c << 5) + lid;
+      const int k = st_0 + ((c - c_st) << 5) + lid;
       if (k < st_1) term_stack<Real>(a, T, s, slots, k, u0[k]);
     } else if (c < c_ch) {
       kind = 1;
@@ -462,7 +464,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         }
         s.ch_part[3 * cc] = axs; s.ch_part[3 * cc + 1] = ays; s.ch_part[3 * cc + 2] = azs;
       }
-    } else if (c < c_hb) {
+    } else if (c < c_bd) {
       kind = 3;
       const int k = ba_0 + ((c - c_ba) << 5) + lid;
       if (k < ba_1) term_angle<Real>(a, T, s, slots, k);
@@ -491,7 +493,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   if (s.misc[MISC_EXCESS]) {
     if (tid == 0 && cu.rank == 0) {
       const double beta = a.hb_beta_global ? (a.rex ? a.rex->beta_global : a.beta_hbond15) : a.lab_beta[label];
-      prune_hbonds<Real>(a, lane, L, T, istep, beta, true);
+      prune_hbonds<Real>(a, lane, L, T, istep, beta, true, s.exc);
     }
     if (CL == 1) __syncthreads(); else cg::this_cluster().sync();
   }
@@ -669,7 +671,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     for (int k = tid; k < 2 * N * s.W; k += nth) s.mask[k] = gm[k];
   }
   if (tid < MISC_UNITS) s.misc[tid] = 0;
-  int *exc = a.site_exc + L.site0;
+  int *exc = s.exc;
   for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
   __syncthreads();
   for (int k = tid; k < NQ; k += nth) s.qidx[s.qb[k]] = k;
@@ -924,9 +926,9 @@ template __global__ void lane_kernel<float, 512, 2>(KArgs);
 // Dynamic shared memory to request for a topology: base layout + bit
 // matrices + incidence lists + slots, capped at the 227 KB a CTA may use.
 size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
-                       bool dbuf) {
-  SmemPlan p = smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit, dbuf);
-  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + p.near + p.cst + 64;
+                       bool dbuf, int nsite) {
+  SmemPlan p = smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit, dbuf, nsite);
+  size_t want = p.base + (p.mask <= MASK_SMEM_MAX ? p.mask : 0) + p.inc + p.slots + p.near + p.cst + p.exc + 64;
   return want < 227 * 1024 ? want : 227 * 1024;
 }
 
