@@ -340,13 +340,17 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
   }
   // chunk ranges, kinds in decreasing cost per chunk (measured on B200):
-  // hbonds (a formed hbond is the longest serial chain of the phase),
   // stacks, tertiary stacks, Debye-Hueckel row chunks, angles, bonds, then
-  // noise
-  const int c_st = (hb_1 - hb_0 + 31) >> 5;
+  // noise.  The hbond chunks go first with two CTAs per lane (a formed
+  // hbond is the longest serial chain of the phase, and the first CTA takes
+  // every hbond) and after the angles with one CTA, where that order
+  // balances the warps better (both measured on B200).
+  const int n_hbc = (hb_1 - hb_0 + 31) >> 5, n_bac = (ba_1 - ba_0 + 31) >> 5;
+  const int c_st = (CL == 2) ? n_hbc : 0;   // first stack chunk
   const int c_ts = c_st + ((st_1 - st_0 + 31) >> 5), c_ch = c_ts + ((ts_1 - ts_0 + 31) >> 5);
   const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
-  const int c_bd = c_ba + ((ba_1 - ba_0 + 31) >> 5);
+  const int c_hb = (CL == 2) ? 0 : c_ba + n_bac;   // first hbond chunk
+  const int c_bd = c_ba + n_bac + ((CL == 2) ? 0 : n_hbc);
   const int c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
   // the sink's Gaussian noise of the own beads, drawn here where warps have slack
   const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
@@ -360,9 +364,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (c >= c_end) break;
     PHASE_T0(t_item);
     int kind;
-    if (c < c_st) {
+    if (c >= c_hb && c < c_hb + n_hbc) {
       kind = 0;
-      const int h = hb_0 + (c << 5) + lid;
+      const int h = hb_0 + ((c - c_hb) << 5) + lid;
       if (h < hb_1) {
         uint8_t f = hbf[h] & 1;
         if (f) {
@@ -464,7 +468,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         }
         s.ch_part[3 * cc] = axs; s.ch_part[3 * cc + 1] = ays; s.ch_part[3 * cc + 2] = azs;
       }
-    } else if (c < c_bd) {
+    } else if (c < c_ba + n_bac) {
       kind = 3;
       const int k = ba_0 + ((c - c_ba) << 5) + lid;
       if (k < ba_1) term_angle<Real>(a, T, s, slots, k);
