@@ -404,56 +404,62 @@ __global__ void __launch_bounds__(256) rex_exchange_kernel(KArgs a, RexState *re
                                                            const double *e_own, const double *e_opp,
                                                            const double *u, double *scale, double *velo) {
   const int n = a.nlane, tid = threadIdx.x;
+  const int ip = rex->idx_pair;
+  const unsigned long long ctr = rex->counter;
+  __shared__ int s_npair, s_nacc;
   for (int r = tid; r < n; r += blockDim.x) scale[r] = 0.0;
+  if (tid == 0) { s_npair = 0; s_nacc = 0; }
+  __syncthreads();
+  // simu_replica_exchange.F90:121-267.  The pairs of one exchange are
+  // disjoint, so each is decided by its own thread; the k-th pair in label
+  // order takes the k-th uniform, as the reference's serial loop draws them.
+  for (int li = 1 + tid; li <= n; li += blockDim.x) {
+    const int lj = rex_pair(li, n, ip);
+    if (lj < li) continue;
+    const int k = (ip == 1) ? (li - 1) / 2 : (li - 2) / 2;
+    atomicAdd(&s_npair, 1);
+    double uu;
+    if (u) {
+      uu = u[k];
+    } else {
+      const unsigned long long c = ctr + (unsigned long long)k;
+      const U4 o = philox4x32(U4{(uint32_t)c, (uint32_t)(c >> 32), 0x52454D44u, 0u}, (uint32_t)a.seed,
+                              (uint32_t)(a.seed >> 32));
+      uu = u01_open0(o.x) - 2.3283064365386963e-10;   // [0, 1)
+    }
+    const int ri = lab2rep[li - 1], rj = lab2rep[lj - 1];
+    const double tm = a.lab_T[li - 1], tn = a.lab_T[lj - 1];
+    const double pim = e_own[(size_t)ri * N_ETYPE], pin = e_opp[(size_t)ri * N_ETYPE];
+    const double pjn = e_own[(size_t)rj * N_ETYPE], pjm = e_opp[(size_t)rj * N_ETYPE];
+    const double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / a.boltz;
+    if (delta < 0.0e0 || uu <= exp(-delta)) {
+      rep2lab[ri] = lj - 1; rep2lab[rj] = li - 1;
+      lab2rep[li - 1] = rj; lab2rep[lj - 1] = ri;
+      const double sf = sqrt(tn / tm);
+      scale[ri] = sf;
+      scale[rj] = -sf;
+      atomicAdd(&s_nacc, 1);
+    }
+  }
   __syncthreads();
   if (tid == 0) {
-    const int ip = rex->idx_pair;
-    int nrand = 0, nacc = 0;
-    unsigned long long ctr = rex->counter;
-    for (int li = 1; li <= n; ++li) {
-      const int lj = rex_pair(li, n, ip);
-      if (lj < li) continue;
-      ++nrand;
-      double uu;
-      if (u) {
-        uu = u[nrand - 1];
-      } else {
-        const U4 o = philox4x32(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x52454D44u, 0u}, (uint32_t)a.seed,
-                                (uint32_t)(a.seed >> 32));
-        ++ctr;
-        uu = u01_open0(o.x) - 2.3283064365386963e-10;   // [0, 1)
-      }
-      const int ri = lab2rep[li - 1], rj = lab2rep[lj - 1];
-      const double tm = a.lab_T[li - 1], tn = a.lab_T[lj - 1];
-      const double pim = e_own[(size_t)ri * N_ETYPE], pin = e_opp[(size_t)ri * N_ETYPE];
-      const double pjn = e_own[(size_t)rj * N_ETYPE], pjm = e_opp[(size_t)rj * N_ETYPE];
-      const double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / a.boltz;
-      if (delta < 0.0e0 || uu <= exp(-delta)) {
-        rep2lab[ri] = lj - 1; rep2lab[rj] = li - 1;
-        lab2rep[li - 1] = rj; lab2rep[lj - 1] = ri;
-        const double sf = sqrt(tn / tm);
-        scale[ri] = sf;
-        scale[rj] = -sf;
-        ++nacc;
-      }
-    }
-    rex->counter = ctr;
-    rex->nacc = nacc;
+    rex->counter = u ? ctr : ctr + (unsigned long long)s_npair;
+    rex->nacc = s_nacc;
     rex->idx_pair = (ip == 2) ? 1 : ip + 1;
     rex->beta_global = 1.0e0 / (a.lab_T[rep2lab[n - 1]] * a.boltz);
   }
-  __syncthreads();
   for (int r = tid; r < n; r += blockDim.x) a.lstate[r].label = rep2lab[r];
   // time_integral.F90 velocity rescale of a swapped replica (scale > 0
-  // multiplies, scale < 0 divides by -scale)
-  for (int r = 0; r < n; ++r) {
+  // multiplies, scale < 0 divides by -scale), one warp per replica
+  const int warp = tid >> 5, lid = tid & 31, nw = blockDim.x >> 5;
+  for (int r = warp; r < n; r += nw) {
     const double f = scale[r];
     if (f == 0.0) continue;
     const LaneDesc L = a.lanes[r];
     const int N = a.tops[L.top].nmp;
     double *v = velo + 3 * (size_t)L.state0;
-    if (f > 0.0) for (int k = tid; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
-    else for (int k = tid; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
+    if (f > 0.0) for (int k = lid; k < 3 * N; k += 32) v[k] = f * v[k];
+    else for (int k = lid; k < 3 * N; k += 32) v[k] = v[k] / (-f);
   }
 }
 
