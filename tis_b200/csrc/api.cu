@@ -44,8 +44,6 @@ void bd_update_items(const std::vector<int> &lane_T, std::vector<int> &items, st
 long long bd_plane_floats(int nmp);
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp);
 cudaError_t bd_force_launch(cudaStream_t st, const KArgs &a, int max_nmp);
-cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
-                              const double *scale);
 }  // namespace tis
 
 using namespace tis;

@@ -318,32 +318,9 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   }
 }
 
-// velocity rescale after an accepted temperature swap
-// (simu_replica_exchange.F90:272-300): scale > 0 multiplies, scale < 0
-// divides by -scale, 0 leaves the lane alone.
-__global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const TopDesc *tops, const double *scale, int nlane);
-
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a) {
   energy_kernel<<<grid, 256, 0, st>>>(a);
   return cudaGetLastError();
-}
-
-cudaError_t scale_velo_launch(int nlane, cudaStream_t st, double *velo, const LaneDesc *lanes, const TopDesc *tops,
-                              const double *scale) {
-  scale_velo_kernel<<<nlane, 128, 0, st>>>(velo, lanes, tops, scale, nlane);
-  return cudaGetLastError();
-}
-
-__global__ void scale_velo_kernel(double *velo, const LaneDesc *lanes, const TopDesc *tops, const double *scale, int nlane) {
-  const int lane = blockIdx.x;
-  if (lane >= nlane) return;
-  const double f = scale[lane];
-  if (f == 0.0) return;
-  const LaneDesc L = lanes[lane];
-  const int N = tops[L.top].nmp;
-  double *v = velo + 3 * (size_t)L.state0;
-  if (f > 0.0) for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
-  else for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
 }
 
 // ----------------------------------------------------------------------
