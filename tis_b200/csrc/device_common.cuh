@@ -302,6 +302,10 @@ template <typename Real> __device__ __forceinline__ Real dot(R3<Real> a, R3<Real
 template <typename Real> __device__ __forceinline__ R3<Real> crs(R3<Real> a, R3<Real> b) {
   return R3<Real>{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
+// Interaction tables are constant for a launch: read them through the
+// read-only data path, which the cluster barriers' acquire does not discard.
+template <typename T> __device__ __forceinline__ T ldro(const T *p) { return __ldg(p); }
+
 template <typename Real> __device__ __forceinline__ Real wrap_pi(Real d) {
   const Real PI = (Real)3.14159265358979323846, TPI = (Real)(2.0 * 3.14159265358979323846);
   if (d > PI) d -= TPI; else if (d < -PI) d += TPI;
@@ -311,11 +315,12 @@ template <typename Real> __device__ __forceinline__ Real wrap_pi(Real d) {
 // force_bond.F90:41-56
 template <typename Real>
 __device__ void term_bond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
-  const int *m = a.bd_idx + 2 * (size_t)(T.bd0 + k);
+  const int *mp = a.bd_idx + 2 * (size_t)(T.bd0 + k);
+  const int m[2] = {ldro(mp), ldro(mp + 1)};
   R3<Real> v = dvec(s, m[0], m[1]);
   Real dist = sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
-  Real dd = dist - (Real)a.bd_nat[T.bd0 + k];
-  Real f = (Real)a.bd_coef[T.bd0 + k] * ((Real)-2.0 * fdiv(dd, dist));
+  Real dd = dist - (Real)ldro(a.bd_nat + T.bd0 + k);
+  Real f = (Real)ldro(a.bd_coef + T.bd0 + k) * ((Real)-2.0 * fdiv(dd, dist));
   put_slot<Real>(slots, 2 * k, m[0], -f * v.x, -f * v.y, -f * v.z);
   put_slot<Real>(slots, 2 * k + 1, m[1], f * v.x, f * v.y, f * v.z);
 }
@@ -324,8 +329,9 @@ __device__ void term_bond(const KArgs &a, const TopDesc &T, const Smem<Real> &s,
 template <typename Real>
 __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
   const size_t sb = T.slot_ba + 3 * (size_t)k;
-  const Real cf = (Real)a.ba_coef[T.ba0 + k];
-  const int *m = a.ba_idx + 3 * (size_t)(T.ba0 + k);
+  const Real cf = (Real)ldro(a.ba_coef + T.ba0 + k);
+  const int *mp = a.ba_idx + 3 * (size_t)(T.ba0 + k);
+  const int m[3] = {ldro(mp), ldro(mp + 1), ldro(mp + 2)};
   if (cf < (Real)1.0e-6) {
     put_slot<Real>(slots, sb, m[0], 0, 0, 0); put_slot<Real>(slots, sb + 1, m[1], 0, 0, 0);
     put_slot<Real>(slots, sb + 2, m[2], 0, 0, 0);
@@ -335,7 +341,7 @@ __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   Real c11 = dot(v21, v21), c22 = dot(v32, v32), c21 = dot(v32, v21);
   Real co = -c21 * frsq(c11 * c22);
   if (co > (Real)1) co = 1; else if (co < (Real)-1) co = -1;
-  Real dba = acos(co) - (Real)a.ba_nat[T.ba0 + k];
+  Real dba = acos(co) - (Real)ldro(a.ba_nat + T.ba0 + k);
   Real t3 = c11 * c22 - c21 * c21;
   if (t3 <= (Real)1) t3 = 1;
   Real f = (Real)2 * cf * dba * frsq(t3);
@@ -481,15 +487,17 @@ __device__ void term_tstack(const KArgs &a, const TopDesc &T, const Smem<Real> &
 // force_dtrna_stack.F90:54-165 (skipped when st_status is off)
 template <typename Real>
 __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, double u0) {
-  const int *m = a.st_idx + 7 * (size_t)(T.st0 + k);
+  const int *mp = a.st_idx + 7 * (size_t)(T.st0 + k);
+  const int m[7] = {ldro(mp), ldro(mp + 1), ldro(mp + 2), ldro(mp + 3), ldro(mp + 4), ldro(mp + 5), ldro(mp + 6)};
   if (stack_excluded<Real>(a, T, s, k)) {
     const size_t sb = T.slot_st + 7 * (size_t)k;
 #pragma unroll
     for (int p = 0; p < 7; ++p) put_slot<Real>(slots, sb + p, m[p], 0, 0, 0);
     return;
   }
-  const double *nat = a.st_nat + 3 * (size_t)(T.st0 + k);
-  const double *cf = a.st_coef + 3 * (size_t)(T.st0 + k);
+  const double *natp = a.st_nat + 3 * (size_t)(T.st0 + k), *cfp = a.st_coef + 3 * (size_t)(T.st0 + k);
+  const double nat[3] = {ldro(natp), ldro(natp + 1), ldro(natp + 2)};
+  const double cf[3] = {ldro(cfp), ldro(cfp + 1), ldro(cfp + 2)};
   R3<Real> v21 = dvec(s, m[0], m[1]);
   R3<Real> v34 = dvec(s, m[3], m[2]);
   R3<Real> v54 = dvec(s, m[3], m[4]);
@@ -550,9 +558,14 @@ __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s
 // Returns the energy; active = |d| <= hb_cutoff_dist.
 template <typename Real>
 __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, bool &active) {
-  const int *m = a.hb_idx + 6 * (size_t)(T.hb0 + k);
-  const double *nat = a.hb_nat + 6 * (size_t)(T.hb0 + k);
-  const double *cf = a.hb_coef + 7 * (size_t)(T.hb0 + k);
+  const int *mp = a.hb_idx + 6 * (size_t)(T.hb0 + k);
+  const int m[6] = {ldro(mp), ldro(mp + 1), ldro(mp + 2), ldro(mp + 3), ldro(mp + 4), ldro(mp + 5)};
+  const double *natp = a.hb_nat + 6 * (size_t)(T.hb0 + k), *cfp = a.hb_coef + 7 * (size_t)(T.hb0 + k);
+  double nat[6], cf[7];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) nat[q] = ldro(natp + q);
+#pragma unroll
+  for (int q = 0; q < 7; ++q) cf[q] = ldro(cfp + q);
   // v12 = x1 - x2 (pxyz + minimum image when periodic)
   double w0 = s.PX[m[0]] - s.PX[m[1]], w1 = s.PY[m[0]] - s.PY[m[1]], w2 = s.PZ[m[0]] - s.PZ[m[1]];
   if (a.periodic) { pb1(w0, a.psize[0], a.psizeh[0]); pb1(w1, a.psize[1], a.psizeh[1]); pb1(w2, a.psize[2], a.psizeh[2]); }

@@ -378,10 +378,10 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const int *sites = a.hb_site + 6 * (size_t)(T.hb0 + h);
 #pragma unroll
             for (int q = 0; q < 6; ++q) {
-              int sid = sites[q];
+              int sid = ldro(sites + q);
               if (sid >= 0) {
                 int old = atomicAdd(&exc[sid], 1);
-                if (old + 1 > a.site_val[T.site0 + sid]) {
+                if (old + 1 > ldro(a.site_val + T.site0 + sid)) {
                   s.misc[MISC_EXCESS] = 1;
                   if (CL == 2) peer_ptr(s.misc, cu)[MISC_EXCESS] = 1;
                 }
@@ -396,7 +396,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     } else if (c < c_ts) {
       kind = 1;
       const int k = st_0 + ((c - c_st) << 5) + lid;
-      if (k < st_1) term_stack<Real>(a, T, s, slots, k, u0[k]);
+      if (k < st_1) term_stack<Real>(a, T, s, slots, k, ldro(u0 + k));
     } else if (c < c_ch) {
       kind = 1;
       const int k = ts_0 + ((c - c_ts) << 5) + lid;
