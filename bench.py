@@ -49,8 +49,11 @@ def parse():
     ap.add_argument("--period", type=int, default=None, help="MD steps per bench step (C3: exchange period)")
     ap.add_argument("--precision", type=int, default=None, choices=[0, 1],
                     help="override the workload's arithmetic (0 FP64, 1 mixed)")
-    ap.add_argument("--ref-sample", type=int, default=200,
-                    help="reference arm: MD steps per replica in one timed step")
+    ap.add_argument("--ref-sample", type=int, default=None,
+                    help="reference arm: MD steps per replica in one timed step (default: the CPU leg's sample)")
+    ap.add_argument("--neighbor", default="cadence", choices=["cadence", "skin"],
+                    help="neighbour rebuild rule: every 10 steps (the configs' cadence) or the reference's "
+                         "Verlet skin (neigh_margin 8 A, time_integral.F90:57-93)")
     ap.add_argument("--quick", action="store_true",
                     help="device timing only (no CPU leg, e2e or plain path): small profiling runs")
     return ap.parse_args()
@@ -131,34 +134,95 @@ def bdhi_bytes(systems, every, mixed):
 
 
 # ------------------------------------------------------------------ CPU leg
-def _cpu_replica(job):
-    """One replica of the workload on one core with the CPU restatement."""
+def _fleet_worker(jobs, nsteps, variant, barrier, cmd, res):
+    """One host process: sets up its share of the replicas once (not timed),
+    then for every command steps all of them nsteps after a barrier that
+    every process passes together, and reports its start and end times."""
     import numpy as np
-    from oracle.oracle import Oracle
-    sysd, par, T, nsteps, seed = job
-    par = dict(par, precision=0)
-    o = Oracle(sysd, par, [T])
-    o.set_state(sysd["xyz"][None])
-    rng = np.random.default_rng(seed)
-    noise = rng.normal(size=(nsteps + 1, 1, sysd["nmp"], 3))
-    o.set_noise(noise)
-    t0 = time.perf_counter()
-    o.time_integral_pre()
-    o.step(nsteps)
-    return time.perf_counter() - t0
+    from oracle import oracle as om
+    orcs, noise = [], {}
+    for sysd, par, T, seed in jobs:
+        o = om.Oracle(sysd, dict(par, precision=0), [T], variant=variant)
+        o.set_state(sysd["xyz"][None])
+        if o.nmp not in noise:
+            noise[o.nmp] = np.random.default_rng(seed).normal(size=(nsteps + 1, 1, o.nmp, 3))
+        o.set_noise(noise[o.nmp])
+        o.time_integral_pre()
+        orcs.append(o)
+    res.put(("ready", len(orcs)))
+    while True:
+        n = cmd.get()
+        if n is None:
+            break
+        for o in orcs:
+            o.set_noise(noise[o.nmp][1:])
+        barrier.wait()
+        t0 = time.perf_counter()
+        for o in orcs:
+            o.step(n)
+        t1 = time.perf_counter()
+        res.put((t0, t1))
 
 
-def cpu_run(systems, par, temps, nrep, nsteps, cores, pool):
-    jobs = []
-    lane = 0
-    for s, r in zip(systems, nrep):
-        for _ in range(r):
-            jobs.append((s, par, temps[lane], nsteps, lane))
-            lane += 1
-    t0 = time.perf_counter()
-    list(pool.map(_cpu_replica, jobs))
-    wall = time.perf_counter() - t0
-    return len(jobs) * nsteps / wall
+class CpuFleet:
+    """The CPU restatement of the path on the host cores: one process per
+    core, each owning a fixed share of the replicas (largest first, to the
+    least loaded process), set up once.  A pass steps every replica n MD
+    steps; its rate is replica-steps over the wall time from the first
+    process's start to the last one's end (perf_counter is one clock for
+    every process of the host)."""
+
+    def __init__(self, systems, par, temps, nrep, nsteps, variant):
+        import multiprocessing as mp
+        reps = []
+        lane = 0
+        for s, r in zip(systems, nrep):
+            for _ in range(r):
+                reps.append((s, par, temps[lane], 1000 + lane))
+                lane += 1
+        self.nrep = len(reps)
+        self.cores = max(1, min(os.cpu_count() or 1, self.nrep))
+        load = [0.0] * self.cores
+        share = [[] for _ in range(self.cores)]
+        for job in sorted(reps, key=lambda j: -j[0]["nmp"]):
+            k = load.index(min(load))
+            share[k].append(job)
+            load[k] += job[0]["nmp"]
+        ctx = mp.get_context("spawn")
+        self.barrier = ctx.Barrier(self.cores)
+        self.cmd = [ctx.Queue() for _ in range(self.cores)]
+        self.res = ctx.Queue()
+        self.nsteps = nsteps
+        self.procs = [ctx.Process(target=_fleet_worker, args=(share[k], nsteps, variant, self.barrier,
+                                                              self.cmd[k], self.res), daemon=True)
+                      for k in range(self.cores)]
+        for p in self.procs:
+            p.start()
+        for _ in range(self.cores):
+            self.res.get()
+
+    def run(self, n):
+        n = min(n, self.nsteps)
+        for q in self.cmd:
+            q.put(n)
+        spans = [self.res.get() for _ in range(self.cores)]
+        wall = max(t1 for _, t1 in spans) - min(t0 for t0, _ in spans)
+        return self.nrep * n / wall
+
+    def close(self):
+        for q in self.cmd:
+            q.put(None)
+        for p in self.procs:
+            p.join(timeout=30)
+
+
+def cpu_variant():
+    """The -O3 -march=native copy built on this host, else the checker build."""
+    from oracle import oracle as om
+    return ("native", "-O3 -march=native -ffp-contract=off") if om.build_native() else ("checker", "-O2 -ffp-contract=off")
+
+
+CPU_SAMPLE = {"c3": 2000, "c4": 1000, "c2": 20, "c5": 10}
 
 
 # ------------------------------------------------------------------ clocks
@@ -251,33 +315,47 @@ def peaks():
 # ------------------------------------------------------------------ arms
 def run_reference(args, rank, world):
     """The reference's CPU implementation of the path (the C++ restatement:
-    the Fortran reference cannot be compiled here), all host cores, one
-    replica per process, on a bounded sample of the workload."""
-    if rank != 0:
-        return
-    import multiprocessing as mp
-    systems, par, temps, nrep, desc = workload(args.workload)
-    cores = os.cpu_count() or 1
-    sample = args.ref_sample
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
+    no Fortran compiler exists on this image or the GPU host), all host
+    cores, one process per core, on a bounded sample of the workload.  Under
+    several ranks every rank joins a gloo group and rank 0 alone runs."""
+    joined = 1
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        t = torch.ones(1)
+        tdist.all_reduce(t)
+        joined = int(t.item())
+    if rank == 0:
+        systems, par, temps, nrep, desc = workload(args.workload)
+        sample = args.ref_sample or CPU_SAMPLE[args.workload]
+        variant, flags = cpu_variant()
+        fleet = CpuFleet(systems, par, temps, nrep, sample, variant)
         for _ in range(max(args.warmup, 0)):
-            cpu_run(systems, par, temps, nrep, 20, cores, pool)
-        vals = [cpu_run(systems, par, temps, nrep, sample, cores, pool) for _ in range(args.steps)]
-    value = statistics.median(vals)
-    nlane = sum(nrep)
-    line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": nlane * sample / value * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded random-walk DT15 chains)",
-        "config": {"workload": desc, "parallelism": f"{cores} host processes"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{nlane} replicas x {sample} MD steps per step (C++ FP64 restatement; "
-                                   "no Fortran compiler on this image)"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
+            fleet.run(min(sample, 100))
+        vals = [fleet.run(sample) for _ in range(args.steps)]
+        fleet.close()
+        value = statistics.median(vals)
+        nlane = sum(nrep)
+        line = {
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "ranks_joined": joined,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": nlane * sample / value * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded random-walk DT15 chains)",
+            "config": {"workload": desc, "parallelism": f"{fleet.cores} host processes"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": fleet.cores, "kind": "port",
+                             "sample": f"{nlane} replicas x {sample} MD steps per step, median of {args.steps} "
+                                       f"(C++ FP64 restatement built {flags}; no Fortran compiler on this "
+                                       "image or the GPU host)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as tdist
+        tdist.barrier()
+        tdist.destroy_process_group()
 
 
 def run_ours(args, rank, world, local_rank):
@@ -290,16 +368,18 @@ def run_ours(args, rank, world, local_rank):
         args.no_cpu_baseline = True
         args.no_plain = True
     if rank == 0 and not args.no_cpu_baseline:
-        # CPU leg first, in spawned processes, before this process touches the GPU
-        import multiprocessing as mp
+        # CPU leg first, in spawned processes, before this process touches the
+        # GPU; timed exactly as the reference arm times it
         systems, par, temps, nrep, _ = workload(args.workload)
-        cores = os.cpu_count() or 1
-        sample = {"c3": 1000, "c4": 1000, "c2": 20, "c5": 10}[args.workload]
-        with mp.get_context("spawn").Pool(cores) as pool:
-            v = cpu_run(systems, par, temps, nrep, sample, cores, pool)
-        cpu_line = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                    "sample": f"{sum(nrep)} replicas x {sample} MD steps (C++ FP64 restatement of the "
-                              "reference loops, one replica per process)"}
+        sample = CPU_SAMPLE[args.workload]
+        variant, flags = cpu_variant()
+        fleet = CpuFleet(systems, par, temps, nrep, sample, variant)
+        fleet.run(min(sample, 100))
+        v = statistics.median([fleet.run(sample) for _ in range(3)])
+        fleet.close()
+        cpu_line = {"value": v, "unit": UNIT, "cores": fleet.cores, "kind": "port",
+                    "sample": f"{sum(nrep)} replicas x {sample} MD steps, median of 3 after a warm pass "
+                              f"(C++ FP64 restatement of the reference loops built {flags}, one process per core)"}
     import torch
     torch.cuda.set_device(local_rank)
     dist = None
@@ -311,19 +391,40 @@ def run_ours(args, rank, world, local_rank):
     from tis_b200.engine import Engine
 
     systems, par, temps, nrep, desc = workload(args.workload)
-    par = dict(par, seed=1234 + rank)
+    if args.neighbor == "skin":
+        par["n_step_neighbor"] = 0
     if args.precision is not None:
         par["precision"] = args.precision
-    eng = Engine(systems, par, temps, nrep=nrep)
+    remd = args.workload == "c3"
+    ladder = None
+    if remd and world > 1:
+        # one ladder of 64 replicas per GPU, split over the ranks: noise is
+        # keyed by the global replica (one seed for all), and each exchange
+        # all-gathers replica_energy(2, .) over NCCL (tis_b200.remd)
+        from tis_b200 import remd as rx
+        from tis_b200 import synth
+        nall = len(temps) * world
+        tall = synth.temperature_ladder(nall, 280.0, 400.0)
+        first, count = rx.ladder_share(nall, world, rank)
+        temps = tall[first - 1:first - 1 + count]
+        nrep = [count]
+        par = dict(par, seed=1234)
+        eng = Engine(systems, par, temps, nrep=nrep, ladder=(tall, first))
+        ladder = rx.LadderExchange(eng, nall, dist, "cuda")
+        desc += f"; the {nall}-replica ladder (280-400 K) split over {world} GPUs, exchanges all-gather energies"
+    else:
+        par = dict(par, seed=1234 + rank)
+        eng = Engine(systems, par, temps, nrep=nrep)
     x0 = np.vstack([np.tile(s["xyz"], (r, 1)) for s, r in zip(systems, nrep)])
     eng.set_state(x0)
     eng.time_integral_pre()
-    remd = args.workload == "c3"
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
 
     def period():
         eng.step(period_len)
-        if remd:
+        if ladder is not None:
+            ladder.exchange()
+        elif remd:
             eng.replica_exchange(count=False)
 
     for _ in range(args.warmup):
@@ -413,7 +514,10 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic (seeded random-walk DT15 chains, reference parameter tables)",
             "config": {"workload": desc, "replicas_per_gpu": nlane, "beads_per_replica": int(systems[0]["nmp"]),
                        "md_steps_per_step": period_len, "l2": "flushed between timed steps (256 MiB write)",
-                       "parallelism": f"replicas only, {nlane} lanes per GPU"},
+                       "neighbor_rule": ("Verlet skin, neigh_margin 8 A (the reference's rule)"
+                                         if args.neighbor == "skin" else "rebuild every 10 steps"),
+                       "parallelism": (f"ladder split, {nlane} replicas per GPU, NCCL all-gather at exchanges"
+                                       if ladder is not None else f"replicas only, {nlane} lanes per GPU")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": profiled_traffic() if (args.workload == "c3" and period_len == PERIOD) else None,
@@ -440,8 +544,20 @@ def run_ours(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def free_port():
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch this command under torch.distributed.run
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__)]
+        sys.exit(subprocess.call(cmd + sys.argv[1:]))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

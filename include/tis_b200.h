@@ -49,6 +49,8 @@ enum {
   TIS_E_WCA_REP = 23, TIS_E_WCA_ATT = 24,
   TIS_ETYPE_MAX = 25
 };
+/* i_hydro_tensor values (src/const_index.F90:39-45 HI_TENSOR). */
+enum { TIS_HI_RPY = 1, TIS_HI_RPY_OVER = 2, TIS_HI_ERMAK_OVER = 3, TIS_HI_ZUK_RPY = 4 };
 /* i_simulate_type values used here (src/const_index.F90 SIM). */
 enum { TIS_SIM_LANGEVIN = 1, TIS_SIM_BROWNIAN_HI = 6 };
 /* electrostatics: 0 none, DH = i_function_form 0, EWALD = i_function_form 2,
@@ -129,6 +131,8 @@ typedef struct tis_topology {
                                       every hydrogen bond is secondary ('S') */
   const int32_t *flg_charge_fixed; /* (ncharge) nonzero: a CHARGE_CHANGE value, kept when i_charge = 1
                                       (simu_ele_set.F90:152-158).  NULL: none fixed */
+  const double *radius;            /* (nmp) Brownian-HI: hydrodynamic radius of each bead (var_struct radius,
+                                      setp_mass_fric.F90:91).  NULL: tis_params.hi_radius for every bead */
 } tis_topology;
 
 /* ---------------------------------------------------------------- params */
@@ -170,6 +174,9 @@ typedef struct tis_params {
   double pmf_rmin, pmf_rbin, pmf_rmax; /* first point, spacing, last point read */
   double pmf_rmerge;               /* pmf_merge: the switch from PMF to DH (simu_ele_set.F90:242-250) */
   const double *pmf_mg_p;          /* (pmf_nbin) PMF values; NULL when the system has no Mg */
+  int32_t i_hydro_tensor;          /* Brownian-HI diffusion tensor (HI_TENSOR, const_index.F90:39-45): 1 (or 0)
+                                      RPY, 2 RPY_OVER, 3 ERMAK_OVER (radius of bead 1), 4 ZUK_RPY (per-bead
+                                      radii), simu_hydro_tensors.F90:50-324 */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */
@@ -202,6 +209,18 @@ int tis_init(const tis_topology *top, const tis_params *par, int32_t nrep,
  * beyond running the systems as separate processes (MXUNIT = 20). */
 int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_params *par,
                    const int32_t *nrep, const double *tempk, tis_ctx **out);
+
+/* One rank's share of a replica-exchange ladder split over processes (one
+ * per GPU), as the reference distributes replicas over MPI ranks
+ * (n_replica_mpi local replicas, irep2grep, var_replica.F90): the context
+ * holds global replicas irep_first .. irep_first + nrep_local - 1 of an
+ * nrep_all-replica ladder with temperatures tempk_all[0 .. nrep_all-1];
+ * replica g starts at label g.  Counter-based noise is keyed by the global
+ * replica, so a replica moves exactly as it would in one context holding the
+ * whole ladder.  Exchanges go through tis_rex_energies and
+ * tis_rex_exchange_all; every rank passes the same seed. */
+int tis_init_ladder(const tis_topology *top, const tis_params *par, int32_t nrep_all, const double *tempk_all,
+                    int32_t irep_first, int32_t nrep_local, tis_ctx **out);
 
 void tis_destroy(tis_ctx *ctx);
 
@@ -256,14 +275,22 @@ int tis_force_sumup(tis_ctx *ctx, int32_t irep, double *force_mp);
  * irep for caller-owned DEVICE arrays xyz_dev (in) and force_dev (out), each
  * 3*nmp doubles laid out like xyz_mp, without allocating device memory: all
  * per-call scratch comes from one fixed 1 MiB array that every GPU loading
- * the library holds until exit.  Topology, parameters and the replica's
- * temperature label come from ctx; ctx's own state and lists are untouched.
- * The first call on each device looks up that array's address (set-up) and
- * should come before any stream capture.  Replicas whose scratch would not
- * fit return TIS_E_UNSUPPORTED.  All calls on a GPU share the array: calls
- * that overlap on the GPU (other threads, other contexts) race.  Runs on
- * ctx's stream; xyz_dev must be ready when called, force_dev is ready on
- * return.  Returns like tis_force_sumup. */
+ * the library holds until exit.  It serves hosts whose device memory is held
+ * by their own pool allocator, or that must not grow device memory after
+ * start-up.  Topology, parameters and the replica's temperature label come
+ * from ctx; ctx's own state, lists and flags are untouched.  The scratch of
+ * one call is, rounded up to 256-byte blocks, 2 descriptors per replica of
+ * ctx + 120 nmp + 8 nmp ceil(nmp/32) + 3 nslot (4 or 8 bytes: mixed or FP64)
+ * + 9 nhb + 4 nhbsite bytes, plus 24 nmp + nmp^2 with a periodic box: about
+ * 1,700 beads fit without a periodic box and about 840 with one.  Larger
+ * replicas, Ewald and Brownian-HI contexts return TIS_E_UNSUPPORTED.  The
+ * first call on each device looks up that array's address (set-up) and
+ * should come before any stream capture; the address belongs to the
+ * device's primary context, so a process that resets the device must not
+ * call this afterwards.  All calls on a GPU share the array: calls that
+ * overlap on the GPU (other threads, other contexts) race.  Runs on ctx's
+ * stream; xyz_dev must be ready when called, force_dev is ready on return.
+ * Returns like tis_force_sumup. */
 int tis_force_sumup_static(tis_ctx *ctx, int32_t irep, const double *xyz_dev, double *force_dev);
 
 /* energy_sumup(irep, ...) -> energy(E_TYPE%MAX) (src/energy_sumup.F90:11-530). */
@@ -277,6 +304,34 @@ int tis_time_integral_pre(tis_ctx *ctx);
  * trigger, noise, x update, force_sumup, v/a update, for every replica. */
 int tis_step(tis_ctx *ctx, int64_t nsteps);
 
+/* time_integral(flg_step_each_replica) called nsteps times
+ * (src/time_integral.F90:13-473 with :134 and :460-465): a replica whose
+ * flg_step_each_replica[irep-1] is nonzero on entry does not move; a
+ * replica whose step counter reaches exchange_step[irep-1] stops there and
+ * gets its flag set (exchange_step(grep) of var_replica, indexed by
+ * replica; NULL: no replica stops early).  The caller clears the flags and
+ * moves exchange_step on after each exchange, as time_integral_post does
+ * (src/time_integral_post.F90:275,363).  Not available on the
+ * Brownian-HI path (TIS_E_UNSUPPORTED). */
+int tis_time_integral(tis_ctx *ctx, int64_t nsteps, int32_t *flg_step_each_replica,
+                      const int64_t *exchange_step);
+
+/* Step counter (istep) of every replica, istep[nrep]. */
+int tis_get_steps(tis_ctx *ctx, int64_t *istep);
+
+/* The Gaussian noise r_boxmuller(3, nmp, nrep) that the library's
+ * counter-based generator (Philox4x32-10 with the Box-Muller transform,
+ * keyed by seed, replica and step) gives every bead of every replica at
+ * steps istep .. istep + nstep - 1, as the reference's get_random_number
+ * fills it each step (src/time_integral.F90:121-127); r_boxmuller is
+ * (3, nmp_total, nstep).  Injected noise (tis_set_noise) does not affect it. */
+int tis_get_random_number(tis_ctx *ctx, int64_t istep, int32_t nstep, double *r_boxmuller);
+
+/* Neighbour rebuilds of replica irep since init and the step of the last
+ * one (-1: none): the information of the reference's neighbour-list record
+ * (outfile%neigh, src/time_integral.F90:76-84).  Either pointer may be NULL. */
+int tis_get_rebuild_info(tis_ctx *ctx, int32_t irep, int64_t *n_rebuild, int64_t *last_step);
+
 /* Replica exchange over temperature labels (src/energy_allrep.F90:123-260 and
  * src/simu_replica_exchange.F90:18-300): energies at the own and the partner
  * label's temperature, Metropolis with uniform u[k] for the k-th pair, label
@@ -284,6 +339,30 @@ int tis_step(tis_ctx *ctx, int64_t nsteps);
  * u == NULL draws counter-based uniforms.  n_accept receives the number of
  * accepted swaps. */
 int tis_replica_exchange(tis_ctx *ctx, const double *u, int32_t *n_accept);
+/* Ladder contexts, step 1 of an exchange: replica_energy(2, nrep_local) of
+ * the context's replicas, the energy at the own label and at the exchange
+ * partner's label (0 without a partner), as energy_allrep computes it before
+ * the ranks gather it (src/energy_allrep.F90:123-217,
+ * src/time_integral_post.F90:279).  The caller gathers the ranks' arrays in
+ * replica order into replica_energy(2, nrep_all). */
+int tis_rex_energies(tis_ctx *ctx, double *replica_energy);
+
+/* Ladder contexts, step 2: the exchange of the whole ladder from the
+ * gathered replica_energy(2, nrep_all) (src/simu_replica_exchange.F90:
+ * 121-267): every rank takes the same decisions (u == NULL: counter-based
+ * uniforms from the shared seed), keeps the ladder's label maps, and
+ * relabels and rescales the velocities of its own replicas. */
+int tis_rex_exchange_all(tis_ctx *ctx, const double *replica_energy_all, const double *u, int32_t *n_accept);
+
+/* The Metropolis decisions of one exchange of an nrep_all ladder on the host,
+ * without a context or a GPU (src/simu_replica_exchange.F90:121-267): pairs
+ * of the odd/even alternation idx_pair (1 or 2) in label order, the k-th
+ * taking u[k]; rep2lab (1-based, in/out) is updated; vscale[r] (may be NULL)
+ * is sqrt(T_new/T_old) for a replica that moved up the ladder, minus it for
+ * its partner (whose velocities are divided by it), 0 otherwise. */
+int tis_rex_decide(int32_t nrep_all, const double *tempk_all, int32_t idx_pair, const double *replica_energy,
+                   const double *u, int32_t *rep2lab, double *vscale, int32_t *n_accept);
+
 /* rep2lab(nrep), 1-based labels. */
 int tis_get_labels(tis_ctx *ctx, int32_t *rep2lab);
 

@@ -18,7 +18,29 @@ from tis_b200.abi import (ETYPE_MAX, Params, Topology, make_params, make_topolog
                           ptr_f64, ptr_i32)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = None
+_LIBS = {}
+
+
+def _host_tag() -> str:
+    """The host CPU's model and feature flags, hashed: a -march=native build
+    is used only on the kind of CPU it was built on."""
+    import hashlib
+    info = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                if line.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
+
+
+# the checker (-O2, built with the package) and the copy timed as the CPU
+# baseline (-O3 -march=native, built on the host that runs it)
+_FILES = {"checker": "libtis_oracle.so", "native": f"libtis_oracle_native-{_host_tag()}.so"}
 
 
 def build(quiet: bool = True):
@@ -26,12 +48,18 @@ def build(quiet: bool = True):
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
 
 
-def lib():
-    global _LIB
-    if _LIB is None:
-        path = os.path.join(_HERE, "libtis_oracle.so")
+def build_native() -> bool:
+    """Builds the timing copy for this host; False when that fails."""
+    r = subprocess.run(["make", "-C", _HERE, "native", f"NATIVE_SO={_FILES['native']}"],
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    return r.returncode == 0 and os.path.exists(os.path.join(_HERE, _FILES["native"]))
+
+
+def lib(variant: str = "checker"):
+    if variant not in _LIBS:
+        path = os.path.join(_HERE, _FILES[variant])
         if not os.path.exists(path):
-            build()
+            build() if variant == "checker" else build_native()
         L = C.CDLL(path)
         vp = C.c_void_p
         i32p, f64p = C.POINTER(C.c_int32), C.POINTER(C.c_double)
@@ -59,17 +87,21 @@ def lib():
         L.orc_ewald_table.argtypes = [vp, f64p, f64p, C.c_int]
         L.orc_coulomb_direct.argtypes = [vp, C.c_int, C.c_int]
         L.orc_coulomb_direct.restype = C.c_double
-        L.orc_hydro_tensors.argtypes = [vp, C.c_int, C.c_double, f64p, f64p]
+        L.orc_hydro_tensors.argtypes = [vp, C.c_int, f64p, f64p]
         L.orc_not_spd.argtypes = [vp]
         L.orc_nclamp.argtypes = [vp]
+        L.orc_replica_energy.argtypes = [vp, C.c_int, f64p]
+        L.orc_rex_apply.argtypes = [vp, i32p, f64p]
+        L.orc_rebuild_info.argtypes = [vp, C.c_int, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.orc_rebuild_info.restype = None
         L.orc_pmf_range.argtypes = [vp]
         L.orc_pmf_range.restype = C.c_int
         L.orc_label_pmf.argtypes = [vp, C.c_int, f64p, f64p, f64p, C.c_int]
         L.orc_label_pmf.restype = C.c_int
         L.orc_nclamp.restype = C.c_long
         L.orc_boltz_kcal_mol.restype = C.c_double
-        _LIB = L
-    return _LIB
+        _LIBS[variant] = L
+    return _LIBS[variant]
 
 
 TERMS = {"bond": 0, "angle": 1, "stack": 2, "hbond": 3, "exv": 4, "dh": 5, "ewald": 6, "fene": 7, "wca": 8,
@@ -79,8 +111,8 @@ TERMS = {"bond": 0, "angle": 1, "stack": 2, "hbond": 3, "exv": 4, "dh": 5, "ewal
 class Oracle:
     """One topology, nrep replicas (labels = temperatures tempk)."""
 
-    def __init__(self, sysd: dict, par: dict, tempk):
-        self.L = lib()
+    def __init__(self, sysd: dict, par: dict, tempk, variant: str = "checker"):
+        self.L = lib(variant)
         self.sysd = sysd
         self.nmp = int(sysd["nmp"])
         self.nrep = len(tempk)
@@ -184,6 +216,17 @@ class Oracle:
         self.L.orc_replica_exchange(self.h, ptr_f64(u), C.byref(na))
         return na.value
 
+    def replica_energy(self, irep):
+        """(E at the own label, E at the exchange partner's label or 0)."""
+        out = np.zeros(2)
+        self.L.orc_replica_energy(self.h, irep, ptr_f64(out))
+        return out
+
+    def rex_apply(self, rep2lab, vscale):
+        r = np.ascontiguousarray(rep2lab, dtype=np.int32)
+        v = np.ascontiguousarray(vscale, dtype=np.float64)
+        self.L.orc_rex_apply(self.h, ptr_i32(r), ptr_f64(v))
+
     def labels(self):
         out = np.zeros(self.nrep, dtype=np.int32)
         self.L.orc_get_labels(self.h, ptr_i32(out))
@@ -204,11 +247,13 @@ class Oracle:
     def coulomb_direct(self, irep=1, nlat=10):
         return self.L.orc_coulomb_direct(self.h, irep, nlat)
 
-    def hydro_tensors(self, rad, irep=1, cholesky=True):
+    def hydro_tensors(self, irep=1, cholesky=True):
+        """(D, L, rc) of replica irep at its current coordinates: the
+        tensor tis_params.i_hydro_tensor selects, with the bead radii."""
         n = 3 * self.nmp
         D = np.zeros((n, n))
         Lm = np.zeros((n, n)) if cholesky else None
-        rc = self.L.orc_hydro_tensors(self.h, irep, rad, ptr_f64(D), None if Lm is None else ptr_f64(Lm))
+        rc = self.L.orc_hydro_tensors(self.h, irep, ptr_f64(D), None if Lm is None else ptr_f64(Lm))
         # column-major (3N, 3N) buffers: transpose to row-major views
         return D.T.copy(), (None if Lm is None else Lm.T.copy()), rc
 
@@ -217,6 +262,12 @@ class Oracle:
 
     def nclamp(self):
         return self.L.orc_nclamp(self.h)
+
+    def rebuild_info(self, irep=1):
+        """(neighbour rebuilds of replica irep, istep of the last one)."""
+        n, last = C.c_long(0), C.c_long(0)
+        self.L.orc_rebuild_info(self.h, irep, C.byref(n), C.byref(last))
+        return n.value, last.value
 
     def pmf_range(self):
         return self.L.orc_pmf_range(self.h)

@@ -79,6 +79,7 @@ struct Rep {
   bool unif_exhausted = false;
   long nclamp = 0;
   long nrebuild = 0;
+  long last_rebuild = -1;          // istep of the last neighbour rebuild
   int pmf_range = 0;              // a Mg-P pair below the PMF table's first point
   std::vector<double> hD, hL;     // Brownian-HI: diffuse_tensor, random_tensor (3N x 3N, column-major)
   int not_spd = 0;
@@ -108,6 +109,7 @@ struct orc_ctx {
   std::vector<std::vector<int>> hb_at_site;   // static per-site hb lists (ascending ihb)
   int nfene = 0; std::vector<int> fene2mp; std::vector<double> fene_nat, coef_fene, dist2_fene;
   int nwca = 0; std::vector<int> wca2mp; std::vector<double> wca_nat, coef_wca;
+  std::vector<double> radius;      // var_struct radius: hydrodynamic radius per bead (Brownian-HI)
   int ntst = 0; std::vector<int> tst2mp; std::vector<double> tst_nat, tst_coef;
   std::vector<int> tst2st;         // (2, ntst) 0-based secondary stack of each side, -1: none
   std::vector<char> tst_excl;      // (2, ntst) after mloop_dtrna.F90:74-140
@@ -429,6 +431,7 @@ void neighbor(orc_ctx &c, Rep &r) {
   neighbor_ele(c, r);
   neighbor_hb(c, r);
   r.nrebuild++;
+  r.last_rebuild = r.istep;
 }
 
 // ------------------------------------------------------------ force terms
@@ -1458,6 +1461,8 @@ orc_ctx *orc_create(const tis_topology *t, const tis_params *p, int nrep, const 
   c->fric.assign(t->fric, t->fric + t->nmp);
   c->exv_radius.assign(t->exv_radius, t->exv_radius + t->nmp);
   c->exv_epsilon.assign(t->exv_epsilon, t->exv_epsilon + t->nmp);
+  if (t->radius) c->radius.assign(t->radius, t->radius + t->nmp);
+  else c->radius.assign(t->nmp, p->hi_radius);
   c->rcmass.resize(t->nmp);
   for (int i = 0; i < t->nmp; ++i) c->rcmass[i] = 1.0e0 / c->cmass[i];
   c->ncharge = t->ncharge;
@@ -1720,24 +1725,58 @@ int orc_energy_sumup(orc_ctx *c, int irep, double *energy, int reuse_hb) {
 
 // simu_hydro_tensors.F90:139-182 (HI_TENSOR%RPY, one radius) and 304-324
 // (Cholesky); D and L are (3N, 3N) column-major.  Returns 0 or TIS_E_NOT_SPD.
-int hydro_tensors(const orc_ctx *c, const Rep &r, double rad, double *D, double *Lc) {
+int hydro_tensors(const orc_ctx *c, const Rep &r, double *D, double *Lc) {
   double tempk = c->lab[r.label - 1].tempk;
   int N = c->nmp, n = 3 * N;
   double c6 = BOLTZ_KCAL_MOL * tempk / (6.0e0 * F_PI * c->par.viscosity);
   double c8 = BOLTZ_KCAL_MOL * tempk / (8.0e0 * F_PI * c->par.viscosity);
+  const int type = c->par.i_hydro_tensor == 0 ? TIS_HI_RPY : c->par.i_hydro_tensor;
+  const double rad = c->radius[0];   // radius(1): RPY, RPY_OVER, ERMAK_OVER
   auto Dm = [&](int i, int j) -> double & { return D[(size_t)j * n + i]; };
   std::fill(D, D + (size_t)n * n, 0.0);
   for (int i = 0; i < N; ++i) {
     int i0 = 3 * i;
+    const double rad_i = c->radius[i];
     for (int j = i + 1; j < N; ++j) {
       int j0 = 3 * j;
+      const double rad_j = c->radius[j];
       double rv[3];
       for (int d = 0; d < 3; ++d) rv[d] = r.xyz[3 * j + d] - r.xyz[3 * i + d];
       double r_sq = dot3(rv, rv), r_abs = std::sqrt(r_sq);
-      double rad_sq = rad * rad;
-      double pre1 = c8 / r_abs * (1.0 + 2.0 * rad_sq / (3.0 * r_sq));
-      double pre2 = c8 / r_abs * (1.0 - 2.0 * rad_sq / r_sq) / r_sq;
+      double pre1, pre2;
+      bool diag_only = false;
+      if (type == TIS_HI_ZUK_RPY) {   // simu_hydro_tensors.F90:50-124
+        if ((rad_i + rad_j) < r_abs) {
+          double rad_i_sq = rad_i * rad_i, rad_j_sq = rad_j * rad_j;
+          pre1 = c8 / r_abs * (1.0 + (rad_i_sq + rad_j_sq) / (3.0 * r_sq));
+          pre2 = c8 / r_abs * (1.0 - (rad_i_sq + rad_j_sq) / r_sq) / r_sq;
+        } else {
+          double rad_s, rad_l;
+          if (rad_i < rad_j) { rad_s = rad_i; rad_l = rad_j; } else { rad_s = rad_j; rad_l = rad_i; }
+          if ((rad_l - rad_s) < r_abs) {
+            double r_cb = r_sq * r_abs;
+            double dr2 = (rad_i - rad_j) * (rad_i - rad_j);
+            double y1 = dr2 + 3 * r_sq, y2 = dr2 - r_sq;
+            pre1 = c6 / rad_i / rad_j * (16.0 * r_cb * (rad_i + rad_j) - y1 * y1) / 32.0 / r_cb;
+            pre2 = c6 / rad_i / rad_j * 3.0 * (y2 * y2) / 32.0 / r_cb / r_sq;
+          } else {
+            pre1 = c6 / rad_l; pre2 = 0.0;
+            diag_only = true;
+          }
+        }
+      } else if (type == TIS_HI_RPY || 2.0 * rad < r_abs) {   // :139-182, and the far pairs of :187-300
+        double rad_sq = rad * rad;
+        pre1 = c8 / r_abs * (1.0 + 2.0 * rad_sq / (3.0 * r_sq));
+        pre2 = c8 / r_abs * (1.0 - 2.0 * rad_sq / r_sq) / r_sq;
+      } else if (type == TIS_HI_RPY_OVER) {   // :216-217
+        pre1 = c6 / rad * (1.0 - 9.0 / 32.0 * r_abs / rad);
+        pre2 = c6 / rad * 3.0 / 32.0 / rad / r_abs;
+      } else {   // ERMAK_OVER :269-270
+        pre1 = c8 / 2.0 / rad * 7.0 / 6.0;
+        pre2 = c8 / 2.0 / 2.0 / r_sq;
+      }
       for (int ii = 0; ii < 3; ++ii) {
+        if (diag_only) { Dm(i0 + ii, j0 + ii) = pre1; continue; }
         Dm(i0 + ii, j0 + ii) = pre1 + pre2 * rv[ii] * rv[ii];
         for (int jj = ii + 1; jj < 3; ++jj) {
           Dm(i0 + ii, j0 + jj) = pre2 * rv[ii] * rv[jj];
@@ -1752,7 +1791,7 @@ int hydro_tensors(const orc_ctx *c, const Rep &r, double rad, double *D, double 
       double s = Dm(i, j) + Dm(j, i);
       Dm(i, j) = s; Dm(j, i) = s;
     }
-  for (int i = 0; i < n; ++i) Dm(i, i) = c6 / rad;
+  for (int i = 0; i < n; ++i) Dm(i, i) = c6 / (type == TIS_HI_ZUK_RPY ? c->radius[i / 3] : rad);
   if (!Lc) return 0;
   auto Lm = [&](int i, int j) -> double & { return Lc[(size_t)j * n + i]; };
   std::fill(Lc, Lc + (size_t)n * n, 0.0);
@@ -1822,6 +1861,7 @@ int orc_step(orc_ctx *c, long nsteps) {
       }
       if (rebuild) {
         neighbor(*c, r);
+        r.last_rebuild = istep;   // the step whose trigger fired (outfile%neigh record, time_integral.F90:76-84)
         if (c->par.n_step_neighbor <= 0) std::fill(r.dxyz.begin(), r.dxyz.end(), 0.0);
       }
     }
@@ -1838,7 +1878,7 @@ int orc_step(orc_ctx *c, long nsteps) {
         if ((r.istep - 1) % every == 0) {
           r.hD.resize((size_t)n * n);
           r.hL.resize((size_t)n * n);
-          if (hydro_tensors(c, r, c->par.hi_radius, r.hD.data(), r.hL.data()) != 0) r.not_spd = 1;
+          if (hydro_tensors(c, r, r.hD.data(), r.hL.data()) != 0) r.not_spd = 1;
         }
         const double rl1 = c->par.tstep / (BOLTZ_KCAL_MOL * T), rl2 = std::sqrt(2.0e0 * c->par.tstep);
         const double *xi = &rbm[n3 * i];
@@ -1943,6 +1983,48 @@ int orc_replica_exchange(orc_ctx *c, const double *u, int *n_accept) {
   return 0;
 }
 
+// energy_allrep.F90:130-217 for replica irep alone: out2 = (energy at its
+// own label with the hbond energies of the last force call, energy at the
+// exchange partner's label or 0 without one), labels unchanged
+int orc_replica_energy(orc_ctx *c, int irep, double *out2) {
+  const int n = c->nrep;
+  Rep &r = c->rep[irep - 1];
+  double E[TIS_ETYPE_MAX];
+  energy_sumup(*c, r, E, true);
+  out2[0] = E[TIS_E_TOTAL - 1];
+  int lo;
+  if (c->idx_pair == 1) lo = (r.label % 2 == 1) ? ((r.label + 1 <= n) ? r.label + 1 : 0) : r.label - 1;
+  else if (r.label == 1) lo = 0;
+  else lo = (r.label % 2 == 0) ? ((r.label + 1 <= n) ? r.label + 1 : 0) : r.label - 1;
+  if (lo == 0) { out2[1] = 0.0; return 0; }
+  const int keep = r.label;
+  const double bkeep = c->beta_hbond15;
+  r.label = lo;
+  c->beta_hbond15 = 1.0e0 / (c->lab[lo - 1].tempk * BOLTZ_KCAL_MOL);
+  energy_sumup(*c, r, E, false);
+  out2[1] = E[TIS_E_TOTAL - 1];
+  r.label = keep;
+  c->beta_hbond15 = bkeep;
+  return 0;
+}
+
+// The outcome of an exchange decided elsewhere: the new rep2lab (1-based),
+// velocities times vscale[r] (> 0) or divided by -vscale[r] (< 0), the pair
+// alternation and the label-dependent parameters, as orc_replica_exchange
+// leaves them.
+int orc_rex_apply(orc_ctx *c, const int *rep2lab, const double *vscale) {
+  for (int i = 0; i < c->nrep; ++i) {
+    Rep &r = c->rep[i];
+    r.label = rep2lab[i];
+    c->lab2rep[rep2lab[i] - 1] = i + 1;
+    if (vscale[i] > 0.0) for (auto &v : r.velo) v = vscale[i] * v;
+    else if (vscale[i] < 0.0) for (auto &v : r.velo) v = v / (-vscale[i]);
+  }
+  c->idx_pair = (c->idx_pair == 2) ? 1 : c->idx_pair + 1;
+  para2(*c);
+  return 0;
+}
+
 int orc_get_labels(orc_ctx *c, int *rep2lab) {
   for (int i = 0; i < c->nrep; ++i) rep2lab[i] = c->rep[i].label;
   return 0;
@@ -1995,14 +2077,21 @@ double orc_coulomb_direct(orc_ctx *c, int irep, int nlat) {
   return L.coef * e;
 }
 
-int orc_hydro_tensors(orc_ctx *c, int irep, double rad, double *D, double *Lc) {
-  return hydro_tensors(c, c->rep[irep - 1], rad, D, Lc);
+int orc_hydro_tensors(orc_ctx *c, int irep, double *D, double *Lc) {
+  return hydro_tensors(c, c->rep[irep - 1], D, Lc);
 }
 
 int orc_not_spd(orc_ctx *c) {
   int f = 0;
   for (auto &r : c->rep) f |= r.not_spd;
   return f;
+}
+
+// neighbour rebuilds of replica irep and the step of the last one
+void orc_rebuild_info(orc_ctx *c, int irep, long *n, long *last) {
+  const Rep &r = c->rep[irep - 1];
+  if (n) *n = r.nrebuild;
+  if (last) *last = r.last_rebuild;
 }
 
 long orc_nclamp(orc_ctx *c) {

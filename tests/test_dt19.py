@@ -13,7 +13,9 @@ from tis_b200 import ninfo, synth
 from tis_b200.abi import MP_ION_MG, MP_RNA_PHOS
 from oracle.oracle import Oracle
 
-REF = "/root/reference"
+# the reference source tree (Hori-Lab/TIS), when present: its input files
+# are read as test data; the tests that need it skip otherwise
+REF = os.environ.get("TIS_REFERENCE_DIR", "")
 ELE, EPSI_0, BOLTZ_J, N_AVO = 1.6021766208e-19, 8.854187817e-12, 1.38064852e-23, 6.022140857e23
 JOUL2KCAL_MOL = 1.0 / 4184.0 * N_AVO
 BOX = 80.0
@@ -165,7 +167,7 @@ def test_read_pmf_text():
         ninfo.read_pmf(bad)
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="TIS_REFERENCE_DIR not set")
 def test_read_reference_pmf_file():
     d = ninfo.read_pmf(f"{REF}/para/PMF_RISM/pmf_Mg_P_1264")
     assert d["pmf_nbin"] == 1930 and d["pmf_rmin"] == 1.775 and d["pmf_rmax"] == 50.0
@@ -179,7 +181,7 @@ def test_synthetic_table_matches_reference_grid():
     assert v[0] > 300 and v.min() < -0.5 and abs(v[-1]) < 0.2
 
 
-@pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+@pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="TIS_REFERENCE_DIR not set")
 def test_reference_bwyv19_force_check_input(oracle_lib):
     """The reference's DT19 force-check input (inp/bwyv19_force_check.inp:
     bwyv19.ninfo on the RNA and 206-Mg PDBs, the RISM Mg-P table,

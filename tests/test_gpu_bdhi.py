@@ -89,7 +89,7 @@ def test_bdhi_reports_non_spd_tensor(tis_lib):
     par = synth.bdhi_params()
     orc = Oracle(s, par, [300.0])
     orc.set_state(x[None])
-    _, _, rc = orc.hydro_tensors(par["hi_radius"])
+    _, _, rc = orc.hydro_tensors()
     assert rc == TIS_E_NOT_SPD
     eng = Engine([s], par, [300.0])
     eng.set_state(x)
@@ -118,7 +118,7 @@ def test_bdhi_cholesky_factor(tis_lib, precision, tol):
     D, L = eng.hydro_tensors()
     orc = Oracle(s, dict(par, precision=0), [300.0])
     orc.set_state(x0[None])
-    Dr, Lr, rc = orc.hydro_tensors(par["hi_radius"])
+    Dr, Lr, rc = orc.hydro_tensors()
     assert rc == 0
     dtol = 1e-12 if precision == 0 else 1e-7   # precision 1 keeps D in FP32 for the step
     assert np.abs(D - Dr).max() <= dtol * np.abs(Dr).max()
@@ -172,4 +172,83 @@ def test_bdhi_tensor_core_trajectory(tis_lib):
     xr = orc.get_state()[0].reshape(-1, 3)
     assert np.abs(xr - s["xyz"]).max() > 1e-3
     assert np.abs(x - xr).max() < 1e-6
+    eng.close()
+
+
+def _variant_chain(kind, n, seed, nest):
+    """Bead chain squeezed so that neighbours overlap; Zuk-RPY gets per-bead
+    radii and, with nest, one small bead inside a large one (its WCA record
+    with that bead removed, so forces stay finite)."""
+    s = dict(synth.bead_chain(n, seed))
+    x = s["xyz"] * 0.85
+    if kind == 4:
+        rng = np.random.default_rng(seed)
+        r = rng.uniform(1.2, 2.8, n)
+        if nest:
+            i, j = n // 2 - 3, n // 2
+            r[i], r[j] = 2.6, 1.0
+            x = x.copy()
+            x[j] = x[i] + np.array([0.3, 0.1, -0.2])
+            keep = ~((s["iwca2mp"][:, 0] == i + 1) & (s["iwca2mp"][:, 1] == j + 1))
+            s["iwca2mp"] = s["iwca2mp"][keep]
+            s["wca_nat"] = s["wca_nat"][keep]
+            s["coef_wca"] = s["coef_wca"][:, keep]
+            s["nwca"] = int(keep.sum())
+        s["radius"] = r
+    s["xyz"] = x
+    return s
+
+
+@pytest.mark.parametrize("kind", [1, 2, 3, 4])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_bdhi_tensor_variants(tis_lib, kind, precision):
+    """HI_TENSOR RPY, RPY_OVER, ERMAK_OVER and Zuk-RPY with per-bead radii
+    (simu_hydro_tensors.F90:50-300): D of the refresh against the oracle
+    (FP64: the same rounded operations, relative 1e-15; mixed keeps D in
+    FP32: 1e-7) and its factor (FP64 1e-12, mixed 1e-5)."""
+    s = _variant_chain(kind, 90, 40 + kind, nest=True)
+    par = synth.bdhi_params(precision=precision, i_hydro_tensor=kind)
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(np.zeros((2, s["nmp"], 3)))
+    eng.time_integral_pre()
+    assert eng.step(1) >= 0
+    D, L = eng.hydro_tensors()
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(s["xyz"][None])
+    Dr, Lr, rc = orc.hydro_tensors()
+    if kind == 3:
+        # the Ermak-McCammon overlap formula is not positive definite on
+        # every squeezed chain: both sides must then agree on the failure
+        if rc != 0:
+            eng.close()
+            return
+    assert rc == 0
+    dtol = 1e-15 if precision == 0 else 1e-7
+    assert np.abs(D - Dr).max() <= dtol * np.abs(Dr).max()
+    ltol = 1e-12 if precision == 0 else 1e-5
+    assert np.abs(L - Lr).max() <= ltol * np.abs(Lr).max()
+    eng.close()
+
+
+@pytest.mark.parametrize("kind", [2, 4])
+def test_bdhi_tensor_variant_trajectory(tis_lib, kind):
+    s = _variant_chain(kind, 50, 60 + kind, nest=False)
+    par = synth.bdhi_params(i_hydro_tensor=kind, n_step_hydro=2)
+    nsteps = 6
+    noise = np.random.default_rng(kind).normal(size=(nsteps + 1, s["nmp"], 3))
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(noise)
+    eng.time_integral_pre()
+    assert eng.step(nsteps) >= 0
+    x = eng.get_state()[0]
+    orc = Oracle(s, par, [300.0])
+    orc.set_state(s["xyz"][None])
+    orc.set_noise(noise.reshape(nsteps + 1, 1, s["nmp"], 3))
+    orc.time_integral_pre()
+    orc.step(nsteps)
+    xr = orc.get_state()[0].reshape(-1, 3)
+    assert np.abs(xr - s["xyz"]).max() > 1e-3
+    assert np.abs(x - xr).max() < 1e-9
     eng.close()

@@ -109,3 +109,31 @@ def test_reference_arm_prints_contract_line():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_bench_gpus_2_spawns_two_ranks():
+    """bench.py --gpus 2 without a launcher relaunches itself as two ranks
+    (torch.distributed.run); the reference arm joins them in a gloo group and
+    rank 0 alone prints the line."""
+    env = dict(os.environ, PYTHONPATH=ROOT)
+    env.pop("WORLD_SIZE", None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                          "--steps", "1", "--warmup", "0", "--ref-sample", "5"],
+                         check=True, capture_output=True, text=True, timeout=600, env=env).stdout
+    lines = [json.loads(x) for x in out.strip().splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == 2 and lines[0]["ranks_joined"] == 2
+
+
+def test_cpu_fleet_times_only_the_steps():
+    """The CPU leg's processes set up their replicas before the timed passes;
+    a pass of n steps reports the replica-steps over its wall time."""
+    s, par, temps = synth.workload_c1()
+    fleet = bench.CpuFleet(s * 1, par, temps * 3, [3], 40, "checker")
+    try:
+        assert fleet.cores == min(os.cpu_count() or 1, 3)
+        r1 = fleet.run(20)
+        r2 = fleet.run(40)
+        assert r1 > 0 and r2 > 0
+    finally:
+        fleet.close()

@@ -12,7 +12,9 @@ from tis_b200 import ninfo as N
 from tis_b200 import synth
 from tis_b200.abi import CLASS_ION, CLASS_RNA, MP_ION_CL, MP_ION_MG, MP_RNA_BASE, MP_RNA_PHOS, MP_RNA_SUGAR
 
-REF = "/root/reference"
+# the reference source tree (Hori-Lab/TIS), when present: its input files
+# are read as test data; the tests that need it skip otherwise
+REF = os.environ.get("TIS_REFERENCE_DIR", "")
 
 # A 4-nucleotide chain with a 5' phosphate (P S B per nucleotide, beads 1-12)
 # and an ion unit, in the fixed columns of read_pdb_cg.F90 (coordinates
@@ -221,7 +223,7 @@ def test_writer_round_trip():
             assert a.shape == b.shape and np.allclose(a, b, rtol=1e-15, atol=0), k
 
 
-needs_ref = pytest.mark.skipif(not os.path.isdir(REF), reason="reference tree not present")
+needs_ref = pytest.mark.skipif(not REF or not os.path.isdir(REF), reason="TIS_REFERENCE_DIR not set")
 
 
 @needs_ref

@@ -20,6 +20,7 @@ E_STACK_DTRNA, E_HBOND_DTRNA, E_EXV_DT15 = 16, 17, 18
 E_TSTACK_DTRNA, E_THBOND_DTRNA, E_WCA_REP, E_WCA_ATT = 19, 20, 23, 24
 ETYPE_MAX = 25
 SIM_LANGEVIN, SIM_BROWNIAN_HI = 1, 6
+HI_RPY, HI_RPY_OVER, HI_ERMAK_OVER, HI_ZUK_RPY = 1, 2, 3, 4
 ELE_NONE, ELE_DH, ELE_EWALD = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 
@@ -56,7 +57,7 @@ class Topology(C.Structure):
         ("nwca", C.c_int32), ("iwca2mp", _i32p), ("wca_nat", _f64p), ("coef_wca", _f64p),
         ("ntst", C.c_int32), ("idtrna_tst2mp", _i32p), ("dtrna_tst_nat", _f64p),
         ("coef_dtrna_tst", _f64p), ("idtrna_tst2side", _i32p), ("flg_tst_exclusive", _i32p),
-        ("flg_hb_tertiary", _i32p), ("flg_charge_fixed", _i32p),
+        ("flg_hb_tertiary", _i32p), ("flg_charge_fixed", _i32p), ("radius", _f64p),
     ]
 
 
@@ -77,7 +78,7 @@ class Params(C.Structure):
         ("hi_radius", C.c_double), ("n_step_hydro", C.c_int32),
         ("i_dtrna_model", C.c_int32), ("i_charge", C.c_int32), ("length_per_unit_P", C.c_double),
         ("pmf_nbin", C.c_int32), ("pmf_rmin", C.c_double), ("pmf_rbin", C.c_double), ("pmf_rmax", C.c_double),
-        ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p),
+        ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p), ("i_hydro_tensor", C.c_int32),
     ]
 
 
@@ -115,10 +116,10 @@ _TOPO_ARRAYS = {
     "iwca2mp": np.int32, "wca_nat": np.float64, "coef_wca": np.float64,
     "idtrna_tst2mp": np.int32, "dtrna_tst_nat": np.float64, "coef_dtrna_tst": np.float64,
     "idtrna_tst2side": np.int32, "flg_tst_exclusive": np.int32,
-    "flg_hb_tertiary": np.int32, "flg_charge_fixed": np.int32,
+    "flg_hb_tertiary": np.int32, "flg_charge_fixed": np.int32, "radius": np.float64,
 }
 # Arrays the library accepts as NULL (their absence has a meaning of its own).
-_TOPO_OPTIONAL = ("flg_hb_tertiary", "flg_charge_fixed")
+_TOPO_OPTIONAL = ("flg_hb_tertiary", "flg_charge_fixed", "radius")
 _TOPO_COUNTS = ("nmp", "nunit", "ncharge", "nbd", "nba", "nst", "nhb", "nhbsite", "nfene", "nwca", "ntst")
 
 
@@ -194,6 +195,8 @@ EXPORTED = [
     "tis_replica_exchange", "tis_get_labels", "tis_status", "tis_last_step_ms",
     "tis_last_error", "tis_timer", "tis_force_sumup_static", "tis_launch_count",
     "tis_get_hydro_tensors", "tis_set_step", "tis_get_dtrna_status",
+    "tis_time_integral", "tis_get_steps", "tis_get_rebuild_info", "tis_get_random_number",
+    "tis_init_ladder", "tis_rex_energies", "tis_rex_exchange_all", "tis_rex_decide",
 ]
 
 
@@ -229,5 +232,14 @@ def _declare(lib):
     lib.tis_get_hydro_tensors.argtypes = [vp, C.c_int32, _f64p, _f64p]
     lib.tis_set_step.argtypes = [vp, C.c_int64]
     lib.tis_get_dtrna_status.argtypes = [vp, C.c_int32, _i32p, _i32p]
+    lib.tis_time_integral.argtypes = [vp, C.c_int64, _i32p, C.POINTER(C.c_int64)]
+    lib.tis_init_ladder.argtypes = [C.POINTER(Topology), C.POINTER(Params), C.c_int32, _f64p, C.c_int32, C.c_int32,
+                                    C.POINTER(vp)]
+    lib.tis_rex_energies.argtypes = [vp, _f64p]
+    lib.tis_rex_exchange_all.argtypes = [vp, _f64p, _f64p, _i32p]
+    lib.tis_rex_decide.argtypes = [C.c_int32, _f64p, C.c_int32, _f64p, _f64p, _i32p, _f64p, _i32p]
+    lib.tis_get_random_number.argtypes = [vp, C.c_int64, C.c_int32, _f64p]
+    lib.tis_get_steps.argtypes = [vp, C.POINTER(C.c_int64)]
+    lib.tis_get_rebuild_info.argtypes = [vp, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     lib.tis_launch_count.argtypes = [vp]
     lib.tis_launch_count.restype = C.c_int64

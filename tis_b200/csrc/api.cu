@@ -13,6 +13,7 @@
 #include <map>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -30,9 +31,11 @@ cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, con
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t noise_launch(cudaStream_t st, KArgs a, long long istep0, int nstep, double *out);
 cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst, int *out);
 cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
                        double *ebeta);
+cudaError_t vscale_launch(cudaStream_t st, const KArgs &a, const double *scale, double *velo);
 cudaError_t rex_exchange_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep,
                                 const double *e_own, const double *e_opp, const double *u, double *scale,
                                 double *velo);
@@ -106,6 +109,9 @@ struct tis_ctx {
   std::vector<int> rep2lab;          // per lane, global label index
   std::vector<int> lab2rep;          // per label, lane
   int idx_pair = 1;                  // odd/even alternation (var_replica.F90:134,165-183)
+  int rep_first = 0;                 // ladder context: global replica of lane 0 (irep2grep(1) - 1)
+  std::vector<int> g_rep2lab, g_lab2rep;   // ladder context: label maps of the whole ladder (0-based)
+  unsigned long long g_counter = 0;  // ladder context: counter of the exchange uniforms
   bool hb_energy_valid = false;      // flg_hb_energy
   double beta_global = 0.0;
   // device buffers
@@ -137,6 +143,7 @@ struct tis_ctx {
   DBuf<double> hb_ene;
   DBuf<unsigned char> slots;
   DBuf<double> noise, unif;
+  DBuf<int> lane_n;                  // per-lane step counts of the last tis_time_integral
   int noise_nsteps = 0, noise_base = 0, n_unif = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, tev0 = nullptr, tev1 = nullptr;
@@ -158,7 +165,7 @@ struct tis_ctx {
   long long bd_istep = 0;
   DBuf<int> fene_idx, wca_idx, bd_ptr, d_not_spd;
   DBuf<int2> bd_ent;
-  DBuf<double> fene_cls, wca_cls;
+  DBuf<double> fene_cls, wca_cls, b_hrad;
   DBuf<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef, bd_D, bd_L, bd_F, bd_xi;
   DBuf<float> bd_P, bd_D32, bd_L32;
   DBuf<int> bd_items;               // tensor-core update work items, per launch
@@ -303,9 +310,17 @@ void ewald_table(double L, double alpha, double hmax, std::vector<int8_t> &hv, s
 }  // namespace
 
 // --------------------------------------------------------------------- init
-extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_params *par,
-                              const int32_t *nrep, const double *tempk, tis_ctx **out) {
-  if (!out || !tops || !par || !nrep || !tempk || ntop <= 0) return TIS_E_ARG;
+namespace {
+// the whole ladder of a context that holds only some of its replicas
+struct Ladder {
+  int nall;
+  const double *tempk_all;
+  int first;
+};
+
+int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, const int32_t *nrep,
+              const double *tempk, const Ladder *lad, tis_ctx **out) {
+  if (!out || !tops || !par || !nrep || (!tempk && !lad) || ntop <= 0) return TIS_E_ARG;
   *out = nullptr;
   tis_ctx *c = new tis_ctx();
   c->par = *par;
@@ -318,7 +333,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   // the Brownian-HI path evaluates FENE and WCA records (the C5 bead chains):
   // no electrostatics, no DT15 or harmonic terms
   if (p.i_ele < TIS_ELE_NONE || p.i_ele > TIS_ELE_COULOMB) { tis_destroy(c); return TIS_E_ARG; }
-  if (c->bdhi && (p.i_ele != TIS_ELE_NONE || !(p.viscosity > 0.0) || !(p.hi_radius > 0.0))) {
+  if (c->bdhi && (p.i_ele != TIS_ELE_NONE || !(p.viscosity > 0.0) || p.i_hydro_tensor < 0 || p.i_hydro_tensor > 4)) {
     tis_destroy(c);
     return TIS_E_UNSUPPORTED;
   }
@@ -378,6 +393,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   std::vector<double> fene_cls, wca_cls;
   std::map<std::array<double, 3>, int> fene_cmap, wca_cmap;
   std::vector<double> fene_nat, fene_coef, fene_d2, wca_nat, wca_coef;
+  std::vector<double> b_hrad;   // Brownian-HI: hydrodynamic radius of every bead
   int maxN = 0;
   for (int k = 0; k < ntop; ++k) {
     const tis_topology &t = tops[k];
@@ -412,6 +428,11 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     d.wc0 = (int)wca_nat.size(); d.nwc = t.nwca;
     d.bp0 = (int)bdp.size(); d.be0 = (int)bde.size();
     if (c->bdhi) {
+      for (int i = 0; i < t.nmp; ++i) {
+        const double r = t.radius ? t.radius[i] : p.hi_radius;
+        if (!(r > 0.0)) { tis_destroy(c); return TIS_E_ARG; }
+        b_hrad.push_back(r);
+      }
       std::vector<std::vector<int2>> per(t.nmp);
       auto cls_of = [](std::map<std::array<double, 3>, int> &m, std::vector<double> &tab, double p0, double p1,
                        double p2) {
@@ -631,23 +652,64 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     d.ninc = ip - ip0;
     c->tops.push_back(d);
   }
-  // ---- lanes and labels
+  // ---- labels (temperatures) and lanes (replicas).  Normally lane l starts
+  // with label l; a ladder context holds labels for the whole ladder and
+  // lanes for its share of the replicas (lane l is global replica first + l)
   int nlane = 0;
   for (int k = 0; k < ntop; ++k) {
     if (nrep[k] <= 0) { tis_destroy(c); return TIS_E_ARG; }
     nlane += nrep[k];
   }
+  const int nlabel = lad ? lad->nall : nlane;
+  const double *lab_temp = lad ? lad->tempk_all : tempk;
   c->nlane = nlane;
-  c->nlabel = nlane;
-  std::vector<double> lab_T(nlane), lab_coef(nlane), lab_cdist(nlane), lab_beta(nlane), lab_rele2(nlane);
-  std::vector<double> lab_zp(nlane, 0.0), pmf_e, pmf_f;
+  c->nlabel = nlabel;
+  c->rep_first = lad ? lad->first : 0;
+  std::vector<double> lab_T(nlabel), lab_coef(nlabel), lab_cdist(nlabel), lab_beta(nlabel), lab_rele2(nlabel);
+  std::vector<double> lab_zp(nlabel, 0.0), pmf_e, pmf_f;
   const bool pmf_on = dt19 && n_mg_any > 0;
-  if (pmf_on) { pmf_e.assign((size_t)nlane * p.pmf_nbin, 0.0); pmf_f.assign((size_t)nlane * p.pmf_nbin, 0.0); }
-  std::vector<int> lab_u0off(nlane), lab_c1off(nlane);
+  if (pmf_on) { pmf_e.assign((size_t)nlabel * p.pmf_nbin, 0.0); pmf_f.assign((size_t)nlabel * p.pmf_nbin, 0.0); }
+  std::vector<int> lab_u0off(nlabel), lab_c1off(nlabel);
   std::vector<double> lab_u0, lab_c1;
-  c->label_top.resize(nlane);
+  c->label_top.resize(nlabel);
   c->rep2lab.resize(nlane);
-  c->lab2rep.resize(nlane);
+  c->lab2rep.resize(nlabel);
+  {
+    int label = 0;
+    for (int k = 0; k < ntop; ++k) {
+      TopDesc &d = c->tops[k];
+      d.nlabel = lad ? nlabel : nrep[k];
+      c->top_first_label.push_back(label);
+      const int N = d.nmp;
+      for (int r = 0; r < d.nlabel; ++r, ++label) {
+        const double T = lab_temp[label];
+        double ek, coef, cdist;
+        ele_params(p, T, ek, coef, cdist);
+        lab_T[label] = T;
+        lab_coef[label] = coef;
+        lab_cdist[label] = cdist;
+        if (p.i_charge == 1) lab_zp[label] = manning_zp(p, T, ek, top_nmg[k], dt19);
+        if (pmf_on && top_nmg[k] > 0)
+          pmf_table(p, coef, cdist, lab_zp[label], &pmf_e[(size_t)label * p.pmf_nbin],
+                    &pmf_f[(size_t)label * p.pmf_nbin]);
+        lab_beta[label] = 1.0e0 / (T * BOLTZ_KCAL_MOL);
+        double rr = (p.i_ele == TIS_ELE_DH) ? (p.neigh_margin + p.cutoff_ele * cdist) : (p.neigh_margin + p.cutoff_ele);
+        lab_rele2[label] = rr * rr;
+        lab_u0off[label] = (int)lab_u0.size();
+        for (int s = 0; s < d.nst; ++s) {   // simu_set_dtrna.F90:48-53
+          const double *hst = &st_hsTm_all[3 * (size_t)(d.st0 + s)];
+          lab_u0.push_back(-hst[0] + BOLTZ_KCAL_MOL * (T - hst[2]) * hst[1]);
+        }
+        lab_c1off[label] = (int)lab_c1.size();
+        for (int i = 0; i < N; ++i) {   // time_integral_pre.F90:166-167
+          const int b = d.bead0 + i;
+          lab_c1.push_back(std::sqrt(2.0e0 * b_fric[b] * BOLTZ_KCAL_MOL * T / (p.tstep * b_cmass[b])));
+        }
+        c->label_top[label] = k;
+        c->lab2rep[label] = label;
+      }
+    }
+  }
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
@@ -655,35 +717,10 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
-    d.nlabel = nrep[k];
-    c->top_first_label.push_back(lane);
     const int N = d.nmp;
     for (int r = 0; r < nrep[k]; ++r, ++lane) {
-      const double T = tempk[lane];
-      double ek, coef, cdist;
-      ele_params(p, T, ek, coef, cdist);
-      lab_T[lane] = T;
-      lab_coef[lane] = coef;
-      lab_cdist[lane] = cdist;
-      if (p.i_charge == 1) lab_zp[lane] = manning_zp(p, T, ek, top_nmg[k], dt19);
-      if (pmf_on && top_nmg[k] > 0)
-        pmf_table(p, coef, cdist, lab_zp[lane], &pmf_e[(size_t)lane * p.pmf_nbin], &pmf_f[(size_t)lane * p.pmf_nbin]);
-      lab_beta[lane] = 1.0e0 / (T * BOLTZ_KCAL_MOL);
-      double rr = (p.i_ele == TIS_ELE_DH) ? (p.neigh_margin + p.cutoff_ele * cdist) : (p.neigh_margin + p.cutoff_ele);
-      lab_rele2[lane] = rr * rr;
-      lab_u0off[lane] = (int)lab_u0.size();
-      for (int s = 0; s < d.nst; ++s) {   // simu_set_dtrna.F90:48-53
-        const double *hst = &st_hsTm_all[3 * (size_t)(d.st0 + s)];
-        lab_u0.push_back(-hst[0] + BOLTZ_KCAL_MOL * (T - hst[2]) * hst[1]);
-      }
-      lab_c1off[lane] = (int)lab_c1.size();
-      for (int i = 0; i < N; ++i) {   // time_integral_pre.F90:166-167
-        const int b = d.bead0 + i;
-        lab_c1.push_back(std::sqrt(2.0e0 * b_fric[b] * BOLTZ_KCAL_MOL * T / (p.tstep * b_cmass[b])));
-      }
-      c->label_top[lane] = k;
-      c->rep2lab[lane] = lane;
-      c->lab2rep[lane] = lane;
+      const int grep = c->rep_first + lane;   // global replica (0-based)
+      c->rep2lab[lane] = grep;
       LaneDesc L{};
       L.top = k;
       L.state0 = state_off;
@@ -698,6 +735,8 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
       L.bd0 = bd_off;
       L.bdp0 = bdp_off;
       L.bd32 = bd32_off;
+      L.key_lane = grep;
+      L.key_bead0 = lad ? grep * N : state_off;
       if (c->bdhi) bd_off += 9LL * N * N;
       if (c->bdhi && p.precision == TIS_PREC_MIXED) {
         bdp_off += bd_plane_floats(N);
@@ -720,7 +759,12 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   c->nbead_total = state_off;
   c->lab_T = lab_T;
   // the global beta_hbond15 is the value set for the last replica (simu_set_dtrna.F90:58)
-  c->beta_global = lab_beta[nlane - 1];
+  c->beta_global = lab_beta[nlabel - 1];
+  if (lad) {
+    c->g_rep2lab.resize(nlabel);
+    c->g_lab2rep.resize(nlabel);
+    for (int g = 0; g < nlabel; ++g) { c->g_rep2lab[g] = g; c->g_lab2rep[g] = g; }
+  }
   c->threads = choose_threads(maxN, p.precision == TIS_PREC_MIXED);
   c->group = choose_group(c->threads, maxN);
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
@@ -745,15 +789,15 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   }
   c->smem = smem;
   // two CTAs per lane (a cluster) when the lanes fill at most half of the
-  // SMs: mixed precision, no periodic box, fixed rebuild cadence, DH or no
-  // electrostatics; TIS_CLUSTER=0 turns it off
+  // SMs: mixed precision, no periodic box, DH, Coulomb or no electrostatics
+  // (either rebuild rule); TIS_CLUSTER=0 turns it off
   {
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const char *env = std::getenv("TIS_CLUSTER");
     const bool allow = !(env && env[0] == '0');
-    c->pair = allow && !c->bdhi && p.precision == TIS_PREC_MIXED && !periodic && !skin &&
+    c->pair = allow && !c->bdhi && p.precision == TIS_PREC_MIXED && !periodic &&
               p.i_ele != TIS_ELE_EWALD && minN >= 64 && nsm > 0 && 2 * nlane <= nsm && smem2 <= 227 * 1024;
     c->smem2 = c->pair ? smem2 : 0;
   }
@@ -766,7 +810,11 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(c->d_tops.upload(c->tops));
   CK(c->d_lanes.upload(c->lanes));
   std::vector<LaneState> ls(nlane);
-  for (int i = 0; i < nlane; ++i) { std::memset(&ls[i], 0, sizeof(LaneState)); ls[i].label = i; }
+  for (int i = 0; i < nlane; ++i) {
+    std::memset(&ls[i], 0, sizeof(LaneState));
+    ls[i].label = c->rep2lab[i];
+    ls[i].last_rebuild = -1;
+  }
   CK(c->d_lstate.upload(ls));
   CK(c->b_type.upload(b_type)); CK(c->b_class.upload(b_class)); CK(c->b_unit.upload(b_unit));
   CK(c->b_rcmass.upload(b_rcmass)); CK(c->b_cmass.upload(b_cmass)); CK(c->b_fric.upload(b_fric));
@@ -798,6 +846,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   CK(cudaMemset(c->dxyz.p, 0, n3 * 8));
   CK(c->out_energy.alloc((size_t)nlane * N_ETYPE));
   CK(c->scale.alloc(nlane));
+  CK(c->lane_n.alloc(nlane));
   CK(c->ebeta.alloc(nlane));
   CK(c->elabel.alloc(nlane));
   CK(c->e_opp.alloc((size_t)nlane * N_ETYPE));
@@ -824,7 +873,7 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
     CK(c->fene_idx.upload(fene_idx)); CK(c->fene_nat.upload(fene_nat)); CK(c->fene_coef.upload(fene_coef));
     CK(c->fene_d2.upload(fene_d2));
     CK(c->wca_idx.upload(wca_idx)); CK(c->wca_nat.upload(wca_nat)); CK(c->wca_coef.upload(wca_coef));
-    CK(c->bd_ptr.upload(bdp)); CK(c->bd_ent.upload(bde));
+    CK(c->bd_ptr.upload(bdp)); CK(c->bd_ent.upload(bde)); CK(c->b_hrad.upload(b_hrad));
     if (fene_cls.empty()) fene_cls.assign(3, 0.0);
     if (wca_cls.empty()) wca_cls.assign(3, 0.0);
     CK(c->fene_cls.upload(fene_cls)); CK(c->wca_cls.upload(wca_cls));
@@ -874,6 +923,22 @@ extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_
   *out = c;
   return TIS_OK;
 }
+}  // namespace
+
+extern "C" int tis_init_batch(int32_t ntop, const tis_topology *tops, const tis_params *par,
+                              const int32_t *nrep, const double *tempk, tis_ctx **out) {
+  return init_impl(ntop, tops, par, nrep, tempk, nullptr, out);
+}
+
+extern "C" int tis_init_ladder(const tis_topology *top, const tis_params *par, int32_t nrep_all,
+                               const double *tempk_all, int32_t irep_first, int32_t nrep_local, tis_ctx **out) {
+  if (!out || !tempk_all || nrep_all <= 0 || nrep_local <= 0 || irep_first < 1 ||
+      irep_first - 1 + nrep_local > nrep_all)
+    return TIS_E_ARG;
+  if (par && par->i_simulate_type == TIS_SIM_BROWNIAN_HI) return TIS_E_UNSUPPORTED;
+  const Ladder lad{nrep_all, tempk_all, irep_first - 1};
+  return init_impl(1, top, par, &nrep_local, nullptr, &lad, out);
+}
 
 extern "C" int tis_init(const tis_topology *top, const tis_params *par, int32_t nrep, const double *tempk,
                         tis_ctx **out) {
@@ -901,9 +966,9 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free(); c->p0xyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
-  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free();
+  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free(); c->lane_n.free();
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
-  c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->d_not_spd.free();
+  c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->b_hrad.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
   c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_items.free(); c->bd_D32.free(); c->bd_L32.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1054,6 +1119,8 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_P = c->bd_P.p; a.bd_D32 = c->bd_D32.p; a.bd_L32 = c->bd_L32.p; a.bd_W = c->bd_W.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
   a.not_spd = c->d_not_spd.p;
   a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
+  a.i_hydro_tensor = p.i_hydro_tensor == 0 ? TIS_HI_RPY : p.i_hydro_tensor;
+  a.b_hrad = c->b_hrad.p;
   a.boltz = BOLTZ_KCAL_MOL; a.pi = F_PI;
   a.bd_istep = c->bd_istep; a.bd_kpanel = 0;
   a.bd_tc = (c->bdhi && p.precision == TIS_PREC_MIXED) ? 1 : 0;
@@ -1104,6 +1171,8 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_unif = c->n_unif;
   a.nbead_total = c->nbead_total;
   a.noise_in_sweep = 0;
+  a.lane_nsteps = nullptr;
+  a.step_k = 0;
   return a;
 }
 
@@ -1361,10 +1430,17 @@ extern "C" int tis_time_integral_pre(tis_ctx *c) {
   return check_lanes(c);
 }
 
-extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
-  if (!c || nsteps < 0 || nsteps > 0x7fffffff) return TIS_E_ARG;
-  if (nsteps == 0) return TIS_OK;
-  KArgs a = make_args(c, KM_STEP, (int)nsteps, -1);
+namespace {
+// nsteps calls of time_integral for every lane; lane_n (host, per lane, may
+// be null) lets lane l take only lane_n[l] of them (replicas that wait for
+// their exchange step, time_integral.F90:134).
+int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
+  KArgs a = make_args(c, KM_STEP, nsteps, -1);
+  if (lane_n) {
+    if (c->bdhi) return fail(c, TIS_E_UNSUPPORTED, "per-replica step counts on the Brownian-HI path");
+    CK(cudaMemcpyAsync(c->lane_n.p, lane_n->data(), c->nlane * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    a.lane_nsteps = c->lane_n.p;
+  }
   CK(cudaEventRecord(c->ev0, c->stream));
   if (c->pair) {
     a.smem_total = (int)c->smem2;
@@ -1397,9 +1473,13 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
     // x update -> reciprocal forces -> forces, v / a update
     for (int64_t k = 0; k < nsteps; ++k) {
       KArgs x = make_args(c, KM_XSTEP, 1, -1);
+      x.lane_nsteps = a.lane_nsteps;
+      x.step_k = (int)k;
       int rc = launch_lane(c, x);
       if (rc < 0) return rc;
       KArgs v = make_args(c, KM_VSTEP, 1, -1);
+      v.lane_nsteps = a.lane_nsteps;
+      v.step_k = (int)k;
       v.noise_base = c->noise_base + (int)k;
       rc = ewald_recip(c, v, true);
       if (rc < 0) return rc;
@@ -1416,6 +1496,70 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
   c->hb_energy_valid = true;
   return check_lanes(c);
 }
+}  // namespace
+
+extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
+  if (!c || nsteps < 0 || nsteps > 0x7fffffff) return TIS_E_ARG;
+  if (nsteps == 0) return TIS_OK;
+  return run_steps(c, (int)nsteps, nullptr);
+}
+
+extern "C" int tis_time_integral(tis_ctx *c, int64_t nsteps, int32_t *flg, const int64_t *exchange_step) {
+  if (!c || !flg || nsteps < 0 || nsteps > 0x7fffffff) return TIS_E_ARG;
+  if (nsteps == 0) return TIS_OK;
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int> n(c->nlane);
+  for (int l = 0; l < c->nlane; ++l) {
+    long long k = flg[l] ? 0 : nsteps;
+    if (!flg[l] && exchange_step) {
+      const long long left = exchange_step[l] - ls[l].istep;
+      k = std::max(0LL, std::min(k, left));
+    }
+    n[l] = (int)k;
+  }
+  const int rc = run_steps(c, (int)nsteps, &n);
+  if (rc < 0) return rc;
+  // time_integral.F90:460-465: a replica at its exchange step waits
+  if (exchange_step)
+    for (int l = 0; l < c->nlane; ++l)
+      if (!flg[l] && ls[l].istep + n[l] == exchange_step[l]) flg[l] = 1;
+  return rc;
+}
+
+extern "C" int tis_get_steps(tis_ctx *c, int64_t *istep) {
+  if (!c || !istep) return TIS_E_ARG;
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int l = 0; l < c->nlane; ++l) istep[l] = ls[l].istep;
+  return TIS_OK;
+}
+
+extern "C" int tis_get_random_number(tis_ctx *c, int64_t istep, int32_t nstep, double *r_boxmuller) {
+  if (!c || !r_boxmuller || nstep <= 0 || nstep > 65535) return TIS_E_ARG;
+  const size_t n = 3 * (size_t)c->nbead_total * nstep;
+  DBuf<double> out;
+  CK(out.alloc(n));
+  KArgs a = make_args(c, 0, 0, -1);
+  ++c->launches;
+  CK(noise_launch(c->stream, a, istep, nstep, out.p));
+  CK(cudaMemcpyAsync(r_boxmuller, out.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  out.free();
+  return TIS_OK;
+}
+
+extern "C" int tis_get_rebuild_info(tis_ctx *c, int32_t irep, int64_t *n_rebuild, int64_t *last_step) {
+  if (!c || irep < 1 || irep > c->nlane) return TIS_E_ARG;
+  LaneState l{};
+  CK(cudaMemcpyAsync(&l, c->d_lstate.p + (irep - 1), sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (n_rebuild) *n_rebuild = l.nrebuild;
+  if (last_step) *last_step = l.last_rebuild;
+  return TIS_OK;
+}
 
 // energy_allrep.F90:123-260 + simu_replica_exchange.F90:87-300 +
 // time_integral_post.F90:293-349 (labels refresh rlan_const(1) and the
@@ -1423,6 +1567,8 @@ extern "C" int tis_step(tis_ctx *c, int64_t nsteps) {
 extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_accept) {
   if (!c) return TIS_E_ARG;
   if (c->ntop != 1) return fail(c, TIS_E_UNSUPPORTED, "replica exchange needs one topology");
+  if (c->nlabel != c->nlane)
+    return fail(c, TIS_E_UNSUPPORTED, "a ladder context exchanges through tis_rex_energies and tis_rex_exchange_all");
   const int n = c->nlane;
   // own energies (hbond energies of the last force call reused when valid),
   // then the energies at the partner labels with the partner's beta for the
@@ -1481,10 +1627,132 @@ extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_acce
 
 extern "C" int tis_get_labels(tis_ctx *c, int32_t *rep2lab) {
   if (!c || !rep2lab) return TIS_E_ARG;
-  std::vector<int> r(c->nlane);
-  CK(cudaMemcpyAsync(r.data(), c->d_rep2lab.p, r.size() * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < c->nlane; ++k) rep2lab[k] = r[k] + 1;
+  for (int k = 0; k < c->nlane; ++k) rep2lab[k] = ls[k].label + 1;
+  return TIS_OK;
+}
+
+// ------------------------------------------------ ladder split over ranks
+// simu_replica_exchange.F90:121-267 for one exchange of a whole ladder on
+// the host, after every rank's replica_energy has been gathered
+// (time_integral_post.F90:279): the pairs of this exchange's odd/even
+// alternation in label order, the k-th taking uniform u[k]; an accepted
+// pair swaps the labels of its two replicas and rescales their velocities.
+extern "C" int tis_rex_decide(int32_t nrep_all, const double *tempk_all, int32_t idx_pair,
+                              const double *replica_energy, const double *u, int32_t *rep2lab, double *vscale,
+                              int32_t *n_accept) {
+  if (nrep_all <= 0 || !tempk_all || !replica_energy || !u || !rep2lab || (idx_pair != 1 && idx_pair != 2))
+    return TIS_E_ARG;
+  const int n = nrep_all;
+  std::vector<int> lab2rep(n, -1);
+  for (int r = 0; r < n; ++r) {
+    const int l = rep2lab[r];
+    if (l < 1 || l > n || lab2rep[l - 1] >= 0) return TIS_E_ARG;
+    lab2rep[l - 1] = r;
+  }
+  if (vscale) for (int r = 0; r < n; ++r) vscale[r] = 0.0;
+  int k = 0, nacc = 0;
+  for (int li = 1; li <= n; ++li) {
+    const int lj = rex_pair(li, n, idx_pair);
+    if (lj < li) continue;
+    const int ri = lab2rep[li - 1], rj = lab2rep[lj - 1];
+    const double tm = tempk_all[li - 1], tn = tempk_all[lj - 1];
+    const double pim = replica_energy[2 * ri], pin = replica_energy[2 * ri + 1];
+    const double pjn = replica_energy[2 * rj], pjm = replica_energy[2 * rj + 1];
+    const double delta = ((pjm - pim) / tm - (pjn - pin) / tn) / BOLTZ_KCAL_MOL;
+    const double uu = u[k++];
+    if (delta < 0.0e0 || uu <= std::exp(-delta)) {
+      rep2lab[ri] = lj; rep2lab[rj] = li;
+      lab2rep[li - 1] = rj; lab2rep[lj - 1] = ri;
+      const double sf = std::sqrt(tn / tm);
+      if (vscale) { vscale[ri] = sf; vscale[rj] = -sf; }
+      ++nacc;
+    }
+  }
+  if (n_accept) *n_accept = nacc;
+  return TIS_OK;
+}
+
+extern "C" int tis_rex_energies(tis_ctx *c, double *replica_energy) {
+  if (!c || !replica_energy) return TIS_E_ARG;
+  if (c->g_rep2lab.empty()) return fail(c, TIS_E_UNSUPPORTED, "tis_rex_energies: not a ladder context");
+  // energy_allrep.F90:123-217: the own label's energy (hbond energies of the
+  // last force call reused), then the partner label's with its beta
+  std::vector<double> E, E2;
+  int rc = run_energy(c, -1, nullptr, c->hb_energy_valid, c->beta_global, E);
+  if (rc < 0) return rc;
+  std::vector<int> elab(c->nlane);
+  std::vector<double> beta(c->nlane);
+  for (int l = 0; l < c->nlane; ++l) {
+    const int lo = rex_pair(c->g_rep2lab[c->rep_first + l] + 1, c->nlabel, c->idx_pair);
+    elab[l] = lo ? lo - 1 : -1;
+    beta[l] = lo ? 1.0e0 / (c->lab_T[lo - 1] * BOLTZ_KCAL_MOL) : c->beta_global;
+  }
+  rc = run_energy(c, -1, elab.data(), false, c->beta_global, E2, beta.data());
+  if (rc < 0) return rc;
+  c->hb_energy_valid = false;
+  for (int l = 0; l < c->nlane; ++l) {
+    replica_energy[2 * l] = E[(size_t)l * N_ETYPE + TIS_E_TOTAL - 1];
+    replica_energy[2 * l + 1] = elab[l] >= 0 ? E2[(size_t)l * N_ETYPE + TIS_E_TOTAL - 1] : 0.0;
+  }
+  return check_lanes(c);
+}
+
+extern "C" int tis_rex_exchange_all(tis_ctx *c, const double *replica_energy_all, const double *u,
+                                    int32_t *n_accept) {
+  if (!c || !replica_energy_all) return TIS_E_ARG;
+  if (c->g_rep2lab.empty()) return fail(c, TIS_E_UNSUPPORTED, "tis_rex_exchange_all: not a ladder context");
+  const int n = c->nlabel;
+  int npair = 0;
+  for (int li = 1; li <= n; ++li) npair += rex_pair(li, n, c->idx_pair) > li;
+  std::vector<double> uu(std::max(npair, 1));
+  if (u) {
+    for (int k = 0; k < npair; ++k) uu[k] = u[k];
+  } else {   // the device exchange's counter-based uniforms (same seed on every rank)
+    for (int k = 0; k < npair; ++k) {
+      const unsigned long long ctr = c->g_counter + (unsigned long long)k;
+      const U4 o = philox4x32(U4{(uint32_t)ctr, (uint32_t)(ctr >> 32), 0x52454D44u, 0u}, (uint32_t)c->par.seed,
+                              (uint32_t)(c->par.seed >> 32));
+      uu[k] = u01_open0(o.x) - 2.3283064365386963e-10;
+    }
+    c->g_counter += (unsigned long long)npair;
+  }
+  std::vector<int> r2l(n);
+  for (int g = 0; g < n; ++g) r2l[g] = c->g_rep2lab[g] + 1;
+  std::vector<double> vs(n);
+  int nacc = 0;
+  int rc = tis_rex_decide(n, c->lab_T.data(), c->idx_pair, replica_energy_all, uu.data(), r2l.data(), vs.data(),
+                          &nacc);
+  if (rc < 0) return fail(c, rc, "tis_rex_exchange_all: inconsistent label maps");
+  for (int g = 0; g < n; ++g) { c->g_rep2lab[g] = r2l[g] - 1; c->g_lab2rep[r2l[g] - 1] = g; }
+  c->idx_pair = (c->idx_pair == 2) ? 1 : c->idx_pair + 1;
+  // beta_hbond15 of the last replica's label (simu_set_dtrna.F90:58)
+  c->beta_global = 1.0e0 / (c->lab_T[c->g_rep2lab[n - 1]] * BOLTZ_KCAL_MOL);
+  // the local replicas' labels and velocities
+  std::vector<LaneState> ls(c->nlane);
+  CK(cudaMemcpyAsync(ls.data(), c->d_lstate.p, ls.size() * sizeof(LaneState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> sc(c->nlane);
+  for (int l = 0; l < c->nlane; ++l) {
+    ls[l].label = c->g_rep2lab[c->rep_first + l];
+    c->rep2lab[l] = ls[l].label;
+    sc[l] = vs[c->rep_first + l];
+  }
+  CK(cudaMemcpyAsync(c->d_lstate.p, ls.data(), ls.size() * sizeof(LaneState), cudaMemcpyHostToDevice, c->stream));
+  RexState r{};
+  r.beta_global = c->beta_global;
+  r.counter = c->g_counter;
+  r.idx_pair = c->idx_pair;
+  r.nacc = nacc;
+  CK(cudaMemcpyAsync(c->rex.p, &r, sizeof(RexState), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->scale.p, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  KArgs a = make_args(c, 0, 0, -1);
+  ++c->launches;
+  CK(vscale_launch(c->stream, a, c->scale.p, c->velo.p));
+  CK(cudaStreamSynchronize(c->stream));
+  if (n_accept) *n_accept = nacc;
   return TIS_OK;
 }
 
@@ -1578,6 +1846,9 @@ unsigned char *g_static_ptr[STATIC_MAX_DEVICES] = {};
 
 // Set-up, once per device with that device current: the address of the
 // array on the current device.  Runs inside the first call on each device.
+// The cached address belongs to the device's primary context, which the
+// CUDA runtime keeps for the whole process; a process that resets a device
+// (cudaDeviceReset) must not call tis_force_sumup_static on it afterwards.
 int static_scratch_ptr(tis_ctx *c, unsigned char **out) {
   int dev = 0;
   CK(cudaGetDevice(&dev));
@@ -1630,6 +1901,10 @@ StaticLayout static_layout(const tis_ctx *c, int lane) {
 
 extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xyz_dev, double *force_dev) {
   if (!c || irep < 1 || irep > c->nlane || !xyz_dev || !force_dev) return TIS_E_ARG;
+  // Brownian-HI contexts never size the lane kernel's shared memory and
+  // evaluate FENE / WCA records, not the DT15 terms this call computes
+  if (c->bdhi)
+    return fail(c, TIS_E_UNSUPPORTED, "tis_force_sumup_static: not available on a Brownian-HI context");
   if (c->par.i_ele == TIS_ELE_EWALD)
     return fail(c, TIS_E_UNSUPPORTED, "tis_force_sumup_static: Ewald needs the context's reciprocal-space buffers");
   const int lane = irep - 1;
@@ -1652,6 +1927,10 @@ extern "C" int tis_force_sumup_static(tis_ctx *c, int32_t irep, const double *xy
                      c->stream));
   CK(cudaMemcpyAsync(base + lay.lstate + lane * sizeof(LaneState), c->d_lstate.p + lane, sizeof(LaneState),
                      cudaMemcpyDeviceToDevice, c->stream));
+  // the context's sticky flags (an earlier NAN, overflow or exhausted noise)
+  // do not belong to this call
+  CK(cudaMemsetAsync(base + lay.lstate + lane * sizeof(LaneState) + offsetof(LaneState, flags), 0, sizeof(int),
+                     c->stream));
   CK(cudaMemcpyAsync(base + lay.xyz, xyz_dev, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(base + lay.pxyz, xyz_dev, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   LaneState before{};

@@ -33,38 +33,92 @@ constexpr int CT = 64;          // Cholesky tile
 constexpr int CTP = CT + 1;     // padded shared-memory row
 
 // ------------------------------------------------------------ RPY tensor
+// The 3x3 block pre1 I + pre2 r r^T of the bead pair (i < j, r = x_j - x_i)
+// in simu_hydro_tensors.F90:50-300, each variant's expressions in the
+// reference's evaluation order with explicitly rounded operations (the FP64
+// D is bit-identical to the reference's arithmetic).  diag_only: the block
+// is val I (Zuk-RPY, one bead inside the other).
+struct HiBlock { double pre1, pre2; bool diag_only; };
+
+__device__ __forceinline__ HiBlock hi_pair(int type, double rad, double rad_i, double rad_j, double r_sq, double c6,
+                                           double c8) {
+  const double r_abs = sqrt(r_sq);
+  HiBlock b{0.0, 0.0, false};
+  auto rpy = [&](double rs) {   // rad_sq-sum form shared by RPY and Zuk-RPY apart
+    b.pre1 = __dmul_rn(__ddiv_rn(c8, r_abs), __dadd_rn(1.0, __ddiv_rn(rs, __dmul_rn(3.0, r_sq))));
+    b.pre2 = __ddiv_rn(__dmul_rn(__ddiv_rn(c8, r_abs), __dsub_rn(1.0, __ddiv_rn(rs, r_sq))), r_sq);
+  };
+  if (type == TIS_HI_ZUK_RPY_DEV) {
+    if (__dadd_rn(rad_i, rad_j) < r_abs) {
+      rpy(__dadd_rn(__dmul_rn(rad_i, rad_i), __dmul_rn(rad_j, rad_j)));
+    } else {
+      const double rad_s = rad_i < rad_j ? rad_i : rad_j, rad_l = rad_i < rad_j ? rad_j : rad_i;
+      if (__dsub_rn(rad_l, rad_s) < r_abs) {
+        const double r_cb = __dmul_rn(r_sq, r_abs);
+        const double dr = __dsub_rn(rad_i, rad_j), dr2 = __dmul_rn(dr, dr);
+        const double y1 = __dadd_rn(dr2, __dmul_rn(3.0, r_sq));
+        const double x1 = __dsub_rn(__dmul_rn(__dmul_rn(16.0, r_cb), __dadd_rn(rad_i, rad_j)), __dmul_rn(y1, y1));
+        const double cij = __ddiv_rn(__ddiv_rn(c6, rad_i), rad_j);
+        b.pre1 = __ddiv_rn(__ddiv_rn(__dmul_rn(cij, x1), 32.0), r_cb);
+        const double y2 = __dsub_rn(dr2, r_sq);
+        b.pre2 = __ddiv_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(cij, 3.0), __dmul_rn(y2, y2)), 32.0), r_cb), r_sq);
+      } else {
+        b.pre1 = __ddiv_rn(c6, rad_l);
+        b.diag_only = true;
+      }
+    }
+    return b;
+  }
+  const double rad_sq = __dmul_rn(rad, rad);
+  if (type == TIS_HI_RPY_DEV || __dmul_rn(2.0, rad) < r_abs) {
+    rpy(__dmul_rn(2.0, rad_sq));
+  } else if (type == TIS_HI_RPY_OVER_DEV) {
+    b.pre1 = __dmul_rn(__ddiv_rn(c6, rad), __dsub_rn(1.0, __ddiv_rn(__dmul_rn(0.28125, r_abs), rad)));
+    b.pre2 = __ddiv_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(__ddiv_rn(c6, rad), 3.0), 32.0), rad), r_abs);
+  } else {   // ERMAK_OVER
+    b.pre1 = __ddiv_rn(__dmul_rn(__ddiv_rn(__ddiv_rn(c8, 2.0), rad), 7.0), 6.0);
+    b.pre2 = __ddiv_rn(__ddiv_rn(__ddiv_rn(c8, 2.0), 2.0), r_sq);
+  }
+  return b;
+}
+
 // grid (ceil(N*N / 256), nlane): thread per ordered bead pair (i, j); writes
 // the 3x3 block of D and the lower part of L (L = tril(D) before factoring)
 __global__ void __launch_bounds__(256) rpy_kernel(KArgs a) {
   const int lane = blockIdx.y;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
-  const int N = a.tops[L.top].nmp, n = 3 * N;
+  const TopDesc Tp = a.tops[L.top];
+  const int N = Tp.nmp, n = 3 * N;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (long long)N * N) return;
   const int i = (int)(e / N), j = (int)(e - (long long)i * N);
   const double T = a.lab_T[a.lstate[lane].label];
   const double c6 = a.boltz * T / (6.0 * a.pi * a.viscosity);
   const double c8 = a.boltz * T / (8.0 * a.pi * a.viscosity);
-  const double rad = a.hi_radius;
+  const double *hr = a.b_hrad + Tp.bead0;
+  const double rad = hr[0];   // radius(1) of RPY, RPY_OVER and ERMAK_OVER
+  const int type = a.i_hydro_tensor;
   double blk[3][3];
   if (i == j) {
+    const double dv = c6 / (type == TIS_HI_ZUK_RPY_DEV ? hr[i] : rad);
     for (int p = 0; p < 3; ++p)
-      for (int q = 0; q < 3; ++q) blk[p][q] = (p == q) ? c6 / rad : 0.0;
+      for (int q = 0; q < 3; ++q) blk[p][q] = (p == q) ? dv : 0.0;
   } else {
     // the reference fills i < j with r = x_j - x_i and mirrors the block;
     // the block is even in r, so both orders give the same numbers
     const int lo = i < j ? i : j, hi = i < j ? j : i;
     const double *x = a.xyz + 3 * (size_t)L.state0;
     double r[3];
-    for (int d = 0; d < 3; ++d) r[d] = x[3 * hi + d] - x[3 * lo + d];
-    const double r_sq = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    const double r_abs = sqrt(r_sq);
-    const double rad_sq = rad * rad;
-    const double pre1 = c8 / r_abs * (1.0 + 2.0 * rad_sq / (3.0 * r_sq));
-    const double pre2 = c8 / r_abs * (1.0 - 2.0 * rad_sq / r_sq) / r_sq;
+    for (int d = 0; d < 3; ++d) r[d] = __dsub_rn(x[3 * hi + d], x[3 * lo + d]);
+    const double r_sq = __dadd_rn(__dadd_rn(__dmul_rn(r[0], r[0]), __dmul_rn(r[1], r[1])), __dmul_rn(r[2], r[2]));
+    const HiBlock hb = hi_pair(type, rad, hr[lo], hr[hi], r_sq, c6, c8);
     for (int p = 0; p < 3; ++p)
-      for (int q = 0; q < 3; ++q) blk[p][q] = (p == q ? pre1 : 0.0) + pre2 * r[p] * r[q];
+      for (int q = 0; q < 3; ++q) {
+        if (hb.diag_only) blk[p][q] = (p == q) ? hb.pre1 : 0.0;
+        else if (p == q) blk[p][q] = __dadd_rn(hb.pre1, __dmul_rn(__dmul_rn(hb.pre2, r[p]), r[q]));
+        else blk[p][q] = __dmul_rn(__dmul_rn(hb.pre2, r[p]), r[q]);
+      }
   }
   // D in FP64 (or FP32, rows padded to 4, for the mixed-precision step),
   // the lower part of L (its upper part is never read)
@@ -688,7 +742,7 @@ __global__ void __launch_bounds__(128) bd_noise_kernel(KArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   double n0, n1, n2;
-  noise3(a, lane, L.state0 + i, a.bd_istep, a.noise_base, n0, n1, n2);
+  noise3(a, lane, L, i, a.bd_istep, a.noise_base, n0, n1, n2);
   double *xi = a.bd_xi + 3 * (size_t)(L.state0 + i);
   xi[0] = n0; xi[1] = n1; xi[2] = n2;
 }
@@ -809,7 +863,7 @@ __global__ void __launch_bounds__(256) bd_force_kernel(KArgs a) {
       const double ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro8 * ro4 * ro2;
       const double coef = (ro2 > 1.0) ? pc[1] : pc[2];
       f = 12.0 * coef / nat2 * (ro14 - ro8);
-      if (f > 50.0) { f = 50.0; ++nclamp; }   // DE_MAX
+      if (f > 50.0) { f = 50.0; nclamp += j > i; }   // DE_MAX; the record is counted once, from its lower bead
     }
     fx += f * v0; fy += f * v1; fz += f * v2;
   }

@@ -19,6 +19,8 @@ namespace tis {
 constexpr int MAX_THREADS = 1024;
 constexpr int N_ETYPE = 25;   // E_TYPE%MAX
 constexpr int CHMAX = 1024;   // electrostatic row chunks per lane (at least one per charged bead)
+// HI_TENSOR (const_index.F90:39-45)
+constexpr int TIS_HI_RPY_DEV = 1, TIS_HI_RPY_OVER_DEV = 2, TIS_HI_ERMAK_OVER_DEV = 3, TIS_HI_ZUK_RPY_DEV = 4;
 
 // per-topology descriptor (offsets into the concatenated topology arrays)
 struct TopDesc {
@@ -59,6 +61,8 @@ struct LaneDesc {
   long long bd0;    // Brownian-HI: first element of this lane's (3N)^2 diffusion / Cholesky matrices
   long long bdp0;   // Brownian-HI, tensor cores: first float of this lane's TF32 panel planes
   long long bd32;   // Brownian-HI, mixed precision: first float of this lane's FP32 D and L (rows padded to 4)
+  int key_lane;     // counter-based noise and uniforms: the replica's key (its global replica number - 1)
+  int key_bead0;    // and the counter of its first bead (so a replica draws the same numbers in any context)
 };
 
 // Mutable per-lane scalar state, kept in global memory between launches.
@@ -66,6 +70,7 @@ struct LaneState {
   long long istep;
   long long nrebuild;
   long long nclamp;
+  long long last_rebuild;   // istep of the last neighbour rebuild (-1: none)
   int label;          // global label index
   int unif_pos;
   int flags;          // bit 0 list overflow, 1 nan, 2 uniforms exhausted, 3 noise exhausted
@@ -127,6 +132,8 @@ struct KArgs {
   double *bd_W;                    // per lane: 64 x 64 transposed inverse of the current diagonal tile
   int *not_spd;                    // per lane: a Cholesky pivot was <= 0
   double hi_radius, viscosity;
+  int i_hydro_tensor;              // HI_TENSOR: 1 RPY, 2 RPY_OVER, 3 ERMAK_OVER, 4 ZUK_RPY
+  const double *b_hrad;            // per bead: hydrodynamic radius (ZUK_RPY; the others take bead 1's)
   double boltz, pi;                // BOLTZ_KCAL_MOL and F_PI of const_physical.F90
   long long bd_istep;              // step being taken (1-based)
   int bd_kpanel;                   // Cholesky panel of this launch
@@ -200,6 +207,9 @@ struct KArgs {
   int n_unif;
   int nbead_total;
   int noise_in_sweep;      // 1: the sink's noise is drawn in the bonded sweep (kept in shared memory)
+  const int *lane_nsteps;  // per lane: steps of this launch (KM_STEP) or 1 + the last step index that
+                           // moves the lane (KM_XSTEP / KM_VSTEP); null: every lane takes nsteps
+  int step_k;              // KM_XSTEP / KM_VSTEP: index of this step within the call
 };
 
 #ifdef __CUDACC__
@@ -235,6 +245,15 @@ struct RexState {
   int idx_pair;                // odd/even pair alternation (var_replica.F90:134,165-183)
   int nacc;                    // swaps accepted by the last exchange
 };
+
+// exchange_pair_tb of one temperature dimension (var_replica.F90:165-183):
+// the partner of label l (1-based) among n under the odd/even alternation
+// idx_pair, 0 = no partner
+__host__ __device__ inline int rex_pair(int l, int n, int idx_pair) {
+  if (idx_pair == 1) return (l % 2 == 1) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
+  if (l == 1) return 0;
+  return (l % 2 == 0) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
+}
 
 struct U4 { uint32_t x, y, z, w; };
 

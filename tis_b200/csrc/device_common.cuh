@@ -240,13 +240,15 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
 }
 
 // --------------------------------------------------------------- noise
-// Gaussian triple for (lane, step, bead): counter-based Philox + Box-Muller,
-// or the injected r_boxmuller array when one is set.
-__device__ __forceinline__ void noise3(const KArgs &a, int lane, int gbead, long long istep, int noise_step,
-                                       double &n0, double &n1, double &n2) {
+// Gaussian triple for (replica, step, bead i): counter-based Philox +
+// Box-Muller keyed by the replica's key_lane / key_bead0, or the injected
+// r_boxmuller array (indexed by the bead's place in this context) when one
+// is set.
+__device__ __forceinline__ void noise3(const KArgs &a, int lane, const LaneDesc &L, int i, long long istep,
+                                       int noise_step, double &n0, double &n1, double &n2) {
   if (a.noise) {
     if (noise_step < a.noise_nsteps) {
-      const double *r = a.noise + ((size_t)noise_step * a.nbead_total + gbead) * 3;
+      const double *r = a.noise + ((size_t)noise_step * a.nbead_total + L.state0 + i) * 3;
       n0 = r[0]; n1 = r[1]; n2 = r[2];
     } else {
       n0 = n1 = n2 = 0.0;
@@ -254,8 +256,8 @@ __device__ __forceinline__ void noise3(const KArgs &a, int lane, int gbead, long
     }
     return;
   }
-  U4 c = {(uint32_t)istep, (uint32_t)((unsigned long long)istep >> 32), (uint32_t)gbead, 0x4E4F4953u};
-  U4 o = philox4x32(c, (uint32_t)a.seed ^ (0x9E3779B9u * (uint32_t)(lane + 1)), (uint32_t)(a.seed >> 32));
+  U4 c = {(uint32_t)istep, (uint32_t)((unsigned long long)istep >> 32), (uint32_t)(L.key_bead0 + i), 0x4E4F4953u};
+  U4 o = philox4x32(c, (uint32_t)a.seed ^ (0x9E3779B9u * (uint32_t)(L.key_lane + 1)), (uint32_t)(a.seed >> 32));
   float u1 = u01f_open0(o.x), u2 = u01f_open0(o.y), u3 = u01f_open0(o.z), u4 = u01f_open0(o.w);
   float r1 = sqrtf(-2.0f * logf(u1)), r2 = sqrtf(-2.0f * logf(u3));
   float s1, c1, s2, c2;
@@ -273,7 +275,8 @@ __device__ __forceinline__ double lane_uniform(const KArgs &a, int lane, const L
     return 0.5;
   }
   U4 c = {(uint32_t)istep, (uint32_t)((unsigned long long)istep >> 32), (uint32_t)draw++, 0x50524E45u};
-  U4 o = philox4x32(c, (uint32_t)a.seed ^ (0x85EBCA6Bu * (uint32_t)(lane + 1)), (uint32_t)(a.seed >> 32) ^ 0x5bd1e995u);
+  U4 o = philox4x32(c, (uint32_t)a.seed ^ (0x85EBCA6Bu * (uint32_t)(L.key_lane + 1)),
+                    (uint32_t)(a.seed >> 32) ^ 0x5bd1e995u);
   return u01_open0(o.x);
 }
 

@@ -363,11 +363,6 @@ cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst,
 // label maps, the pair alternation and beta_hbond15; then the CTA writes the
 // lanes' labels and rescales the velocities of the swapped lanes.
 
-__device__ __forceinline__ int rex_pair(int l, int n, int idx_pair) {   // 1-based, 0 = no partner
-  if (idx_pair == 1) return (l % 2 == 1) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
-  if (l == 1) return 0;
-  return (l % 2 == 0) ? ((l + 1 <= n) ? l + 1 : 0) : l - 1;
-}
 
 __global__ void rex_prep_kernel(KArgs a, const int *rep2lab, int *elabel, double *ebeta) {
   const int lane = blockIdx.x * blockDim.x + threadIdx.x;
@@ -438,6 +433,25 @@ __global__ void __launch_bounds__(256) rex_exchange_kernel(KArgs a, RexState *re
     if (f > 0.0) for (int k = lid; k < 3 * N; k += 32) v[k] = f * v[k];
     else for (int k = lid; k < 3 * N; k += 32) v[k] = v[k] / (-f);
   }
+}
+
+// velocity rescale of the lanes a ladder exchange swapped: lane l's
+// velocities times scale[l] (> 0) or divided by -scale[l] (< 0), as the
+// device exchange does; one block per lane
+__global__ void vscale_kernel(KArgs a, const double *scale, double *velo) {
+  const int lane = blockIdx.x;
+  const double f = scale[lane];
+  if (f == 0.0) return;
+  const LaneDesc L = a.lanes[lane];
+  const int N = a.tops[L.top].nmp;
+  double *v = velo + 3 * (size_t)L.state0;
+  if (f > 0.0) for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = f * v[k];
+  else for (int k = threadIdx.x; k < 3 * N; k += blockDim.x) v[k] = v[k] / (-f);
+}
+
+cudaError_t vscale_launch(cudaStream_t st, const KArgs &a, const double *scale, double *velo) {
+  vscale_kernel<<<a.nlane, 128, 0, st>>>(a, scale, velo);
+  return cudaGetLastError();
 }
 
 cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,

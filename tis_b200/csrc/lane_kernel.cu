@@ -44,6 +44,47 @@ __device__ __forceinline__ T *peer_ptr(T *p, const Clu &cu) {
   return cg::this_cluster().map_shared_rank(p, cu.rank ^ 1);
 }
 
+// ------------------------------------------------------------ skin rule
+// time_integral.F90:57-93: rebuild when sqrt(d2max) + sqrt(d2max_2nd) >
+// neigh_margin, d2 = dot_product(dxyz_mp, dxyz_mp) of each bead.  The pair
+// (d2max, d2max_2nd) is the top two of the multiset of d2 values, so partial
+// results merge exactly in any order: each warp folds its beads, every warp
+// then folds the per-warp pairs (of both CTAs of a cluster) and reaches the
+// same decision without another barrier.
+__device__ __forceinline__ void top2_add(double &m1, double &m2, double d2) {
+  if (d2 > m1) { m2 = m1; m1 = d2; } else if (d2 > m2) m2 = d2;
+}
+__device__ __forceinline__ void top2_merge(double &m1, double &m2, double o1, double o2) {
+  const double n1 = fmax(m1, o1), n2 = fmax(fmin(m1, o1), fmax(m2, o2));
+  m1 = n1; m2 = n2;
+}
+__device__ __forceinline__ void top2_warp(double &m1, double &m2) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double o1 = __shfl_xor_sync(0xffffffffu, m1, o), o2 = __shfl_xor_sync(0xffffffffu, m2, o);
+    top2_merge(m1, m2, o1, o2);
+  }
+}
+// dot_product(dxyz, dxyz) in the Fortran operation order, no contraction
+__device__ __forceinline__ double disp2(double x, double y, double z) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+// per-warp pair of this thread's (m1, m2) into red[2 w], red[2 w + 1]; every
+// thread of the CTA calls it
+__device__ __forceinline__ void top2_store(double m1, double m2, double *red) {
+  top2_warp(m1, m2);
+  if ((threadIdx.x & 31) == 0) { red[2 * (threadIdx.x >> 5)] = m1; red[2 * (threadIdx.x >> 5) + 1] = m2; }
+}
+// the trigger from the per-warp pairs of this CTA (lanes 0 .. nwarp - 1) and,
+// with two CTAs, of the other one (lanes 16 .. 16 + nwarp - 1, nwarp <= 16)
+__device__ __forceinline__ bool skin_fires(const double *red, const double *peer_red, int nwarp, double margin) {
+  const int lid = threadIdx.x & 31;
+  double m1 = 0.0, m2 = 0.0;
+  if (lid < nwarp) { m1 = red[2 * lid]; m2 = red[2 * lid + 1]; }
+  else if (peer_red && lid >= 16 && lid - 16 < nwarp) { m1 = peer_red[2 * (lid - 16)]; m2 = peer_red[2 * (lid - 16) + 1]; }
+  top2_warp(m1, m2);
+  return __dadd_rn(sqrt(m1), sqrt(m2)) > margin;
+}
+
 // ------------------------------------------------------------ list build
 // neighbor_list.F90:49-90 + neighbor_assign.F90:481-559 (the EXV_DT15 type
 // sort keeps the generation order) and neighbor_list_ele.F90:123-210: every
@@ -52,7 +93,7 @@ __device__ __forceinline__ T *peer_ptr(T *p, const Clu &cu) {
 // canonical (min, max) orientation (neighbor_assign.F90:742-770).
 template <typename Real, int CL>
 __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
-                            const Clu &cu) {
+                            const Clu &cu, long long istep) {
   const int N = T.nmp, W = s.W;
   const int tid = threadIdx.x, nth = blockDim.x;
   const int warp = tid >> 5, lid = tid & 31, nwarp = nth >> 5;
@@ -216,6 +257,7 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
     int ne = s.misc[MISC_NEXV], nl = s.misc[MISC_NELE];
     if (CL == 2) { ne += peer_ptr(s.misc, cu)[MISC_NEXV]; nl += peer_ptr(s.misc, cu)[MISC_NELE]; }
     st.nrebuild++;
+    st.last_rebuild = istep;
     st.nexv = ne;
     st.nele = nl;
   }
@@ -428,9 +470,17 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             const int j1 = two ? (w << 5) + __ffs(m) - 1 : j0;
             if (two) m &= m - 1;
             const V p0 = s.A4[j0], p1 = s.A4[j1];
-            Real ax = p0.x - pi.x, ay = p0.y - pi.y, az = p0.z - pi.z;
-            Real bx = p1.x - pi.x, by = p1.y - pi.y, bz = p1.z - pi.z;
-            if (mir) { mirror_shift<Real>(a, s, i, j0, ax, ay, az); mirror_shift<Real>(a, s, i, j1, bx, by, bz); }
+            Real ax, ay, az, bx, by, bz;
+            if (mir) {   // FP64 difference and image shift (see the exv gather)
+              double ex = (double)p0.x - (double)pi.x, ey = (double)p0.y - (double)pi.y, ez = (double)p0.z - (double)pi.z;
+              double fx_ = (double)p1.x - (double)pi.x, fy_ = (double)p1.y - (double)pi.y, fz_ = (double)p1.z - (double)pi.z;
+              mirror_shift<double>(a, s, i, j0, ex, ey, ez);
+              mirror_shift<double>(a, s, i, j1, fx_, fy_, fz_);
+              ax = (Real)ex; ay = (Real)ey; az = (Real)ez; bx = (Real)fx_; by = (Real)fy_; bz = (Real)fz_;
+            } else {
+              ax = p0.x - pi.x; ay = p0.y - pi.y; az = p0.z - pi.z;
+              bx = p1.x - pi.x; by = p1.y - pi.y; bz = p1.z - pi.z;
+            }
             const Real ra2 = ax * ax + ay * ay + az * az, rb2 = bx * bx + by * by + bz * bz;
             const Real ria = rsq<Real>(ra2), rib = rsq<Real>(rb2);
             const Real da = ra2 * ria, db = rb2 * rib;
@@ -457,9 +507,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
             }
             if (!(ra2 <= cut2)) fa = 0;
             if (!(rb2 <= cut2) || !two) fb = 0;
-            if (!ewald && !coul) {
-              if (fa > (Real)50) { fa = 50; ++nclamp; }
-              if (fb > (Real)50) { fb = 50; ++nclamp; }
+            if (!ewald && !coul) {   // DE_MAX clamp, each pair counted once (from its lower bead)
+              if (fa > (Real)50) { fa = 50; nclamp += j0 > i; }
+              if (fb > (Real)50) { fb = 50; nclamp += j1 > i; }
             }
             axs -= fa * ax + fb * bx;
             ays -= fa * ay + fb * by;
@@ -481,7 +531,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       const int i = cu.lo + ((c - c_nz) << 5) + lid;
       if (i < cu.hi) {
         double n0, n1, n2;
-        noise3(a, lane, L.state0 + i, istep, noise_step, n0, n1, n2);
+        noise3(a, lane, L, i, istep, noise_step, n0, n1, n2);
         s.NX[i] = n0; s.NY[i] = n1; s.NZ[i] = n2;
       }
     }
@@ -527,8 +577,16 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       // it is within the near radius.
       auto visit = [&](int j, bool rec, int &cnt, uint16_t *lst, int ncap) {
         const V pj = s.A4[j];
-        Real sx = pj.x - pi.x, sy = pj.y - pi.y, sz = pj.z - pi.z;
-        if (mir) mirror_shift<Real>(a, s, i, j, sx, sy, sz);
+        Real sx, sy, sz;
+        if (mir) {
+          // across the box the two coordinates are ~L apart: difference and
+          // image shift in FP64, so only the short result is rounded
+          double ex = (double)pj.x - (double)pi.x, ey = (double)pj.y - (double)pi.y, ez = (double)pj.z - (double)pi.z;
+          mirror_shift<double>(a, s, i, j, ex, ey, ez);
+          sx = (Real)ex; sy = (Real)ey; sz = (Real)ez;
+        } else {
+          sx = pj.x - pi.x; sy = pj.y - pi.y; sz = pj.z - pi.z;
+        }
         const Real d2s = sx * sx + sy * sy + sz * sz;
         if (rec && d2s <= nscr2) {
           if (cnt < ncap) lst[cnt] = (uint16_t)j;
@@ -553,7 +611,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         const Real ro2 = fdiv(ra2, dr * dr);
         const Real ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro2 * ro4 * ro8;
         Real f = fabs((Real)12 * coef * (ro14 - ro8) * dr * inv_ra2 * rinv);
-        if (f > (Real)50) { f = 50; ++nclamp; }
+        // DE_MAX clamp; each pair is visited from both beads and counted once
+        if (f > (Real)50) { f = 50; nclamp += j > i; }
         fx -= (double)(f * wx); fy -= (double)(f * wy); fz -= (double)(f * wz);
       };
       const int ncap = NEAR_CAP / GA;
@@ -629,6 +688,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)(blockIdx.x / CL);
   if (lane >= a.nlane) return;
   if (CL == 2 && a.mode != KM_STEP) return;
+  // replicas that have reached their exchange step wait (time_integral.F90:134)
+  if (a.lane_nsteps && (a.mode == KM_XSTEP || a.mode == KM_VSTEP) && a.step_k >= a.lane_nsteps[lane]) return;
+  const int lane_steps = (a.lane_nsteps && a.mode == KM_STEP) ? min(a.nsteps, a.lane_nsteps[lane]) : a.nsteps;
   const LaneDesc L = a.lanes[lane];
   const TopDesc T = a.tops[L.top];
   const int N = T.nmp, NQ = T.nq;
@@ -690,7 +752,6 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
 
   const int label0 = st.label;
   const double *c1 = a.lab_c1 + a.lab_c1off[label0];
-  const int gb0 = L.state0;
   if (s.cst_on) {
     for (int i = tid; i < N; i += nth) {
       const int b = T.bead0 + i;
@@ -704,42 +765,71 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       double n0, n1, n2, rc, cc, c2, c3;
       if (s.cst_on) {
         if (a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }   // drawn in the bonded sweep
-        else noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
+        else noise3(a, lane, L, i, istep, nstep_noise, n0, n1, n2);
         rc = s.RC[i]; cc = s.C1[i]; c2 = s.C2[i]; c3 = s.C3[i];
       } else {
-        noise3(a, lane, gb0 + i, istep, nstep_noise, n0, n1, n2);
+        noise3(a, lane, L, i, istep, nstep_noise, n0, n1, n2);
         const int b = T.bead0 + i;
         rc = a.b_rcmass[b]; cc = c1[i]; c2 = a.b_c2[b]; c3 = a.b_c3[b];
       }
-      const double ax = fx * rc + cc * n0, ay = fy * rc + cc * n1, az = fz * rc + cc * n2;
-      s.VX[i] = c2 * s.VX[i] + c3 * (s.AX[i] + ax);
-      s.VY[i] = c2 * s.VY[i] + c3 * (s.AY[i] + ay);
-      s.VZ[i] = c2 * s.VZ[i] + c3 * (s.AZ[i] + az);
+      // each product rounded, as the reference evaluates it (no contraction)
+      const double ax = __dadd_rn(__dmul_rn(fx, rc), __dmul_rn(cc, n0));
+      const double ay = __dadd_rn(__dmul_rn(fy, rc), __dmul_rn(cc, n1));
+      const double az = __dadd_rn(__dmul_rn(fz, rc), __dmul_rn(cc, n2));
+      s.VX[i] = __dadd_rn(__dmul_rn(c2, s.VX[i]), __dmul_rn(c3, __dadd_rn(s.AX[i], ax)));
+      s.VY[i] = __dadd_rn(__dmul_rn(c2, s.VY[i]), __dmul_rn(c3, __dadd_rn(s.AY[i], ay)));
+      s.VZ[i] = __dadd_rn(__dmul_rn(c2, s.VZ[i]), __dmul_rn(c3, __dadd_rn(s.AZ[i], az)));
       s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
       if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
     };
   };
 
+  // skin rule: the trigger of the first step from the displacements loaded
+  // above (the other CTA's pairs are read after the cluster barrier below)
+  bool skin_fire = false;
+  if (skin && (a.mode == KM_STEP || a.mode == KM_XSTEP)) {
+    double m1 = 0.0, m2 = 0.0;
+    for (int i = cu.lo + tid; i < cu.hi; i += nth) top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+    top2_store(m1, m2, s.red);
+    if (CL == 1) {
+      __syncthreads();
+      skin_fire = skin_fires(s.red, nullptr, nth >> 5, a.neigh_margin);
+    }
+  }
+
   if constexpr (CL == 2) {
     typedef typename V4<Real>::T V;
     cg::this_cluster().sync();   // both CTAs are running before any distributed access
+    const double *peer_red = peer_ptr(s.red, cu);
+    if (skin) skin_fire = skin_fires(s.red, peer_red, nth >> 5, a.neigh_margin);
     double *pXN = peer_ptr(s.XN, cu), *pYN = peer_ptr(s.YN, cu), *pZN = peer_ptr(s.ZN, cu);
     V *pA4N = peer_ptr(s.A4N, cu), *pL4N = peer_ptr(s.L4N, cu);
-    for (int step = 0; step < a.nsteps; ++step) {
+    for (int step = 0; step < lane_steps; ++step) {
       const long long istep = istep0 + step + 1;
-      // time_integral.F90:94 fixed cadence (the two-CTA path has no skin rule)
+      // neighbour trigger: the skin rule (time_integral.F90:57-93) or the
+      // fixed cadence (:94); the decision is the same in both CTAs
       PHASE_T0(t_reb);
-      if ((istep % a.n_step_neighbor) == 1 || istep == 1) build_lists<Real, 2>(a, lane, L, T, s, cu);
+      const bool rebuild = skin ? skin_fire : ((istep % a.n_step_neighbor) == 1 || istep == 1);
+      if (rebuild) {
+        build_lists<Real, 2>(a, lane, L, T, s, cu, istep);
+        // dxyz_mp(:,:,irep) = 0 (time_integral.F90:89), own beads
+        if (skin) for (int i = cu.lo + tid; i < cu.hi; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
+      }
       PHASE_ADD(1, t_reb);
       PHASE_T0(t_xu);
       // swap in the double buffers after both CTAs wrote them; the other
       // CTA's copy of the own beads is written through distributed memory
+      double m1 = 0.0, m2 = 0.0;
       for (int i = cu.lo + tid; i < cu.hi; i += nth) {
         const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-        const double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
-        const double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
-        const double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
+        const double dx = __dadd_rn(__dmul_rn(c4, s.VX[i]), __dmul_rn(a.tstep2, s.AX[i]));
+        const double dy = __dadd_rn(__dmul_rn(c4, s.VY[i]), __dmul_rn(a.tstep2, s.AY[i]));
+        const double dz = __dadd_rn(__dmul_rn(c4, s.VZ[i]), __dmul_rn(a.tstep2, s.AZ[i]));
         const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
+        if (skin) {
+          s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
+          top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+        }
         s.XN[i] = nx; s.YN[i] = ny; s.ZN[i] = nz;
         pXN[i] = nx; pYN[i] = ny; pZN[i] = nz;
         V av = s.A4[i], lv;
@@ -754,12 +844,16 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
           if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
         }
       }
+      // the per-warp pairs are read by both CTAs right after the barrier
+      // below and rewritten only after the force pass's cluster barrier
+      if (skin) top2_store(m1, m2, s.red);
       if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
       if (tid == 0) s.misc[MISC_EXCESS] = 0;
       PHASE_ADD(2, t_xu);
       PHASE_T0(t_b1);
       cg::this_cluster().sync();
       PHASE_ADD(8, t_b1);
+      if (skin) skin_fire = skin_fires(s.red, peer_red, nth >> 5, a.neigh_margin);
       { double *t; t = s.X; s.X = s.XN; s.XN = t; t = s.Y; s.Y = s.YN; s.YN = t; t = s.Z; s.Z = s.ZN; s.ZN = t; }
       s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
       { V *t; t = s.A4; s.A4 = s.A4N; s.A4N = t; t = s.L4; s.L4 = s.L4N; s.L4N = t; }
@@ -774,7 +868,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     }
     cg::this_cluster().sync();   // no distributed shared-memory access after this
   } else if (a.mode == KM_NEIGHBOR) {
-    build_lists<Real, 1>(a, lane, L, T, s, cu);
+    build_lists<Real, 1>(a, lane, L, T, s, cu, st.istep);
   } else if (a.mode == KM_FORCE) {
     double *out = a.out_force;
     force_pass<Real, 1>(a, lane, L, T, s, st.istep, cu, -1, [&](int i, double fx, double fy, double fz) {
@@ -782,7 +876,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       out[o] = fx; out[o + 1] = fy; out[o + 2] = fz;
     });
   } else if (a.mode == KM_PRE) {
-    build_lists<Real, 1>(a, lane, L, T, s, cu);
+    build_lists<Real, 1>(a, lane, L, T, s, cu, st.istep);
     // dxyz_mp = 0 (time_integral_pre.F90:79)
     if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
     __syncthreads();
@@ -790,65 +884,44 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     force_pass<Real, 1>(a, lane, L, T, s, is, cu, a.noise_base, [&](int i, double fx, double fy, double fz) {
       double n0, n1, n2;
       if (s.cst_on && a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }
-      else noise3(a, lane, gb0 + i, is, a.noise_base, n0, n1, n2);
+      else noise3(a, lane, L, i, is, a.noise_base, n0, n1, n2);
       const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
-      s.AX[i] = fx * rc + cc * n0; s.AY[i] = fy * rc + cc * n1; s.AZ[i] = fz * rc + cc * n2;
+      s.AX[i] = __dadd_rn(__dmul_rn(fx, rc), __dmul_rn(cc, n0));
+      s.AY[i] = __dadd_rn(__dmul_rn(fy, rc), __dmul_rn(cc, n1));
+      s.AZ[i] = __dadd_rn(__dmul_rn(fz, rc), __dmul_rn(cc, n2));
     });
   } else {  // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step)
-    const int nloop = (a.mode == KM_STEP) ? a.nsteps : 1;
+    const int nloop = (a.mode == KM_STEP) ? lane_steps : 1;
     for (int step = 0; step < nloop; ++step) {
       const long long istep = st.istep + 1;
       if (a.mode != KM_VSTEP) {
         // time_integral.F90:57-161: neighbour trigger, rebuild, x update
         PHASE_T0(t_trig);
-        // neighbour trigger (time_integral.F90:57-110)
-        bool rebuild;
-        if (!skin) {
-          rebuild = (istep % a.n_step_neighbor) == 1 || istep == 1;
-        } else {
-          double m1 = 0, m2 = 0;
-          for (int i = tid; i < N; i += nth) {
-            double d2 = s.DX[i] * s.DX[i] + s.DY[i] * s.DY[i] + s.DZ[i] * s.DZ[i];
-            if (d2 > m1) { m2 = m1; m1 = d2; } else if (d2 > m2) m2 = d2;
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            double o1 = __shfl_xor_sync(0xffffffffu, m1, o), o2 = __shfl_xor_sync(0xffffffffu, m2, o);
-            double n1 = fmax(m1, o1), n2 = fmax(fmin(m1, o1), fmax(m2, o2));
-            m1 = n1; m2 = n2;
-          }
-          if ((tid & 31) == 0) { s.red[2 * (tid >> 5)] = m1; s.red[2 * (tid >> 5) + 1] = m2; }
-          __syncthreads();
-          if (tid == 0) {
-            double b1 = 0, b2 = 0;
-            for (int w = 0; w < (nth >> 5); ++w) {
-              double o1 = s.red[2 * w], o2 = s.red[2 * w + 1];
-              double n1 = fmax(b1, o1), n2 = fmax(fmin(b1, o1), fmax(b2, o2));
-              b1 = n1; b2 = n2;
-            }
-            s.misc[MISC_REBUILD] = (sqrt(b1) + sqrt(b2) > a.neigh_margin) ? 1 : 0;
-          }
-          __syncthreads();
-          rebuild = s.misc[MISC_REBUILD] != 0;
-        }
+        const bool rebuild = skin ? skin_fire : ((istep % a.n_step_neighbor) == 1 || istep == 1);
         PHASE_ADD(0, t_trig);
         PHASE_T0(t_reb);
         if (rebuild) {
-          build_lists<Real, 1>(a, lane, L, T, s, cu);
+          build_lists<Real, 1>(a, lane, L, T, s, cu, istep);
           // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
           if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
           __syncthreads();
         }
         PHASE_ADD(1, t_reb);
         PHASE_T0(t_xu);
-        // x update (time_integral.F90:152-161); clear hbond-site counters
+        // x update (time_integral.F90:152-161), each product rounded as the
+        // reference evaluates it; clear hbond-site counters
+        double m1 = 0.0, m2 = 0.0;
         for (int i = tid; i < N; i += nth) {
           const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-          double dx = c4 * s.VX[i] + a.tstep2 * s.AX[i];
-          double dy = c4 * s.VY[i] + a.tstep2 * s.AY[i];
-          double dz = c4 * s.VZ[i] + a.tstep2 * s.AZ[i];
+          const double dx = __dadd_rn(__dmul_rn(c4, s.VX[i]), __dmul_rn(a.tstep2, s.AX[i]));
+          const double dy = __dadd_rn(__dmul_rn(c4, s.VY[i]), __dmul_rn(a.tstep2, s.AY[i]));
+          const double dz = __dadd_rn(__dmul_rn(c4, s.VZ[i]), __dmul_rn(a.tstep2, s.AZ[i]));
           s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
           if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
-          if (skin) { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
+          if (skin) {
+            s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
+            top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+          }
           set_pos<Real>(s, i);
           if (s.near_on) {
             const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
@@ -857,9 +930,13 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
             if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
           }
         }
+        // per-warp pairs for the next step's trigger: read by every warp
+        // right after the barrier below, rewritten only in the next x update
+        if (skin) top2_store(m1, m2, s.red);
         for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
         if (tid == 0) s.misc[MISC_EXCESS] = 0;
         __syncthreads();
+        if (skin) skin_fire = skin_fires(s.red, nullptr, nth >> 5, a.neigh_margin);
         PHASE_ADD(2, t_xu);
       }
       if (a.mode != KM_XSTEP) {
@@ -911,9 +988,30 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       if (s.misc[MISC_CLAMP]) atomicAdd((unsigned long long *)&st.nclamp, (unsigned long long)s.misc[MISC_CLAMP]);
       if (s.misc[MISC_NAN]) atomicOr(&st.flags, LF_NAN);
       if (s.misc[MISC_PMF]) atomicOr(&st.flags, LF_PMF);
-      if (cu.rank == 0) st.istep = istep0 + a.nsteps;
+      if (cu.rank == 0) st.istep = istep0 + lane_steps;
     }
   }
+}
+
+// r_boxmuller(3, nmp, nrep) of the counter-based generator for steps
+// istep0 .. istep0 + gridDim.y - 1 (the noise the lane kernel draws at
+// those steps): block (lane, k) writes out[k][bead][3]
+__global__ void noise_kernel(KArgs a, long long istep0, double *out) {
+  const int lane = blockIdx.x, k = blockIdx.y;
+  const LaneDesc L = a.lanes[lane];
+  const int N = a.tops[L.top].nmp;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    double n0, n1, n2;
+    noise3(a, lane, L, i, istep0 + k, 0, n0, n1, n2);
+    const size_t o = ((size_t)k * a.nbead_total + L.state0 + i) * 3;
+    out[o] = n0; out[o + 1] = n1; out[o + 2] = n2;
+  }
+}
+
+cudaError_t noise_launch(cudaStream_t st, KArgs a, long long istep0, int nstep, double *out) {
+  a.noise = nullptr;   // always the counter-based generator
+  noise_kernel<<<dim3(a.nlane, nstep), 256, 0, st>>>(a, istep0, out);
+  return cudaGetLastError();
 }
 
 #ifdef TIS_PHASE_TIMING

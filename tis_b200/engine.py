@@ -23,9 +23,13 @@ class TisError(RuntimeError):
 
 
 class Engine:
-    def __init__(self, systems, par: dict, tempk, nrep=None):
+    def __init__(self, systems, par: dict, tempk, nrep=None, ladder=None):
         """systems: list of topology dicts (tis_b200.synth); nrep[k] replicas of
-        systems[k] (default 1 each) with temperatures tempk (one per lane)."""
+        systems[k] (default 1 each) with temperatures tempk (one per lane).
+        ladder=(tempk_all, irep_first): this engine holds replicas irep_first
+        .. irep_first + len(tempk) - 1 (1-based) of the ladder tempk_all of one
+        system split over ranks (tis_init_ladder); tempk are their starting
+        temperatures."""
         self.L = load_library()
         if isinstance(systems, dict):
             systems = [systems]
@@ -47,8 +51,16 @@ class Engine:
         nr = np.ascontiguousarray(np.asarray(self.nrep, dtype=np.int32))
         self._nr = nr
         h = C.c_void_p()
-        rc = self.L.tis_init_batch(len(self.systems), tops, C.byref(self._par), ptr_i32(nr), ptr_f64(self.tempk),
-                                   C.byref(h))
+        self.ladder = None
+        if ladder is not None:
+            tall = np.ascontiguousarray(np.asarray(ladder[0], dtype=np.float64))
+            self.ladder = (tall, int(ladder[1]))
+            assert len(self.systems) == 1
+            rc = self.L.tis_init_ladder(tops, C.byref(self._par), len(tall), ptr_f64(tall), int(ladder[1]),
+                                        len(self.tempk), C.byref(h))
+        else:
+            rc = self.L.tis_init_batch(len(self.systems), tops, C.byref(self._par), ptr_i32(nr),
+                                       ptr_f64(self.tempk), C.byref(h))
         if rc != 0 or not h.value:
             raise TisError(rc, "tis_init_batch failed")
         self.h = h
@@ -151,6 +163,37 @@ class Engine:
     def step(self, n):
         return self._check(self.L.tis_step(self.h, int(n)), "step")
 
+    def time_integral(self, n, flags, exchange_step=None):
+        """n calls of time_integral(flg_step_each_replica): flags (nrep int32,
+        updated in place) freeze replicas; exchange_step (nrep int64) stops
+        a replica there and sets its flag."""
+        assert flags.dtype == np.int32 and flags.shape == (self.nlane,)
+        ex = None
+        if exchange_step is not None:
+            ex = np.ascontiguousarray(exchange_step, dtype=np.int64)
+            self._keep_ex = ex
+        return self._check(self.L.tis_time_integral(self.h, int(n), ptr_i32(flags),
+                                                    None if ex is None else ex.ctypes.data_as(C.POINTER(C.c_int64))),
+                           "time_integral")
+
+    def random_number(self, istep, nstep):
+        """(nstep, nbead, 3) Gaussian noise of the counter-based generator at
+        steps istep .. istep + nstep - 1."""
+        out = np.zeros((nstep, self.nbead, 3))
+        self._check(self.L.tis_get_random_number(self.h, int(istep), int(nstep), ptr_f64(out)), "random_number")
+        return out
+
+    def steps(self):
+        out = np.zeros(self.nlane, dtype=np.int64)
+        self._check(self.L.tis_get_steps(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))), "get_steps")
+        return out
+
+    def rebuild_info(self, irep=1):
+        """(neighbour rebuilds of replica irep, step of the last one)."""
+        n, last = C.c_int64(0), C.c_int64(0)
+        self._check(self.L.tis_get_rebuild_info(self.h, irep, C.byref(n), C.byref(last)), "rebuild_info")
+        return n.value, last.value
+
     def last_step_ms(self):
         return self.L.tis_last_step_ms(self.h)
 
@@ -173,6 +216,22 @@ class Engine:
             up = ptr_f64(uu)
         self._check(self.L.tis_replica_exchange(self.h, up, C.byref(na) if count else None), "replica_exchange")
         return na.value if count else None
+
+    def rex_energies(self):
+        """(nrep_local, 2): energy at the own label and at the exchange
+        partner's label of this ladder engine's replicas."""
+        out = np.zeros((self.nlane, 2))
+        self._check(self.L.tis_rex_energies(self.h, ptr_f64(out)), "rex_energies")
+        return out
+
+    def rex_exchange_all(self, energies_all, u=None):
+        """The exchange of the whole ladder from the gathered (nrep_all, 2)
+        energies; returns the number of accepted swaps."""
+        e = np.ascontiguousarray(energies_all, dtype=np.float64)
+        na = C.c_int32(0)
+        up = None if u is None else ptr_f64(np.ascontiguousarray(u, dtype=np.float64))
+        self._check(self.L.tis_rex_exchange_all(self.h, ptr_f64(e), up, C.byref(na)), "rex_exchange_all")
+        return na.value
 
     def hydro_tensors(self, irep=1):
         """(D, L) of the last Brownian-HI refresh, row-major (3N, 3N) arrays."""
