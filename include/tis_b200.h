@@ -177,6 +177,19 @@ typedef struct tis_params {
   int32_t i_hydro_tensor;          /* Brownian-HI diffusion tensor (HI_TENSOR, const_index.F90:39-45): 1 (or 0)
                                       RPY, 2 RPY_OVER, 3 ERMAK_OVER (radius of bead 1), 4 ZUK_RPY (per-bead
                                       radii), simu_hydro_tensors.F90:50-324 */
+  /* Launch configuration of the step kernel (no reference counterpart).  Each
+   * field left 0 comes from the environment (TIS_THREADS, TIS_GROUP,
+   * TIS_CLUSTER, TIS_NOISE_SWEEP), else from the measured table the
+   * autotuner writes (launch_table, or tuned_launch.tsv next to the
+   * library), else from a built-in rule.  The results do not depend on it
+   * beyond the summation order of each bead's force. */
+  int32_t launch_threads;          /* threads per CTA: 128, 256, 512, or 1024 (mixed, one CTA per replica) */
+  int32_t launch_group;            /* threads per bead in the force gather: 1, 2, 4 or 8 */
+  int32_t launch_ctas;             /* CTAs per replica: 1, or 2 (a cluster: mixed precision, 512 threads,
+                                      no periodic box, no Ewald, >= 64 beads) */
+  int32_t launch_noise_sweep;      /* two CTAs: 1 draws the noise in the bonded sweep, 2 in the update */
+  int32_t launch_order;            /* 1: replicas launched in context order, 2: largest first */
+  const char *launch_table;        /* NULL: tuned_launch.tsv next to the library */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */
@@ -192,6 +205,11 @@ typedef struct tis_status_t {
   int32_t exv_pairs_max;           /* largest exv half list among replicas */
   int32_t ele_pairs_max;           /* largest ele half list among replicas */
   int32_t ctas_per_lane;           /* CTAs (one cluster) that tis_step gives each replica: 1 or 2 */
+  int32_t threads_per_cta;         /* the launch configuration in use (see tis_params.launch_*) */
+  int32_t group;                   /* threads per bead in the force gather, 0: per-replica rule */
+  int32_t noise_sweep;
+  int32_t lane_order;
+  int32_t launch_source;           /* 0 built-in rule, 1 tuned table, 2 caller or environment */
 } tis_status_t;
 
 typedef struct tis_ctx tis_ctx;

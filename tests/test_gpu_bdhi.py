@@ -208,22 +208,24 @@ def test_bdhi_tensor_variants(tis_lib, kind, precision):
     FP32: 1e-7) and its factor (FP64 1e-12, mixed 1e-5)."""
     s = _variant_chain(kind, 90, 40 + kind, nest=True)
     par = synth.bdhi_params(precision=precision, i_hydro_tensor=kind)
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(s["xyz"][None])
+    Dr, Lr, rc = orc.hydro_tensors()
     eng = Engine([s], par, [300.0])
     eng.set_state(s["xyz"])
     eng.set_noise(np.zeros((2, s["nmp"], 3)))
     eng.time_integral_pre()
+    if rc != 0:
+        # the Ermak-McCammon overlap formula is not positive definite on
+        # every squeezed chain: the GPU must then report the same failure
+        assert kind == 3 and rc == TIS_E_NOT_SPD
+        with pytest.raises(TisError) as e:
+            eng.step(1)
+        assert e.value.code == TIS_E_NOT_SPD
+        eng.close()
+        return
     assert eng.step(1) >= 0
     D, L = eng.hydro_tensors()
-    orc = Oracle(s, dict(par, precision=0), [300.0])
-    orc.set_state(s["xyz"][None])
-    Dr, Lr, rc = orc.hydro_tensors()
-    if kind == 3:
-        # the Ermak-McCammon overlap formula is not positive definite on
-        # every squeezed chain: both sides must then agree on the failure
-        if rc != 0:
-            eng.close()
-            return
-    assert rc == 0
     dtol = 1e-15 if precision == 0 else 1e-7
     assert np.abs(D - Dr).max() <= dtol * np.abs(Dr).max()
     ltol = 1e-12 if precision == 0 else 1e-5

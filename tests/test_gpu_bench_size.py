@@ -17,8 +17,6 @@
   every chain within the tolerances above.  Chains above 512 beads keep their
   bit matrices in global memory.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -38,15 +36,7 @@ def rel_force_err(f, ref):
 
 
 def engine(systems, par, temps, nrep, pair):
-    old = os.environ.get("TIS_CLUSTER")
-    os.environ["TIS_CLUSTER"] = "1" if pair else "0"
-    try:
-        eng = Engine(systems, par, temps, nrep=nrep)
-    finally:
-        if old is None:
-            del os.environ["TIS_CLUSTER"]
-        else:
-            os.environ["TIS_CLUSTER"] = old
+    eng = Engine(systems, dict(par, launch_ctas=2 if pair else 1), temps, nrep=nrep)
     return eng
 
 

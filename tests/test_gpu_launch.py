@@ -1,0 +1,80 @@
+"""Launch configurations of the step kernel (tis_params.launch_*, the tuned
+table tis_b200/autotune.py writes, the environment overrides): the source of
+the configuration in use, and forces and trajectories that stay within the
+parity tolerances for every configuration, against the oracle.  The
+configurations differ only in the summation order of each bead's force."""
+import os
+
+import numpy as np
+import pytest
+
+from tis_b200 import autotune, synth
+from tis_b200.engine import Engine
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def test_table_caller_and_environment(tis_lib, tmp_path, monkeypatch):
+    systems, par, temps = synth.workload_c1()
+    key = autotune.workload_key(systems, par, [1])
+    table = tmp_path / "t.tsv"
+    cfg = dict(launch_threads=256, launch_group=4, launch_ctas=1, launch_noise_sweep=1, launch_order=1)
+    autotune.merge_rows(str(table), {key: autotune.format_row(key, cfg, 1.0)})
+    eng = Engine(systems, dict(par, launch_table=str(table)), temps)
+    st = eng.status()
+    assert (st["launch_source"], st["threads_per_cta"], st["group"]) == (1, 256, 4)
+    eng.close()
+    eng = Engine(systems, dict(par, launch_table=str(table), launch_threads=128), temps)
+    st = eng.status()
+    assert (st["launch_source"], st["threads_per_cta"], st["group"]) == (2, 128, 4)
+    eng.close()
+    monkeypatch.setenv("TIS_GROUP", "2")
+    eng = Engine(systems, dict(par, launch_table=str(table)), temps)
+    assert (eng.status()["launch_source"], eng.status()["group"]) == (2, 2)
+    eng.close()
+    monkeypatch.delenv("TIS_GROUP")
+    eng = Engine(systems, dict(par, launch_table=str(tmp_path / "absent.tsv")), temps)
+    assert eng.status()["launch_source"] == 0
+    eng.close()
+
+
+@pytest.mark.parametrize("cfg", [dict(launch_threads=128, launch_group=1), dict(launch_threads=256, launch_group=8),
+                                 dict(launch_threads=1024, launch_group=2), dict(launch_ctas=2, launch_group=4,
+                                                                                 launch_noise_sweep=2)])
+def test_configurations_keep_parity(tis_lib, cfg):
+    systems, par, ladder = synth.workload_c3()
+    s = systems[0]
+    temps = list(ladder[::16])
+    nrep, n, nsteps = len(temps), s["nmp"], 25
+    eng = Engine([s], dict(par, **cfg), temps, nrep=[nrep])
+    noise = np.random.default_rng(3).normal(size=(nsteps + 1, nrep * n, 3))
+    eng.set_state(np.tile(s["xyz"], (nrep, 1)))
+    eng.set_noise(noise)
+    eng.time_integral_pre()
+    eng.step(nsteps)
+    x, _, _ = eng.get_state()
+    orc = Oracle(s, dict(par, precision=0), temps)
+    orc.set_state(np.tile(s["xyz"], (nrep, 1, 1)))
+    orc.set_noise(noise.reshape(nsteps + 1, nrep, n, 3))
+    orc.time_integral_pre()
+    orc.step(nsteps)
+    assert np.abs(x - orc.get_state()[0].reshape(-1, 3)).max() < 1e-4
+    eng.close()
+
+
+def test_largest_first_order_on_uneven_batch(tis_lib):
+    """Batches launch their largest replicas first; the order changes which
+    SM runs a replica, not its numbers."""
+    systems = [synth.set_friction(synth.dt15_chain(k, 100 + k, hb_fraction=0.3), 0.5) for k in (9, 41, 23, 60)]
+    par = synth.dt15_params(ionic_strength=0.15, precision=1)
+    out = []
+    for order in (1, 2):
+        eng = Engine(systems, dict(par, launch_order=order), [300.0] * 4, nrep=[1] * 4)
+        assert eng.status()["lane_order"] == order
+        eng.set_state(np.vstack([s["xyz"] for s in systems]))
+        eng.time_integral_pre()
+        eng.step(30)
+        out.append(eng.get_state()[0])
+        eng.close()
+    assert np.array_equal(out[0], out[1])

@@ -2,14 +2,12 @@
 bonded items) against one CTA per replica and against the CPU restatement,
 through the C-ABI.  The split is used by tis_step for mixed precision,
 non-periodic systems of >= 64 beads with a fixed rebuild cadence when the
-replicas fill at most half of the SMs; TIS_CLUSTER=0 turns it off.
+replicas fill at most half of the SMs; tis_params.launch_ctas chooses it.
 
 Tolerances: two-CTA vs one-CTA positions 1e-9 A after 25 steps (the same
 FP32 pair forces, FP64 sums grouped differently); against the oracle the
 mixed-precision trajectory tolerance 1e-4 A.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -21,15 +19,7 @@ pytestmark = pytest.mark.gpu
 
 
 def run(system, par, temps, noise, nsteps, pair, uniforms=None):
-    old = os.environ.get("TIS_CLUSTER")
-    os.environ["TIS_CLUSTER"] = "1" if pair else "0"
-    try:
-        eng = Engine([system], par, temps, nrep=[len(temps)])
-    finally:
-        if old is None:
-            del os.environ["TIS_CLUSTER"]
-        else:
-            os.environ["TIS_CLUSTER"] = old
+    eng = Engine([system], dict(par, launch_ctas=2 if pair else 1), temps, nrep=[len(temps)])
     assert eng.status()["ctas_per_lane"] == (2 if pair else 1)
     eng.set_state(np.tile(system["xyz"], (len(temps), 1)))
     eng.set_noise(noise, uniforms)

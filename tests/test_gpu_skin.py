@@ -13,8 +13,6 @@ the two-CTA cluster are both run.  A margin of 2 A makes the rule fire every
 ~85 steps; the default 8 A fires about once per 1,300 steps, which the
 64-replica run covers.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -28,15 +26,7 @@ POS_TOL = {0: 1e-8, 1: 1e-4}
 
 
 def engine(system, par, temps, pair):
-    old = os.environ.get("TIS_CLUSTER")
-    os.environ["TIS_CLUSTER"] = "1" if pair else "0"
-    try:
-        eng = Engine([system], par, temps, nrep=[len(temps)])
-    finally:
-        if old is None:
-            del os.environ["TIS_CLUSTER"]
-        else:
-            os.environ["TIS_CLUSTER"] = old
+    eng = Engine([system], dict(par, launch_ctas=2 if pair else 1), temps, nrep=[len(temps)])
     assert eng.status()["ctas_per_lane"] == (2 if pair else 1)
     return eng
 

@@ -79,6 +79,8 @@ class Params(C.Structure):
         ("i_dtrna_model", C.c_int32), ("i_charge", C.c_int32), ("length_per_unit_P", C.c_double),
         ("pmf_nbin", C.c_int32), ("pmf_rmin", C.c_double), ("pmf_rbin", C.c_double), ("pmf_rmax", C.c_double),
         ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p), ("i_hydro_tensor", C.c_int32),
+        ("launch_threads", C.c_int32), ("launch_group", C.c_int32), ("launch_ctas", C.c_int32),
+        ("launch_noise_sweep", C.c_int32), ("launch_order", C.c_int32), ("launch_table", C.c_char_p),
     ]
 
 
@@ -88,6 +90,8 @@ class Status(C.Structure):
         ("list_overflow", C.c_int32), ("nan_seen", C.c_int32), ("wait_timeout", C.c_int32),
         ("not_spd", C.c_int32), ("last_error", C.c_int32),
         ("exv_pairs_max", C.c_int32), ("ele_pairs_max", C.c_int32), ("ctas_per_lane", C.c_int32),
+        ("threads_per_cta", C.c_int32), ("group", C.c_int32), ("noise_sweep", C.c_int32),
+        ("lane_order", C.c_int32), ("launch_source", C.c_int32),
     ]
 
 
@@ -155,6 +159,11 @@ def make_params(**kw) -> Params:
         if k == "psize":
             for i in range(3):
                 p.psize[i] = float(v[i])
+        elif k == "launch_table":
+            if v is not None:
+                b = str(v).encode()
+                p._keep.append(b)
+                p.launch_table = b
         elif k == "pmf_mg_p":
             if v is not None:
                 a = np.ascontiguousarray(np.asarray(v, dtype=np.float64))

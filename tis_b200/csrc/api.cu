@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <dlfcn.h>
+
 #include "../../include/tis_b200.h"
 #include "common.cuh"
 
@@ -154,6 +156,9 @@ struct tis_ctx {
   std::vector<long long> clamp_seen;
   long long launches = 0;            // kernels this context has launched
   bool pair = false;                 // tis_step runs two CTAs (a cluster) per lane
+  int noise_sweep = 1, order = 1, launch_source = 0;
+  std::vector<int> h_order;          // launch order of the lanes (order 2: largest first)
+  DBuf<int> d_order;
   size_t smem2 = 0;
   // Ewald
   int nk = 0, hmax = 0, nqblk = 1, nq_max = 0;
@@ -245,26 +250,68 @@ void append(std::vector<T> &dst, const T *src, size_t n) {
   if (n) dst.insert(dst.end(), src, src + n);
 }
 
-int choose_threads(int maxN, bool mixed) {
-  const char *env = std::getenv("TIS_THREADS");
-  if (env) {
-    int t = std::atoi(env);
-    if (t >= 64 && t <= (mixed ? 1024 : 512) && t % 32 == 0) return t;
+// ------------------------------------------------------------ launch configuration
+// The step kernel's launch configuration: threads per CTA, threads per bead
+// in the force gather, CTAs per replica, where the two-CTA step draws its
+// noise, and the launch order of the replicas.  Measured choices come from
+// the table the autotuner (tis_b200/autotune.py) writes; each row is a
+// workload key and the fastest configuration measured for it:
+//   nmp nlane precision i_ele periodic skin | threads group ctas noise_sweep order | rate
+struct LaunchCfg {
+  int threads = 0, group = 0, ctas = 0, noise_sweep = 0, order = 0;
+};
+
+struct TuneRow {
+  int nmp, nlane, precision, ele, periodic, skin;
+  LaunchCfg cfg;
+};
+
+std::string library_dir() {
+  Dl_info info;
+  if (dladdr((void *)&library_dir, &info) && info.dli_fname) {
+    const std::string p = info.dli_fname;
+    const size_t k = p.rfind('/');
+    return k == std::string::npos ? std::string(".") : p.substr(0, k);
   }
-  if (maxN <= 96) return 128;
-  if (maxN <= 160) return 256;
-  return 512;
+  return ".";
 }
 
-int choose_group(int threads, int maxN) {
-  const char *env = std::getenv("TIS_GROUP");
-  if (env) {
-    int g = std::atoi(env);
-    if (g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32) return g;
+std::vector<TuneRow> read_tune_table(const std::string &path) {
+  std::vector<TuneRow> rows;
+  FILE *f = std::fopen(path.c_str(), "r");
+  if (!f) return rows;
+  char line[512];
+  while (std::fgets(line, sizeof line, f)) {
+    if (line[0] == '#' || line[0] == '\n') continue;
+    TuneRow r{};
+    double rate = 0.0;
+    const int n = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %lf", &r.nmp, &r.nlane, &r.precision, &r.ele,
+                              &r.periodic, &r.skin, &r.cfg.threads, &r.cfg.group, &r.cfg.ctas, &r.cfg.noise_sweep,
+                              &r.cfg.order, &rate);
+    if (n >= 11 && r.nmp > 0 && r.nlane > 0) rows.push_back(r);
   }
-  int g = 1;
-  while (g < 8 && (threads / (2 * g)) >= maxN) g *= 2;
-  return g;
+  std::fclose(f);
+  return rows;
+}
+
+// the measured row of the same arithmetic, electrostatics, box and rebuild
+// rule nearest in (log nmp, log nlane)
+bool tune_lookup(const std::vector<TuneRow> &rows, int nmp, int nlane, int precision, int ele, int periodic, int skin,
+                 LaunchCfg &out) {
+  double best = 1e300;
+  for (int pass = 0; pass < 2 && best == 1e300; ++pass)
+    for (const TuneRow &r : rows) {
+      if (r.precision != precision || r.ele != ele || r.periodic != periodic) continue;
+      if (pass == 0 && r.skin != skin) continue;   // the other rule only when none matches
+      const double d = std::fabs(std::log((double)nmp / r.nmp)) + std::fabs(std::log((double)nlane / r.nlane));
+      if (d < best) { best = d; out = r.cfg; }
+    }
+  return best < 1e300;
+}
+
+int env_int(const char *name) {
+  const char *e = std::getenv(name);
+  return e ? std::atoi(e) : 0;
 }
 
 // Reciprocal vectors of mloop_ewld.F90:56-156: every integer h != 0 with
@@ -765,8 +812,6 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     c->g_lab2rep.resize(nlabel);
     for (int g = 0; g < nlabel; ++g) { c->g_rep2lab[g] = g; c->g_lab2rep[g] = g; }
   }
-  c->threads = choose_threads(maxN, p.precision == TIS_PREC_MIXED);
-  c->group = choose_group(c->threads, maxN);
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
   size_t smem = 0, smem2 = 0;
   int minN = 1 << 30;
@@ -788,18 +833,63 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     minN = std::min(minN, d.nmp);
   }
   c->smem = smem;
-  // two CTAs per lane (a cluster) when the lanes fill at most half of the
-  // SMs: mixed precision, no periodic box, DH, Coulomb or no electrostatics
-  // (either rebuild rule); TIS_CLUSTER=0 turns it off
+  // launch configuration: caller fields, then the environment, then the
+  // tuned table, then the built-in rule (one CTA per replica up to 96 beads
+  // on 128 threads, 256 up to 160, else 512; two CTAs per replica when the
+  // replicas fill at most half of the SMs; largest replica first in batches)
   {
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const char *env = std::getenv("TIS_CLUSTER");
-    const bool allow = !(env && env[0] == '0');
-    c->pair = allow && !c->bdhi && p.precision == TIS_PREC_MIXED && !periodic &&
-              p.i_ele != TIS_ELE_EWALD && minN >= 64 && nsm > 0 && 2 * nlane <= nsm && smem2 <= 227 * 1024;
+    const bool mixed = p.precision == TIS_PREC_MIXED;
+    const bool pair_ok = !c->bdhi && mixed && !periodic && p.i_ele != TIS_ELE_EWALD && minN >= 64 &&
+                         smem2 <= 227 * 1024;
+    LaunchCfg cfg;
+    int source = 0;
+    {
+      const std::string path = p.launch_table ? std::string(p.launch_table) : library_dir() + "/tuned_launch.tsv";
+      const std::vector<TuneRow> rows = read_tune_table(path);
+      if (!c->bdhi && tune_lookup(rows, maxN, nlane, mixed ? 1 : 0, p.i_ele, periodic ? 1 : 0, skin ? 1 : 0, cfg))
+        source = 1;
+    }
+    const int env_t = env_int("TIS_THREADS"), env_g = env_int("TIS_GROUP");
+    const char *env_c = std::getenv("TIS_CLUSTER"), *env_n = std::getenv("TIS_NOISE_SWEEP");
+    if (env_t) { cfg.threads = env_t; source = 2; }
+    if (env_g) { cfg.group = env_g; source = 2; }
+    if (env_c) { cfg.ctas = env_c[0] == '0' ? 1 : 2; source = 2; }
+    if (env_n) { cfg.noise_sweep = env_n[0] == '0' ? 2 : 1; source = 2; }
+    if (p.launch_threads) { cfg.threads = p.launch_threads; source = 2; }
+    if (p.launch_group) { cfg.group = p.launch_group; source = 2; }
+    if (p.launch_ctas) { cfg.ctas = p.launch_ctas; source = 2; }
+    if (p.launch_noise_sweep) { cfg.noise_sweep = p.launch_noise_sweep; source = 2; }
+    if (p.launch_order) { cfg.order = p.launch_order; source = 2; }
+    if (cfg.ctas == 0) cfg.ctas = (pair_ok && nsm > 0 && 2 * nlane <= nsm) ? 2 : 1;
+    if (cfg.ctas == 2 && !pair_ok) cfg.ctas = 1;
+    if (cfg.ctas == 2) cfg.threads = 512;   // the cluster kernel runs 512 threads per CTA
+    if (cfg.threads == 0) cfg.threads = maxN <= 96 ? 128 : (maxN <= 160 ? 256 : 512);
+    if (cfg.threads < 64 || cfg.threads > (mixed ? 1024 : 512) || cfg.threads % 32) {
+      tis_destroy(c);
+      return TIS_E_ARG;
+    }
+    if (!(cfg.group == 0 || cfg.group == 1 || cfg.group == 2 || cfg.group == 4 || cfg.group == 8)) {
+      tis_destroy(c);
+      return TIS_E_ARG;
+    }
+    if (cfg.noise_sweep == 0) cfg.noise_sweep = 1;
+    if (cfg.order == 0) cfg.order = ntop > 1 ? 2 : 1;
+    c->threads = cfg.threads;
+    c->group = cfg.group;
+    c->pair = cfg.ctas == 2;
+    c->noise_sweep = cfg.noise_sweep;
+    c->order = cfg.order;
+    c->launch_source = source;
     c->smem2 = c->pair ? smem2 : 0;
+    // replicas largest first: a CTA that frees its SM takes the next one
+    std::vector<int> order(nlane);
+    for (int l = 0; l < nlane; ++l) order[l] = l;
+    if (c->order == 2)
+      std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return c->lane_nmp[x] > c->lane_nmp[y]; });
+    c->h_order = order;
   }
 
   // ---- device
@@ -807,6 +897,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
   CK(cudaEventCreate(&c->ev0));
   CK(cudaEventCreate(&c->ev1));
   if (!c->bdhi) CK(lane_kernel_set_smem(p.precision == TIS_PREC_MIXED, (int)smem, (int)c->smem2));
+  CK(c->d_order.upload(c->h_order));
   CK(c->d_tops.upload(c->tops));
   CK(c->d_lanes.upload(c->lanes));
   std::vector<LaneState> ls(nlane);
@@ -966,7 +1057,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free(); c->p0xyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
-  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free(); c->lane_n.free();
+  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free(); c->lane_n.free(); c->d_order.free();
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
   c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->b_hrad.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
@@ -1173,6 +1264,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.noise_in_sweep = 0;
   a.lane_nsteps = nullptr;
   a.step_k = 0;
+  a.lane_order = (c->order == 2 && only_lane < 0) ? c->d_order.p : nullptr;
   return a;
 }
 
@@ -1445,8 +1537,7 @@ int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
   if (c->pair) {
     a.smem_total = (int)c->smem2;
     // the two-CTA sweep has idle warps: the sink's noise is drawn there
-    const char *env = std::getenv("TIS_NOISE_SWEEP");
-    a.noise_in_sweep = (env && env[0] == '0') ? 0 : 1;
+    a.noise_in_sweep = c->noise_sweep == 1 ? 1 : 0;
     ++c->launches;
     CK(lane_kernel_launch_pair(c->nlane, c->smem2, c->stream, a));
   } else if (c->bdhi) {
@@ -1771,6 +1862,11 @@ extern "C" int tis_status(tis_ctx *c, tis_status_t *st) {
     st->ele_pairs_max = std::max(st->ele_pairs_max, ls[i].nele);
   }
   st->ctas_per_lane = c->pair ? 2 : 1;
+  st->threads_per_cta = c->pair ? 512 : c->threads;
+  st->group = c->group;
+  st->noise_sweep = c->noise_sweep;
+  st->lane_order = c->order;
+  st->launch_source = c->launch_source;
   st->wait_timeout = c->wait_timeout;
   st->not_spd = c->not_spd;
   st->last_error = c->last_error;

@@ -210,6 +210,7 @@ struct KArgs {
   const int *lane_nsteps;  // per lane: steps of this launch (KM_STEP) or 1 + the last step index that
                            // moves the lane (KM_XSTEP / KM_VSTEP); null: every lane takes nsteps
   int step_k;              // KM_XSTEP / KM_VSTEP: index of this step within the call
+  const int *lane_order;   // lane of each CTA (or cluster) of a launch over every lane; null: in order
 };
 
 #ifdef __CUDACC__

@@ -85,6 +85,20 @@ __device__ __forceinline__ bool skin_fires(const double *red, const double *peer
   return __dadd_rn(sqrt(m1), sqrt(m2)) > margin;
 }
 
+// a b + c d of the integration: in the FP64 path each product rounded as
+// the reference evaluates it (no contraction), so the update is the
+// reference's to the last bit; the mixed path lets the compiler contract
+template <typename Real>
+__device__ __forceinline__ double mad2(double a, double b, double c, double d) {
+  if constexpr (sizeof(Real) == 8) return __dadd_rn(__dmul_rn(a, b), __dmul_rn(c, d));
+  else return a * b + c * d;
+}
+template <typename Real>
+__device__ __forceinline__ double add_rn(double a, double b) {
+  if constexpr (sizeof(Real) == 8) return __dadd_rn(a, b);
+  else return a + b;
+}
+
 // ------------------------------------------------------------ list build
 // neighbor_list.F90:49-90 + neighbor_assign.F90:481-559 (the EXV_DT15 type
 // sort keeps the generation order) and neighbor_list_ele.F90:123-210: every
@@ -554,7 +568,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   PHASE_T0(t_p2);
   // ---- phase 2: exv pairs + bonded slots + Debye-Hueckel chunk partials
   const int nown = cu.hi - cu.lo;
-  const int GA = pow2_floor_clamp(nth / nown, 8);
+  const int GA = a.group > 0 ? a.group : pow2_floor_clamp(nth / nown, 8);
   const int g = tid & (GA - 1), grp = tid / GA, ngrp = nth / GA;
   const Real ra = (Real)a.exv_adjust, ra2 = ra * ra, inv_ra2 = (Real)(1.0 / (a.exv_adjust * a.exv_adjust));
   const Real dist_ps = (Real)a.exv_dist_PS, dist_rr = (Real)a.exv_dist;
@@ -683,9 +697,10 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
 // the x update, one after the bonded sweep (two more at a rebuild, one more
 // after a valence pruning).  Every branch that decides a cluster barrier is
 // uniform over both CTAs.
-template <typename Real, int NT, int CL>
+template <typename Real, int NT, int CL, bool SKIN2 = false>
 __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
-  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)(blockIdx.x / CL);
+  const int lane = (a.only_lane >= 0) ? a.only_lane
+                                      : (a.lane_order ? a.lane_order[blockIdx.x / CL] : (int)(blockIdx.x / CL));
   if (lane >= a.nlane) return;
   if (CL == 2 && a.mode != KM_STEP) return;
   // replicas that have reached their exchange step wait (time_integral.F90:134)
@@ -695,7 +710,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   const TopDesc T = a.tops[L.top];
   const int N = T.nmp, NQ = T.nq;
   const int tid = threadIdx.x, nth = blockDim.x;
-  const bool skin = a.n_step_neighbor <= 0;
+  // the two-CTA kernel is compiled once per rebuild rule (its registers are
+  // scarce); the one-CTA kernel decides at run time
+  const bool skin = (CL == 2) ? SKIN2 : a.n_step_neighbor <= 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<Real> s = carve<Real>(smem_raw, a.smem_total, a, L, T, a.periodic != 0, skin, CL == 2);
   LaneState &st = a.lstate[lane];
@@ -773,12 +790,12 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         rc = a.b_rcmass[b]; cc = c1[i]; c2 = a.b_c2[b]; c3 = a.b_c3[b];
       }
       // each product rounded, as the reference evaluates it (no contraction)
-      const double ax = __dadd_rn(__dmul_rn(fx, rc), __dmul_rn(cc, n0));
-      const double ay = __dadd_rn(__dmul_rn(fy, rc), __dmul_rn(cc, n1));
-      const double az = __dadd_rn(__dmul_rn(fz, rc), __dmul_rn(cc, n2));
-      s.VX[i] = __dadd_rn(__dmul_rn(c2, s.VX[i]), __dmul_rn(c3, __dadd_rn(s.AX[i], ax)));
-      s.VY[i] = __dadd_rn(__dmul_rn(c2, s.VY[i]), __dmul_rn(c3, __dadd_rn(s.AY[i], ay)));
-      s.VZ[i] = __dadd_rn(__dmul_rn(c2, s.VZ[i]), __dmul_rn(c3, __dadd_rn(s.AZ[i], az)));
+      const double ax = mad2<Real>(fx, rc, cc, n0);
+      const double ay = mad2<Real>(fy, rc, cc, n1);
+      const double az = mad2<Real>(fz, rc, cc, n2);
+      s.VX[i] = mad2<Real>(c2, s.VX[i], c3, add_rn<Real>(s.AX[i], ax));
+      s.VY[i] = mad2<Real>(c2, s.VY[i], c3, add_rn<Real>(s.AY[i], ay));
+      s.VZ[i] = mad2<Real>(c2, s.VZ[i], c3, add_rn<Real>(s.AZ[i], az));
       s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
       if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
     };
@@ -822,9 +839,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       double m1 = 0.0, m2 = 0.0;
       for (int i = cu.lo + tid; i < cu.hi; i += nth) {
         const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-        const double dx = __dadd_rn(__dmul_rn(c4, s.VX[i]), __dmul_rn(a.tstep2, s.AX[i]));
-        const double dy = __dadd_rn(__dmul_rn(c4, s.VY[i]), __dmul_rn(a.tstep2, s.AY[i]));
-        const double dz = __dadd_rn(__dmul_rn(c4, s.VZ[i]), __dmul_rn(a.tstep2, s.AZ[i]));
+        const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
+        const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
+        const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
         const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
         if (skin) {
           s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
@@ -886,9 +903,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       if (s.cst_on && a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }
       else noise3(a, lane, L, i, is, a.noise_base, n0, n1, n2);
       const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
-      s.AX[i] = __dadd_rn(__dmul_rn(fx, rc), __dmul_rn(cc, n0));
-      s.AY[i] = __dadd_rn(__dmul_rn(fy, rc), __dmul_rn(cc, n1));
-      s.AZ[i] = __dadd_rn(__dmul_rn(fz, rc), __dmul_rn(cc, n2));
+      s.AX[i] = mad2<Real>(fx, rc, cc, n0);
+      s.AY[i] = mad2<Real>(fy, rc, cc, n1);
+      s.AZ[i] = mad2<Real>(fz, rc, cc, n2);
     });
   } else {  // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step)
     const int nloop = (a.mode == KM_STEP) ? lane_steps : 1;
@@ -913,9 +930,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         double m1 = 0.0, m2 = 0.0;
         for (int i = tid; i < N; i += nth) {
           const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-          const double dx = __dadd_rn(__dmul_rn(c4, s.VX[i]), __dmul_rn(a.tstep2, s.AX[i]));
-          const double dy = __dadd_rn(__dmul_rn(c4, s.VY[i]), __dmul_rn(a.tstep2, s.AY[i]));
-          const double dz = __dadd_rn(__dmul_rn(c4, s.VZ[i]), __dmul_rn(a.tstep2, s.AZ[i]));
+          const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
+          const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
+          const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
           s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
           if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
           if (skin) {
@@ -1023,7 +1040,8 @@ extern "C" int tis_phase_read(unsigned long long *out) {
 template __global__ void lane_kernel<double, 512, 1>(KArgs);
 template __global__ void lane_kernel<float, 512, 1>(KArgs);
 template __global__ void lane_kernel<float, 1024, 1>(KArgs);
-template __global__ void lane_kernel<float, 512, 2>(KArgs);
+template __global__ void lane_kernel<float, 512, 2, false>(KArgs);
+template __global__ void lane_kernel<float, 512, 2, true>(KArgs);
 
 // Dynamic shared memory to request for a topology: base layout + bit
 // matrices + incidence lists + slots, capped at the 227 KB a CTA may use.
@@ -1045,8 +1063,11 @@ cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2) {
     if (e != cudaSuccess) return e;
     e = cudaFuncSetAttribute(lane_kernel<float, 1024, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e != cudaSuccess) return e;
-    if (bytes2 > 0)
-      return cudaFuncSetAttribute(lane_kernel<float, 512, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes2);
+    if (bytes2 > 0) {
+      e = cudaFuncSetAttribute(lane_kernel<float, 512, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes2);
+      if (e != cudaSuccess) return e;
+      return cudaFuncSetAttribute(lane_kernel<float, 512, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes2);
+    }
     return cudaSuccess;
   }
   return cudaFuncSetAttribute(lane_kernel<double, 512, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -1074,7 +1095,8 @@ cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, con
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, lane_kernel<float, 512, 2>, a);
+  if (a.n_step_neighbor <= 0) return cudaLaunchKernelEx(&cfg, lane_kernel<float, 512, 2, true>, a);
+  return cudaLaunchKernelEx(&cfg, lane_kernel<float, 512, 2, false>, a);
 }
 
 } // namespace tis
