@@ -480,6 +480,30 @@ def run_ours(args, rank, world, local_rank):
         e2e_value = aggregate_rate(rs_rank, world, e2e_total)
     nbytes = 3 * eng.nbead * 3 * 8
 
+    # C3 under the other neighbour rule, the same periods (no exchange kernel
+    # differences): the headline uses args.neighbor
+    other_rule = None
+    if remd and ladder is None and not args.quick:
+        alt = dict(par, n_step_neighbor=0 if par["n_step_neighbor"] > 0 else 10)
+        e2 = Engine(systems, alt, temps, nrep=nrep)
+        e2.set_state(x0)
+        e2.time_integral_pre()
+        for _ in range(args.warmup):
+            e2.step(period_len)
+            e2.replica_exchange(count=False)
+        t2 = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e2.timer_start()
+            e2.step(period_len)
+            e2.replica_exchange(count=False)
+            t2.append(e2.timer_stop())
+        other_rule = {"rule": "Verlet skin, neigh_margin 8 A" if alt["n_step_neighbor"] <= 0 else "every 10 steps",
+                      "value": nlane * period_len * args.steps / (sum(t2) * 1e-3), "unit": UNIT,
+                      "n_rebuild_per_replica_step": e2.status()["n_rebuild"] / (nlane * period_len * (args.steps + args.warmup))}
+        e2.close()
+
     plain = None
     if rank == 0 and not args.no_plain:
         from tis_b200 import synth
@@ -536,6 +560,7 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": ck,
             "plain_fp64": plain,
+            "other_neighbor_rule": other_rule,
             "status": eng.status(),
         }
         print(json.dumps(line), flush=True)

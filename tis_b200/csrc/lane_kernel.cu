@@ -817,8 +817,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   if constexpr (CL == 2) {
     typedef typename V4<Real>::T V;
     cg::this_cluster().sync();   // both CTAs are running before any distributed access
-    const double *peer_red = peer_ptr(s.red, cu);
-    if (skin) skin_fire = skin_fires(s.red, peer_red, nth >> 5, a.neigh_margin);
+    if (skin) skin_fire = skin_fires(s.red, peer_ptr(s.red, cu), nth >> 5, a.neigh_margin);
     double *pXN = peer_ptr(s.XN, cu), *pYN = peer_ptr(s.YN, cu), *pZN = peer_ptr(s.ZN, cu);
     V *pA4N = peer_ptr(s.A4N, cu), *pL4N = peer_ptr(s.L4N, cu);
     for (int step = 0; step < lane_steps; ++step) {
@@ -870,7 +869,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       PHASE_T0(t_b1);
       cg::this_cluster().sync();
       PHASE_ADD(8, t_b1);
-      if (skin) skin_fire = skin_fires(s.red, peer_red, nth >> 5, a.neigh_margin);
+      if (skin) skin_fire = skin_fires(s.red, peer_ptr(s.red, cu), nth >> 5, a.neigh_margin);
       { double *t; t = s.X; s.X = s.XN; s.XN = t; t = s.Y; s.Y = s.YN; s.YN = t; t = s.Z; s.Z = s.ZN; s.ZN = t; }
       s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
       { V *t; t = s.A4; s.A4 = s.A4N; s.A4N = t; t = s.L4; s.L4 = s.L4N; s.L4N = t; }
