@@ -51,6 +51,8 @@ def parse():
                     help="override the workload's arithmetic (0 FP64, 1 mixed)")
     ap.add_argument("--ref-sample", type=int, default=None,
                     help="reference arm: MD steps per replica in one timed step (default: the CPU leg's sample)")
+    ap.add_argument("--refine", action="store_true",
+                    help="C5: refine the mixed-precision correlated noise once per step (tis_params.hi_refine)")
     ap.add_argument("--neighbor", default="cadence", choices=["cadence", "skin"],
                     help="neighbour rebuild rule: every 10 steps (the configs' cadence) or the reference's "
                          "Verlet skin (neigh_margin 8 A, time_integral.F90:57-93)")
@@ -395,6 +397,8 @@ def run_ours(args, rank, world, local_rank):
         par["n_step_neighbor"] = 0
     if args.precision is not None:
         par["precision"] = args.precision
+    if args.refine:
+        par["hi_refine"] = 1
     remd = args.workload == "c3"
     ladder = None
     if remd and world > 1:

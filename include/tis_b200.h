@@ -174,6 +174,10 @@ typedef struct tis_params {
   double pmf_rmin, pmf_rbin, pmf_rmax; /* first point, spacing, last point read */
   double pmf_rmerge;               /* pmf_merge: the switch from PMF to DH (simu_ele_set.F90:242-250) */
   const double *pmf_mg_p;          /* (pmf_nbin) PMF values; NULL when the system has no Mg */
+  int32_t hi_refine;               /* Brownian-HI, mixed precision: 1 refines the correlated noise once per step.
+                                      The step's factor L (split-TF32 tensor-core factorisation, kept in FP32)
+                                      has L L^T = D + E, |E| ~ 1e-7 |D|; the sample L xi - E L^-T xi / 2 has
+                                      covariance D + O(E^2).  E is formed in FP64 at each refresh. 0: off */
   int32_t i_hydro_tensor;          /* Brownian-HI diffusion tensor (HI_TENSOR, const_index.F90:39-45): 1 (or 0)
                                       RPY, 2 RPY_OVER, 3 ERMAK_OVER (radius of bead 1), 4 ZUK_RPY (per-bead
                                       radii), simu_hydro_tensors.F90:50-324 */

@@ -254,3 +254,65 @@ def test_bdhi_tensor_variant_trajectory(tis_lib, kind):
     assert np.abs(xr - s["xyz"]).max() > 1e-3
     assert np.abs(x - xr).max() < 1e-9
     eng.close()
+
+
+@pytest.mark.parametrize("refine", [0, 1])
+def test_bdhi_refined_noise_covariance(tis_lib, refine):
+    """hi_refine (mixed precision): the matrix M the step applies to the
+    noise, read column by column (unit noise vectors, no forces, one
+    refresh at x0), has ||M M^T - D|| / ||D|| ~ 1e-7 with the FP32 factor
+    alone and below 1e-10 with the refinement (D: the oracle's FP64 tensor
+    at x0)."""
+    s = dict(synth.bead_chain(100, 77))
+    s.update(nfene=0, nwca=0)                         # no forces: dx = sqrt(2 dt) M xi
+    par = synth.bdhi_params(precision=1, n_step_hydro=1 << 30, hi_refine=refine)
+    n = 3 * s["nmp"]
+    noise = np.zeros((n + 1, s["nmp"], 3))
+    for i in range(n):
+        noise[1 + i].reshape(-1)[i] = 1.0
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(noise)
+    eng.time_integral_pre()
+    rl2 = np.sqrt(2.0 * par["tstep"])
+    M = np.zeros((n, n))
+    x_prev = eng.get_state()[0].reshape(-1)
+    for i in range(n):
+        assert eng.step(1) >= 0
+        x = eng.get_state()[0].reshape(-1)
+        M[:, i] = (x - x_prev) / rl2
+        x_prev = x
+    eng.close()
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(s["xyz"][None])
+    D, _, rc = orc.hydro_tensors(cholesky=False)
+    cov = np.linalg.norm(M @ M.T - D) / np.linalg.norm(D)
+    if refine:
+        assert cov < 1e-10, cov
+    else:
+        assert 1e-9 < cov < 1e-5, cov
+    print({"refine": refine, "covariance_error": cov})
+
+
+def test_bdhi_refined_trajectory(tis_lib):
+    """The refined mixed-precision step against the FP64 restatement with
+    the same injected noise (the correction is of order 1e-7)."""
+    s = _variant_chain(1, 70, 19, nest=False)
+    par = synth.bdhi_params(precision=1, n_step_hydro=2, hi_refine=1)
+    nsteps = 6
+    noise = np.random.default_rng(12).normal(size=(nsteps + 1, s["nmp"], 3))
+    eng = Engine([s], par, [300.0])
+    eng.set_state(s["xyz"])
+    eng.set_noise(noise)
+    eng.time_integral_pre()
+    assert eng.step(nsteps) >= 0
+    x = eng.get_state()[0]
+    orc = Oracle(s, dict(par, precision=0), [300.0])
+    orc.set_state(s["xyz"][None])
+    orc.set_noise(noise.reshape(nsteps + 1, 1, s["nmp"], 3))
+    orc.time_integral_pre()
+    orc.step(nsteps)
+    xr = orc.get_state()[0].reshape(-1, 3)
+    assert np.abs(xr - s["xyz"]).max() > 1e-3
+    assert np.abs(x - xr).max() < 1e-6
+    eng.close()

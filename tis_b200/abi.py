@@ -78,7 +78,7 @@ class Params(C.Structure):
         ("hi_radius", C.c_double), ("n_step_hydro", C.c_int32),
         ("i_dtrna_model", C.c_int32), ("i_charge", C.c_int32), ("length_per_unit_P", C.c_double),
         ("pmf_nbin", C.c_int32), ("pmf_rmin", C.c_double), ("pmf_rbin", C.c_double), ("pmf_rmax", C.c_double),
-        ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p), ("i_hydro_tensor", C.c_int32),
+        ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p), ("hi_refine", C.c_int32), ("i_hydro_tensor", C.c_int32),
         ("launch_threads", C.c_int32), ("launch_group", C.c_int32), ("launch_ctas", C.c_int32),
         ("launch_noise_sweep", C.c_int32), ("launch_order", C.c_int32), ("launch_table", C.c_char_p),
     ]

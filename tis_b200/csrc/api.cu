@@ -176,6 +176,9 @@ struct tis_ctx {
   DBuf<int> bd_items;               // tensor-core update work items, per launch
   std::vector<int> bd_koff;
   DBuf<double> bd_W;
+  bool refine = false;               // Brownian-HI: refined noise (tis_params.hi_refine)
+  DBuf<double> bd_D64, bd_z;
+  DBuf<float> bd_E32, bd_W32;
 };
 
 namespace {
@@ -380,6 +383,8 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
   // the Brownian-HI path evaluates FENE and WCA records (the C5 bead chains):
   // no electrostatics, no DT15 or harmonic terms
   if (p.i_ele < TIS_ELE_NONE || p.i_ele > TIS_ELE_COULOMB) { tis_destroy(c); return TIS_E_ARG; }
+  if (p.hi_refine != 0 && p.hi_refine != 1) { tis_destroy(c); return TIS_E_ARG; }
+  c->refine = c->bdhi && p.precision == TIS_PREC_MIXED && p.hi_refine == 1;
   if (c->bdhi && (p.i_ele != TIS_ELE_NONE || !(p.viscosity > 0.0) || p.i_hydro_tensor < 0 || p.i_hydro_tensor > 4)) {
     tis_destroy(c);
     return TIS_E_UNSUPPORTED;
@@ -760,7 +765,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
   size_t mask_off = 0, slot_off = 0;
   long long mirror_off = 0;
   int hb_off = 0, site_off = 0, state_off = 0, ew_off = 0;
-  long long bd_off = 0, bdp_off = 0, bd32_off = 0;
+  long long bd_off = 0, bdp_off = 0, bd32_off = 0, bdw_off = 0;
   int lane = 0;
   for (int k = 0; k < ntop; ++k) {
     TopDesc &d = c->tops[k];
@@ -785,9 +790,11 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
       L.key_lane = grep;
       L.key_bead0 = lad ? grep * N : state_off;
       if (c->bdhi) bd_off += 9LL * N * N;
+      L.bdw0 = bdw_off;
       if (c->bdhi && p.precision == TIS_PREC_MIXED) {
         bdp_off += bd_plane_floats(N);
         bd32_off += 3LL * N * ((3LL * N + 3) / 4 * 4);
+        if (p.hi_refine == 1) bdw_off += (long long)((3 * N + 63) / 64) * 64 * 64;
       }
       state_off += N;
       mask_off += 2 * (size_t)N * ((N + 31) / 32);
@@ -979,6 +986,13 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
       if (items.empty()) items.push_back(0);
       CK(c->bd_items.upload(items));
       CK(c->bd_D32.alloc((size_t)bd32_off)); CK(c->bd_L32.alloc((size_t)bd32_off));
+      if (c->refine) {
+        // z of a lane is staged in one CTA's shared memory
+        if (3 * (size_t)maxN * 8 + 17 * 64 * 8 > 227 * 1024) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
+        CK(c->bd_D64.alloc((size_t)bd_off)); CK(c->bd_E32.alloc((size_t)bd32_off));
+        CK(c->bd_W32.alloc((size_t)bdw_off)); CK(c->bd_z.alloc(n3));
+        CK(cudaMemset(c->bd_E32.p, 0, (size_t)bd32_off * sizeof(float)));
+      }
       // padding columns and the factor's upper part are never written
       CK(cudaMemset(c->bd_D32.p, 0, (size_t)bd32_off * sizeof(float)));
       CK(cudaMemset(c->bd_L32.p, 0, (size_t)bd32_off * sizeof(float)));
@@ -1061,6 +1075,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
   c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->b_hrad.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
+  c->bd_D64.free(); c->bd_z.free(); c->bd_E32.free(); c->bd_W32.free();
   c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_items.free(); c->bd_D32.free(); c->bd_L32.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1209,6 +1224,8 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.bd_ptr = c->bd_ptr.p; a.bd_ent = c->bd_ent.p; a.fene_cls = c->fene_cls.p; a.wca_cls = c->wca_cls.p;
   a.bd_D = c->bd_D.p; a.bd_L = c->bd_L.p; a.bd_P = c->bd_P.p; a.bd_D32 = c->bd_D32.p; a.bd_L32 = c->bd_L32.p; a.bd_W = c->bd_W.p; a.bd_F = c->bd_F.p; a.bd_xi = c->bd_xi.p;
   a.not_spd = c->d_not_spd.p;
+  a.bd_refine = c->refine ? 1 : 0;
+  a.bd_D64 = c->bd_D64.p; a.bd_E32 = c->bd_E32.p; a.bd_W32 = c->bd_W32.p; a.bd_z = c->bd_z.p;
   a.hi_radius = p.hi_radius; a.viscosity = p.viscosity;
   a.i_hydro_tensor = p.i_hydro_tensor == 0 ? TIS_HI_RPY : p.i_hydro_tensor;
   a.b_hrad = c->b_hrad.p;
@@ -1549,10 +1566,10 @@ int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
       b.bd_istep = istep;
       b.noise_base = c->noise_base + (int)k;
       if ((istep - 1) % every == 0) {
-        c->launches += bd_refactor_launches(c->max_nmp, b.bd_tc != 0);
+        c->launches += bd_refactor_launches(c->max_nmp, b.bd_tc != 0) + (c->refine ? 2 : 0);
         CK(bd_refactor_launch(c->stream, b, c->max_nmp, c->bd_items.p, c->bd_koff.data()));
       }
-      c->launches += 3;
+      c->launches += 3 + (c->refine ? 1 : 0);
       CK(bd_step_launch(c->stream, b, c->max_nmp));
       c->bd_istep = istep;
     }

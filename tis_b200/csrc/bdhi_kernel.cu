@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(256) rpy_kernel(KArgs a) {
     for (int q = 0; q < 3; ++q) {
       if (a.bd_tc) a.bd_D32[L.bd32 + (size_t)(3 * i + p) * ((n + 3) & ~3) + 3 * j + q] = (float)blk[p][q];
       else a.bd_D[L.bd0 + row + q] = blk[p][q];
+      if (a.bd_refine) a.bd_D64[L.bd0 + row + q] = blk[p][q];
       if (3 * j + q <= 3 * i + p) Lm[row + q] = blk[p][q];
     }
   }
@@ -808,6 +809,18 @@ __global__ void __launch_bounds__(256) bd_update_kernel(KArgs a) {
   if (a.bd_tc) {
     const size_t row = L.bd32 + (size_t)k * ((n + 3) & ~3);
     row_dots32(a.bd_D32 + row, a.bd_L32 + row, F, xi, n, k, lid, df, dr);
+    if (a.bd_refine) {   // - (E z)_k / 2
+      const float4 *E4 = (const float4 *)(a.bd_E32 + row);
+      const double *z = a.bd_z + 3 * (size_t)L.state0;
+      const int n4 = n >> 2;
+      double ez = 0.0;
+      for (int g = lid; g < n4; g += 32) {
+        const float4 e = E4[g];
+        ez += (double)e.x * z[4 * g] + (double)e.y * z[4 * g + 1] + (double)e.z * z[4 * g + 2] + (double)e.w * z[4 * g + 3];
+      }
+      if (lid < n - 4 * n4) ez += (double)a.bd_E32[row + 4 * n4 + lid] * z[4 * n4 + lid];
+      dr -= 0.5 * ez;
+    }
   } else {
     const size_t row = L.bd0 + (size_t)k * n;
     row_dots64(a.bd_D + row, a.bd_L + row, F, xi, n, k, lid, df, dr);
@@ -825,6 +838,144 @@ __global__ void __launch_bounds__(256) bd_update_kernel(KArgs a) {
     a.pxyz[o] += dx;
     a.dxyz[o] += dx;
   }
+}
+
+// ------------------------------------------------------------ refinement
+// The mixed-precision step samples L xi with the FP32 factor L, whose
+// L L^T = D + E differs from D by the rounding of the split-TF32 updates and
+// of the FP32 copy (|E| ~ 1e-7 |D|).  M = L - E L^-T / 2 has
+// M M^T = D + E L^-T L^-1 E / 4, so the step samples M xi = L xi - E z / 2
+// with z = L^-T xi.  E is formed at each refresh with FP64 sums; z and E z
+// are FP32 data with FP64 sums (errors of order 1e-7 of a 1e-7 correction).
+constexpr int RT = 64;
+constexpr int RT_SMEM = 2 * RT * (RT + 1) * (int)sizeof(double);
+
+// grid (Tmax (Tmax + 1) / 2, nlane), 256 threads: tile (I, J), I >= J, of
+// E = L L^T - D in FP64, written to both halves of the FP32 E
+__global__ void __launch_bounds__(256) refine_residual_kernel(KArgs a) {
+  const int lane = blockIdx.y;
+  if (lane >= a.nlane) return;
+  const LaneDesc L = a.lanes[lane];
+  const int n = 3 * a.tops[L.top].nmp, T = (n + RT - 1) / RT, ld = (n + 3) & ~3;
+  const int p = blockIdx.x;
+  if (p >= T * (T + 1) / 2) return;
+  int I = (int)((sqrt(8.0 * p + 1.0) - 1.0) * 0.5);
+  while ((I + 1) * (I + 2) / 2 <= p) ++I;
+  while (I * (I + 1) / 2 > p) --I;
+  const int J = p - I * (I + 1) / 2;
+  extern __shared__ double rsm[];
+  double *As = rsm, *Bs = rsm + RT * (RT + 1);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) acc[q][w] = 0.0;
+  const float *Lm = a.bd_L32 + L.bd32;
+  for (int K = 0; K <= J; ++K) {   // L_IK L_JK^T; L is zero above its diagonal
+    for (int e = threadIdx.x; e < RT * RT; e += 256) {
+      const int r = e / RT, c = e - r * RT, gc = K * RT + c, ra = I * RT + r, rb = J * RT + r;
+      As[r * (RT + 1) + c] = (ra < n && gc < n) ? (double)Lm[(size_t)ra * ld + gc] : 0.0;
+      Bs[r * (RT + 1) + c] = (rb < n && gc < n) ? (double)Lm[(size_t)rb * ld + gc] : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < RT; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) { av[q] = As[(ty * 4 + q) * (RT + 1) + k]; bv[q] = Bs[(tx * 4 + q) * (RT + 1) + k]; }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) acc[q][w] = fma(av[q], bv[w], acc[q][w]);
+    }
+    __syncthreads();
+  }
+  const double *D = a.bd_D64 + L.bd0;
+  float *E = a.bd_E32 + L.bd32;
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int row = I * RT + ty * 4 + q, col = J * RT + tx * 4 + w;
+      if (row < n && col < n) {
+        const float e = (float)(acc[q][w] - D[(size_t)row * n + col]);
+        E[(size_t)row * ld + col] = e;
+        if (I != J) E[(size_t)col * ld + row] = e;
+      }
+    }
+}
+
+// grid (Tmax, nlane), 64 threads: W_b = inverse of the diagonal tile L_bb of
+// the FP32 factor (FP64 forward substitution, one column per thread; rows
+// past n act as the identity)
+__global__ void __launch_bounds__(64) refine_inverse_kernel(KArgs a) {
+  const int lane = blockIdx.y;
+  if (lane >= a.nlane) return;
+  const LaneDesc L = a.lanes[lane];
+  const int n = 3 * a.tops[L.top].nmp, T = (n + RT - 1) / RT, ld = (n + 3) & ~3;
+  const int b = blockIdx.x;
+  if (b >= T) return;
+  extern __shared__ double inv_buf[];   // L_bb, then its inverse (RT_SMEM bytes)
+  double *Lt = inv_buf, *X = inv_buf + RT * (RT + 1);
+  const float *Lm = a.bd_L32 + L.bd32;
+  const int c = threadIdx.x;
+  for (int r = 0; r < RT; ++r) {
+    const int gr = b * RT + r, gc = b * RT + c;
+    Lt[r * (RT + 1) + c] = (gr < n && gc < n) ? (double)Lm[(size_t)gr * ld + gc] : (r == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  for (int i = 0; i < RT; ++i) {
+    double x = 0.0;
+    if (i >= c) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) s -= Lt[i * (RT + 1) + k] * X[k * (RT + 1) + c];
+      x = s / Lt[i * (RT + 1) + i];
+    }
+    X[i * (RT + 1) + c] = x;
+  }
+  float *W = a.bd_W32 + L.bdw0 + (size_t)b * RT * RT;
+  for (int i = 0; i < RT; ++i) W[i * RT + c] = (float)X[i * (RT + 1) + c];
+}
+
+// grid nlane, 1024 threads: z = L^-T xi by blocked back substitution from
+// the last tile: rhs_b = xi_b - sum over the rows below of L^T z, then
+// z_b = W_b^T rhs_b
+constexpr int TRSV_THREADS = 1024;
+__global__ void __launch_bounds__(TRSV_THREADS) refine_trsv_kernel(KArgs a) {
+  const int lane = blockIdx.x;
+  if (lane >= a.nlane) return;
+  const LaneDesc L = a.lanes[lane];
+  const int n = 3 * a.tops[L.top].nmp, T = (n + RT - 1) / RT, ld = (n + 3) & ~3;
+  extern __shared__ double trsm_buf[];
+  double *zs = trsm_buf;                         // n
+  double *part = trsm_buf + ((n + 1) & ~1);      // 16 x 64
+  double *rhs = part + 16 * RT;             // 64
+  const float *Lm = a.bd_L32 + L.bd32;
+  const double *xi = a.bd_xi + 3 * (size_t)L.state0;
+  const int c = threadIdx.x & (RT - 1), g = threadIdx.x >> 6;
+  for (int b = T - 1; b >= 0; --b) {
+    const int j = b * RT + c;
+    double sacc = 0.0;
+    if (j < n)
+      for (int r = (b + 1) * RT + g; r < n; r += 16) sacc += (double)Lm[(size_t)r * ld + j] * zs[r];
+    part[g * RT + c] = sacc;
+    __syncthreads();
+    if (threadIdx.x < RT) {
+      double t = 0.0;
+      for (int q = 0; q < 16; ++q) t += part[q * RT + c];
+      rhs[c] = (j < n) ? xi[j] - t : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x < RT) {
+      const float *W = a.bd_W32 + L.bdw0 + (size_t)b * RT * RT;
+      double z = 0.0;
+      for (int i = c; i < RT; ++i) z += (double)W[i * RT + c] * rhs[i];
+      if (j < n) zs[j] = z;
+    }
+    __syncthreads();
+  }
+  double *zo = a.bd_z + 3 * (size_t)L.state0;
+  for (int k = threadIdx.x; k < n; k += TRSV_THREADS) zo[k] = zs[k];
 }
 
 // grid (ceil(maxN / 8), nlane), 256 threads: one warp per bead sums its FENE
@@ -955,6 +1106,15 @@ cudaError_t bd_refactor_launch(cudaStream_t st, KArgs a, int max_nmp, const int 
     a.bd_kpanel = T - 1;
     if (T > 1) chol_diag_kernel<<<a.nlane, 256, 0, st>>>(a);
   }
+  if (a.bd_refine) {
+    e = cudaFuncSetAttribute(refine_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, RT_SMEM);
+    if (e != cudaSuccess) return e;
+    const int TR = (3 * max_nmp + RT - 1) / RT;
+    refine_residual_kernel<<<dim3(TR * (TR + 1) / 2, a.nlane), 256, RT_SMEM, st>>>(a);
+    e = cudaFuncSetAttribute(refine_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, RT_SMEM);
+    if (e != cudaSuccess) return e;
+    refine_inverse_kernel<<<dim3(TR, a.nlane), RT, RT_SMEM, st>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -974,6 +1134,12 @@ long long bd_plane_floats(int nmp) {
 
 cudaError_t bd_step_launch(cudaStream_t st, const KArgs &a, int max_nmp) {
   bd_noise_kernel<<<dim3((max_nmp + 127) / 128, a.nlane), 128, 0, st>>>(a);
+  if (a.bd_refine) {
+    const size_t sm = (size_t)((3 * max_nmp + 1) & ~1) * sizeof(double) + (16 * RT + RT) * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(refine_trsv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    refine_trsv_kernel<<<a.nlane, TRSV_THREADS, sm, st>>>(a);
+  }
   bd_update_kernel<<<dim3((3 * max_nmp + 7) / 8, a.nlane), 256, 0, st>>>(a);
   bd_force_kernel<<<dim3((max_nmp + 7) / 8, a.nlane), 256, 0, st>>>(a);
   return cudaGetLastError();

@@ -61,6 +61,7 @@ struct LaneDesc {
   long long bd0;    // Brownian-HI: first element of this lane's (3N)^2 diffusion / Cholesky matrices
   long long bdp0;   // Brownian-HI, tensor cores: first float of this lane's TF32 panel planes
   long long bd32;   // Brownian-HI, mixed precision: first float of this lane's FP32 D and L (rows padded to 4)
+  long long bdw0;   // Brownian-HI refinement: first float of this lane's inverses of the diagonal tiles of L
   int key_lane;     // counter-based noise and uniforms: the replica's key (its global replica number - 1)
   int key_bead0;    // and the counter of its first bead (so a replica draws the same numbers in any context)
 };
@@ -133,6 +134,13 @@ struct KArgs {
   int *not_spd;                    // per lane: a Cholesky pivot was <= 0
   double hi_radius, viscosity;
   int i_hydro_tensor;              // HI_TENSOR: 1 RPY, 2 RPY_OVER, 3 ERMAK_OVER, 4 ZUK_RPY
+  // refinement of the mixed-precision noise: E = L L^T - D (FP32 L of the step, FP64 sums), W = inverses
+  // of the diagonal 64 x 64 tiles of L, z = L^-T xi; the step adds -E z / 2 to L xi
+  int bd_refine;
+  double *bd_D64;                  // per lane (3N x 3N, row-major): D in FP64 (refinement)
+  float *bd_E32;                   // per lane: E, rows padded like bd_D32
+  float *bd_W32;                   // per lane: (T, 64, 64) inverses of the diagonal tiles
+  double *bd_z;                    // per lane (3N): z
   const double *b_hrad;            // per bead: hydrodynamic radius (ZUK_RPY; the others take bead 1's)
   double boltz, pi;                // BOLTZ_KCAL_MOL and F_PI of const_physical.F90
   long long bd_istep;              // step being taken (1-based)

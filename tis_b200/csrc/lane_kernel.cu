@@ -618,10 +618,27 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         else if (ci == 2 && cj == 2) dij = dist_rr;
         else dij = bi.x + bj.x;
         if (r2 > dij * dij) return;
-        const Real rinv = rsq<Real>(r2);
-        const Real dist = r2 * rinv;
+        Real rinv, dr;
+        if constexpr (sizeof(Real) == 4) {
+          // inside contact the potential is steep and dr = dist + a - d_ij
+          // a small difference: the distance and dr in FP64 from the exact
+          // hi + lo difference, so their rounding is not amplified
+          const double ex = (double)sx + ((double)lj.x - (double)li.x);
+          const double ey = (double)sy + ((double)lj.y - (double)li.y);
+          const double ez = (double)sz + ((double)lj.z - (double)li.z);
+          const double d64 = sqrt(ex * ex + ey * ey + ez * ez);
+          double dij64;
+          if (a.dt19) dij64 = (ti == 3 && tj == 3) ? a.exv_dist : (double)bi.x + (double)bj.x;
+          else if ((ti == 2 && tj == 4) || (ti == 4 && tj == 2)) dij64 = a.exv_dist_PS;
+          else if (ci == 2 && cj == 2) dij64 = a.exv_dist;
+          else dij64 = (double)bi.x + (double)bj.x;
+          rinv = (Real)(1.0 / d64);
+          dr = (Real)(d64 + a.exv_adjust - dij64);
+        } else {
+          rinv = rsq<Real>(r2);
+          dr = r2 * rinv + ra - dij;
+        }
         const Real coef = bi.y * bj.y;
-        const Real dr = dist + ra - dij;
         const Real ro2 = fdiv(ra2, dr * dr);
         const Real ro4 = ro2 * ro2, ro8 = ro4 * ro4, ro14 = ro2 * ro4 * ro8;
         Real f = fabs((Real)12 * coef * (ro14 - ro8) * dr * inv_ra2 * rinv);
