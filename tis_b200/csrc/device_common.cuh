@@ -342,10 +342,22 @@ __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   }
   R3<Real> v21 = dvec(s, m[0], m[1]), v32 = dvec(s, m[1], m[2]);
   Real c11 = dot(v21, v21), c22 = dot(v32, v32), c21 = dot(v32, v21);
-  Real co = -c21 * frsq(c11 * c22);
-  if (co > (Real)1) co = 1; else if (co < (Real)-1) co = -1;
-  Real dba = acos(co) - (Real)ldro(a.ba_nat + T.ba0 + k);
-  Real t3 = c11 * c22 - c21 * c21;
+  Real th, t3;
+  if constexpr (sizeof(Real) == 4) {
+    // FP32: the angle as atan2(|v21 x v32|, -v21.v32) and t3 = |v21 x v32|^2
+    // (= c11 c22 - c21^2), the same quantities as the reference's acos of the
+    // clamped cosine, without the rounding that acos and the difference
+    // amplify when the angle nears 0 or 180 degrees
+    const R3<Real> cr = crs(v21, v32);
+    t3 = dot(cr, cr);
+    th = atan2(sqrt(t3), -c21);
+  } else {
+    Real co = -c21 * frsq(c11 * c22);
+    if (co > (Real)1) co = 1; else if (co < (Real)-1) co = -1;
+    th = acos(co);
+    t3 = c11 * c22 - c21 * c21;
+  }
+  Real dba = th - (Real)ldro(a.ba_nat + T.ba0 + k);
   if (t3 <= (Real)1) t3 = 1;
   Real f = (Real)2 * cf * dba * frsq(t3);
   Real a1 = fdiv(c21, c11), a2 = fdiv(c21, c22);
@@ -406,12 +418,21 @@ __device__ void term_tstack(const KArgs &a, const TopDesc &T, const Smem<Real> &
   const Real v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
 #pragma unroll
   for (int q = 0; q < 3; ++q) { fr[2][q] = 0; fr[3][q] = 0; fr[4][q] = 0; fr[5][q] = 0; }
-  // angle 3-1=2
+  // angle 3-1=2 (FP32: from |v13 x v12| as in term_angle)
   {
-    Real co = fdiv(d1213, a13 * a12);
-    co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
-    d = acos(co) - (Real)nat[1];
-    const Real pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
+    Real th, sn2;
+    if constexpr (sizeof(Real) == 4) {
+      const R3<Real> cr = crs(v13, v12);
+      sn2 = dot(cr, cr);
+      th = atan2(sqrt(sn2), d1213);
+    } else {
+      Real co = fdiv(d1213, a13 * a12);
+      co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
+      th = acos(co);
+      sn2 = d1313 * d1212 - d1213 * d1213;
+    }
+    d = th - (Real)nat[1];
+    const Real pre = (Real)2 * (Real)cf[2] * d * frsq(sn2);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const Real fi = pre * (v12a[q] - o1213_1313 * v13a[q]), fk = pre * (v13a[q] - o1213_1212 * v12a[q]);
@@ -421,10 +442,19 @@ __device__ void term_tstack(const KArgs &a, const TopDesc &T, const Smem<Real> &
   }
   // angle 1=2-4
   {
-    Real co = fdiv(d1242, a12 * a42);
-    co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
-    d = acos(co) - (Real)nat[2];
-    const Real pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
+    Real th, sn2;
+    if constexpr (sizeof(Real) == 4) {
+      const R3<Real> cr = crs(v12, v42);
+      sn2 = dot(cr, cr);
+      th = atan2(sqrt(sn2), d1242);
+    } else {
+      Real co = fdiv(d1242, a12 * a42);
+      co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
+      th = acos(co);
+      sn2 = d1212 * d4242 - d1242 * d1242;
+    }
+    d = th - (Real)nat[2];
+    const Real pre = (Real)2 * (Real)cf[3] * d * frsq(sn2);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const Real fi = -pre * (v42a[q] - o1242_1212 * v12a[q]), fk = -pre * (v12a[q] - o1242_4242 * v42a[q]);
@@ -598,11 +628,23 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
   Real d4246o4242 = fdiv(d4246, d4242), d1242o4242 = fdiv(d1242, d4242), d1353o1313 = fdiv(d1353, d1313);
   const Real MAXC = (Real)a.max_abscos;
   const Real v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
-  // angle 3-1=2
+  // angle 3-1=2; the |cos| cap replaces the sine by that of the cap
+  // (FP32: the angle from |v12 x v13| and the sine squared without the
+  // difference, as in term_angle)
   Real cos312 = fdiv(d1213, a13 * a12);
-  if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
-  d = acos(cos312) - (Real)nat[1];
-  Real pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
+  const Real sin2cap = (Real)1 - MAXC * MAXC;
+  Real pre;
+  if constexpr (sizeof(Real) == 4) {
+    const R3<Real> cr = crs(v12, v13);
+    const Real sn2 = dot(cr, cr);
+    d = atan2(sqrt(sn2), d1213) - (Real)nat[1];
+    pre = (Real)2 * (Real)cf[2] * d * frsq(fabs(cos312) > MAXC ? d1313 * d1212 * sin2cap : sn2);
+    if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
+  } else {
+    if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
+    d = acos(cos312) - (Real)nat[1];
+    pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
+  }
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     Real fi = pre * (v12a[q] - d1213o1313 * v13a[q]);
@@ -612,9 +654,17 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
   ex -= (Real)cf[2] * d * d;
   // angle 1=2-4
   Real cos124 = fdiv(d1242, a12 * a42);
-  if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
-  d = acos(cos124) - (Real)nat[2];
-  pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
+  if constexpr (sizeof(Real) == 4) {
+    const R3<Real> cr = crs(v42, v12);
+    const Real sn2 = dot(cr, cr);
+    d = atan2(sqrt(sn2), d1242) - (Real)nat[2];
+    pre = (Real)2 * (Real)cf[3] * d * frsq(fabs(cos124) > MAXC ? d1212 * d4242 * sin2cap : sn2);
+    if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
+  } else {
+    if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
+    d = acos(cos124) - (Real)nat[2];
+    pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
+  }
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     Real fi = -pre * (v42a[q] - d1242o1212 * v12a[q]);
