@@ -879,10 +879,12 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(KArgs a) {
       Bs[r * (RT + 1) + c] = (rb < n && gc < n) ? (double)Lm[(size_t)rb * ld + gc] : 0.0;
     }
     __syncthreads();
+    // thread (ty, tx): rows ty * 4 + q, columns tx + 16 w (consecutive tx
+    // read rows 65 doubles apart: no shared-memory bank conflicts)
     for (int k = 0; k < RT; ++k) {
       double av[4], bv[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) { av[q] = As[(ty * 4 + q) * (RT + 1) + k]; bv[q] = Bs[(tx * 4 + q) * (RT + 1) + k]; }
+      for (int q = 0; q < 4; ++q) { av[q] = As[(ty * 4 + q) * (RT + 1) + k]; bv[q] = Bs[(tx + 16 * q) * (RT + 1) + k]; }
 #pragma unroll
       for (int q = 0; q < 4; ++q)
 #pragma unroll
@@ -896,7 +898,7 @@ __global__ void __launch_bounds__(256) refine_residual_kernel(KArgs a) {
   for (int q = 0; q < 4; ++q)
 #pragma unroll
     for (int w = 0; w < 4; ++w) {
-      const int row = I * RT + ty * 4 + q, col = J * RT + tx * 4 + w;
+      const int row = I * RT + ty * 4 + q, col = J * RT + tx + 16 * w;
       if (row < n && col < n) {
         const float e = (float)(acc[q][w] - D[(size_t)row * n + col]);
         E[(size_t)row * ld + col] = e;

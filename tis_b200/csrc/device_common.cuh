@@ -342,18 +342,18 @@ __device__ void term_angle(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   }
   R3<Real> v21 = dvec(s, m[0], m[1]), v32 = dvec(s, m[1], m[2]);
   Real c11 = dot(v21, v21), c22 = dot(v32, v32), c21 = dot(v32, v21);
+  Real co = -c21 * frsq(c11 * c22);
+  if (co > (Real)1) co = 1; else if (co < (Real)-1) co = -1;
   Real th, t3;
-  if constexpr (sizeof(Real) == 4) {
-    // FP32: the angle as atan2(|v21 x v32|, -v21.v32) and t3 = |v21 x v32|^2
-    // (= c11 c22 - c21^2), the same quantities as the reference's acos of the
-    // clamped cosine, without the rounding that acos and the difference
-    // amplify when the angle nears 0 or 180 degrees
+  if (sizeof(Real) == 4 && fabs(co) > (Real)0.99) {
+    // FP32 near 0 or 180 degrees: the angle as atan2(|v21 x v32|, -v21.v32)
+    // and t3 = |v21 x v32|^2 (= c11 c22 - c21^2), the same quantities as the
+    // reference's acos of the cosine, without the rounding that acos and the
+    // difference amplify there (up to 1e-4 rad at 179.97 degrees)
     const R3<Real> cr = crs(v21, v32);
     t3 = dot(cr, cr);
     th = atan2(sqrt(t3), -c21);
   } else {
-    Real co = -c21 * frsq(c11 * c22);
-    if (co > (Real)1) co = 1; else if (co < (Real)-1) co = -1;
     th = acos(co);
     t3 = c11 * c22 - c21 * c21;
   }
@@ -387,137 +387,199 @@ __device__ __forceinline__ bool stack_excluded(const KArgs &a, const TopDesc &T,
   return false;
 }
 
-// force_dtrna_stack_nlocal.F90:60-263: tertiary stack k into its six slots
+// force_dtrna_stack_nlocal.F90:60-263: tertiary stack k into its six slots,
+// FP64 in both paths for the reason given at term_stack
 template <typename Real>
 __device__ void term_tstack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k) {
   const int *m = a.tst_idx + 6 * (size_t)(T.tst0 + k);
   const double *nat = a.tst_nat + 6 * (size_t)(T.tst0 + k);
   const double *cf = a.tst_coef + 7 * (size_t)(T.tst0 + k);
+  typedef double W;   // working precision of this term
   auto dv = [&](int p, int q) {   // x_p - x_q (pxyz + minimum image when periodic)
     double w0 = s.PX[m[p]] - s.PX[m[q]], w1 = s.PY[m[p]] - s.PY[m[q]], w2 = s.PZ[m[p]] - s.PZ[m[q]];
     if (a.periodic) { pb1(w0, a.psize[0], a.psizeh[0]); pb1(w1, a.psize[1], a.psizeh[1]); pb1(w2, a.psize[2], a.psizeh[2]); }
-    return R3<Real>{(Real)w0, (Real)w1, (Real)w2};
+    return R3<W>{w0, w1, w2};
   };
-  const R3<Real> v12 = dv(0, 1), v13 = dv(0, 2), v53 = dv(4, 2), v42 = dv(3, 1), v46 = dv(3, 5);
-  const Real d1212 = dot(v12, v12), d1313 = dot(v13, v13), d4242 = dot(v42, v42);
-  const Real a12 = sqrt(d1212), a13 = sqrt(d1313), a42 = sqrt(d4242);
-  const Real d1213 = dot(v13, v12), d1242 = dot(v12, v42), d4246 = dot(v42, v46), d1353 = dot(v13, v53);
-  const Real o1213_1212 = fdiv(d1213, d1212), o1213_1313 = fdiv(d1213, d1313);
-  const Real o1242_1212 = fdiv(d1242, d1212), o4246_4242 = fdiv(d4246, d4242);
-  const Real o1242_4242 = fdiv(d1242, d4242), o1353_1313 = fdiv(d1353, d1313);
-  Real fr[6][3];
-  Real ediv = 1;
+  const R3<W> v12 = dv(0, 1), v13 = dv(0, 2), v53 = dv(4, 2), v42 = dv(3, 1), v46 = dv(3, 5);
+  const W d1212 = dot(v12, v12), d1313 = dot(v13, v13), d4242 = dot(v42, v42);
+  const W a12 = sqrt(d1212), a13 = sqrt(d1313), a42 = sqrt(d4242);
+  const W d1213 = dot(v13, v12), d1242 = dot(v12, v42), d4246 = dot(v42, v46), d1353 = dot(v13, v53);
+  const W o1213_1212 = fdiv<W>(d1213, d1212), o1213_1313 = fdiv<W>(d1213, d1313);
+  const W o1242_1212 = fdiv<W>(d1242, d1212), o4246_4242 = fdiv<W>(d4246, d4242);
+  const W o1242_4242 = fdiv<W>(d1242, d4242), o1353_1313 = fdiv<W>(d1353, d1313);
+  W fr[6][3];
+  W ediv = 1;
   // distance 1=2
-  Real d = a12 - (Real)nat[0];
-  ediv += (Real)cf[1] * d * d;
+  W d = a12 - (W)nat[0];
+  ediv += (W)cf[1] * d * d;
   {
-    const Real g = fdiv((Real)2 * (Real)cf[1] * d, a12);
+    const W g = fdiv<W>((W)2 * (W)cf[1] * d, a12);
     fr[0][0] = g * v12.x; fr[0][1] = g * v12.y; fr[0][2] = g * v12.z;
     fr[1][0] = -fr[0][0]; fr[1][1] = -fr[0][1]; fr[1][2] = -fr[0][2];
   }
-  const Real v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
+  const W v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
 #pragma unroll
   for (int q = 0; q < 3; ++q) { fr[2][q] = 0; fr[3][q] = 0; fr[4][q] = 0; fr[5][q] = 0; }
-  // angle 3-1=2 (FP32: from |v13 x v12| as in term_angle)
+  // angle 3-1=2
   {
-    Real th, sn2;
-    if constexpr (sizeof(Real) == 4) {
-      const R3<Real> cr = crs(v13, v12);
-      sn2 = dot(cr, cr);
-      th = atan2(sqrt(sn2), d1213);
-    } else {
-      Real co = fdiv(d1213, a13 * a12);
-      co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
-      th = acos(co);
-      sn2 = d1313 * d1212 - d1213 * d1213;
-    }
-    d = th - (Real)nat[1];
-    const Real pre = (Real)2 * (Real)cf[2] * d * frsq(sn2);
+    W co = fdiv<W>(d1213, a13 * a12);
+    co = co > (W)1 ? (W)1 : (co < (W)-1 ? (W)-1 : co);
+    const W th = acos(co), sn2 = d1313 * d1212 - d1213 * d1213;
+    d = th - (W)nat[1];
+    const W pre = (W)2 * (W)cf[2] * d * frsq<W>(sn2);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const Real fi = pre * (v12a[q] - o1213_1313 * v13a[q]), fk = pre * (v13a[q] - o1213_1212 * v12a[q]);
+      const W fi = pre * (v12a[q] - o1213_1313 * v13a[q]), fk = pre * (v13a[q] - o1213_1212 * v12a[q]);
       fr[2][q] += fi; fr[1][q] += fk; fr[0][q] -= fi + fk;
     }
-    ediv += (Real)cf[2] * d * d;
+    ediv += (W)cf[2] * d * d;
   }
   // angle 1=2-4
   {
-    Real th, sn2;
-    if constexpr (sizeof(Real) == 4) {
-      const R3<Real> cr = crs(v12, v42);
-      sn2 = dot(cr, cr);
-      th = atan2(sqrt(sn2), d1242);
-    } else {
-      Real co = fdiv(d1242, a12 * a42);
-      co = co > (Real)1 ? (Real)1 : (co < (Real)-1 ? (Real)-1 : co);
-      th = acos(co);
-      sn2 = d1212 * d4242 - d1242 * d1242;
-    }
-    d = th - (Real)nat[2];
-    const Real pre = (Real)2 * (Real)cf[3] * d * frsq(sn2);
+    W co = fdiv<W>(d1242, a12 * a42);
+    co = co > (W)1 ? (W)1 : (co < (W)-1 ? (W)-1 : co);
+    const W th = acos(co), sn2 = d1212 * d4242 - d1242 * d1242;
+    d = th - (W)nat[2];
+    const W pre = (W)2 * (W)cf[3] * d * frsq<W>(sn2);
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
-      const Real fi = -pre * (v42a[q] - o1242_1212 * v12a[q]), fk = -pre * (v12a[q] - o1242_4242 * v42a[q]);
+      const W fi = -pre * (v42a[q] - o1242_1212 * v12a[q]), fk = -pre * (v12a[q] - o1242_4242 * v42a[q]);
       fr[0][q] += fi; fr[3][q] += fk; fr[1][q] -= fi + fk;
     }
-    ediv += (Real)cf[3] * d * d;
+    ediv += (W)cf[3] * d * d;
   }
   // dihedral 4-2=1=3
-  const R3<Real> c4212 = crs(v42, v12), c1213 = crs(v12, v13);
-  const Real c4212_2 = dot(c4212, c4212), c1213_2 = dot(c1213, c1213);
+  const R3<W> c4212 = crs(v42, v12), c1213 = crs(v12, v13);
+  const W c4212_2 = dot(c4212, c4212), c1213_2 = dot(c1213, c1213);
   {
-    d = wrap_pi(atan2(dot(v42, c1213) * a12, dot(c4212, c1213)) - (Real)nat[3]);
-    ediv += (Real)cf[4] * d * d;
-    const Real pre = (Real)2 * (Real)cf[4] * d * a12;
-    const Real gi = fdiv(pre, c4212_2), gl = -fdiv(pre, c1213_2);
-    const Real fi[3] = {gi * c4212.x, gi * c4212.y, gi * c4212.z}, fl[3] = {gl * c1213.x, gl * c1213.y, gl * c1213.z};
+    d = wrap_pi(atan2(dot(v42, c1213) * a12, dot(c4212, c1213)) - (W)nat[3]);
+    ediv += (W)cf[4] * d * d;
+    const W pre = (W)2 * (W)cf[4] * d * a12;
+    const W gi = fdiv<W>(pre, c4212_2), gl = -fdiv<W>(pre, c1213_2);
+    const W fi[3] = {gi * c4212.x, gi * c4212.y, gi * c4212.z}, fl[3] = {gl * c1213.x, gl * c1213.y, gl * c1213.z};
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       fr[3][q] += fi[q];
-      fr[1][q] += ((Real)-1 + o1242_1212) * fi[q] - o1213_1212 * fl[q];
-      fr[0][q] += ((Real)-1 + o1213_1212) * fl[q] - o1242_1212 * fi[q];
+      fr[1][q] += ((W)-1 + o1242_1212) * fi[q] - o1213_1212 * fl[q];
+      fr[0][q] += ((W)-1 + o1213_1212) * fl[q] - o1242_1212 * fi[q];
       fr[2][q] += fl[q];
     }
   }
   // dihedral 5-3-1=2
   {
-    const R3<Real> mm = crs(v53, v13), nn{-c1213.x, -c1213.y, -c1213.z};
-    d = wrap_pi(atan2(dot(v53, nn) * a13, dot(mm, nn)) - (Real)nat[4]);
-    ediv += (Real)cf[5] * d * d;
-    const Real pre = (Real)2 * (Real)cf[5] * d * a13;
-    const Real gi = fdiv(pre, dot(mm, mm)), gl = -fdiv(pre, c1213_2);
-    const Real fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
+    const R3<W> mm = crs(v53, v13), nn{-c1213.x, -c1213.y, -c1213.z};
+    d = wrap_pi(atan2(dot(v53, nn) * a13, dot(mm, nn)) - (W)nat[4]);
+    ediv += (W)cf[5] * d * d;
+    const W pre = (W)2 * (W)cf[5] * d * a13;
+    const W gi = fdiv<W>(pre, dot(mm, mm)), gl = -fdiv<W>(pre, c1213_2);
+    const W fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       fr[4][q] += fi[q];
-      fr[2][q] += ((Real)-1 + o1353_1313) * fi[q] - o1213_1313 * fl[q];
-      fr[0][q] += ((Real)-1 + o1213_1313) * fl[q] - o1353_1313 * fi[q];
+      fr[2][q] += ((W)-1 + o1353_1313) * fi[q] - o1213_1313 * fl[q];
+      fr[0][q] += ((W)-1 + o1213_1313) * fl[q] - o1353_1313 * fi[q];
       fr[1][q] += fl[q];
     }
   }
   // dihedral 1=2-4-6
   {
-    const R3<Real> mm{-c4212.x, -c4212.y, -c4212.z}, nn = crs(v42, v46);
-    d = wrap_pi(atan2(dot(v12, nn) * a42, dot(mm, nn)) - (Real)nat[5]);
-    ediv += (Real)cf[6] * d * d;
-    const Real pre = (Real)2 * (Real)cf[6] * d * a42;
-    const Real gi = fdiv(pre, c4212_2), gl = -fdiv(pre, dot(nn, nn));
-    const Real fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
+    const R3<W> mm{-c4212.x, -c4212.y, -c4212.z}, nn = crs(v42, v46);
+    d = wrap_pi(atan2(dot(v12, nn) * a42, dot(mm, nn)) - (W)nat[5]);
+    ediv += (W)cf[6] * d * d;
+    const W pre = (W)2 * (W)cf[6] * d * a42;
+    const W gi = fdiv<W>(pre, c4212_2), gl = -fdiv<W>(pre, dot(nn, nn));
+    const W fi[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, fl[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       fr[0][q] += fi[q];
-      fr[1][q] += ((Real)-1 + o1242_4242) * fi[q] - o4246_4242 * fl[q];
-      fr[3][q] += ((Real)-1 + o4246_4242) * fl[q] - o1242_4242 * fi[q];
+      fr[1][q] += ((W)-1 + o1242_4242) * fi[q] - o4246_4242 * fl[q];
+      fr[3][q] += ((W)-1 + o4246_4242) * fl[q] - o1242_4242 * fi[q];
       fr[5][q] += fl[q];
     }
   }
-  const Real pre = (Real)(cf[0] / ((double)ediv * (double)ediv));
+  const W pre = cf[0] / (ediv * ediv);
   const size_t sb = T.slot_tst + 6 * (size_t)k;
 #pragma unroll
-  for (int p = 0; p < 6; ++p) put_slot<Real>(slots, sb + p, m[p], pre * fr[p][0], pre * fr[p][1], pre * fr[p][2]);
+  for (int p = 0; p < 6; ++p)
+    put_slot<Real>(slots, sb + p, m[p], (Real)(pre * fr[p][0]), (Real)(pre * fr[p][1]), (Real)(pre * fr[p][2]));
 }
 
-// force_dtrna_stack.F90:54-165 (skipped when st_status is off)
+// force_dtrna_stack.F90:54-165 in FP64 whatever Real is, for a stack whose
+// dihedrals run through a nearly straight triple: their cross products of
+// nearly parallel bond vectors, and force terms that cancel, are resolved by
+// FP32 only to ~1e-4 (measured on a C4 chain).
+template <typename Real>
+__device__ void term_stack64(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, double u0) {
+  const int *mp = a.st_idx + 7 * (size_t)(T.st0 + k);
+  const int m[7] = {ldro(mp), ldro(mp + 1), ldro(mp + 2), ldro(mp + 3), ldro(mp + 4), ldro(mp + 5), ldro(mp + 6)};
+  const double *natp = a.st_nat + 3 * (size_t)(T.st0 + k), *cfp = a.st_coef + 3 * (size_t)(T.st0 + k);
+  const double nat[3] = {ldro(natp), ldro(natp + 1), ldro(natp + 2)};
+  const double cf[3] = {ldro(cfp), ldro(cfp + 1), ldro(cfp + 2)};
+  typedef double W;   // working precision of this term
+  auto dv = [&](int i, int j) {   // x_j - x_i (unwrapped), FP64
+    return R3<W>{s.X[j] - s.X[i], s.Y[j] - s.Y[i], s.Z[j] - s.Z[i]};
+  };
+  R3<W> v21 = dv(m[0], m[1]);
+  R3<W> v34 = dv(m[3], m[2]);
+  R3<W> v54 = dv(m[3], m[4]);
+  R3<W> v56 = dv(m[5], m[4]);
+  R3<W> v76 = dv(m[5], m[6]);
+  const W k1 = cf[0], k2 = cf[1], k3 = cf[2];
+  W fr[7][3];
+  W ediv = 1;
+  W dist = sqrt(dot(v21, v21));
+  W dd = dist - (W)nat[0];
+  ediv += k1 * dd * dd;
+  W g = (W)2 * k1 * fdiv<W>(dd, dist);
+  fr[0][0] = -g * v21.x; fr[0][1] = -g * v21.y; fr[0][2] = -g * v21.z;
+  fr[1][0] = g * v21.x; fr[1][1] = g * v21.y; fr[1][2] = g * v21.z;
+  R3<W> mm = crs(v34, v54), nn = crs(v54, v56);
+  W dmm = dot(mm, mm), dnn = dot(nn, nn);
+  W d5454 = dot(v54, v54), abs54 = sqrt(d5454);
+  W d5654 = dot(v56, v54);
+  W d3454o = fdiv<W>(dot(v34, v54), d5454), d5654o = fdiv<W>(d5654, d5454);
+  W dih = atan2(dot(v34, nn) * abs54, dot(mm, nn));
+  W d = wrap_pi(dih - (W)nat[1]);
+  ediv += k2 * d * d;
+  W gi = fdiv<W>((W)2 * k2 * d * abs54, dmm), gl = -fdiv<W>((W)2 * k2 * d * abs54, dnn);
+  R3<W> fi{gi * mm.x, gi * mm.y, gi * mm.z}, fl{gl * nn.x, gl * nn.y, gl * nn.z};
+  const W fiv[3] = {fi.x, fi.y, fi.z}, flv[3] = {fl.x, fl.y, fl.z};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    fr[2][q] = fiv[q];
+    fr[3][q] = ((W)-1 + d3454o) * fiv[q] - d5654o * flv[q];
+    fr[4][q] = ((W)-1 + d5654o) * flv[q] - d3454o * fiv[q];
+    fr[5][q] = flv[q];
+    fr[6][q] = 0;
+  }
+  mm = crs(v76, v56);
+  nn.x = -nn.x; nn.y = -nn.y; nn.z = -nn.z;
+  dmm = dot(mm, mm);
+  W d5656 = dot(v56, v56), abs56 = sqrt(d5656);
+  W d7656o = fdiv<W>(dot(v76, v56), d5656), d5456o = fdiv<W>(d5654, d5656);
+  dih = atan2(dot(v76, nn) * abs56, dot(mm, nn));
+  d = wrap_pi(dih - (W)nat[2]);
+  ediv += k3 * d * d;
+  gi = fdiv<W>((W)2 * k3 * d * abs56, dmm); gl = -fdiv<W>((W)2 * k3 * d * abs56, dnn);
+  const W f2i[3] = {gi * mm.x, gi * mm.y, gi * mm.z}, f2l[3] = {gl * nn.x, gl * nn.y, gl * nn.z};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    fr[6][q] += f2i[q];
+    fr[5][q] += ((W)-1 + d7656o) * f2i[q] - d5456o * f2l[q];
+    fr[4][q] += -d7656o * f2i[q] + ((W)-1 + d5456o) * f2l[q];
+    fr[3][q] += f2l[q];
+  }
+  const W pre = u0 / (ediv * ediv);
+  const size_t sb = T.slot_st + 7 * (size_t)k;
+#pragma unroll
+  for (int p = 0; p < 7; ++p)
+    put_slot<Real>(slots, sb + p, m[p], (Real)(pre * fr[p][0]), (Real)(pre * fr[p][1]), (Real)(pre * fr[p][2]));
+}
+
+// force_dtrna_stack.F90:54-165 (skipped when st_status is off).  The FP64
+// path evaluates it as written; the mixed path in FP32 unless one of the
+// dihedrals' triples is within ~2 degrees of straight (sin^2 < 1e-3), which
+// goes to term_stack64
 template <typename Real>
 __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s, const SlotDst &slots, int k, double u0) {
   const int *mp = a.st_idx + 7 * (size_t)(T.st0 + k);
@@ -536,6 +598,16 @@ __device__ void term_stack(const KArgs &a, const TopDesc &T, const Smem<Real> &s
   R3<Real> v54 = dvec(s, m[3], m[4]);
   R3<Real> v56 = dvec(s, m[5], m[4]);
   R3<Real> v76 = dvec(s, m[5], m[6]);
+  if constexpr (sizeof(Real) == 4) {
+    const R3<Real> c1 = crs(v34, v54), c2 = crs(v54, v56), c3 = crs(v76, v56);
+    const Real l54 = dot(v54, v54), l56 = dot(v56, v56);
+    const Real lim = (Real)1e-3;
+    if (dot(c1, c1) < lim * dot(v34, v34) * l54 || dot(c2, c2) < lim * l54 * l56 ||
+        dot(c3, c3) < lim * dot(v76, v76) * l56) {
+      term_stack64<Real>(a, T, s, slots, k, u0);
+      return;
+    }
+  }
   const Real k1 = (Real)cf[0], k2 = (Real)cf[1], k3 = (Real)cf[2];
   Real fr[7][3];
   Real ediv = 1;
@@ -628,23 +700,12 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
   Real d4246o4242 = fdiv(d4246, d4242), d1242o4242 = fdiv(d1242, d4242), d1353o1313 = fdiv(d1353, d1313);
   const Real MAXC = (Real)a.max_abscos;
   const Real v12a[3] = {v12.x, v12.y, v12.z}, v13a[3] = {v13.x, v13.y, v13.z}, v42a[3] = {v42.x, v42.y, v42.z};
-  // angle 3-1=2; the |cos| cap replaces the sine by that of the cap
-  // (FP32: the angle from |v12 x v13| and the sine squared without the
-  // difference, as in term_angle)
+  // angle 3-1=2 (the |cos| cap keeps acos away from +-1, so FP32 resolves
+  // it: the sine is at least that of the cap)
   Real cos312 = fdiv(d1213, a13 * a12);
-  const Real sin2cap = (Real)1 - MAXC * MAXC;
-  Real pre;
-  if constexpr (sizeof(Real) == 4) {
-    const R3<Real> cr = crs(v12, v13);
-    const Real sn2 = dot(cr, cr);
-    d = atan2(sqrt(sn2), d1213) - (Real)nat[1];
-    pre = (Real)2 * (Real)cf[2] * d * frsq(fabs(cos312) > MAXC ? d1313 * d1212 * sin2cap : sn2);
-    if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
-  } else {
-    if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
-    d = acos(cos312) - (Real)nat[1];
-    pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
-  }
+  if (fabs(cos312) > MAXC) d1213 = copysign(a12 * a13 * MAXC, cos312);
+  d = acos(cos312) - (Real)nat[1];
+  Real pre = (Real)2 * (Real)cf[2] * d * frsq(d1313 * d1212 - d1213 * d1213);
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     Real fi = pre * (v12a[q] - d1213o1313 * v13a[q]);
@@ -654,17 +715,9 @@ __device__ double term_hbond(const KArgs &a, const TopDesc &T, const Smem<Real> 
   ex -= (Real)cf[2] * d * d;
   // angle 1=2-4
   Real cos124 = fdiv(d1242, a12 * a42);
-  if constexpr (sizeof(Real) == 4) {
-    const R3<Real> cr = crs(v42, v12);
-    const Real sn2 = dot(cr, cr);
-    d = atan2(sqrt(sn2), d1242) - (Real)nat[2];
-    pre = (Real)2 * (Real)cf[3] * d * frsq(fabs(cos124) > MAXC ? d1212 * d4242 * sin2cap : sn2);
-    if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
-  } else {
-    if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
-    d = acos(cos124) - (Real)nat[2];
-    pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
-  }
+  if (fabs(cos124) > MAXC) d1242 = copysign(a12 * a42 * MAXC, cos124);
+  d = acos(cos124) - (Real)nat[2];
+  pre = (Real)2 * (Real)cf[3] * d * frsq(d1212 * d4242 - d1242 * d1242);
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     Real fi = -pre * (v42a[q] - d1242o1212 * v12a[q]);

@@ -618,11 +618,12 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         else if (ci == 2 && cj == 2) dij = dist_rr;
         else dij = bi.x + bj.x;
         if (r2 > dij * dij) return;
-        Real rinv, dr;
-        if constexpr (sizeof(Real) == 4) {
-          // inside contact the potential is steep and dr = dist + a - d_ij
-          // a small difference: the distance and dr in FP64 from the exact
-          // hi + lo difference, so their rounding is not amplified
+        Real rinv = rsq<Real>(r2);
+        Real dr = r2 * rinv + ra - dij;
+        if (sizeof(Real) == 4 && dr < (Real)1.5) {
+          // on the steep part of the potential (dr = dist + a - d_ij small)
+          // the rounding of the FP32 distance is amplified ~13 / dr: the
+          // distance and dr in FP64 from the exact hi + lo difference
           const double ex = (double)sx + ((double)lj.x - (double)li.x);
           const double ey = (double)sy + ((double)lj.y - (double)li.y);
           const double ez = (double)sz + ((double)lj.z - (double)li.z);
@@ -634,9 +635,6 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
           else dij64 = (double)bi.x + (double)bj.x;
           rinv = (Real)(1.0 / d64);
           dr = (Real)(d64 + a.exv_adjust - dij64);
-        } else {
-          rinv = rsq<Real>(r2);
-          dr = r2 * rinv + ra - dij;
         }
         const Real coef = bi.y * bj.y;
         const Real ro2 = fdiv(ra2, dr * dr);
