@@ -194,6 +194,9 @@ typedef struct tis_params {
   int32_t launch_noise_sweep;      /* two CTAs: 1 draws the noise in the bonded sweep, 2 in the update */
   int32_t launch_order;            /* 1: replicas launched in context order, 2: largest first */
   const char *launch_table;        /* NULL: tuned_launch.tsv next to the library */
+  int32_t launch_sweep;            /* bonded sweep of one CTA per replica: 1 a fixed deal of item chunks to
+                                      warps, 2 warps take chunks from a shared counter, longest kinds first
+                                      (two CTAs: always 1) */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */
@@ -214,6 +217,7 @@ typedef struct tis_status_t {
   int32_t noise_sweep;
   int32_t lane_order;
   int32_t launch_source;           /* 0 built-in rule, 1 tuned table, 2 caller or environment */
+  int32_t sweep;
 } tis_status_t;
 
 typedef struct tis_ctx tis_ctx;

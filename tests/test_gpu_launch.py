@@ -19,11 +19,19 @@ def test_table_caller_and_environment(tis_lib, tmp_path, monkeypatch):
     systems, par, temps = synth.workload_c1()
     key = autotune.workload_key(systems, par, [1])
     table = tmp_path / "t.tsv"
-    cfg = dict(launch_threads=256, launch_group=4, launch_ctas=1, launch_noise_sweep=1, launch_order=1)
+    cfg = dict(launch_threads=256, launch_group=4, launch_ctas=1, launch_noise_sweep=1, launch_order=1,
+               launch_sweep=2)
     autotune.merge_rows(str(table), {key: autotune.format_row(key, cfg, 1.0)})
     eng = Engine(systems, dict(par, launch_table=str(table)), temps)
     st = eng.status()
-    assert (st["launch_source"], st["threads_per_cta"], st["group"]) == (1, 256, 4)
+    assert (st["launch_source"], st["threads_per_cta"], st["group"], st["sweep"]) == (1, 256, 4, 2)
+    eng.close()
+    # a row without the sweep column leaves the schedule to the built-in rule
+    old = tmp_path / "old.tsv"
+    old.write_text(" ".join(str(v) for v in key) + " 256 4 1 1 1 1.0\n")
+    eng = Engine(systems, dict(par, launch_table=str(old)), temps)
+    st = eng.status()
+    assert (st["launch_source"], st["threads_per_cta"], st["sweep"]) == (1, 256, 1)
     eng.close()
     eng = Engine(systems, dict(par, launch_table=str(table), launch_threads=128), temps)
     st = eng.status()
@@ -41,7 +49,8 @@ def test_table_caller_and_environment(tis_lib, tmp_path, monkeypatch):
 
 @pytest.mark.parametrize("cfg", [dict(launch_threads=128, launch_group=1), dict(launch_threads=256, launch_group=8),
                                  dict(launch_threads=1024, launch_group=2), dict(launch_ctas=2, launch_group=4,
-                                                                                 launch_noise_sweep=2)])
+                                                                                 launch_noise_sweep=2),
+                                 dict(launch_threads=512, launch_sweep=2), dict(launch_threads=1024, launch_sweep=2)])
 def test_configurations_keep_parity(tis_lib, cfg):
     systems, par, ladder = synth.workload_c3()
     s = systems[0]
@@ -78,3 +87,25 @@ def test_largest_first_order_on_uneven_batch(tis_lib):
         out.append(eng.get_state()[0])
         eng.close()
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("threads", [512, 1024])
+def test_sweep_schedules_agree_bitwise(tis_lib, threads):
+    """The fixed deal and the shared counter hand the same item chunks to
+    different warps: every item is computed the same way and every bead's
+    sum keeps its order, so the trajectories are bitwise equal."""
+    systems, par, ladder = synth.workload_c3()
+    s = systems[0]
+    temps = list(ladder[::8])
+    out = []
+    for sweep in (1, 2):
+        eng = Engine([s], dict(par, launch_ctas=1, launch_threads=threads, launch_sweep=sweep), temps,
+                     nrep=[len(temps)])
+        assert eng.status()["sweep"] == sweep
+        eng.set_state(np.tile(s["xyz"], (len(temps), 1)))
+        eng.time_integral_pre()
+        eng.step(200)
+        out.append(eng.get_state())
+        eng.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)

@@ -81,6 +81,7 @@ class Params(C.Structure):
         ("pmf_rmerge", C.c_double), ("pmf_mg_p", _f64p), ("hi_refine", C.c_int32), ("i_hydro_tensor", C.c_int32),
         ("launch_threads", C.c_int32), ("launch_group", C.c_int32), ("launch_ctas", C.c_int32),
         ("launch_noise_sweep", C.c_int32), ("launch_order", C.c_int32), ("launch_table", C.c_char_p),
+        ("launch_sweep", C.c_int32),
     ]
 
 
@@ -91,7 +92,7 @@ class Status(C.Structure):
         ("not_spd", C.c_int32), ("last_error", C.c_int32),
         ("exv_pairs_max", C.c_int32), ("ele_pairs_max", C.c_int32), ("ctas_per_lane", C.c_int32),
         ("threads_per_cta", C.c_int32), ("group", C.c_int32), ("noise_sweep", C.c_int32),
-        ("lane_order", C.c_int32), ("launch_source", C.c_int32),
+        ("lane_order", C.c_int32), ("launch_source", C.c_int32), ("sweep", C.c_int32),
     ]
 
 

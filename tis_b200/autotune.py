@@ -12,6 +12,9 @@ the GPU for every valid configuration of
   update;
 * for batches of different sizes, the launch order (as given, or largest
   first),
+* for one CTA, the schedule of the bonded sweep: a fixed deal of item
+  chunks to warps, or warps taking chunks from a shared counter, longest
+  kinds first (the cluster kernel always deals them),
 
 keeps the fastest, and writes it as a row of the table that tis_init reads
 (tuned_launch.tsv next to libtis_b200.so; one row per workload key:
@@ -33,7 +36,7 @@ import statistics
 
 import numpy as np
 
-HEADER = ("# nmp nlane precision i_ele periodic skin | threads group ctas noise_sweep order | "
+HEADER = ("# nmp nlane precision i_ele periodic skin | threads group ctas noise_sweep order sweep | "
           "replica-steps/s measured by tis_b200.autotune\n")
 
 
@@ -57,9 +60,9 @@ def candidates(systems, par, nrep):
         threads = [512] if ctas == 2 else ([128, 256, 512] + ([1024] if mixed else []))
         sweeps = [1, 2] if ctas == 2 else [1]
         orders = [1, 2] if uneven else [1]
-        for t, g, nz, o in itertools.product(threads, [0, 1, 2, 4, 8], sweeps, orders):
+        for t, g, nz, o, sw in itertools.product(threads, [0, 1, 2, 4, 8], sweeps, orders, [1] if ctas == 2 else [1, 2]):
             out.append(dict(launch_ctas=ctas, launch_threads=t, launch_group=g, launch_noise_sweep=nz,
-                            launch_order=o))
+                            launch_order=o, launch_sweep=sw))
     return out
 
 
@@ -97,9 +100,9 @@ def tune(systems, par, temps, nrep, steps=500, reps=3):
 
 
 def format_row(key, cfg, rate):
-    return ("%d %d %d %d %d %d %d %d %d %d %d %.6g\n" %
+    return ("%d %d %d %d %d %d %d %d %d %d %d %d %.6g\n" %
             (key + (cfg["launch_threads"], cfg["launch_group"], cfg["launch_ctas"], cfg["launch_noise_sweep"],
-                    cfg["launch_order"], rate)))
+                    cfg["launch_order"], cfg["launch_sweep"], rate)))
 
 
 def merge_rows(path, rows):

@@ -156,7 +156,7 @@ struct tis_ctx {
   std::vector<long long> clamp_seen;
   long long launches = 0;            // kernels this context has launched
   bool pair = false;                 // tis_step runs two CTAs (a cluster) per lane
-  int noise_sweep = 1, order = 1, launch_source = 0;
+  int noise_sweep = 1, order = 1, sweep = 1, launch_source = 0;
   std::vector<int> h_order;          // launch order of the lanes (order 2: largest first)
   DBuf<int> d_order;
   size_t smem2 = 0;
@@ -259,9 +259,10 @@ void append(std::vector<T> &dst, const T *src, size_t n) {
 // noise, and the launch order of the replicas.  Measured choices come from
 // the table the autotuner (tis_b200/autotune.py) writes; each row is a
 // workload key and the fastest configuration measured for it:
-//   nmp nlane precision i_ele periodic skin | threads group ctas noise_sweep order | rate
+//   nmp nlane precision i_ele periodic skin | threads group ctas noise_sweep order sweep | rate
+// (rows without the sweep column leave it to the built-in rule)
 struct LaunchCfg {
-  int threads = 0, group = 0, ctas = 0, noise_sweep = 0, order = 0;
+  int threads = 0, group = 0, ctas = 0, noise_sweep = 0, order = 0, sweep = 0;
 };
 
 struct TuneRow {
@@ -287,11 +288,15 @@ std::vector<TuneRow> read_tune_table(const std::string &path) {
   while (std::fgets(line, sizeof line, f)) {
     if (line[0] == '#' || line[0] == '\n') continue;
     TuneRow r{};
-    double rate = 0.0;
-    const int n = std::sscanf(line, "%d %d %d %d %d %d %d %d %d %d %d %lf", &r.nmp, &r.nlane, &r.precision, &r.ele,
-                              &r.periodic, &r.skin, &r.cfg.threads, &r.cfg.group, &r.cfg.ctas, &r.cfg.noise_sweep,
-                              &r.cfg.order, &rate);
-    if (n >= 11 && r.nmp > 0 && r.nlane > 0) rows.push_back(r);
+    double v[13];
+    int n = 0;
+    for (char *tok = std::strtok(line, " \t\r\n"); tok && n < 13; tok = std::strtok(nullptr, " \t\r\n"))
+      v[n++] = std::atof(tok);
+    if (n != 12 && n != 13) continue;   // the rate is the last column
+    int *f[12] = {&r.nmp, &r.nlane, &r.precision, &r.ele, &r.periodic, &r.skin, &r.cfg.threads, &r.cfg.group,
+                  &r.cfg.ctas, &r.cfg.noise_sweep, &r.cfg.order, &r.cfg.sweep};
+    for (int k = 0; k < n - 1; ++k) *f[k] = (int)v[k];
+    if (r.nmp > 0 && r.nlane > 0) rows.push_back(r);
   }
   std::fclose(f);
   return rows;
@@ -870,6 +875,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     if (p.launch_ctas) { cfg.ctas = p.launch_ctas; source = 2; }
     if (p.launch_noise_sweep) { cfg.noise_sweep = p.launch_noise_sweep; source = 2; }
     if (p.launch_order) { cfg.order = p.launch_order; source = 2; }
+    if (p.launch_sweep) { cfg.sweep = p.launch_sweep; source = 2; }
     if (cfg.ctas == 0) cfg.ctas = (pair_ok && nsm > 0 && 2 * nlane <= nsm) ? 2 : 1;
     if (cfg.ctas == 2 && !pair_ok) cfg.ctas = 1;
     if (cfg.ctas == 2) cfg.threads = 512;   // the cluster kernel runs 512 threads per CTA
@@ -884,11 +890,18 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     }
     if (cfg.noise_sweep == 0) cfg.noise_sweep = 1;
     if (cfg.order == 0) cfg.order = ntop > 1 ? 2 : 1;
+    if (cfg.ctas == 2) cfg.sweep = 1;   // the cluster kernel deals its chunks
+    else if (cfg.sweep == 0) cfg.sweep = cfg.threads >= 1024 ? 2 : 1;
+    if (cfg.sweep != 1 && cfg.sweep != 2) {
+      tis_destroy(c);
+      return TIS_E_ARG;
+    }
     c->threads = cfg.threads;
     c->group = cfg.group;
     c->pair = cfg.ctas == 2;
     c->noise_sweep = cfg.noise_sweep;
     c->order = cfg.order;
+    c->sweep = cfg.sweep;
     c->launch_source = source;
     c->smem2 = c->pair ? smem2 : 0;
     // replicas largest first: a CTA that frees its SM takes the next one
@@ -1279,6 +1292,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_unif = c->n_unif;
   a.nbead_total = c->nbead_total;
   a.noise_in_sweep = 0;
+  a.sweep_dynamic = c->sweep == 2 ? 1 : 0;
   a.lane_nsteps = nullptr;
   a.step_k = 0;
   a.lane_order = (c->order == 2 && only_lane < 0) ? c->d_order.p : nullptr;
@@ -1883,6 +1897,7 @@ extern "C" int tis_status(tis_ctx *c, tis_status_t *st) {
   st->group = c->group;
   st->noise_sweep = c->noise_sweep;
   st->lane_order = c->order;
+  st->sweep = c->sweep;
   st->launch_source = c->launch_source;
   st->wait_timeout = c->wait_timeout;
   st->not_spd = c->not_spd;

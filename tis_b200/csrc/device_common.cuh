@@ -10,11 +10,18 @@ namespace tis {
 // Optional per-phase cycle counters (compiled only with -DTIS_PHASE_TIMING,
 // read with tis_phase_read): thread 0 of CTA 0 accumulates clock64 spans.
 #ifdef TIS_PHASE_TIMING
-static __device__ unsigned long long g_phase[64];
+static __device__ unsigned long long g_phase[128];
 #define PHASE_T0(v) long long v = clock64()
 #define PHASE_ADD(k, t0) do { if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(&g_phase[k], (unsigned long long)(clock64() - (t0))); } while (0)
-#define PHASE_ALL(k, t0) do { if (blockIdx.x == 0) { atomicAdd(&g_phase[k], (unsigned long long)(clock64() - (t0))); atomicAdd(&g_phase[(k) + 16], 1ull); } } while (0)
+#ifdef TIS_PHASE_LIGHT
+#define PHASE_ALL(k, t0) do {} while (0)
 #else
+#define PHASE_ALL(k, t0) do { if (blockIdx.x == 0) { atomicAdd(&g_phase[k], (unsigned long long)(clock64() - (t0))); atomicAdd(&g_phase[(k) + 16], 1ull); } } while (0)
+#endif
+// per-warp spans of the first two CTAs: slots base + 16 blockIdx.x + warp
+#define PHASE_WARP(base, t0) do { if (blockIdx.x < 2 && (threadIdx.x & 31) == 0) atomicAdd(&g_phase[(base) + 16 * blockIdx.x + (threadIdx.x >> 5)], (unsigned long long)(clock64() - (t0))); } while (0)
+#else
+#define PHASE_WARP(base, t0) do {} while (0)
 #define PHASE_ALL(k, t0) do {} while (0)
 #define PHASE_T0(v) do {} while (0)
 #define PHASE_ADD(k, t0) do {} while (0)
@@ -68,9 +75,11 @@ template <> struct V4<double> { typedef double4 T; };
 // in shared memory when they fit; otherwise they are used in global memory.
 constexpr size_t MASK_SMEM_MAX = 64 * 1024;    // bit matrices kept in shared memory up to this size
 
-enum { MISC_EXCESS = 0, MISC_REBUILD = 1, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,
-       MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8, MISC_PMF = 9,
-       MISC_UNITS = 10 /* neigh_unit ints start here */ };
+// MISC_EXCESS and MISC_NEAR_DISP have a second copy (+1) for odd steps: the
+// two-CTA kernel sets a flag for the next step while the current one is read.
+enum { MISC_EXCESS = 0, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,
+       MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8, MISC_PMF = 10, MISC_CHUNK = 11,
+       MISC_UNITS = 12 /* neigh_unit ints start here */ };
 
 // Excluded-volume near lists: at a recording pass every bead keeps, per
 // thread of its group, the exv-list partners within (screen radius +

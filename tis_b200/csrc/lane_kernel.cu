@@ -82,6 +82,11 @@ __device__ __forceinline__ bool skin_fires(const double *red, const double *peer
   if (lid < nwarp) { m1 = red[2 * lid]; m2 = red[2 * lid + 1]; }
   else if (peer_red && lid >= 16 && lid - 16 < nwarp) { m1 = peer_red[2 * (lid - 16)]; m2 = peer_red[2 * (lid - 16) + 1]; }
   top2_warp(m1, m2);
+  // FP32 screen: the float sum is within ~4e-7 (relative) of the FP64 one,
+  // so outside a 1e-4 band around the margin it decides the same way
+  const float sf = sqrtf((float)m1) + sqrtf((float)m2), mf = (float)margin;
+  if (sf < mf * 0.9999f) return false;
+  if (sf > mf * 1.0001f) return true;
   return __dadd_rn(sqrt(m1), sqrt(m2)) > margin;
 }
 
@@ -211,6 +216,7 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
       }
       const double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
       bool ex = d2 < (one_unit ? rn2_00 : s.rn2[ui * nu + uj]);
+      const bool el = qi && fabs((double)s.A4[j].w) >= 1.0e-6 && d2 < rele2;
       if (ex) {
         if (ui == uj) {
           if (ci == 2 /* RNA */ && j < i + nsep) ex = false;
@@ -226,8 +232,6 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
           }
         }
       }
-      bool el = false;
-      if (qi && fabs((double)s.A4[j].w) >= 1.0e-6) el = d2 < rele2;
       if (ex || el) {
         const uint32_t bj = 1u << (j & 31), bi = 1u << (i & 31);
         const bool own_i = CL == 1 || (i >= cu.lo && i < cu.hi);
@@ -342,7 +346,7 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
 // chunk partials; the group's owner thread hands the FP64 total to `sink`.
 template <typename Real, int CL, typename Sink>
 __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
-                           long long istep, const Clu &cu, int noise_step, Sink sink) {
+                           long long istep, const Clu &cu, int noise_step, Sink sink, int par = 0) {
   typedef typename V4<Real>::T V;
   const int N = T.nmp, NQ = T.nq, W = s.W;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -358,7 +362,9 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   const uint32_t *mexv = s.mask, *mele = s.mask + (size_t)N * W;
   const uint8_t *mir = a.periodic ? (a.mirror + L.mirror0) : nullptr;
   int nclamp = 0;
-  // (site counters and MISC_EXCESS were cleared by the caller before its barrier)
+  // (site counters and this step's MISC_EXCESS copy were cleared by the
+  // caller before its barrier; par selects the copies of this step)
+  const int f_exc = MISC_EXCESS + par, f_disp = MISC_NEAR_DISP + par;
   const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd, ntst = T.ntst;
   const ChunkGeo geo = chunk_geo(NQ, W);
   const int nch = (a.i_ele != 0) ? geo.nch : 0;
@@ -376,7 +382,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // near-list state: read here (after the caller's barrier), rewritten by
   // thread 0 only after the end-of-phase-1 barrier
   const bool near_rec = s.near_on && (s.misc[MISC_NEAR_BAD] != 0 ||
-                                      __int_as_float(s.misc[MISC_NEAR_DISP]) > NEAR_DISP_MAX * NEAR_DISP_MAX);
+                                      __int_as_float(s.misc[f_disp]) > NEAR_DISP_MAX * NEAR_DISP_MAX);
   PHASE_T0(t_p1);
   // warp-uniform schedule: 32-item chunks of one kind (no divergence between
   // kinds), dealt to the warps as below
@@ -395,29 +401,51 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     bd_0 = cu.rank ? nbd / 2 : 0; bd_1 = cu.rank ? nbd : nbd / 2;
     ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
   }
-  // chunk ranges, kinds in decreasing cost per chunk (measured on B200):
-  // stacks, tertiary stacks, Debye-Hueckel row chunks, angles, bonds, then
-  // noise.  The hbond chunks go first with two CTAs per lane (a formed
-  // hbond is the longest serial chain of the phase, and the first CTA takes
-  // every hbond) and after the angles with one CTA, where that order
-  // balances the warps better (both measured on B200).
-  const int n_hbc = (hb_1 - hb_0 + 31) >> 5, n_bac = (ba_1 - ba_0 + 31) >> 5;
-  const int c_st = (CL == 2) ? n_hbc : 0;   // first stack chunk
-  const int c_ts = c_st + ((st_1 - st_0 + 31) >> 5), c_ch = c_ts + ((ts_1 - ts_0 + 31) >> 5);
-  const int c_ba = c_ch + ((ch_1 - ch_0 + 31) >> 5);
-  const int c_hb = (CL == 2) ? 0 : c_ba + n_bac;   // first hbond chunk
-  const int c_bd = c_ba + n_bac + ((CL == 2) ? 0 : n_hbc);
-  const int c_nz = c_bd + ((bd_1 - bd_0 + 31) >> 5);
+  // Chunks of 32 items of one kind.  Fixed deal (sweep_dynamic 0): kinds in
+  // decreasing cost per chunk (measured on B200) -- stacks, tertiary
+  // stacks, Debye-Hueckel row chunks, angles, bonds, then noise -- with the
+  // hbond chunks first for two CTAs per lane (a formed hbond is the longest
+  // serial chain of the phase, and the first CTA takes every hbond) and
+  // after the angles for one CTA, where that order balances the warps
+  // better; round r gives chunk r nwarp + w to warp w (r even) or to warp
+  // nwarp - 1 - w (r odd), so the costly first chunks and the cheap last
+  // ones even out over the warps and over the SM's four schedulers.
+  // Counter (sweep_dynamic 1): tertiary stacks (FP64) and Debye-Hueckel
+  // chunks first, then stacks, hbonds, angles, bonds, noise; each warp takes
+  // the next chunk from a shared counter as it finishes one (longest first),
+  // which balances CTAs with many chunks per warp better (one CTA per lane).
+  const bool dyn = CL == 1 && a.sweep_dynamic != 0;   // two CTAs per lane: the fixed deal (measured faster)
+  const int n_hbc = (hb_1 - hb_0 + 31) >> 5, n_stc = (st_1 - st_0 + 31) >> 5, n_tsc = (ts_1 - ts_0 + 31) >> 5;
+  const int n_chc = (ch_1 - ch_0 + 31) >> 5, n_bac = (ba_1 - ba_0 + 31) >> 5, n_bdc = (bd_1 - bd_0 + 31) >> 5;
+  int c_hb, c_st, c_ts, c_ch, c_ba, c_bd, c_nz;   // first chunk of each kind
+  if (dyn) {
+    c_ts = 0; c_ch = c_ts + n_tsc; c_st = c_ch + n_chc; c_hb = c_st + n_stc;
+    c_ba = c_hb + n_hbc; c_bd = c_ba + n_bac; c_nz = c_bd + n_bdc;
+  } else {
+    c_st = (CL == 2) ? n_hbc : 0; c_ts = c_st + n_stc; c_ch = c_ts + n_tsc; c_ba = c_ch + n_chc;
+    c_hb = (CL == 2) ? 0 : c_ba + n_bac;
+    c_bd = c_ba + n_bac + ((CL == 2) ? 0 : n_hbc); c_nz = c_bd + n_bdc;
+  }
   // the sink's Gaussian noise of the own beads, drawn here where warps have slack
   const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
   const int c_end = c_nz + ((n_nz + 31) >> 5);
   (void)k_st; (void)k_ch; (void)k_ba; (void)k_bd; (void)total;
-  // snake deal: round r gives chunk r nwarp + w to warp w (r even) or to
-  // warp nwarp - 1 - w (r odd), so the costly first chunks and the cheap
-  // last ones even out over the warps
-  for (int r = 0; r * nwarp < c_end; ++r) {
-    const int c = r * nwarp + ((r & 1) ? nwarp - 1 - warp : warp);
-    if (c >= c_end) break;
+  // (the counter was cleared after the last pass's bonded sweep)
+  int r = 0, c = warp;
+  if (dyn) {
+    if (lid == 0) c = atomicAdd(&s.misc[MISC_CHUNK], 1);
+    c = __shfl_sync(0xffffffffu, c, 0);
+  }
+  while (c < c_end) {
+    // the next chunk of this warp, requested before this one is processed
+    int cn;
+    if (dyn) {
+      cn = 0;
+      if (lid == 0) cn = atomicAdd(&s.misc[MISC_CHUNK], 1);
+    } else {
+      ++r;
+      cn = r * nwarp + ((r & 1) ? nwarp - 1 - warp : warp);
+    }
     PHASE_T0(t_item);
     int kind;
     if (c >= c_hb && c < c_hb + n_hbc) {
@@ -438,8 +466,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
               if (sid >= 0) {
                 int old = atomicAdd(&exc[sid], 1);
                 if (old + 1 > ldro(a.site_val + T.site0 + sid)) {
-                  s.misc[MISC_EXCESS] = 1;
-                  if (CL == 2) peer_ptr(s.misc, cu)[MISC_EXCESS] = 1;
+                  s.misc[f_exc] = 1;
+                  if (CL == 2) peer_ptr(s.misc, cu)[f_exc] = 1;
                 }
               }
             }
@@ -449,15 +477,15 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         }
         hbf[h] = f;
       }
-    } else if (c < c_ts) {
+    } else if (c >= c_st && c < c_st + n_stc) {
       kind = 1;
       const int k = st_0 + ((c - c_st) << 5) + lid;
       if (k < st_1) term_stack<Real>(a, T, s, slots, k, ldro(u0 + k));
-    } else if (c < c_ch) {
+    } else if (c >= c_ts && c < c_ts + n_tsc) {
       kind = 1;
       const int k = ts_0 + ((c - c_ts) << 5) + lid;
       if (k < ts_1) term_tstack<Real>(a, T, s, slots, k);
-    } else if (c < c_ba) {
+    } else if (c >= c_ch && c < c_ch + n_chc) {
       kind = 2;
       const int cc = ch_0 + ((c - c_ch) << 5) + lid;
       if (cc < ch_1) {
@@ -532,11 +560,11 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
         }
         s.ch_part[3 * cc] = axs; s.ch_part[3 * cc + 1] = ays; s.ch_part[3 * cc + 2] = azs;
       }
-    } else if (c < c_ba + n_bac) {
+    } else if (c >= c_ba && c < c_ba + n_bac) {
       kind = 3;
       const int k = ba_0 + ((c - c_ba) << 5) + lid;
       if (k < ba_1) term_angle<Real>(a, T, s, slots, k);
-    } else if (c < c_nz) {
+    } else if (c >= c_bd && c < c_bd + n_bdc) {
       kind = 4;
       const int k = bd_0 + ((c - c_bd) << 5) + lid;
       if (k < bd_1) term_bond<Real>(a, T, s, slots, k);
@@ -550,15 +578,21 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
       }
     }
     PHASE_ALL(32 + kind, t_item);
+    c = dyn ? __shfl_sync(0xffffffffu, cn, 0) : cn;
   }
   PHASE_ADD(3, t_p1);
+  PHASE_WARP(64, t_p1);
   PHASE_T0(t_b2);
   if (CL == 1) __syncthreads(); else cg::this_cluster().sync();
   PHASE_ADD(9, t_b2);
-  if (tid == 0 && s.near_on) { s.misc[MISC_NEAR_BAD] = 0; s.misc[MISC_NEAR_DISP] = 0; }
+  // (two CTAs: the caller clears the displacement flag of the step after next)
+  if (tid == 0) {
+    s.misc[MISC_CHUNK] = 0;   // every warp has taken its last chunk
+    if (s.near_on) { s.misc[MISC_NEAR_BAD] = 0; if (CL == 1) s.misc[f_disp] = 0; }
+  }
   // both CTAs hold the same flag (the first one sets it in both), so both
   // take the same barriers
-  if (s.misc[MISC_EXCESS]) {
+  if (s.misc[f_exc]) {
     if (tid == 0 && cu.rank == 0) {
       const double beta = a.hb_beta_global ? (a.rex ? a.rex->beta_global : a.beta_hbond15) : a.lab_beta[label];
       prune_hbonds<Real>(a, lane, L, T, istep, beta, true, s.exc);
@@ -697,6 +731,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (valid && g == 0) PHASE_ALL(42, t_e1);
   }
   if (nclamp) atomicAdd(&s.misc[MISC_CLAMP], nclamp);
+  PHASE_WARP(96, t_p2);
 #ifdef TIS_PHASE_TIMING
   __syncthreads();
   PHASE_ADD(5, t_p2);
@@ -817,84 +852,105 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   };
 
   // skin rule: the trigger of the first step from the displacements loaded
-  // above (the other CTA's pairs are read after the cluster barrier below)
+  // above (two CTAs: in the copy of the step's parity; the other CTA's pairs
+  // are read after the cluster barrier below)
   bool skin_fire = false;
+  double *red0 = s.red + ((CL == 2) ? 32 * (int)(istep0 & 1) : 0);
   if (skin && (a.mode == KM_STEP || a.mode == KM_XSTEP)) {
     double m1 = 0.0, m2 = 0.0;
     for (int i = cu.lo + tid; i < cu.hi; i += nth) top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
-    top2_store(m1, m2, s.red);
+    top2_store(m1, m2, red0);
     if (CL == 1) {
       __syncthreads();
-      skin_fire = skin_fires(s.red, nullptr, nth >> 5, a.neigh_margin);
+      skin_fire = skin_fires(red0, nullptr, nth >> 5, a.neigh_margin);
     }
   }
 
   if constexpr (CL == 2) {
     typedef typename V4<Real>::T V;
     cg::this_cluster().sync();   // both CTAs are running before any distributed access
-    if (skin) skin_fire = skin_fires(s.red, peer_ptr(s.red, cu), nth >> 5, a.neigh_margin);
-    double *pXN = peer_ptr(s.XN, cu), *pYN = peer_ptr(s.YN, cu), *pZN = peer_ptr(s.ZN, cu);
-    V *pA4N = peer_ptr(s.A4N, cu), *pL4N = peer_ptr(s.L4N, cu);
+    if (skin) skin_fire = skin_fires(red0, peer_ptr(red0, cu), nth >> 5, a.neigh_margin);
+    // x update of step n + 1 of own bead i (time_integral.F90:152-161) from
+    // the v / a of step n: positions into the next-step buffers of both CTAs;
+    // skin rule: dxyz restarts from zero when step n + 1 rebuilds
+    // (time_integral.F90:89), and (m1, m2) collect the top two of the new
+    // dxyz for the trigger of step n + 2; the near-list displacement flag of
+    // step n + 1 goes to the copy of its parity
+    auto xnext = [&](int i, bool fire, int f_disp, double &m1, double &m2) {
+      const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
+      const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
+      const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
+      const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
+      const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
+      if (skin) {
+        if (fire) { s.DX[i] = dx; s.DY[i] = dy; s.DZ[i] = dz; }
+        else { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
+        top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+      }
+      s.XN[i] = nx; s.YN[i] = ny; s.ZN[i] = nz;
+      peer_ptr(s.XN, cu)[i] = nx; peer_ptr(s.YN, cu)[i] = ny; peer_ptr(s.ZN, cu)[i] = nz;
+      V av = s.A4[i], lv;
+      av.x = (Real)nx; av.y = (Real)ny; av.z = (Real)nz;
+      lv.x = (Real)(nx - (double)av.x); lv.y = (Real)(ny - (double)av.y); lv.z = (Real)(nz - (double)av.z);
+      lv.w = (Real)0;
+      s.A4N[i] = av; s.L4N[i] = lv;
+      peer_ptr(s.A4N, cu)[i] = av; peer_ptr(s.L4N, cu)[i] = lv;
+      if (s.near_on) {
+        const float ex = (float)av.x - s.NR4[i].x, ey = (float)av.y - s.NR4[i].y, ez = (float)av.z - s.NR4[i].z;
+        const float e2 = ex * ex + ey * ey + ez * ez;
+        if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[f_disp], 0x7f000000);
+      }
+    };
+    // the first step's x update; the later ones run in the v / a update of
+    // the step before (the lists of a rebuild come from the positions before
+    // the update, which stay in the current buffers until the swap)
+    {
+      const long long is1 = istep0 + 1;
+      double m1 = 0.0, m2 = 0.0;
+      for (int i = cu.lo + tid; i < cu.hi; i += nth) xnext(i, skin_fire, MISC_NEAR_DISP + (int)(is1 & 1), m1, m2);
+      if (skin) top2_store(m1, m2, s.red + 32 * (int)(is1 & 1));
+      if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+      if (tid == 0) s.misc[MISC_EXCESS + (int)(is1 & 1)] = 0;
+    }
     for (int step = 0; step < lane_steps; ++step) {
       const long long istep = istep0 + step + 1;
+      const int par = (int)(istep & 1);
+      const bool last = step + 1 == lane_steps;
       // neighbour trigger: the skin rule (time_integral.F90:57-93) or the
       // fixed cadence (:94); the decision is the same in both CTAs
       PHASE_T0(t_reb);
       const bool rebuild = skin ? skin_fire : ((istep % a.n_step_neighbor) == 1 || istep == 1);
       if (rebuild) {
+        __syncthreads();   // the last force pass has finished with the rows
         build_lists<Real, 2>(a, lane, L, T, s, cu, istep);
-        // dxyz_mp(:,:,irep) = 0 (time_integral.F90:89), own beads
-        if (skin) for (int i = cu.lo + tid; i < cu.hi; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
       }
       PHASE_ADD(1, t_reb);
-      PHASE_T0(t_xu);
-      // swap in the double buffers after both CTAs wrote them; the other
-      // CTA's copy of the own beads is written through distributed memory
-      double m1 = 0.0, m2 = 0.0;
-      for (int i = cu.lo + tid; i < cu.hi; i += nth) {
-        const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-        const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
-        const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
-        const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
-        const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
-        if (skin) {
-          s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
-          top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
-        }
-        s.XN[i] = nx; s.YN[i] = ny; s.ZN[i] = nz;
-        pXN[i] = nx; pYN[i] = ny; pZN[i] = nz;
-        V av = s.A4[i], lv;
-        av.x = (Real)nx; av.y = (Real)ny; av.z = (Real)nz;
-        lv.x = (Real)(nx - (double)av.x); lv.y = (Real)(ny - (double)av.y); lv.z = (Real)(nz - (double)av.z);
-        lv.w = (Real)0;
-        s.A4N[i] = av; s.L4N[i] = lv;
-        pA4N[i] = av; pL4N[i] = lv;
-        if (s.near_on) {
-          const float ex = (float)av.x - s.NR4[i].x, ey = (float)av.y - s.NR4[i].y, ez = (float)av.z - s.NR4[i].z;
-          const float e2 = ex * ex + ey * ey + ez * ez;
-          if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
-        }
-      }
-      // the per-warp pairs are read by both CTAs right after the barrier
-      // below and rewritten only after the force pass's cluster barrier
-      if (skin) top2_store(m1, m2, s.red);
-      if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
-      if (tid == 0) s.misc[MISC_EXCESS] = 0;
-      PHASE_ADD(2, t_xu);
       PHASE_T0(t_b1);
+      // the next-step buffers of both CTAs are complete
       cg::this_cluster().sync();
       PHASE_ADD(8, t_b1);
-      if (skin) skin_fire = skin_fires(s.red, peer_ptr(s.red, cu), nth >> 5, a.neigh_margin);
+      // trigger of the next step from the dxyz of this one (both CTAs' pairs)
+      if (skin) skin_fire = skin_fires(s.red + 32 * par, peer_ptr(s.red + 32 * par, cu), nth >> 5, a.neigh_margin);
+      // flags of the next step: their last readers passed this barrier
+      if (tid == 0) { s.misc[MISC_EXCESS + (par ^ 1)] = 0; s.misc[MISC_NEAR_DISP + (par ^ 1)] = 0; }
       { double *t; t = s.X; s.X = s.XN; s.XN = t; t = s.Y; s.Y = s.YN; s.YN = t; t = s.Z; s.Z = s.ZN; s.ZN = t; }
       s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
       { V *t; t = s.A4; s.A4 = s.A4N; s.A4N = t; t = s.L4; s.L4 = s.L4N; s.L4N = t; }
-      pXN = peer_ptr(s.XN, cu); pYN = peer_ptr(s.YN, cu); pZN = peer_ptr(s.ZN, cu);
-      pA4N = peer_ptr(s.A4N, cu); pL4N = peer_ptr(s.L4N, cu);
       PHASE_T0(t_fp);
-      force_pass<Real, 2>(a, lane, L, T, s, istep, cu, a.noise_base + step, vstep(istep, a.noise_base + step));
-      // the next x update reads v / a and the near-list positions that
-      // other threads of this CTA wrote in the force pass
-      __syncthreads();
+      const int nstep_noise = a.noise_base + step;
+      const bool fire_next = skin_fire;
+      double m1 = 0.0, m2 = 0.0;
+      force_pass<Real, 2>(a, lane, L, T, s, istep, cu, nstep_noise,
+                          [&](int i, double fx, double fy, double fz) {
+                            vstep(istep, nstep_noise)(i, fx, fy, fz);
+                            if (!last) xnext(i, fire_next, MISC_NEAR_DISP + (par ^ 1), m1, m2);
+                          }, par);
+      if (!last) {
+        if (skin) top2_store(m1, m2, s.red + 32 * (par ^ 1));
+        // hbond-site counters of the next step (read only in the bonded sweep
+        // and the valence pruning, both behind this step's cluster barriers)
+        if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+      }
       PHASE_ADD(6, t_fp);
     }
     cg::this_cluster().sync();   // no distributed shared-memory access after this
@@ -1047,7 +1103,7 @@ cudaError_t noise_launch(cudaStream_t st, KArgs a, long long istep0, int nstep, 
 
 #ifdef TIS_PHASE_TIMING
 extern "C" int tis_phase_read(unsigned long long *out) {
-  return (int)cudaMemcpyFromSymbol(out, g_phase, sizeof(unsigned long long) * 64);
+  return (int)cudaMemcpyFromSymbol(out, g_phase, sizeof(unsigned long long) * 128);
 }
 #endif
 
