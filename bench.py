@@ -53,12 +53,35 @@ def parse():
                     help="reference arm: MD steps per replica in one timed step (default: the CPU leg's sample)")
     ap.add_argument("--refine", action="store_true",
                     help="C5: refine the mixed-precision correlated noise once per step (tis_params.hi_refine)")
-    ap.add_argument("--neighbor", default="cadence", choices=["cadence", "skin"],
-                    help="neighbour rebuild rule: every 10 steps (the configs' cadence) or the reference's "
-                         "Verlet skin (neigh_margin 8 A, time_integral.F90:57-93)")
+    ap.add_argument("--neighbor", default=None, choices=["cadence", "skin"],
+                    help="neighbour rebuild rule: every 10 steps, or the reference's Verlet skin (neigh_margin "
+                         "8 A, time_integral.F90:57-93); default: the cadence where the workload's "
+                         "configuration fixes one (C1), else the skin rule")
     ap.add_argument("--quick", action="store_true",
                     help="device timing only (no CPU leg, e2e or plain path): small profiling runs")
     return ap.parse_args()
+
+
+def neighbor_rule(args):
+    """The rebuild rule of the run: --neighbor, else the cadence where the
+    workload's configuration fixes one (C1: every 10 steps), else the
+    reference's own rule, the Verlet skin.  With the 8 A margin both rules
+    keep every pair within the force cutoffs in the lists, so the forces
+    differ only by the rounding of the summation order (pairs beyond a
+    cutoff add zero); the number of rebuilds is what differs."""
+    if args.neighbor:
+        return args.neighbor
+    return "cadence" if args.workload == "c1" else "skin"
+
+
+def apply_rule(par, rule):
+    if rule == "skin":
+        par["n_step_neighbor"] = 0
+    return par
+
+
+RULE_TEXT = {"skin": "Verlet-skin rebuild (neigh_margin 8 A, the reference's rule)",
+             "cadence": "rebuild every 10 steps"}
 
 
 def workload(name):
@@ -68,12 +91,12 @@ def workload(name):
         nrep = [len(temps)]
         desc = ("C3: 64-replica temperature REMD of a 76-nt DT15 chain (227 beads), 20 random stem "
                 "hbond pairs, Debye-Hueckel 100 mM, ladder 280-400 K, Langevin dt 0.05 tau, "
-                "friction 0.5/tau, rebuild every 10 steps, exchange every 1000 steps")
+                "friction 0.5/tau, exchange every 1000 steps")
     elif name == "c4":
         systems, par, temps = synth.workload_c4()
         nrep = [1] * len(systems)
         desc = ("C4: 256 independent DT15 chains, lengths log-uniform 20-400 nt, 30% of residues in "
-                "hbond pairs, Debye-Hueckel 150 mM, 300 K, Langevin dt 0.05 tau, rebuild every 10 steps")
+                "hbond pairs, Debye-Hueckel 150 mM, 300 K, Langevin dt 0.05 tau")
     elif name == "c2":
         systems, par, temps = synth.workload_c2()
         nrep = [1]
@@ -331,6 +354,7 @@ def run_reference(args, rank, world):
         joined = int(t.item())
     if rank == 0:
         systems, par, temps, nrep, desc = workload(args.workload)
+        apply_rule(par, neighbor_rule(args))
         sample = args.ref_sample or CPU_SAMPLE[args.workload]
         variant, flags = cpu_variant()
         fleet = CpuFleet(systems, par, temps, nrep, sample, variant)
@@ -346,7 +370,8 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": nlane * sample / value * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded random-walk DT15 chains)",
-            "config": {"workload": desc, "parallelism": f"{fleet.cores} host processes"},
+            "config": {"workload": desc, "neighbor_rule": RULE_TEXT[neighbor_rule(args)],
+                       "parallelism": f"{fleet.cores} host processes"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": fleet.cores, "kind": "port",
                              "sample": f"{nlane} replicas x {sample} MD steps per step, median of {args.steps} "
                                        f"(C++ FP64 restatement built {flags}; no Fortran compiler on this "
@@ -373,6 +398,7 @@ def run_ours(args, rank, world, local_rank):
         # CPU leg first, in spawned processes, before this process touches the
         # GPU; timed exactly as the reference arm times it
         systems, par, temps, nrep, _ = workload(args.workload)
+        apply_rule(par, neighbor_rule(args))
         sample = CPU_SAMPLE[args.workload]
         variant, flags = cpu_variant()
         fleet = CpuFleet(systems, par, temps, nrep, sample, variant)
@@ -393,8 +419,7 @@ def run_ours(args, rank, world, local_rank):
     from tis_b200.engine import Engine
 
     systems, par, temps, nrep, desc = workload(args.workload)
-    if args.neighbor == "skin":
-        par["n_step_neighbor"] = 0
+    apply_rule(par, neighbor_rule(args))
     if args.precision is not None:
         par["precision"] = args.precision
     if args.refine:
@@ -485,7 +510,7 @@ def run_ours(args, rank, world, local_rank):
     nbytes = 3 * eng.nbead * 3 * 8
 
     # C3 under the other neighbour rule, the same periods (no exchange kernel
-    # differences): the headline uses args.neighbor
+    # differences): the headline uses neighbor_rule(args)
     other_rule = None
     if remd and ladder is None and not args.quick:
         alt = dict(par, n_step_neighbor=0 if par["n_step_neighbor"] > 0 else 10)
@@ -503,7 +528,7 @@ def run_ours(args, rank, world, local_rank):
             e2.step(period_len)
             e2.replica_exchange(count=False)
             t2.append(e2.timer_stop())
-        other_rule = {"rule": "Verlet skin, neigh_margin 8 A" if alt["n_step_neighbor"] <= 0 else "every 10 steps",
+        other_rule = {"rule": RULE_TEXT["skin" if alt["n_step_neighbor"] <= 0 else "cadence"],
                       "value": nlane * period_len * args.steps / (sum(t2) * 1e-3), "unit": UNIT,
                       "n_rebuild_per_replica_step": e2.status()["n_rebuild"] / (nlane * period_len * (args.steps + args.warmup))}
         e2.close()
@@ -542,8 +567,7 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic (seeded random-walk DT15 chains, reference parameter tables)",
             "config": {"workload": desc, "replicas_per_gpu": nlane, "beads_per_replica": int(systems[0]["nmp"]),
                        "md_steps_per_step": period_len, "l2": "flushed between timed steps (256 MiB write)",
-                       "neighbor_rule": ("Verlet skin, neigh_margin 8 A (the reference's rule)"
-                                         if args.neighbor == "skin" else "rebuild every 10 steps"),
+                       "neighbor_rule": RULE_TEXT[neighbor_rule(args)],
                        "parallelism": (f"ladder split, {nlane} replicas per GPU, NCCL all-gather at exchanges"
                                        if ladder is not None else f"replicas only, {nlane} lanes per GPU")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

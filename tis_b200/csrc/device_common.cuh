@@ -275,6 +275,29 @@ __device__ __forceinline__ void noise3(const KArgs &a, int lane, const LaneDesc 
   n0 = (double)(r1 * c1); n1 = (double)(r1 * s1); n2 = (double)(r2 * c2);
 }
 
+// component d of noise3 (the same operations for that component)
+__device__ __forceinline__ double noise1(const KArgs &a, int lane, const LaneDesc &L, int i, long long istep,
+                                         int noise_step, int d) {
+  if (a.noise) {
+    if (noise_step < a.noise_nsteps) return a.noise[((size_t)noise_step * a.nbead_total + L.state0 + i) * 3 + d];
+    atomicOr(&a.lstate[lane].flags, LF_NOISE_EXHAUSTED);
+    return 0.0;
+  }
+  U4 c = {(uint32_t)istep, (uint32_t)((unsigned long long)istep >> 32), (uint32_t)(L.key_bead0 + i), 0x4E4F4953u};
+  U4 o = philox4x32(c, (uint32_t)a.seed ^ (0x9E3779B9u * (uint32_t)(L.key_lane + 1)), (uint32_t)(a.seed >> 32));
+  float sn, cs;
+  if (d < 2) {
+    const float u1 = u01f_open0(o.x), u2 = u01f_open0(o.y);
+    const float r1 = sqrtf(-2.0f * logf(u1));
+    sincospif(2.0f * u2, &sn, &cs);
+    return (double)(r1 * (d ? sn : cs));
+  }
+  const float u3 = u01f_open0(o.z), u4 = u01f_open0(o.w);
+  const float r2 = sqrtf(-2.0f * logf(u3));
+  sincospif(2.0f * u4, &sn, &cs);
+  return (double)(r2 * cs);
+}
+
 __device__ __forceinline__ double lane_uniform(const KArgs &a, int lane, const LaneDesc &L, long long istep,
                                                int &draw) {
   LaneState &st = a.lstate[lane];

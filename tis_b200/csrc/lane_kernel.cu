@@ -110,6 +110,13 @@ __device__ __forceinline__ double add_rn(double a, double b) {
 // unordered pair is tested once and sets its bit in both rows of the exv
 // and/or ele matrix.  Periodic systems also record the mirror index of the
 // canonical (min, max) orientation (neighbor_assign.F90:742-770).
+__device__ __forceinline__ void rebuild_counts(LaneState &st, int nexv, int nele, long long istep) {
+  st.nrebuild++;
+  st.last_rebuild = istep;
+  st.nexv = nexv;
+  st.nele = nele;
+}
+
 template <typename Real, int CL>
 __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
                             const Clu &cu, long long istep) {
@@ -266,18 +273,12 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
     double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
     hbf[h] = (d2 < a.hb_nd2[T.hb0 + h]) ? 1 : 0;
   }
+  // one CTA: the lists and counts are complete after this barrier; two CTAs:
+  // the rows are read only after the step's next cluster barrier, after
+  // which the first CTA adds up both counts (rebuild_counts)
   if (CL == 1) {
     __syncthreads();
-  } else {
-    cg::this_cluster().sync();   // every bit of the own rows is in
-  }
-  if (tid == 0 && cu.rank == 0) {
-    int ne = s.misc[MISC_NEXV], nl = s.misc[MISC_NELE];
-    if (CL == 2) { ne += peer_ptr(s.misc, cu)[MISC_NEXV]; nl += peer_ptr(s.misc, cu)[MISC_NELE]; }
-    st.nrebuild++;
-    st.last_rebuild = istep;
-    st.nexv = ne;
-    st.nele = nl;
+    if (tid == 0) rebuild_counts(st, s.misc[MISC_NEXV], s.misc[MISC_NELE], istep);
   }
 }
 
@@ -344,9 +345,13 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
 // hbonds, bonds.  Phase 2 gives each bead a group of GA
 // threads that sums its exv pairs, its bonded slots and its Debye-Hueckel
 // chunk partials; the group's owner thread hands the FP64 total to `sink`.
-template <typename Real, int CL, typename Sink>
+struct NoFin {
+  __device__ void operator()(int) const {}
+};
+
+template <typename Real, int CL, typename Sink, typename Fin = NoFin>
 __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const TopDesc &T, Smem<Real> &s,
-                           long long istep, const Clu &cu, int noise_step, Sink sink, int par = 0) {
+                           long long istep, const Clu &cu, int noise_step, Sink sink, int par = 0, Fin fin = Fin()) {
   typedef typename V4<Real>::T V;
   const int N = T.nmp, NQ = T.nq, W = s.W;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -722,12 +727,19 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     }
     if (valid) PHASE_ALL(41, t_e2);
     PHASE_T0(t_e1);
+    // every thread of the group holds the same totals: thread d of the group
+    // (d < GA) hands component d (and d + GA, ...) to the sink, then its
+    // first thread finishes the bead after the components are written
     group_reduce<Real>(fx, fy, fz, GA);
-    if (valid && g == 0 && a.f_ext) {
-      const size_t o = 3 * (size_t)(L.state0 + i);
-      fx += a.f_ext[o]; fy += a.f_ext[o + 1]; fz += a.f_ext[o + 2];
+    if (valid) {
+      for (int d = g; d < 3; d += GA) {
+        double f = d == 0 ? fx : (d == 1 ? fy : fz);
+        if (a.f_ext) f += a.f_ext[3 * (size_t)(L.state0 + i) + d];
+        sink(i, d, f);
+      }
     }
-    if (valid && g == 0) sink(i, fx, fy, fz);
+    __syncwarp();
+    if (valid && g == 0) fin(i);
     if (valid && g == 0) PHASE_ALL(42, t_e1);
   }
   if (nclamp) atomicAdd(&s.misc[MISC_CLAMP], nclamp);
@@ -787,6 +799,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     const int b = T.bead0 + i;
     set_pos<Real>(s, i);
     s.A4[i].w = (Real)bead_charge(a, st.label, b);
+    if (s.A4N) { s.A4N[i].w = s.A4[i].w; s.L4N[i].w = (Real)0; }   // the next-step copies keep .w
     s.B4[i].x = (Real)a.b_radius[b]; s.B4[i].y = (Real)a.b_eps[b];
     s.B4[i].z = (Real)(a.b_screen[b] * (1.0 + 1.0e-4) + 1.0e-3); s.B4[i].w = (Real)0;
     s.typ[i] = a.b_type[b]; s.cls[i] = a.b_class[b];
@@ -826,28 +839,26 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     }
     __syncthreads();
   }
-  // time_integral.F90:169-183: v / a update of bead i from its force
+  // time_integral.F90:169-183: v / a update of component d of bead i from
+  // its force (the components of a bead are three independent updates)
   auto vstep = [&](long long istep, int nstep_noise) {
-    return [&, istep, nstep_noise](int i, double fx, double fy, double fz) {
-      double n0, n1, n2, rc, cc, c2, c3;
+    return [&, istep, nstep_noise](int i, int d, double f) {
+      double n, rc, cc, c2, c3;
       if (s.cst_on) {
-        if (a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }   // drawn in the bonded sweep
-        else noise3(a, lane, L, i, istep, nstep_noise, n0, n1, n2);
+        // drawn in the bonded sweep, or here
+        n = a.noise_in_sweep ? s.NX[d * N + i] : noise1(a, lane, L, i, istep, nstep_noise, d);
         rc = s.RC[i]; cc = s.C1[i]; c2 = s.C2[i]; c3 = s.C3[i];
       } else {
-        noise3(a, lane, L, i, istep, nstep_noise, n0, n1, n2);
+        n = noise1(a, lane, L, i, istep, nstep_noise, d);
         const int b = T.bead0 + i;
         rc = a.b_rcmass[b]; cc = c1[i]; c2 = a.b_c2[b]; c3 = a.b_c3[b];
       }
       // each product rounded, as the reference evaluates it (no contraction)
-      const double ax = mad2<Real>(fx, rc, cc, n0);
-      const double ay = mad2<Real>(fy, rc, cc, n1);
-      const double az = mad2<Real>(fz, rc, cc, n2);
-      s.VX[i] = mad2<Real>(c2, s.VX[i], c3, add_rn<Real>(s.AX[i], ax));
-      s.VY[i] = mad2<Real>(c2, s.VY[i], c3, add_rn<Real>(s.AY[i], ay));
-      s.VZ[i] = mad2<Real>(c2, s.VZ[i], c3, add_rn<Real>(s.AZ[i], az));
-      s.AX[i] = ax; s.AY[i] = ay; s.AZ[i] = az;
-      if (!(fx == fx && fy == fy && fz == fz)) s.misc[MISC_NAN] = 1;
+      double *V = s.VX + d * N, *A = s.AX + d * N;
+      const double acc = mad2<Real>(f, rc, cc, n);
+      V[i] = mad2<Real>(c2, V[i], c3, add_rn<Real>(A[i], acc));
+      A[i] = acc;
+      if (!(f == f)) s.misc[MISC_NAN] = 1;
     };
   };
 
@@ -876,26 +887,26 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     // (time_integral.F90:89), and (m1, m2) collect the top two of the new
     // dxyz for the trigger of step n + 2; the near-list displacement flag of
     // step n + 1 goes to the copy of its parity
-    auto xnext = [&](int i, bool fire, int f_disp, double &m1, double &m2) {
+    auto xnext = [&](int i, int d, bool fire) {
       const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-      const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
-      const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
-      const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
-      const double nx = s.X[i] + dx, ny = s.Y[i] + dy, nz = s.Z[i] + dz;
+      const double dx = mad2<Real>(c4, s.VX[d * N + i], a.tstep2, s.AX[d * N + i]);
+      const double nx = s.X[d * N + i] + dx;
       if (skin) {
-        if (fire) { s.DX[i] = dx; s.DY[i] = dy; s.DZ[i] = dz; }
-        else { s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz; }
-        top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+        double *D = s.DX + d * N;
+        D[i] = fire ? dx : D[i] + dx;
       }
-      s.XN[i] = nx; s.YN[i] = ny; s.ZN[i] = nz;
-      peer_ptr(s.XN, cu)[i] = nx; peer_ptr(s.YN, cu)[i] = ny; peer_ptr(s.ZN, cu)[i] = nz;
-      V av = s.A4[i], lv;
-      av.x = (Real)nx; av.y = (Real)ny; av.z = (Real)nz;
-      lv.x = (Real)(nx - (double)av.x); lv.y = (Real)(ny - (double)av.y); lv.z = (Real)(nz - (double)av.z);
-      lv.w = (Real)0;
-      s.A4N[i] = av; s.L4N[i] = lv;
-      peer_ptr(s.A4N, cu)[i] = av; peer_ptr(s.L4N, cu)[i] = lv;
+      s.XN[d * N + i] = nx;
+      peer_ptr(s.XN, cu)[d * N + i] = nx;
+      const Real hi = (Real)nx, lo = (Real)(nx - (double)hi);
+      (&s.A4N[i].x)[d] = hi; (&s.L4N[i].x)[d] = lo;
+      (&peer_ptr(s.A4N, cu)[i].x)[d] = hi; (&peer_ptr(s.L4N, cu)[i].x)[d] = lo;
+    };
+    // after the three components of bead i: its dxyz into (m1, m2), and the
+    // near-list displacement check
+    auto xfin = [&](int i, int f_disp, double &m1, double &m2) {
+      if (skin) top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
       if (s.near_on) {
+        const V av = s.A4N[i];
         const float ex = (float)av.x - s.NR4[i].x, ey = (float)av.y - s.NR4[i].y, ez = (float)av.z - s.NR4[i].z;
         const float e2 = ex * ex + ey * ey + ez * ez;
         if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[f_disp], 0x7f000000);
@@ -907,7 +918,10 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     {
       const long long is1 = istep0 + 1;
       double m1 = 0.0, m2 = 0.0;
-      for (int i = cu.lo + tid; i < cu.hi; i += nth) xnext(i, skin_fire, MISC_NEAR_DISP + (int)(is1 & 1), m1, m2);
+      for (int i = cu.lo + tid; i < cu.hi; i += nth) {
+        for (int d = 0; d < 3; ++d) xnext(i, d, skin_fire);
+        xfin(i, MISC_NEAR_DISP + (int)(is1 & 1), m1, m2);
+      }
       if (skin) top2_store(m1, m2, s.red + 32 * (int)(is1 & 1));
       if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
       if (tid == 0) s.misc[MISC_EXCESS + (int)(is1 & 1)] = 0;
@@ -926,9 +940,13 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       }
       PHASE_ADD(1, t_reb);
       PHASE_T0(t_b1);
-      // the next-step buffers of both CTAs are complete
+      // the next-step buffers (and, after a rebuild, the list rows) of both
+      // CTAs are complete
       cg::this_cluster().sync();
       PHASE_ADD(8, t_b1);
+      if (rebuild && tid == 0 && cu.rank == 0)
+        rebuild_counts(st, s.misc[MISC_NEXV] + peer_ptr(s.misc, cu)[MISC_NEXV],
+                       s.misc[MISC_NELE] + peer_ptr(s.misc, cu)[MISC_NELE], istep);
       // trigger of the next step from the dxyz of this one (both CTAs' pairs)
       if (skin) skin_fire = skin_fires(s.red + 32 * par, peer_ptr(s.red + 32 * par, cu), nth >> 5, a.neigh_margin);
       // flags of the next step: their last readers passed this barrier
@@ -940,11 +958,16 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       const int nstep_noise = a.noise_base + step;
       const bool fire_next = skin_fire;
       double m1 = 0.0, m2 = 0.0;
-      force_pass<Real, 2>(a, lane, L, T, s, istep, cu, nstep_noise,
-                          [&](int i, double fx, double fy, double fz) {
-                            vstep(istep, nstep_noise)(i, fx, fy, fz);
-                            if (!last) xnext(i, fire_next, MISC_NEAR_DISP + (par ^ 1), m1, m2);
-                          }, par);
+      force_pass<Real, 2>(
+          a, lane, L, T, s, istep, cu, nstep_noise,
+          [&](int i, int d, double f) {
+            vstep(istep, nstep_noise)(i, d, f);
+            if (!last) xnext(i, d, fire_next);
+          },
+          par,
+          [&](int i) {
+            if (!last) xfin(i, MISC_NEAR_DISP + (par ^ 1), m1, m2);
+          });
       if (!last) {
         if (skin) top2_store(m1, m2, s.red + 32 * (par ^ 1));
         // hbond-site counters of the next step (read only in the bonded sweep
@@ -958,24 +981,17 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     build_lists<Real, 1>(a, lane, L, T, s, cu, st.istep);
   } else if (a.mode == KM_FORCE) {
     double *out = a.out_force;
-    force_pass<Real, 1>(a, lane, L, T, s, st.istep, cu, -1, [&](int i, double fx, double fy, double fz) {
-      const size_t o = 3 * (size_t)(L.state0 + i);
-      out[o] = fx; out[o + 1] = fy; out[o + 2] = fz;
-    });
+    force_pass<Real, 1>(a, lane, L, T, s, st.istep, cu, -1,
+                        [&](int i, int d, double f) { out[3 * (size_t)(L.state0 + i) + d] = f; });
   } else if (a.mode == KM_PRE) {
     build_lists<Real, 1>(a, lane, L, T, s, cu, st.istep);
     // dxyz_mp = 0 (time_integral_pre.F90:79)
     if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
     __syncthreads();
     const long long is = st.istep;
-    force_pass<Real, 1>(a, lane, L, T, s, is, cu, a.noise_base, [&](int i, double fx, double fy, double fz) {
-      double n0, n1, n2;
-      if (s.cst_on && a.noise_in_sweep) { n0 = s.NX[i]; n1 = s.NY[i]; n2 = s.NZ[i]; }
-      else noise3(a, lane, L, i, is, a.noise_base, n0, n1, n2);
-      const double rc = a.b_rcmass[T.bead0 + i], cc = c1[i];
-      s.AX[i] = mad2<Real>(fx, rc, cc, n0);
-      s.AY[i] = mad2<Real>(fy, rc, cc, n1);
-      s.AZ[i] = mad2<Real>(fz, rc, cc, n2);
+    force_pass<Real, 1>(a, lane, L, T, s, is, cu, a.noise_base, [&](int i, int d, double f) {
+      const double n = (s.cst_on && a.noise_in_sweep) ? s.NX[d * N + i] : noise1(a, lane, L, i, is, a.noise_base, d);
+      s.AX[d * N + i] = mad2<Real>(f, a.b_rcmass[T.bead0 + i], c1[i], n);
     });
   } else {  // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step)
     const int nloop = (a.mode == KM_STEP) ? lane_steps : 1;
