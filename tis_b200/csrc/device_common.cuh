@@ -75,11 +75,12 @@ template <> struct V4<double> { typedef double4 T; };
 // in shared memory when they fit; otherwise they are used in global memory.
 constexpr size_t MASK_SMEM_MAX = 64 * 1024;    // bit matrices kept in shared memory up to this size
 
-// MISC_EXCESS and MISC_NEAR_DISP have a second copy (+1) for odd steps: the
-// two-CTA kernel sets a flag for the next step while the current one is read.
+// MISC_EXCESS, MISC_NEAR_DISP and MISC_DMAX have a second copy (+1) for odd
+// steps: the two-CTA kernel sets a flag for the next step while the current
+// one is read.
 enum { MISC_EXCESS = 0, MISC_CLAMP = 2, MISC_NEXV = 3, MISC_NELE = 4, MISC_NAN = 5,
        MISC_REBUILT = 6, MISC_NEAR_BAD = 7, MISC_NEAR_DISP = 8, MISC_PMF = 10, MISC_CHUNK = 11,
-       MISC_UNITS = 12 /* neigh_unit ints start here */ };
+       MISC_DMAX = 12 /* and 13 */, MISC_UNITS = 14 /* neigh_unit ints start here */ };
 
 // Excluded-volume near lists: at a recording pass every bead keeps, per
 // thread of its group, the exv-list partners within (screen radius +
@@ -101,6 +102,7 @@ struct Smem {
   double *DX, *DY, *DZ;     // dxyz_mp (skin rule only)
   double *QX, *QY, *QZ;     // periodic: pxyz wrapped at the last rebuild
   double *XN, *YN, *ZN;     // two-CTA lanes: next-step positions (double buffer)
+  double *DD;               // skin rule: dot_product(dxyz, dxyz) of every bead
   double *red;              // 64 doubles of reduction scratch
   double *ch_part;          // (3 * CHMAX) partial Debye-Hueckel force of each chunk
   double *rn2;              // rneighbordist2_unit (nunit x nunit)
@@ -136,6 +138,7 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc
   if (periodic) nd += 6 * (size_t)N;
   if (skin) nd += 3 * (size_t)N;
   if (dbuf) nd += 3 * (size_t)N;
+  if (skin) nd += (size_t)N;
   size_t b = nd * 8;
   b += 12 * (size_t)N * real_size;                  // A4, B4, L4
   if (dbuf) b += 8 * (size_t)N * real_size;         // A4N, L4N
@@ -192,6 +195,8 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   else { s.DX = s.DY = s.DZ = nullptr; }
   if (dbuf) { s.XN = d; s.YN = d + N; s.ZN = d + 2 * N; d += 3 * N; }
   else { s.XN = s.YN = s.ZN = nullptr; }
+  if (skin) { s.DD = d; d += N; }
+  else s.DD = nullptr;
   s.red = d; d += 64;
   s.ch_part = d; d += 3 * CHMAX;
   s.rn2 = d; d += T.nunit * T.nunit;

@@ -74,13 +74,9 @@ __device__ __forceinline__ void top2_store(double m1, double m2, double *red) {
   top2_warp(m1, m2);
   if ((threadIdx.x & 31) == 0) { red[2 * (threadIdx.x >> 5)] = m1; red[2 * (threadIdx.x >> 5) + 1] = m2; }
 }
-// the trigger from the per-warp pairs of this CTA (lanes 0 .. nwarp - 1) and,
-// with two CTAs, of the other one (lanes 16 .. 16 + nwarp - 1, nwarp <= 16)
-__device__ __forceinline__ bool skin_fires(const double *red, const double *peer_red, int nwarp, double margin) {
-  const int lid = threadIdx.x & 31;
-  double m1 = 0.0, m2 = 0.0;
-  if (lid < nwarp) { m1 = red[2 * lid]; m2 = red[2 * lid + 1]; }
-  else if (peer_red && lid >= 16 && lid - 16 < nwarp) { m1 = peer_red[2 * (lid - 16)]; m2 = peer_red[2 * (lid - 16) + 1]; }
+// sqrt(d2max) + sqrt(d2max_2nd) > margin from every lane's pair (the
+// decision is the same in every lane)
+__device__ __forceinline__ bool skin_decide(double m1, double m2, double margin) {
   top2_warp(m1, m2);
   // FP32 screen: the float sum is within ~4e-7 (relative) of the FP64 one,
   // so outside a 1e-4 band around the margin it decides the same way
@@ -88,6 +84,26 @@ __device__ __forceinline__ bool skin_fires(const double *red, const double *peer
   if (sf < mf * 0.9999f) return false;
   if (sf > mf * 1.0001f) return true;
   return __dadd_rn(sqrt(m1), sqrt(m2)) > margin;
+}
+// The trigger from the d2 of every bead (DD) and M, their maximum rounded
+// up to float: M rules the skin out while 2 sqrt(M) is 1e-4 below the
+// margin (sqrt(d2max) + sqrt(d2max_2nd) <= 2 sqrt(M)); else every warp
+// takes the top two d2 of DD.  Every thread reaches the same decision.
+__device__ __forceinline__ bool skin_trigger(int Mbits, const double *DD, int N, double margin) {
+  const float M = __int_as_float(Mbits);
+  if (2.0f * sqrtf(M) < (float)margin * 0.9999f) return false;
+  double m1 = 0.0, m2 = 0.0;
+  for (int b = (threadIdx.x & 31); b < N; b += 32) top2_add(m1, m2, DD[b]);
+  return skin_decide(m1, m2, margin);
+}
+// the trigger from the per-warp pairs of this CTA (lanes 0 .. nwarp - 1) and,
+// with two CTAs, of the other one (lanes 16 .. 16 + nwarp - 1, nwarp <= 16)
+__device__ __forceinline__ bool skin_fires(const double *red, const double *peer_red, int nwarp, double margin) {
+  const int lid = threadIdx.x & 31;
+  double m1 = 0.0, m2 = 0.0;
+  if (lid < nwarp) { m1 = red[2 * lid]; m2 = red[2 * lid + 1]; }
+  else if (peer_red && lid >= 16 && lid - 16 < nwarp) { m1 = peer_red[2 * (lid - 16)]; m2 = peer_red[2 * (lid - 16) + 1]; }
+  return skin_decide(m1, m2, margin);
 }
 
 // a b + c d of the integration: in the FP64 path each product rounded as
@@ -594,6 +610,7 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   if (tid == 0) {
     s.misc[MISC_CHUNK] = 0;   // every warp has taken its last chunk
     if (s.near_on) { s.misc[MISC_NEAR_BAD] = 0; if (CL == 1) s.misc[f_disp] = 0; }
+    if (CL == 1) s.misc[MISC_DMAX] = 0;
   }
   // both CTAs hold the same flag (the first one sets it in both), so both
   // take the same barriers
@@ -901,10 +918,18 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       (&s.A4N[i].x)[d] = hi; (&s.L4N[i].x)[d] = lo;
       (&peer_ptr(s.A4N, cu)[i].x)[d] = hi; (&peer_ptr(s.L4N, cu)[i].x)[d] = lo;
     };
-    // after the three components of bead i: its dxyz into (m1, m2), and the
-    // near-list displacement check
-    auto xfin = [&](int i, int f_disp, double &m1, double &m2) {
-      if (skin) top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+    // after the three components of bead i: dot_product(dxyz, dxyz) into DD
+    // of both CTAs and, rounded up to float, into the running maximum of the
+    // step (flag copy f_dmax, both CTAs); the near-list displacement check
+    auto xfin = [&](int i, int f_disp, int f_dmax) {
+      if (skin) {
+        const double d2 = disp2(s.DX[i], s.DY[i], s.DZ[i]);
+        s.DD[i] = d2;
+        peer_ptr(s.DD, cu)[i] = d2;
+        const int bits = __float_as_int(__double2float_ru(d2));   // order-preserving for d2 >= 0
+        atomicMax(&s.misc[f_dmax], bits);
+        atomicMax(&peer_ptr(s.misc, cu)[f_dmax], bits);
+      }
       if (s.near_on) {
         const V av = s.A4N[i];
         const float ex = (float)av.x - s.NR4[i].x, ey = (float)av.y - s.NR4[i].y, ez = (float)av.z - s.NR4[i].z;
@@ -917,12 +942,10 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     // the update, which stay in the current buffers until the swap)
     {
       const long long is1 = istep0 + 1;
-      double m1 = 0.0, m2 = 0.0;
       for (int i = cu.lo + tid; i < cu.hi; i += nth) {
         for (int d = 0; d < 3; ++d) xnext(i, d, skin_fire);
-        xfin(i, MISC_NEAR_DISP + (int)(is1 & 1), m1, m2);
+        xfin(i, MISC_NEAR_DISP + (int)(is1 & 1), MISC_DMAX + (int)(is1 & 1));
       }
-      if (skin) top2_store(m1, m2, s.red + 32 * (int)(is1 & 1));
       if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
       if (tid == 0) s.misc[MISC_EXCESS + (int)(is1 & 1)] = 0;
     }
@@ -947,17 +970,18 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       if (rebuild && tid == 0 && cu.rank == 0)
         rebuild_counts(st, s.misc[MISC_NEXV] + peer_ptr(s.misc, cu)[MISC_NEXV],
                        s.misc[MISC_NELE] + peer_ptr(s.misc, cu)[MISC_NELE], istep);
-      // trigger of the next step from the dxyz of this one (both CTAs' pairs)
-      if (skin) skin_fire = skin_fires(s.red + 32 * par, peer_ptr(s.red + 32 * par, cu), nth >> 5, a.neigh_margin);
+      // trigger of the next step from the dxyz of this one
+      if (skin) skin_fire = skin_trigger(s.misc[MISC_DMAX + par], s.DD, N, a.neigh_margin);
       // flags of the next step: their last readers passed this barrier
-      if (tid == 0) { s.misc[MISC_EXCESS + (par ^ 1)] = 0; s.misc[MISC_NEAR_DISP + (par ^ 1)] = 0; }
+      if (tid == 0) {
+        s.misc[MISC_EXCESS + (par ^ 1)] = 0; s.misc[MISC_NEAR_DISP + (par ^ 1)] = 0; s.misc[MISC_DMAX + (par ^ 1)] = 0;
+      }
       { double *t; t = s.X; s.X = s.XN; s.XN = t; t = s.Y; s.Y = s.YN; s.YN = t; t = s.Z; s.Z = s.ZN; s.ZN = t; }
       s.PX = s.X; s.PY = s.Y; s.PZ = s.Z;
       { V *t; t = s.A4; s.A4 = s.A4N; s.A4N = t; t = s.L4; s.L4 = s.L4N; s.L4N = t; }
       PHASE_T0(t_fp);
       const int nstep_noise = a.noise_base + step;
       const bool fire_next = skin_fire;
-      double m1 = 0.0, m2 = 0.0;
       force_pass<Real, 2>(
           a, lane, L, T, s, istep, cu, nstep_noise,
           [&](int i, int d, double f) {
@@ -966,10 +990,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
           },
           par,
           [&](int i) {
-            if (!last) xfin(i, MISC_NEAR_DISP + (par ^ 1), m1, m2);
+            if (!last) xfin(i, MISC_NEAR_DISP + (par ^ 1), MISC_DMAX + (par ^ 1));
           });
       if (!last) {
-        if (skin) top2_store(m1, m2, s.red + 32 * (par ^ 1));
         // hbond-site counters of the next step (read only in the bonded sweep
         // and the valence pruning, both behind this step's cluster barriers)
         if (cu.rank == 0) for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
@@ -1013,7 +1036,6 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         PHASE_T0(t_xu);
         // x update (time_integral.F90:152-161), each product rounded as the
         // reference evaluates it; clear hbond-site counters
-        double m1 = 0.0, m2 = 0.0;
         for (int i = tid; i < N; i += nth) {
           const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
           const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
@@ -1023,7 +1045,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
           if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
           if (skin) {
             s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
-            top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
+            const double d2 = disp2(s.DX[i], s.DY[i], s.DZ[i]);
+            s.DD[i] = d2;
+            atomicMax(&s.misc[MISC_DMAX], __float_as_int(__double2float_ru(d2)));   // order-preserving for d2 >= 0
           }
           set_pos<Real>(s, i);
           if (s.near_on) {
@@ -1033,13 +1057,12 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
             if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
           }
         }
-        // per-warp pairs for the next step's trigger: read by every warp
-        // right after the barrier below, rewritten only in the next x update
-        if (skin) top2_store(m1, m2, s.red);
         for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
         if (tid == 0) s.misc[MISC_EXCESS] = 0;
         __syncthreads();
-        if (skin) skin_fire = skin_fires(s.red, nullptr, nth >> 5, a.neigh_margin);
+        // the next step's trigger (MISC_DMAX is cleared after the force
+        // pass's first barrier, before the next x update)
+        if (skin) skin_fire = skin_trigger(s.misc[MISC_DMAX], s.DD, N, a.neigh_margin);
         PHASE_ADD(2, t_xu);
       }
       if (a.mode != KM_XSTEP) {
