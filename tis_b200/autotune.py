@@ -24,7 +24,7 @@ order of each bead's sum, so the choice is a speed choice only.  The
 neighbour rebuild rule (Verlet skin or a fixed cadence) is part of the
 model the caller sets; the tuner times the workload as given.
 
-    python -m tis_b200.autotune --workload c3 c4 c1 [--out PATH]
+    python -m tis_b200.autotune --workload c1 c3 c3skin c3fp64 c4 c4skin [--out PATH]
 """
 from __future__ import annotations
 
@@ -132,18 +132,22 @@ def _workload(name):
         if name == "c3fp64":
             par = dict(par, precision=0)
         return systems, par, temps, [len(temps)]
-    if name == "c4":
+    if name in ("c4", "c4skin"):
         systems, par, temps = synth.workload_c4()
+        if name == "c4skin":
+            par = dict(par, n_step_neighbor=0)
         return systems, par, temps, [1] * len(systems)
-    if name == "c2":
+    if name in ("c2", "c2skin"):
         systems, par, temps = synth.workload_c2()
+        if name == "c2skin":
+            par = dict(par, n_step_neighbor=0)
         return systems, par, temps, [1]
     raise ValueError(name)
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", nargs="+", default=["c1", "c3", "c3skin", "c3fp64", "c4"])
+    ap.add_argument("--workload", nargs="+", default=["c1", "c3", "c3skin", "c3fp64", "c4", "c4skin"])
     ap.add_argument("--out", default=table_path())
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--reps", type=int, default=3)
