@@ -194,9 +194,9 @@ typedef struct tis_params {
   int32_t launch_noise_sweep;      /* two CTAs: 1 draws the noise in the bonded sweep, 2 in the update */
   int32_t launch_order;            /* 1: replicas launched in context order, 2: largest first */
   const char *launch_table;        /* NULL: tuned_launch.tsv next to the library */
-  int32_t launch_sweep;            /* bonded sweep of one CTA per replica: 1 a fixed deal of item chunks to
-                                      warps, 2 warps take chunks from a shared counter, longest kinds first
-                                      (two CTAs: always 1) */
+  int32_t launch_sweep;            /* bonded sweep of one CTA per replica: 1 item chunks dealt to the warps
+                                      in turn, 2 warps take chunks from a shared counter, longest kinds
+                                      first, 3 a longest-first deal made once per launch (two CTAs: 1) */
 } tis_params;
 
 /* ---------------------------------------------------------------- status */

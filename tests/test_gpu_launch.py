@@ -50,7 +50,8 @@ def test_table_caller_and_environment(tis_lib, tmp_path, monkeypatch):
 @pytest.mark.parametrize("cfg", [dict(launch_threads=128, launch_group=1), dict(launch_threads=256, launch_group=8),
                                  dict(launch_threads=1024, launch_group=2), dict(launch_ctas=2, launch_group=4,
                                                                                  launch_noise_sweep=2),
-                                 dict(launch_threads=512, launch_sweep=2), dict(launch_threads=1024, launch_sweep=2)])
+                                 dict(launch_threads=512, launch_sweep=2), dict(launch_threads=1024, launch_sweep=2),
+                                 dict(launch_threads=512, launch_sweep=3)])
 def test_configurations_keep_parity(tis_lib, cfg):
     systems, par, ladder = synth.workload_c3()
     s = systems[0]
@@ -91,14 +92,15 @@ def test_largest_first_order_on_uneven_batch(tis_lib):
 
 @pytest.mark.parametrize("threads", [512, 1024])
 def test_sweep_schedules_agree_bitwise(tis_lib, threads):
-    """The fixed deal and the shared counter hand the same item chunks to
+    """The three schedules of the bonded sweep (chunks dealt in turn, taken
+    from a shared counter, dealt longest first) hand the same item chunks to
     different warps: every item is computed the same way and every bead's
     sum keeps its order, so the trajectories are bitwise equal."""
     systems, par, ladder = synth.workload_c3()
     s = systems[0]
     temps = list(ladder[::8])
     out = []
-    for sweep in (1, 2):
+    for sweep in (1, 2, 3):
         eng = Engine([s], dict(par, launch_ctas=1, launch_threads=threads, launch_sweep=sweep), temps,
                      nrep=[len(temps)])
         assert eng.status()["sweep"] == sweep
@@ -107,5 +109,6 @@ def test_sweep_schedules_agree_bitwise(tis_lib, threads):
         eng.step(200)
         out.append(eng.get_state())
         eng.close()
-    for a, b in zip(out[0], out[1]):
-        assert np.array_equal(a, b)
+    for other in out[1:]:
+        for a, b in zip(out[0], other):
+            assert np.array_equal(a, b)

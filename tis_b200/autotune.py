@@ -12,9 +12,10 @@ the GPU for every valid configuration of
   update;
 * for batches of different sizes, the launch order (as given, or largest
   first),
-* for one CTA, the schedule of the bonded sweep: a fixed deal of item
-  chunks to warps, or warps taking chunks from a shared counter, longest
-  kinds first (the cluster kernel always deals them),
+* for one CTA, the schedule of the bonded sweep: item chunks dealt to the
+  warps in turn, warps taking chunks from a shared counter (longest kinds
+  first), or a longest-first deal made once per launch (the cluster kernel
+  always deals them in turn),
 
 keeps the fastest, and writes it as a row of the table that tis_init reads
 (tuned_launch.tsv next to libtis_b200.so; one row per workload key:
@@ -60,7 +61,7 @@ def candidates(systems, par, nrep):
         threads = [512] if ctas == 2 else ([128, 256, 512] + ([1024] if mixed else []))
         sweeps = [1, 2] if ctas == 2 else [1]
         orders = [1, 2] if uneven else [1]
-        for t, g, nz, o, sw in itertools.product(threads, [0, 1, 2, 4, 8], sweeps, orders, [1] if ctas == 2 else [1, 2]):
+        for t, g, nz, o, sw in itertools.product(threads, [0, 1, 2, 4, 8], sweeps, orders, [1] if ctas == 2 else [1, 2, 3]):
             out.append(dict(launch_ctas=ctas, launch_threads=t, launch_group=g, launch_noise_sweep=nz,
                             launch_order=o, launch_sweep=sw))
     return out

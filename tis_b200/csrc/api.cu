@@ -890,9 +890,9 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     }
     if (cfg.noise_sweep == 0) cfg.noise_sweep = 1;
     if (cfg.order == 0) cfg.order = ntop > 1 ? 2 : 1;
-    if (cfg.ctas == 2) cfg.sweep = 1;   // the cluster kernel deals its chunks
-    else if (cfg.sweep == 0) cfg.sweep = cfg.threads >= 1024 ? 2 : 1;
-    if (cfg.sweep != 1 && cfg.sweep != 2) {
+    if (cfg.ctas == 2) cfg.sweep = 1;   // the cluster kernel deals its chunks snake-wise
+    else if (cfg.sweep == 0) cfg.sweep = cfg.threads >= 1024 ? 3 : 1;
+    if (cfg.sweep < 1 || cfg.sweep > 3) {
       tis_destroy(c);
       return TIS_E_ARG;
     }
@@ -1292,7 +1292,7 @@ KArgs make_args(tis_ctx *c, int mode, int nsteps, int only_lane) {
   a.n_unif = c->n_unif;
   a.nbead_total = c->nbead_total;
   a.noise_in_sweep = 0;
-  a.sweep_dynamic = c->sweep == 2 ? 1 : 0;
+  a.sweep_mode = c->sweep - 1;
   a.lane_nsteps = nullptr;
   a.step_k = 0;
   a.lane_order = (c->order == 2 && only_lane < 0) ? c->d_order.p : nullptr;

@@ -215,7 +215,7 @@ struct KArgs {
   int n_unif;
   int nbead_total;
   int noise_in_sweep;      // 1: the sink's noise is drawn in the bonded sweep (kept in shared memory)
-  int sweep_dynamic;       // bonded sweep: 0 a fixed deal of chunks to warps, 1 warps take them from a counter
+  int sweep_mode;          // bonded sweep of one CTA per lane: 0 snake deal, 1 shared counter, 2 longest-first deal
   const int *lane_nsteps;  // per lane: steps of this launch (KM_STEP) or 1 + the last step index that
                            // moves the lane (KM_XSTEP / KM_VSTEP); null: every lane takes nsteps
   int step_k;              // KM_XSTEP / KM_VSTEP: index of this step within the call

@@ -126,8 +126,18 @@ struct Smem {
   double *C1, *C2, *C3, *C4, *RC;   // rlan_const(1..4) and 1/m of each bead (cst_on)
   double *NX, *NY, *NZ;              // this step's Gaussian noise, drawn in the bonded sweep (cst_on)
   int *exc;                 // hbond-site occupancy counters (shared when they fit, else the lane's global copy)
+  int16_t *sched;           // fixed deal of the bonded sweep: warp w takes chunks sched[33 + sched[w] ..]
+  int sched_cap;
   bool mask_smem, slots_smem, inc_smem, near_on, cst_on, exc_smem;
 };
+
+// Entries of the bonded sweep's fixed deal: 33 per-warp offsets, then the
+// chunk ids (at most sched_cap: every kind's items, at most nslot / 2, the
+// electrostatic row chunks, at most CHMAX, and the noise of N beads, in
+// chunks of 32, one partial chunk per kind) and as many scratch entries
+__host__ __device__ inline int sched_cap(int N, int nslot) {
+  return (nslot + CHMAX + N) / 32 + 16;
+}
 
 struct SmemPlan { size_t base, mask, slots, inc, near, cst, exc; };
 
@@ -145,6 +155,8 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int nq, int nslot, int ninc
   b = (b + 15) & ~(size_t)15;
   b += 4 * ((size_t)nq + N + (N + 1) + MISC_UNITS + (size_t)nunit * nunit + 8);
   b += 4 * (size_t)N;                               // unit, typ, cls
+  b = (b + 15) & ~(size_t)15;
+  b += 2 * (33 + 2 * (size_t)sched_cap(N, nslot));  // sweep deal
   b = (b + 15) & ~(size_t)15;
   SmemPlan p;
   p.base = b;
@@ -213,7 +225,10 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   s.unit = (int16_t *)ip;
   int8_t *b = (int8_t *)(s.unit + N);
   s.typ = b; s.cls = b + N; b += 2 * N;
-  unsigned char *u = (unsigned char *)(((uintptr_t)b + 15) & ~(uintptr_t)15);
+  s.sched = (int16_t *)(((uintptr_t)b + 15) & ~(uintptr_t)15);
+  s.sched_cap = sched_cap(N, T.nslot);
+  unsigned char *u = (unsigned char *)(s.sched + 33 + 2 * s.sched_cap);
+  u = (unsigned char *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
   size_t used = (size_t)(u - base);
   size_t left = (size_t)total > used ? (size_t)total - used : 0;
   s.W = (N + 31) >> 5;

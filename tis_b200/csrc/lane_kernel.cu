@@ -355,6 +355,96 @@ __device__ __forceinline__ ChunkGeo chunk_geo(int NQ, int W) {
   return g;
 }
 
+// Items of the bonded sweep of this CTA, [x0, x1) per kind (all of them
+// for one CTA per lane; with two CTAs every hbond goes to the first one, as
+// the valence pruning that may follow is serial, the rows of the own
+// charged beads, and halves of the stacks, angles and bonds), cut into
+// chunks of 32 items of one kind, and dealt to the warps in one of three
+// ways (sweep_mode; two CTAs per lane always take the first):
+//  0  chunks numbered hbonds (two CTAs), stacks, tertiary stacks,
+//     Debye-Hueckel row chunks, angles, hbonds (one CTA), bonds, noise --
+//     kinds in measured cost order, with a formed hbond the longest serial
+//     chain -- and round r gives chunk r nwarp + w to warp w (r even) or to
+//     warp nwarp - 1 - w (r odd), so the costly first chunks and the cheap
+//     last ones even out over the warps and the SM's four schedulers;
+//  1  tertiary stacks (FP64), Debye-Hueckel chunks, stacks, hbonds, angles,
+//     bonds, noise -- longest first -- each warp taking the next chunk from
+//     a shared counter as it finishes one;
+//  2  the numbering of 0, dealt once per launch by sweep_deal.
+// Measured on B200: 0 for C3 (one or two chunks per warp, where the cost of
+// an hbond chunk depends on how many hbonds are formed), 1 and 2 for
+// C4's long chains (many chunks per warp).
+struct Sweep {
+  int hb_0, hb_1, st_0, st_1, ts_0, ts_1, ch_0, ch_1, ba_0, ba_1, bd_0, bd_1, nz_0, nz_1;
+  int c_hb, c_st, c_ts, c_ch, c_ba, c_bd, c_nz, c_end;
+  int n_hbc, n_stc, n_tsc, n_chc, n_bac, n_bdc, n_nzc;
+};
+
+template <int CL>
+__device__ __forceinline__ Sweep sweep_plan(const KArgs &a, const TopDesc &T, const Clu &cu, int nch, int cpr,
+                                            bool noise, bool dyn) {
+  Sweep w;
+  const int nhb = T.nhb, nst = T.nst, nba = T.nba, nbd = T.nbd, ntst = T.ntst;
+  w.hb_0 = 0; w.hb_1 = nhb; w.st_0 = 0; w.st_1 = nst; w.ts_0 = 0; w.ts_1 = ntst;
+  w.ch_0 = 0; w.ch_1 = nch; w.ba_0 = 0; w.ba_1 = nba; w.bd_0 = 0; w.bd_1 = nbd;
+  if (CL == 2) {
+    if (cu.rank == 1) w.hb_1 = 0;
+    w.st_0 = cu.rank ? nst / 2 : 0; w.st_1 = cu.rank ? nst : nst / 2;
+    w.ts_0 = cu.rank ? ntst / 2 : 0; w.ts_1 = cu.rank ? ntst : ntst / 2;
+    w.ba_0 = cu.rank ? nba / 2 : 0; w.ba_1 = cu.rank ? nba : nba / 2;
+    w.bd_0 = cu.rank ? nbd / 2 : 0; w.bd_1 = cu.rank ? nbd : nbd / 2;
+    w.ch_0 = nch ? cu.kq_lo * cpr : 0; w.ch_1 = nch ? cu.kq_hi * cpr : 0;
+  }
+  w.nz_0 = cu.lo; w.nz_1 = noise ? cu.hi : cu.lo;
+  w.n_hbc = (w.hb_1 - w.hb_0 + 31) >> 5; w.n_stc = (w.st_1 - w.st_0 + 31) >> 5;
+  w.n_tsc = (w.ts_1 - w.ts_0 + 31) >> 5; w.n_chc = (w.ch_1 - w.ch_0 + 31) >> 5;
+  w.n_bac = (w.ba_1 - w.ba_0 + 31) >> 5; w.n_bdc = (w.bd_1 - w.bd_0 + 31) >> 5;
+  w.n_nzc = (w.nz_1 - w.nz_0 + 31) >> 5;
+  if (dyn) {
+    w.c_ts = 0; w.c_ch = w.c_ts + w.n_tsc; w.c_st = w.c_ch + w.n_chc; w.c_hb = w.c_st + w.n_stc;
+    w.c_ba = w.c_hb + w.n_hbc; w.c_bd = w.c_ba + w.n_bac; w.c_nz = w.c_bd + w.n_bdc;
+  } else {
+    w.c_st = (CL == 2) ? w.n_hbc : 0; w.c_ts = w.c_st + w.n_stc; w.c_ch = w.c_ts + w.n_tsc;
+    w.c_ba = w.c_ch + w.n_chc; w.c_hb = (CL == 2) ? 0 : w.c_ba + w.n_bac;
+    w.c_bd = w.c_ba + w.n_bac + ((CL == 2) ? 0 : w.n_hbc); w.c_nz = w.c_bd + w.n_bdc;
+  }
+  w.c_end = w.c_nz + w.n_nzc;
+  return w;
+}
+
+// The fixed deal (thread 0, once per launch): chunks in decreasing
+// estimated latency -- per kind, relative to a bond chunk (measured on
+// B200): tertiary stack 16, stack 9, Debye-Hueckel 1 + 10 per word of a
+// row, hbond and angle 5, bond 4, noise 3 -- each to the warp with
+// the least estimated load (ties: the least loaded of the SM's four
+// schedulers, then the lowest warp); warp w's chunks are
+// sched[33 + sched[w] .. 33 + sched[w + 1]).
+__device__ void sweep_deal(const Sweep &w, int gw, int nwarp, int16_t *sched, int cap) {
+  struct K { int c0, n, wt; } k[7] = {{w.c_ts, w.n_tsc, 16}, {w.c_st, w.n_stc, 9}, {w.c_ch, w.n_chc, 1 + 10 * gw},
+                                      {w.c_hb, w.n_hbc, 5},  {w.c_ba, w.n_bac, 5},  {w.c_bd, w.n_bdc, 4},
+                                      {w.c_nz, w.n_nzc, 3}};
+  for (int x = 1; x < 7; ++x)   // stable insertion sort by weight, descending
+    for (int y = x; y > 0 && k[y].wt > k[y - 1].wt; --y) { K t = k[y]; k[y] = k[y - 1]; k[y - 1] = t; }
+  int load[32], cnt[33], sm[4] = {0, 0, 0, 0};
+  for (int v = 0; v < 32; ++v) { load[v] = 0; cnt[v] = 0; }
+  int16_t *asg = sched + 33 + cap;   // warp of each chunk id
+  const int nc = w.c_end < cap ? w.c_end : cap;
+  for (int x = 0; x < 7; ++x)
+    for (int c = k[x].c0; c < k[x].c0 + k[x].n && c < nc; ++c) {
+      int best = 0;
+      for (int v = 1; v < nwarp; ++v)
+        if (load[v] < load[best] || (load[v] == load[best] && sm[v & 3] < sm[best & 3])) best = v;
+      load[best] += k[x].wt; sm[best & 3] += k[x].wt; ++cnt[best];
+      asg[c] = (int16_t)best;
+    }
+  int o = 0;
+  for (int v = 0; v < nwarp; ++v) { sched[v] = (int16_t)o; o += cnt[v]; cnt[v] = sched[v]; }
+  sched[nwarp] = (int16_t)o;
+  // each warp's chunks in the order the deal gave them (longest first)
+  for (int x = 0; x < 7; ++x)
+    for (int c = k[x].c0; c < k[x].c0 + k[x].n && c < nc; ++c) sched[33 + cnt[asg[c]]++] = (int16_t)c;
+}
+
 // Phase 1 runs every interaction-level item in one balanced sweep: stacks,
 // tertiary stacks, Debye-Hueckel chunks (force_ele_DH.F90:72-117 over a word range of one
 // charged bead's ele row, summed by one thread into ch_part), angles,
@@ -408,54 +498,26 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
   // warp-uniform schedule: 32-item chunks of one kind (no divergence between
   // kinds), dealt to the warps as below
   const int nwarp = nth >> 5, warp = tid >> 5, lid = tid & 31;
-  // items of this CTA, [x0, x1) per kind: all of them for one CTA per lane;
-  // with two CTAs every hbond goes to the first one (the valence pruning that
-  // may follow is serial), the rows of the own charged beads, and halves of
-  // the stacks, angles and bonds
-  int hb_0 = 0, hb_1 = nhb, st_0 = 0, st_1 = nst, ch_0 = 0, ch_1 = nch, ba_0 = 0, ba_1 = nba, bd_0 = 0, bd_1 = nbd;
-  int ts_0 = 0, ts_1 = ntst;
-  if (CL == 2) {
-    if (cu.rank == 1) hb_1 = 0;
-    st_0 = cu.rank ? nst / 2 : 0; st_1 = cu.rank ? nst : nst / 2;
-    ts_0 = cu.rank ? ntst / 2 : 0; ts_1 = cu.rank ? ntst : ntst / 2;
-    ba_0 = cu.rank ? nba / 2 : 0; ba_1 = cu.rank ? nba : nba / 2;
-    bd_0 = cu.rank ? nbd / 2 : 0; bd_1 = cu.rank ? nbd : nbd / 2;
-    ch_0 = nch ? cu.kq_lo * geo.cpr : 0; ch_1 = nch ? cu.kq_hi * geo.cpr : 0;
-  }
-  // Chunks of 32 items of one kind.  Fixed deal (sweep_dynamic 0): kinds in
-  // decreasing cost per chunk (measured on B200) -- stacks, tertiary
-  // stacks, Debye-Hueckel row chunks, angles, bonds, then noise -- with the
-  // hbond chunks first for two CTAs per lane (a formed hbond is the longest
-  // serial chain of the phase, and the first CTA takes every hbond) and
-  // after the angles for one CTA, where that order balances the warps
-  // better; round r gives chunk r nwarp + w to warp w (r even) or to warp
-  // nwarp - 1 - w (r odd), so the costly first chunks and the cheap last
-  // ones even out over the warps and over the SM's four schedulers.
-  // Counter (sweep_dynamic 1): tertiary stacks (FP64) and Debye-Hueckel
-  // chunks first, then stacks, hbonds, angles, bonds, noise; each warp takes
-  // the next chunk from a shared counter as it finishes one (longest first),
-  // which balances CTAs with many chunks per warp better (one CTA per lane).
-  const bool dyn = CL == 1 && a.sweep_dynamic != 0;   // two CTAs per lane: the fixed deal (measured faster)
-  const int n_hbc = (hb_1 - hb_0 + 31) >> 5, n_stc = (st_1 - st_0 + 31) >> 5, n_tsc = (ts_1 - ts_0 + 31) >> 5;
-  const int n_chc = (ch_1 - ch_0 + 31) >> 5, n_bac = (ba_1 - ba_0 + 31) >> 5, n_bdc = (bd_1 - bd_0 + 31) >> 5;
-  int c_hb, c_st, c_ts, c_ch, c_ba, c_bd, c_nz;   // first chunk of each kind
-  if (dyn) {
-    c_ts = 0; c_ch = c_ts + n_tsc; c_st = c_ch + n_chc; c_hb = c_st + n_stc;
-    c_ba = c_hb + n_hbc; c_bd = c_ba + n_bac; c_nz = c_bd + n_bdc;
-  } else {
-    c_st = (CL == 2) ? n_hbc : 0; c_ts = c_st + n_stc; c_ch = c_ts + n_tsc; c_ba = c_ch + n_chc;
-    c_hb = (CL == 2) ? 0 : c_ba + n_bac;
-    c_bd = c_ba + n_bac + ((CL == 2) ? 0 : n_hbc); c_nz = c_bd + n_bdc;
-  }
-  // the sink's Gaussian noise of the own beads, drawn here where warps have slack
-  const int n_nz = (noise_step >= 0 && s.cst_on && a.noise_in_sweep) ? cu.hi - cu.lo : 0;
-  const int c_end = c_nz + ((n_nz + 31) >> 5);
+  const int mode = (CL == 1) ? a.sweep_mode : 0;
+  const bool dyn = mode == 1;
+  // the sink's Gaussian noise of the own beads is drawn in the sweep, where warps have slack
+  const Sweep sw = sweep_plan<CL>(a, T, cu, nch, geo.cpr, noise_step >= 0 && s.cst_on && a.noise_in_sweep, dyn);
+  const int hb_0 = sw.hb_0, hb_1 = sw.hb_1, st_0 = sw.st_0, st_1 = sw.st_1, ts_0 = sw.ts_0, ts_1 = sw.ts_1;
+  const int ch_0 = sw.ch_0, ch_1 = sw.ch_1, ba_0 = sw.ba_0, ba_1 = sw.ba_1, bd_0 = sw.bd_0, bd_1 = sw.bd_1;
+  const int c_hb = sw.c_hb, c_st = sw.c_st, c_ts = sw.c_ts, c_ch = sw.c_ch, c_ba = sw.c_ba, c_bd = sw.c_bd;
+  const int c_nz = sw.c_nz, c_end = sw.c_end;
+  const int n_hbc = sw.n_hbc, n_stc = sw.n_stc, n_tsc = sw.n_tsc, n_chc = sw.n_chc, n_bac = sw.n_bac,
+            n_bdc = sw.n_bdc;
   (void)k_st; (void)k_ch; (void)k_ba; (void)k_bd; (void)total;
-  // (the counter was cleared after the last pass's bonded sweep)
-  int r = 0, c = warp;
+  // (the counter was cleared after the last pass's bonded sweep; the deal
+  // was made at the start of the launch)
+  int k = 0, kend = 0, c = warp;
   if (dyn) {
     if (lid == 0) c = atomicAdd(&s.misc[MISC_CHUNK], 1);
     c = __shfl_sync(0xffffffffu, c, 0);
+  } else if (mode == 2) {
+    k = s.sched[warp]; kend = s.sched[warp + 1];
+    c = (k < kend) ? s.sched[33 + k] : c_end;
   }
   while (c < c_end) {
     // the next chunk of this warp, requested before this one is processed
@@ -463,9 +525,11 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (dyn) {
       cn = 0;
       if (lid == 0) cn = atomicAdd(&s.misc[MISC_CHUNK], 1);
+    } else if (mode == 2) {
+      cn = (++k < kend) ? s.sched[33 + k] : c_end;
     } else {
-      ++r;
-      cn = r * nwarp + ((r & 1) ? nwarp - 1 - warp : warp);
+      ++k;
+      cn = k * nwarp + ((k & 1) ? nwarp - 1 - warp : warp);
     }
     PHASE_T0(t_item);
     int kind;
@@ -845,6 +909,16 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
     int ql = 0, qh = 0;
     for (int k = 0; k < NQ; ++k) { ql += s.qb[k] < cu.lo; qh += s.qb[k] < cu.hi; }
     cu.kq_lo = ql; cu.kq_hi = qh;
+  }
+  // the fixed deal of the bonded sweep, for the launch (modes with a force pass)
+  if (CL == 1 && a.mode != KM_NEIGHBOR && a.sweep_mode == 2) {
+    if (tid == 0) {
+      const ChunkGeo geo = chunk_geo(NQ, s.W);
+      const Sweep sw = sweep_plan<CL>(a, T, cu, a.i_ele != 0 ? geo.nch : 0, geo.cpr,
+                                      a.mode != KM_FORCE && s.cst_on && a.noise_in_sweep, false);
+      sweep_deal(sw, geo.gw, nth >> 5, s.sched, s.sched_cap);
+    }
+    __syncthreads();
   }
 
   const int label0 = st.label;
