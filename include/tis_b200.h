@@ -342,6 +342,21 @@ int tis_step(tis_ctx *ctx, int64_t nsteps);
 int tis_time_integral(tis_ctx *ctx, int64_t nsteps, int32_t *flg_step_each_replica,
                       const int64_t *exchange_step);
 
+/* The time-integral loop of mloop_simulator (src/mloop_simulator.F90:
+ * 123-150) for replicas that step together: nperiod times [nstep calls of
+ * time_integral for every replica; when exchange is nonzero, the replica
+ * exchange of time_integral_post (src/time_integral_post.F90:275-363) with
+ * counter-based uniforms, as tis_replica_exchange(ctx, NULL, NULL)].  The
+ * kernels of one period are recorded once as a CUDA graph on the library's
+ * stream (again when nstep or exchange differ from the last call) and
+ * replayed, so a period costs one graph launch and no host wait; the host
+ * waits once at the end and reports the replicas' errors (NaN, list
+ * overflow) of the whole run there; tis_last_step_ms then gives the device
+ * time of the last period's steps.  nstep >= 1.  Returns like tis_step.
+ * TIS_E_UNSUPPORTED: Brownian-HI contexts, injected noise or uniforms
+ * (tis_set_noise), and exchange on a context tis_replica_exchange refuses. */
+int tis_run(tis_ctx *ctx, int32_t nperiod, int64_t nstep, int32_t exchange);
+
 /* Step counter (istep) of every replica, istep[nrep]. */
 int tis_get_steps(tis_ctx *ctx, int64_t *istep);
 
@@ -394,8 +409,8 @@ int tis_get_labels(tis_ctx *ctx, int32_t *rep2lab);
 
 int tis_status(tis_ctx *ctx, tis_status_t *st);
 
-/* Milliseconds of the last tis_step measured with CUDA events on the
- * library's stream. */
+/* Milliseconds of the last tis_step (or of the steps of tis_run's last
+ * period) measured with CUDA events on the library's stream. */
 double tis_last_step_ms(tis_ctx *ctx);
 
 /* Device timer on the library's stream: op 0 records the start event; op 1

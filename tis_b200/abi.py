@@ -201,7 +201,7 @@ EXPORTED = [
     "tis_init", "tis_init_batch", "tis_destroy", "tis_nrep", "tis_nmp",
     "tis_set_state", "tis_get_state", "tis_get_pxyz", "tis_set_noise",
     "tis_neighbor", "tis_get_exv_list", "tis_get_ele_list", "tis_get_hb_list",
-    "tis_force_sumup", "tis_energy_sumup", "tis_time_integral_pre", "tis_step",
+    "tis_force_sumup", "tis_energy_sumup", "tis_time_integral_pre", "tis_step", "tis_run",
     "tis_replica_exchange", "tis_get_labels", "tis_status", "tis_last_step_ms",
     "tis_last_error", "tis_timer", "tis_force_sumup_static", "tis_launch_count",
     "tis_get_hydro_tensors", "tis_set_step", "tis_get_dtrna_status",
@@ -230,6 +230,7 @@ def _declare(lib):
     lib.tis_energy_sumup.argtypes = [vp, C.c_int32, _f64p]
     lib.tis_time_integral_pre.argtypes = [vp]
     lib.tis_step.argtypes = [vp, C.c_int64]
+    lib.tis_run.argtypes = [vp, C.c_int32, C.c_int64, C.c_int32]
     lib.tis_replica_exchange.argtypes = [vp, _f64p, _i32p]
     lib.tis_get_labels.argtypes = [vp, _i32p]
     lib.tis_status.argtypes = [vp, C.POINTER(Status)]

@@ -160,6 +160,11 @@ struct tis_ctx {
   std::vector<int> h_order;          // launch order of the lanes (order 2: largest first)
   DBuf<int> d_order;
   size_t smem2 = 0;
+  // tis_run: the recorded period (nstep steps [+ exchange]) and its launches
+  cudaGraphExec_t g_exec = nullptr;
+  cudaEvent_t g_ev0 = nullptr, g_ev1 = nullptr;   // recorded around the period's steps
+  long long g_nstep = -1, g_launches = 0;
+  int g_exchange = -1;
   // Ewald
   int nk = 0, hmax = 0, nqblk = 1, nq_max = 0;
   DBuf<int8_t> ew_h;
@@ -1090,6 +1095,9 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
   c->bd_D64.free(); c->bd_z.free(); c->bd_E32.free(); c->bd_W32.free();
   c->bd_D.free(); c->bd_L.free(); c->bd_P.free(); c->bd_items.free(); c->bd_D32.free(); c->bd_L32.free(); c->bd_W.free(); c->bd_F.free(); c->bd_xi.free();
+  if (c->g_exec) cudaGraphExecDestroy(c->g_exec);
+  if (c->g_ev0) cudaEventDestroy(c->g_ev0);
+  if (c->g_ev1) cudaEventDestroy(c->g_ev1);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->tev0) cudaEventDestroy(c->tev0);
@@ -1554,17 +1562,14 @@ extern "C" int tis_time_integral_pre(tis_ctx *c) {
 }
 
 namespace {
-// nsteps calls of time_integral for every lane; lane_n (host, per lane, may
-// be null) lets lane l take only lane_n[l] of them (replicas that wait for
-// their exchange step, time_integral.F90:134).
-int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
+// The kernels of nsteps steps of every lane, queued on the context's stream
+// without a host wait (lane_n_dev: per-lane step counts on the device, or
+// NULL).  Outside the Brownian-HI path (whose refresh schedule is counted
+// on the host) every launch argument is fixed when it is queued, so the
+// same sequence can be recorded into a CUDA graph (tis_run).
+int enqueue_steps(tis_ctx *c, int nsteps, const int *lane_n_dev) {
   KArgs a = make_args(c, KM_STEP, nsteps, -1);
-  if (lane_n) {
-    if (c->bdhi) return fail(c, TIS_E_UNSUPPORTED, "per-replica step counts on the Brownian-HI path");
-    CK(cudaMemcpyAsync(c->lane_n.p, lane_n->data(), c->nlane * sizeof(int), cudaMemcpyHostToDevice, c->stream));
-    a.lane_nsteps = c->lane_n.p;
-  }
-  CK(cudaEventRecord(c->ev0, c->stream));
+  a.lane_nsteps = lane_n_dev;
   if (c->pair) {
     a.smem_total = (int)c->smem2;
     // the two-CTA sweep has idle warps: the sink's noise is drawn there
@@ -1609,6 +1614,22 @@ int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
       if (rc < 0) return rc;
     }
   }
+  return TIS_OK;
+}
+
+// nsteps calls of time_integral for every lane; lane_n (host, per lane, may
+// be null) lets lane l take only lane_n[l] of them (replicas that wait for
+// their exchange step, time_integral.F90:134).
+int run_steps(tis_ctx *c, int nsteps, const std::vector<int> *lane_n) {
+  const int *lane_n_dev = nullptr;
+  if (lane_n) {
+    if (c->bdhi) return fail(c, TIS_E_UNSUPPORTED, "per-replica step counts on the Brownian-HI path");
+    CK(cudaMemcpyAsync(c->lane_n.p, lane_n->data(), c->nlane * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    lane_n_dev = c->lane_n.p;
+  }
+  CK(cudaEventRecord(c->ev0, c->stream));
+  const int rc = enqueue_steps(c, nsteps, lane_n_dev);
+  if (rc < 0) return rc;
   CK(cudaEventRecord(c->ev1, c->stream));
   CK(cudaEventSynchronize(c->ev1));
   float ms = 0.f;
@@ -1686,11 +1707,17 @@ extern "C" int tis_get_rebuild_info(tis_ctx *c, int32_t irep, int64_t *n_rebuild
 // energy_allrep.F90:123-260 + simu_replica_exchange.F90:87-300 +
 // time_integral_post.F90:293-349 (labels refresh rlan_const(1) and the
 // electrostatic / stack parameters: the kernels read them by label).
-extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_accept) {
-  if (!c) return TIS_E_ARG;
+namespace {
+int exchange_check(tis_ctx *c) {
   if (c->ntop != 1) return fail(c, TIS_E_UNSUPPORTED, "replica exchange needs one topology");
   if (c->nlabel != c->nlane)
     return fail(c, TIS_E_UNSUPPORTED, "a ladder context exchanges through tis_rex_energies and tis_rex_exchange_all");
+  return TIS_OK;
+}
+
+// The kernels of one exchange, queued without a host wait (u: injected
+// uniforms on the host, or NULL for the device's counter-based ones).
+int enqueue_exchange(tis_ctx *c, const double *u) {
   const int n = c->nlane;
   // own energies (hbond energies of the last force call reused when valid),
   // then the energies at the partner labels with the partner's beta for the
@@ -1738,6 +1765,16 @@ extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_acce
   ++c->launches;
   CK(rex_exchange_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->out_energy.p, c->e_opp.p, du,
                          c->scale.p, c->velo.p));
+  return TIS_OK;
+}
+}  // namespace
+
+extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_accept) {
+  if (!c) return TIS_E_ARG;
+  int rc = exchange_check(c);
+  if (rc < 0) return rc;
+  rc = enqueue_exchange(c, u);
+  if (rc < 0) return rc;
   if (n_accept) {   // the only host wait of an exchange
     RexState r;
     CK(cudaMemcpyAsync(&r, c->rex.p, sizeof(RexState), cudaMemcpyDeviceToHost, c->stream));
@@ -1745,6 +1782,76 @@ extern "C" int tis_replica_exchange(tis_ctx *c, const double *u, int32_t *n_acce
     *n_accept = r.nacc;
   }
   return TIS_OK;
+}
+
+// mloop_simulator.F90:123-150, the time-integral loop, for replicas that
+// step together: nperiod times [nstep calls of time_integral; with exchange,
+// the replica exchange of time_integral_post].  One period's kernels are
+// recorded once as a CUDA graph on the context's stream (again when nstep or
+// exchange change) and replayed nperiod times; the host waits once, at the
+// end, where the replicas' error flags (sticky) are read.  last_ms: the
+// device time of the last period's steps (event nodes of the graph).
+extern "C" int tis_run(tis_ctx *c, int32_t nperiod, int64_t nstep, int32_t exchange) {
+  if (!c || nperiod < 0 || nstep < 1 || nstep > 0x7fffffff) return TIS_E_ARG;
+  if (c->bdhi)
+    return fail(c, TIS_E_UNSUPPORTED, "tis_run on the Brownian-HI path (its refresh schedule is counted on the host)");
+  if (c->noise_nsteps || c->n_unif)
+    return fail(c, TIS_E_UNSUPPORTED, "tis_run with injected noise or uniforms (tis_set_noise)");
+  exchange = exchange ? 1 : 0;
+  if (exchange) {
+    const int rc = exchange_check(c);
+    if (rc < 0) return rc;
+  }
+  if (nperiod == 0) return TIS_OK;
+  if (!c->g_exec || c->g_nstep != nstep || c->g_exchange != exchange) {
+    if (c->g_exec) { cudaGraphExecDestroy(c->g_exec); c->g_exec = nullptr; }
+    // recording queues nothing: the host's counters are put back after it
+    const long long launches0 = c->launches;
+    const int idx_pair0 = c->idx_pair;
+    const bool hb_valid0 = c->hb_energy_valid;
+    if (!c->g_ev0) { CK(cudaEventCreate(&c->g_ev0)); CK(cudaEventCreate(&c->g_ev1)); }
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    // event nodes around the steps: their last replay times the last period's steps
+    cudaError_t er = cudaEventRecordWithFlags(c->g_ev0, c->stream, cudaEventRecordExternal);
+    int rc = er == cudaSuccess ? enqueue_steps(c, (int)nstep, nullptr)
+                               : fail(c, TIS_E_CUDA, std::string("cudaEventRecordWithFlags: ") + cudaGetErrorString(er));
+    if (rc >= 0) {
+      er = cudaEventRecordWithFlags(c->g_ev1, c->stream, cudaEventRecordExternal);
+      if (er != cudaSuccess) rc = fail(c, TIS_E_CUDA, std::string("cudaEventRecordWithFlags: ") + cudaGetErrorString(er));
+    }
+    if (rc >= 0 && exchange) {
+      c->hb_energy_valid = true;   // the steps' last force call left the hbond energies
+      rc = enqueue_exchange(c, nullptr);
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    c->g_launches = c->launches - launches0;
+    c->launches = launches0;
+    c->idx_pair = idx_pair0;
+    c->hb_energy_valid = hb_valid0;
+    if (rc < 0 || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return rc < 0 ? rc : fail(c, TIS_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&c->g_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      c->g_exec = nullptr;
+      return fail(c, TIS_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ei));
+    }
+    c->g_nstep = nstep;
+    c->g_exchange = exchange;
+  }
+  for (int p = 0; p < nperiod; ++p) CK(cudaGraphLaunch(c->g_exec, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->g_ev0, c->g_ev1));
+  c->last_ms = ms;
+  c->launches += (long long)nperiod * c->g_launches;
+  c->hb_energy_valid = !exchange;
+  if (exchange)
+    for (int p = 0; p < nperiod; ++p) c->idx_pair = (c->idx_pair == 2) ? 1 : c->idx_pair + 1;
+  return check_lanes(c);
 }
 
 extern "C" int tis_get_labels(tis_ctx *c, int32_t *rep2lab) {

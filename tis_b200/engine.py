@@ -163,6 +163,12 @@ class Engine:
     def step(self, n):
         return self._check(self.L.tis_step(self.h, int(n)), "step")
 
+    def run(self, nperiod, nstep, exchange=True):
+        """nperiod periods of nstep steps of every replica, each followed by
+        a replica exchange with counter-based uniforms when exchange is set,
+        replayed from one recorded CUDA graph; one host wait at the end."""
+        return self._check(self.L.tis_run(self.h, int(nperiod), int(nstep), 1 if exchange else 0), "run")
+
     def time_integral(self, n, flags, exchange_step=None):
         """n calls of time_integral(flg_step_each_replica): flags (nrep int32,
         updated in place) freeze replicas; exchange_step (nrep int64) stops
