@@ -32,7 +32,7 @@ cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2);
 cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, const KArgs &a);
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
-cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a);
+cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a);
 cudaError_t noise_launch(cudaStream_t st, KArgs a, long long istep0, int nstep, double *out);
 cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst, int *out);
 cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
@@ -1514,7 +1514,7 @@ int run_energy(tis_ctx *c, int only_lane, const int *labels, bool reuse, double 
   a.reuse_hb = reuse ? 1 : 0;
   a.ebeta = beta;
   ++c->launches;
-  CK(energy_kernel_launch(only_lane >= 0 ? 1 : c->nlane, c->stream, a));
+  CK(energy_kernel_launch(only_lane >= 0 ? 1 : c->nlane, c->max_nmp, c->stream, a));
   if (c->par.i_ele == TIS_ELE_EWALD) {
     int rc = ewald_recip(c, a, false);
     if (rc < 0) return rc;
@@ -1729,7 +1729,7 @@ int enqueue_exchange(tis_ctx *c, const double *u) {
   a.ebeta_lane = nullptr;
   a.out_energy = c->out_energy.p;
   ++c->launches;
-  CK(energy_kernel_launch(n, c->stream, a));
+  CK(energy_kernel_launch(n, c->max_nmp, c->stream, a));
   if (c->par.i_ele == TIS_ELE_EWALD) {
     int rc = ewald_recip(c, a, false);
     if (rc < 0) return rc;
@@ -1744,7 +1744,7 @@ int enqueue_exchange(tis_ctx *c, const double *u) {
   b.ebeta_lane = c->ebeta.p;
   b.out_energy = c->e_opp.p;
   ++c->launches;
-  CK(energy_kernel_launch(n, c->stream, b));
+  CK(energy_kernel_launch(n, c->max_nmp, c->stream, b));
   if (c->par.i_ele == TIS_ELE_EWALD) {
     int rc = ewald_recip(c, b, false);
     if (rc < 0) return rc;
@@ -1762,7 +1762,7 @@ int enqueue_exchange(tis_ctx *c, const double *u) {
       CK(cudaMemcpyAsync(c->rex_u.p, u, (size_t)npair * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     du = c->rex_u.p;
   }
-  ++c->launches;
+  c->launches += 2;   // the decisions, then the velocity rescale
   CK(rex_exchange_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->out_energy.p, c->e_opp.p, du,
                          c->scale.p, c->velo.p));
   return TIS_OK;

@@ -27,7 +27,10 @@ __device__ __forceinline__ double wrapd(double d) {
 
 enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_TST, ES_THB, ES_N };
 
-__global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
+constexpr int EK_THREADS = 512;
+constexpr int EK_STAGE_MAX = 1536;   // beads whose (pxyz, charge) fit the 48 KB of default shared memory
+
+__global__ void __launch_bounds__(EK_THREADS) energy_kernel(KArgs a) {
   const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
@@ -39,7 +42,16 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const double *X = a.xyz + 3 * (size_t)L.state0;
   const double *P = a.pxyz + 3 * (size_t)L.state0;
   const double *V = a.velo + 3 * (size_t)L.state0;
-  __shared__ double red[ES_N][8];
+  __shared__ double red[ES_N][EK_THREADS / 32];
+  // the pair loops read pxyz and the charge of every partner: staged in
+  // shared memory (the same doubles) when the lane fits
+  extern __shared__ double4 ek_pq[];
+  const bool staged = N <= EK_STAGE_MAX;
+  if (staged)
+    for (int i = tid; i < N; i += nth) {
+      const double3 p = gpos(P, i);
+      ek_pq[i] = make_double4(p.x, p.y, p.z, bead_charge(a, label, T.bead0 + i));
+    }
   __shared__ int excess_flag;
   double es[ES_N];
   for (int k = 0; k < ES_N; ++k) es[k] = 0.0;
@@ -162,8 +174,13 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   const double cut2 = (a.i_ele == 1 && a.i_DH_cutoff_type == 0) ? (a.cutoff_ele * cdist) * (a.cutoff_ele * cdist)
                                                                 : a.cutoff_ele * a.cutoff_ele;
   const double rcd = 1.0 / cdist;
+  auto ppos = [&](int i) {
+    if (staged) { const double4 v = ek_pq[i]; return make_double3(v.x, v.y, v.z); }
+    return gpos(P, i);
+  };
+  auto pq = [&](int i) { return staged ? ek_pq[i].w : bead_charge(a, label, T.bead0 + i); };
   auto shifted = [&](int i, int j) {   // j > i: canonical orientation
-    double3 w = sub3(gpos(P, j), gpos(P, i));
+    double3 w = sub3(ppos(j), ppos(i));
     if (mir) {
       const int im = (int)mir[(size_t)i * N + j] - 1;
       const int m0 = im / 9, m1 = (im / 3) % 3, m2 = im % 3;
@@ -173,11 +190,15 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
     }
     return w;
   };
-  for (int i = tid; i < N; i += nth) {
+  // one item per (row i, word w) of the upper triangle, so the rows of
+  // charged beads with many partners spread over many threads
+  for (int it = tid; it < N * W; it += nth) {
+    const int i = it / W, w = it - i * W;
+    if (w < ((i + 1) >> 5)) continue;
     const int ti = a.b_type[T.bead0 + i], ci = a.b_class[T.bead0 + i];
-    const double q_i = bead_charge(a, label, T.bead0 + i);
+    const double q_i = pq(i);
     const bool qi = fabs(q_i) >= 1.0e-6;
-    for (int w = (i + 1) >> 5; w < W; ++w) {
+    {
       uint32_t me = mexv[(size_t)i * W + w], ml = (a.i_ele != 0 && qi) ? mele[(size_t)i * W + w] : 0u;
       if (w == ((i + 1) >> 5)) {   // keep bits j > i only
         const uint32_t keep = ((i + 1) & 31) ? ~((1u << ((i + 1) & 31)) - 1u) : 0xffffffffu;
@@ -222,7 +243,7 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
             es[ES_ELE] += pe[ib] - pf[ib] * (dist1 - (a.pmf_rmin + (double)ib * a.pmf_rbin));
             continue;
           }
-          const double ce = q_i * bead_charge(a, label, T.bead0 + j) * coefT;
+          const double ce = q_i * pq(j) * coefT;
           if (a.i_ele == 1) es[ES_ELE] += ce / dist1 * exp(-dist1 * rcd);
           else if (a.i_ele == 3) es[ES_ELE] += ce * (1.0e0 / dist1 - 1.0e0 / a.cutoff_ele);   // energy_ele_coulomb.F90:66
           else es[ES_ELE] += ce * erfc(a.ewld_alpha * dist1) / dist1;
@@ -318,8 +339,9 @@ __global__ void __launch_bounds__(256) energy_kernel(KArgs a) {
   }
 }
 
-cudaError_t energy_kernel_launch(int grid, cudaStream_t st, const KArgs &a) {
-  energy_kernel<<<grid, 256, 0, st>>>(a);
+cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a) {
+  const size_t smem = (size_t)(max_nmp <= EK_STAGE_MAX ? max_nmp : 0) * sizeof(double4);
+  energy_kernel<<<grid, EK_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
@@ -361,7 +383,8 @@ cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst,
 // rex_exchange_kernel (one CTA): thread 0 runs the Metropolis decisions in
 // label order with counter-based uniforms (or injected ones), updates the
 // label maps, the pair alternation and beta_hbond15; then the CTA writes the
-// lanes' labels and rescales the velocities of the swapped lanes.
+// lanes' labels.  vscale_kernel then rescales the velocities of the swapped
+// lanes, one block per lane.
 
 
 __global__ void rex_prep_kernel(KArgs a, const int *rep2lab, int *elabel, double *ebeta) {
@@ -421,18 +444,7 @@ __global__ void __launch_bounds__(256) rex_exchange_kernel(KArgs a, RexState *re
     rex->beta_global = 1.0e0 / (a.lab_T[rep2lab[n - 1]] * a.boltz);
   }
   for (int r = tid; r < n; r += blockDim.x) a.lstate[r].label = rep2lab[r];
-  // time_integral.F90 velocity rescale of a swapped replica (scale > 0
-  // multiplies, scale < 0 divides by -scale), one warp per replica
-  const int warp = tid >> 5, lid = tid & 31, nw = blockDim.x >> 5;
-  for (int r = warp; r < n; r += nw) {
-    const double f = scale[r];
-    if (f == 0.0) continue;
-    const LaneDesc L = a.lanes[r];
-    const int N = a.tops[L.top].nmp;
-    double *v = velo + 3 * (size_t)L.state0;
-    if (f > 0.0) for (int k = lid; k < 3 * N; k += 32) v[k] = f * v[k];
-    else for (int k = lid; k < 3 * N; k += 32) v[k] = v[k] / (-f);
-  }
+  (void)velo;   // the velocities of the swapped replicas are rescaled by vscale_kernel
 }
 
 // velocity rescale of the lanes a ladder exchange swapped: lane l's
@@ -465,6 +477,8 @@ cudaError_t rex_exchange_launch(cudaStream_t st, const KArgs &a, RexState *rex, 
                                 const double *e_own, const double *e_opp, const double *u, double *scale,
                                 double *velo) {
   rex_exchange_kernel<<<1, 256, 0, st>>>(a, rex, rep2lab, lab2rep, e_own, e_opp, u, scale, velo);
+  // time_integral.F90 velocity rescale of the swapped replicas, one block each
+  vscale_kernel<<<a.nlane, 128, 0, st>>>(a, scale, velo);
   return cudaGetLastError();
 }
 
