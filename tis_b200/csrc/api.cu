@@ -33,6 +33,7 @@ cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, con
 size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a);
+cudaError_t energy_pair_launch(int nlane, int max_nmp, cudaStream_t st, const KArgs &a, const KArgs &b);
 cudaError_t noise_launch(cudaStream_t st, KArgs a, long long istep0, int nstep, double *out);
 cudaError_t st_status_launch(cudaStream_t st, const KArgs &a, int lane, int nst, int *out);
 cudaError_t rex_launch(cudaStream_t st, const KArgs &a, RexState *rex, int *rep2lab, int *lab2rep, int *elabel,
@@ -143,6 +144,9 @@ struct tis_ctx {
   DBuf<uint8_t> b_qkind;            // (bead) 1: phosphate charge -Zp of the label (i_charge = 1)
   DBuf<double> lab_zp, pmf_e, pmf_f; // per label: Zp; Mg-P table (pmf_nbin per label)
   DBuf<double> hb_ene;
+  DBuf<uint8_t> hb_flag2;            // hbond scratch of an exchange's partner-label energy pass
+  DBuf<double> hb_ene2;
+  DBuf<int> site_exc2;
   DBuf<unsigned char> slots;
   DBuf<double> noise, unif;
   DBuf<int> lane_n;                  // per-lane step counts of the last tis_time_integral
@@ -982,6 +986,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
   CK(c->mirror.alloc(periodic ? (size_t)mirror_off : 1));
   CK(c->slots.alloc(slot_off * 3 * real_size));
   CK(c->hb_flag.alloc(hb_off)); CK(c->hb_ene.alloc(hb_off)); CK(c->site_exc.alloc(site_off));
+  CK(c->hb_flag2.alloc(hb_off)); CK(c->hb_ene2.alloc(hb_off)); CK(c->site_exc2.alloc(site_off));
   CK(cudaMemset(c->hb_flag.p, 0, std::max(hb_off, 1)));
   CK(cudaMemset(c->hb_ene.p, 0, std::max(hb_off, 1) * sizeof(double)));
   c->max_nmp = maxN;
@@ -1089,7 +1094,7 @@ extern "C" void tis_destroy(tis_ctx *c) {
   c->xyz.free(); c->pxyz.free(); c->velo.free(); c->accel.free(); c->dxyz.free(); c->p0xyz.free();
   c->out_force.free(); c->out_energy.free(); c->scale.free();
   c->mask.free(); c->site_exc.free(); c->mirror.free(); c->hb_flag.free();
-  c->hb_ene.free(); c->slots.free(); c->noise.free(); c->unif.free(); c->lane_n.free(); c->d_order.free();
+  c->hb_ene.free(); c->hb_flag2.free(); c->hb_ene2.free(); c->site_exc2.free(); c->slots.free(); c->noise.free(); c->unif.free(); c->lane_n.free(); c->d_order.free();
   c->ew_h.free(); c->ew_coef.free(); c->ew_tab.free(); c->ew_S.free(); c->f_ext.free();
   c->fene_idx.free(); c->wca_idx.free(); c->bd_ptr.free(); c->bd_ent.free(); c->fene_cls.free(); c->wca_cls.free(); c->b_hrad.free(); c->d_not_spd.free();
   c->fene_nat.free(); c->fene_coef.free(); c->fene_d2.free(); c->wca_nat.free(); c->wca_coef.free();
@@ -1728,25 +1733,32 @@ int enqueue_exchange(tis_ctx *c, const double *u) {
   a.elabel = nullptr;
   a.ebeta_lane = nullptr;
   a.out_energy = c->out_energy.p;
-  ++c->launches;
-  CK(energy_kernel_launch(n, c->max_nmp, c->stream, a));
-  if (c->par.i_ele == TIS_ELE_EWALD) {
-    int rc = ewald_recip(c, a, false);
-    if (rc < 0) return rc;
-    ++c->launches;
-    CK(ewald_energy_launch(c->stream, a));
-  }
-  ++c->launches;
-  CK(rex_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->elabel.p, c->ebeta.p));
   KArgs b = a;
   b.reuse_hb = 0;
   b.elabel = c->elabel.p;
   b.ebeta_lane = c->ebeta.p;
   b.out_energy = c->e_opp.p;
-  ++c->launches;
-  CK(energy_kernel_launch(n, c->max_nmp, c->stream, b));
-  if (c->par.i_ele == TIS_ELE_EWALD) {
-    int rc = ewald_recip(c, b, false);
+  if (c->par.i_ele != TIS_ELE_EWALD) {
+    // the partner labels first, then both passes in one launch (the partner
+    // pass recomputes the hbonds in its own scratch)
+    ++c->launches;
+    CK(rex_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->elabel.p, c->ebeta.p));
+    b.hb_flag = c->hb_flag2.p; b.hb_ene = c->hb_ene2.p; b.site_exc = c->site_exc2.p;
+    b.hb_flag_src = c->hb_flag.p;
+    ++c->launches;
+    CK(energy_pair_launch(n, c->max_nmp, c->stream, a, b));
+  } else {
+    ++c->launches;
+    CK(energy_kernel_launch(n, c->max_nmp, c->stream, a));
+    int rc = ewald_recip(c, a, false);
+    if (rc < 0) return rc;
+    ++c->launches;
+    CK(ewald_energy_launch(c->stream, a));
+    ++c->launches;
+    CK(rex_launch(c->stream, a, c->rex.p, c->d_rep2lab.p, c->d_lab2rep.p, c->elabel.p, c->ebeta.p));
+    ++c->launches;
+    CK(energy_kernel_launch(n, c->max_nmp, c->stream, b));
+    rc = ewald_recip(c, b, false);
     if (rc < 0) return rc;
     ++c->launches;
     CK(ewald_energy_launch(c->stream, b));

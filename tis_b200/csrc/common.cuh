@@ -201,6 +201,8 @@ struct KArgs {
   // energy evaluation (energy_kernel)
   const int *elabel;       // per lane label override (-1: own label)
   int reuse_hb;            // 1: sum the hbond energies of the last force pass (flg_hb_energy)
+  const uint8_t *hb_flag_src; // energy pass with its own hbond scratch (hb_flag, hb_ene, site_exc):
+                              // the list bits of the lanes' hb_flag are read from here; null: hb_flag
   double ebeta;            // beta_hbond15 for a recomputed hbond pruning
   const double *ebeta_lane;// per lane beta (overrides ebeta when set)
   double *out_energy;      // (N_ETYPE) per lane

@@ -30,9 +30,7 @@ enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_
 constexpr int EK_THREADS = 512;
 constexpr int EK_STAGE_MAX = 1536;   // beads whose (pxyz, charge) fit the 48 KB of default shared memory
 
-__global__ void __launch_bounds__(EK_THREADS) energy_kernel(KArgs a) {
-  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
-  if (lane >= a.nlane) return;
+__device__ __forceinline__ void energy_lane(const KArgs &a, int lane) {
   const LaneDesc L = a.lanes[lane];
   const TopDesc T = a.tops[L.top];
   const int N = T.nmp;
@@ -254,7 +252,7 @@ __global__ void __launch_bounds__(EK_THREADS) energy_kernel(KArgs a) {
   // hydrogen bonds (energy_dtrna_hbond15.F90)
   if (!a.reuse_hb) {
     for (int h = tid; h < T.nhb; h += nth) {
-      uint8_t f = hbf[h] & 1;
+      uint8_t f = (a.hb_flag_src ? a.hb_flag_src + L.hb0 : hbf)[h] & 1;
       hbe[h] = 0.0;
       if (f) {
         const int *m = a.hb_idx + 6 * (size_t)(T.hb0 + h);
@@ -339,9 +337,31 @@ __global__ void __launch_bounds__(EK_THREADS) energy_kernel(KArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(EK_THREADS) energy_kernel(KArgs a) {
+  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.x;
+  if (lane >= a.nlane) return;
+  energy_lane(a, lane);
+}
+
+// The two energy passes of an exchange in one launch: block l < nlane the
+// own label of lane l (args a), block nlane + l the partner label (args b,
+// whose hbond recomputation uses its own scratch, so the passes can run
+// together)
+__global__ void __launch_bounds__(EK_THREADS) energy_pair_kernel(KArgs a, KArgs b) {
+  const int l = (int)blockIdx.x;
+  if (l < a.nlane) energy_lane(a, l);
+  else if (l < 2 * a.nlane) energy_lane(b, l - a.nlane);
+}
+
 cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a) {
   const size_t smem = (size_t)(max_nmp <= EK_STAGE_MAX ? max_nmp : 0) * sizeof(double4);
   energy_kernel<<<grid, EK_THREADS, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t energy_pair_launch(int nlane, int max_nmp, cudaStream_t st, const KArgs &a, const KArgs &b) {
+  const size_t smem = (size_t)(max_nmp <= EK_STAGE_MAX ? max_nmp : 0) * sizeof(double4);
+  energy_pair_kernel<<<2 * nlane, EK_THREADS, smem, st>>>(a, b);
   return cudaGetLastError();
 }
 
