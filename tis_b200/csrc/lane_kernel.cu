@@ -121,6 +121,7 @@ __device__ __forceinline__ double add_rn(double a, double b) {
 }
 
 // ------------------------------------------------------------ list build
+constexpr int CELL_MIN = 384;   // beads of a one-CTA lane from which the build bins them
 // neighbor_list.F90:49-90 + neighbor_assign.F90:481-559 (the EXV_DT15 type
 // sort keeps the generation order) and neighbor_list_ele.F90:123-210: every
 // unordered pair is tested once and sets its bit in both rows of the exv
@@ -214,63 +215,203 @@ __device__ void build_lists(const KArgs &a, int lane, const LaneDesc &L, const T
     if (s.mask_smem) { pexv = peer_ptr(mexv, cu); pele = peer_ptr(mele, cu); }
   }
   PHASE_T0(t_pairs);
-  // warp w takes rows i = w, w + nwarp, ...; its lanes take j > i (two CTAs:
-  // CTA r takes the rows of parity r and sets each bit in the copy of the
-  // row's owner)
   const bool one_unit = nu == 1;
   const double rn2_00 = s.rn2[0];
-  const int rstep = nwarp * CL;
-  for (int i = warp * CL + cu.rank; i < N - 1; i += rstep) {
-    const int ui = s.unit[i];
-    const int ci = s.cls[i];
-    const int nsep = (s.typ[i] == 2) ? a.nsep[0] : (s.typ[i] == 4 ? a.nsep[1] : (s.typ[i] == 3 ? a.nsep[2] : -1));
-    const double xi = s.PX[i], yi = s.PY[i], zi = s.PZ[i];
-    const bool qi = a.i_ele != 0 && fabs((double)s.A4[i].w) >= 1.0e-6;
-    for (int j = i + 1 + lid; j < N; j += 32) {
-      const int uj = one_unit ? 0 : s.unit[j];
-      if (!one_unit && !nunit_ok[ui * nu + uj]) continue;
-      double v0 = __dsub_rn(s.PX[j], xi), v1 = __dsub_rn(s.PY[j], yi), v2 = __dsub_rn(s.PZ[j], zi);
-      int im = 27;
-      if (a.periodic) {
-        int m0 = pb1(v0, a.psize[0], a.psizeh[0]);
-        int m1 = pb1(v1, a.psize[1], a.psizeh[1]);
-        int m2 = pb1(v2, a.psize[2], a.psizeh[2]);
-        im = 9 * m0 + 3 * m1 + m2 + 1;
+  // the pair test of row i, partner j > i
+  auto pair = [&](int i, int j, int ui, int ci, int nsep, double xi, double yi, double zi, bool qi) {
+    const int uj = one_unit ? 0 : s.unit[j];
+    if (!one_unit && !nunit_ok[ui * nu + uj]) return;
+    double v0 = __dsub_rn(s.PX[j], xi), v1 = __dsub_rn(s.PY[j], yi), v2 = __dsub_rn(s.PZ[j], zi);
+    int im = 27;
+    if (a.periodic) {
+      int m0 = pb1(v0, a.psize[0], a.psizeh[0]);
+      int m1 = pb1(v1, a.psize[1], a.psizeh[1]);
+      int m2 = pb1(v2, a.psize[2], a.psizeh[2]);
+      im = 9 * m0 + 3 * m1 + m2 + 1;
+    }
+    const double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
+    bool ex = d2 < (one_unit ? rn2_00 : s.rn2[ui * nu + uj]);
+    const bool el = qi && fabs((double)s.A4[j].w) >= 1.0e-6 && d2 < rele2;
+    if (ex) {
+      if (ui == uj) {
+        if (ci == 2 /* RNA */ && j < i + nsep) ex = false;
+      } else {
+        const int cj = s.cls[j];
+        if (!((ci == 2 && cj == 2) || (ci == 2 && cj == 4) || (ci == 4 && cj == 2) ||
+              (ci == 4 && cj == 3) || (ci == 3 && cj == 4)))
+          ex = false;
+        else if (a.dt19 && ((ci == 2 && cj == 4) || (ci == 4 && cj == 2))) {
+          // neighbor_assign.F90:524-537: no exv between a charged phosphate and an ion
+          const int pb = (s.typ[i] == 2) ? i : ((s.typ[j] == 2) ? j : -1);
+          if (pb >= 0 && fabs((double)s.A4[pb].w) > 1.0e-6) ex = false;
+        }
       }
-      const double d2 = __dadd_rn(__dadd_rn(sqr_rn(v0), sqr_rn(v1)), sqr_rn(v2));
-      bool ex = d2 < (one_unit ? rn2_00 : s.rn2[ui * nu + uj]);
-      const bool el = qi && fabs((double)s.A4[j].w) >= 1.0e-6 && d2 < rele2;
+    }
+    if (ex || el) {
+      const uint32_t bj = 1u << (j & 31), bi = 1u << (i & 31);
+      const bool own_i = CL == 1 || (i >= cu.lo && i < cu.hi);
+      const bool own_j = CL == 1 || (j >= cu.lo && j < cu.hi);
       if (ex) {
-        if (ui == uj) {
-          if (ci == 2 /* RNA */ && j < i + nsep) ex = false;
+        atomicOr(&(own_i ? mexv : pexv)[(size_t)i * W + (j >> 5)], bj);
+        atomicOr(&(own_j ? mexv : pexv)[(size_t)j * W + (i >> 5)], bi);
+        ++nexv_l;
+      }
+      if (el) {
+        atomicOr(&(own_i ? mele : pele)[(size_t)i * W + (j >> 5)], bj);
+        atomicOr(&(own_j ? mele : pele)[(size_t)j * W + (i >> 5)], bi);
+        ++nele_l;
+      }
+      if (mir) mir[(size_t)i * N + j] = (uint8_t)im;
+    }
+  };
+  auto nsep_of = [&](int i) {
+    return (s.typ[i] == 2) ? a.nsep[0] : (s.typ[i] == 4 ? a.nsep[1] : (s.typ[i] == 3 ? a.nsep[2] : -1));
+  };
+  auto q_of = [&](int i) { return a.i_ele != 0 && fabs((double)s.A4[i].w) >= 1.0e-6; };
+  // ---- cell list (one CTA, large lanes): bins at least as wide as the
+  // largest list cutoff, so a pair within it lies in the same or a
+  // neighbouring bin (across the box when periodic); a row tests only the
+  // beads of the 27 bins around its own.  The test is the all-pairs one, so
+  // are the lists.  Scratch: the Debye-Hueckel partials, unused while the
+  // lists are built.
+  int *cl = (int *)s.ch_part;
+  int nb[3] = {0, 0, 0};
+  double blo[3] = {0, 0, 0}, bw[3] = {1, 1, 1};
+  bool cells = false;
+  if (CL == 1 && N >= CELL_MIN) {
+    double rc2 = rele2;
+    for (int k = 0; k < nu * nu; ++k) rc2 = fmax(rc2, s.rn2[k]);
+    const double wmin = sqrt(rc2) * (1.0 + 1.0e-9) + 1.0e-9;
+    double ext[3];
+    if (a.periodic) {
+      for (int d = 0; d < 3; ++d) { blo[d] = -a.psizeh[d]; ext[d] = a.psize[d]; }
+    } else {
+      // bounding box of the lane: per-warp extremes, then every thread
+      double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+      for (int i = tid; i < N; i += nth) {
+        const double q[3] = {s.PX[i], s.PY[i], s.PZ[i]};
+        for (int d = 0; d < 3; ++d) { mn[d] = fmin(mn[d], q[d]); mx[d] = fmax(mx[d], q[d]); }
+      }
+      for (int o = 16; o > 0; o >>= 1)
+        for (int d = 0; d < 3; ++d) {
+          mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+          mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+        }
+      double *red = (double *)cl;
+      if (lid == 0)
+        for (int d = 0; d < 3; ++d) { red[d * 32 + warp] = mn[d]; red[(3 + d) * 32 + warp] = mx[d]; }
+      __syncthreads();
+      for (int d = 0; d < 3; ++d) {
+        for (int w = 0; w < nwarp; ++w) { mn[d] = fmin(mn[d], red[d * 32 + w]); mx[d] = fmax(mx[d], red[(3 + d) * 32 + w]); }
+        blo[d] = mn[d];
+        ext[d] = mx[d] - mn[d];
+      }
+      __syncthreads();   // red is overwritten below
+    }
+    // bins of width >= wmin, widened until their tables fit the scratch
+    const long long room = 6 * CHMAX - 1 - N - 56 * nwarp;
+    double w = wmin;
+    for (int tries = 0; tries < 40 && !cells; ++tries, w *= 1.25) {
+      long long ncell = 1;
+      bool ok = true;
+      for (int d = 0; d < 3; ++d) {
+        const double nf = floor(ext[d] / w) + (a.periodic ? 0.0 : 1.0);
+        nb[d] = nf < 1.0 ? 1 : (nf > 4096.0 ? 4096 : (int)nf);
+        bw[d] = a.periodic ? ext[d] / nb[d] : w;
+        if (a.periodic && nb[d] < 3) ok = false;   // neighbouring bins must be distinct
+        ncell *= nb[d];
+      }
+      if (!ok || ncell <= 27) break;   // too few bins to gain over the all-pairs scan
+      cells = 2 * ncell <= room;
+    }
+  }
+  if (cells) {
+    const int ncell = nb[0] * nb[1] * nb[2];
+    int *start = cl, *fill = cl + ncell + 1, *cb = fill + ncell, *wsc = cb + N;
+    auto bin_of = [&](int i, int &x, int &y, int &z) {
+      x = min(max((int)floor((s.PX[i] - blo[0]) / bw[0]), 0), nb[0] - 1);
+      y = min(max((int)floor((s.PY[i] - blo[1]) / bw[1]), 0), nb[1] - 1);
+      z = min(max((int)floor((s.PZ[i] - blo[2]) / bw[2]), 0), nb[2] - 1);
+    };
+    for (int k = tid; k <= ncell; k += nth) start[k] = 0;
+    __syncthreads();
+    for (int i = tid; i < N; i += nth) {
+      int x, y, z;
+      bin_of(i, x, y, z);
+      atomicAdd(&start[(z * nb[1] + y) * nb[0] + x + 1], 1);
+    }
+    __syncthreads();
+    if (warp == 0) {   // inclusive scan: start[c] = first slot of bin c, start[ncell] = N
+      const int seg = (ncell + 1 + 31) / 32, k0 = lid * seg, k1 = min(k0 + seg, ncell + 1);
+      int sum = 0;
+      for (int k = k0; k < k1; ++k) sum += start[k];
+      int incl = sum;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lid >= o) incl += t;
+      }
+      int run = incl - sum;
+      for (int k = k0; k < k1; ++k) { run += start[k]; start[k] = run; }
+    }
+    __syncthreads();
+    for (int c = tid; c < ncell; c += nth) fill[c] = start[c];
+    __syncthreads();
+    for (int i = tid; i < N; i += nth) {
+      int x, y, z;
+      bin_of(i, x, y, z);
+      cb[atomicAdd(&fill[(z * nb[1] + y) * nb[0] + x], 1)] = i;
+    }
+    __syncthreads();
+    int *wp = wsc + 56 * warp;   // per warp: 28 candidate offsets, 27 bin starts
+    for (int i = warp; i < N - 1; i += nwarp) {
+      int x, y, z;
+      bin_of(i, x, y, z);
+      int n_l = 0, st_l = 0;
+      if (lid < 27) {
+        int bx = x + lid % 3 - 1, by = y + (lid / 3) % 3 - 1, bz = z + lid / 9 - 1;
+        bool in = true;
+        if (a.periodic) {
+          bx = (bx + nb[0]) % nb[0]; by = (by + nb[1]) % nb[1]; bz = (bz + nb[2]) % nb[2];
         } else {
-          const int cj = s.cls[j];
-          if (!((ci == 2 && cj == 2) || (ci == 2 && cj == 4) || (ci == 4 && cj == 2) ||
-                (ci == 4 && cj == 3) || (ci == 3 && cj == 4)))
-            ex = false;
-          else if (a.dt19 && ((ci == 2 && cj == 4) || (ci == 4 && cj == 2))) {
-            // neighbor_assign.F90:524-537: no exv between a charged phosphate and an ion
-            const int pb = (s.typ[i] == 2) ? i : ((s.typ[j] == 2) ? j : -1);
-            if (pb >= 0 && fabs((double)s.A4[pb].w) > 1.0e-6) ex = false;
-          }
+          in = bx >= 0 && bx < nb[0] && by >= 0 && by < nb[1] && bz >= 0 && bz < nb[2];
+        }
+        if (in) {
+          const int c = (bz * nb[1] + by) * nb[0] + bx;
+          st_l = start[c];
+          n_l = start[c + 1] - st_l;
         }
       }
-      if (ex || el) {
-        const uint32_t bj = 1u << (j & 31), bi = 1u << (i & 31);
-        const bool own_i = CL == 1 || (i >= cu.lo && i < cu.hi);
-        const bool own_j = CL == 1 || (j >= cu.lo && j < cu.hi);
-        if (ex) {
-          atomicOr(&(own_i ? mexv : pexv)[(size_t)i * W + (j >> 5)], bj);
-          atomicOr(&(own_j ? mexv : pexv)[(size_t)j * W + (i >> 5)], bi);
-          ++nexv_l;
-        }
-        if (el) {
-          atomicOr(&(own_i ? mele : pele)[(size_t)i * W + (j >> 5)], bj);
-          atomicOr(&(own_j ? mele : pele)[(size_t)j * W + (i >> 5)], bi);
-          ++nele_l;
-        }
-        if (mir) mir[(size_t)i * N + j] = (uint8_t)im;
+      int incl = n_l;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lid >= o) incl += t;
       }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (lid < 28) wp[lid] = incl - n_l;
+      if (lid < 27) wp[28 + lid] = st_l;
+      __syncwarp();
+      const int ui = s.unit[i], ci = s.cls[i], nsep = nsep_of(i);
+      const double xi = s.PX[i], yi = s.PY[i], zi = s.PZ[i];
+      const bool qi = q_of(i);
+      for (int k = lid; k < total; k += 32) {
+        int b = 0;   // the last bin whose candidates start at or before k
+        for (int st = 16; st > 0; st >>= 1)
+          if (b + st < 27 && wp[b + st] <= k) b += st;
+        const int j = cb[wp[28 + b] + k - wp[b]];
+        if (j > i) pair(i, j, ui, ci, nsep, xi, yi, zi, qi);
+      }
+      __syncwarp();
+    }
+  } else {
+    // every pair: warp w takes rows i = w, w + nwarp, ...; its lanes take
+    // j > i (two CTAs: CTA r takes the rows of parity r and sets each bit
+    // in the copy of the row's owner)
+    const int rstep = nwarp * CL;
+    for (int i = warp * CL + cu.rank; i < N - 1; i += rstep) {
+      const int ui = s.unit[i], ci = s.cls[i], nsep = nsep_of(i);
+      const double xi = s.PX[i], yi = s.PY[i], zi = s.PZ[i];
+      const bool qi = q_of(i);
+      for (int j = i + 1 + lid; j < N; j += 32) pair(i, j, ui, ci, nsep, xi, yi, zi, qi);
     }
   }
   if (nexv_l) atomicAdd(&s.misc[MISC_NEXV], nexv_l);
