@@ -1044,8 +1044,8 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     CK(c->ew_coef.upload(coef));
     CK(c->ew_tab.alloc(std::max<size_t>((size_t)ew_off * 3 * (c->hmax + 1) * 2, 1)));
     CK(c->ew_S.alloc(std::max<size_t>((size_t)nlane * c->nqblk * c->nk * 2, 1)));
-    CK(c->f_ext.alloc(n3));
-    CK(cudaMemset(c->f_ext.p, 0, n3 * 8));
+    CK(c->f_ext.alloc(n3 * EW_F_SPLIT));
+    CK(cudaMemset(c->f_ext.p, 0, n3 * EW_F_SPLIT * 8));
   }
   c->clamp_seen.assign(nlane, 0);
   *out = c;

@@ -19,6 +19,8 @@ namespace tis {
 constexpr int MAX_THREADS = 1024;
 constexpr int N_ETYPE = 25;   // E_TYPE%MAX
 constexpr int CHMAX = 1024;   // electrostatic row chunks per lane (at least one per charged bead)
+constexpr int EW_F_SPLIT = 4; // k ranges of the reciprocal-space forces: f_ext holds one (3, nbead_total)
+                              // plane of partial forces per range, added in range order
 // HI_TENSOR (const_index.F90:39-45)
 constexpr int TIS_HI_RPY_DEV = 1, TIS_HI_RPY_OVER_DEV = 2, TIS_HI_ERMAK_OVER_DEV = 3, TIS_HI_ZUK_RPY_DEV = 4;
 

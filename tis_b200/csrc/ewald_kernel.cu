@@ -12,8 +12,9 @@
 //   ewald_sk_kernel     per k and charge block: partial S_c(k) = sum q cos,
 //                       S_s(k) = sum q sin (charges in ascending order)
 //   ewald_sk_sum_kernel S(k) = the charge-block partials summed in block order
-//   ewald_force_kernel  per charge (one warp): F = sum_k coef 2 C(k)
-//                       q (sin S_c - cos S_s) k
+//   ewald_force_kernel  per charge (one warp) and k range (EW_F_SPLIT of
+//                       them): partial F = sum_k coef 2 C(k) q (sin S_c -
+//                       cos S_s) k, added by the lane kernel in range order
 //   ewald_energy_kernel per lane: coef (sum_k C(k) (S_c^2 + S_s^2) + self)
 //
 // All sums run in a fixed order, so the results do not depend on scheduling.
@@ -115,10 +116,12 @@ __global__ void __launch_bounds__(256) ewald_sk_sum_kernel(KArgs a) {
 
 constexpr int EW_F_KCHUNK = 512;     // k vectors staged in shared memory at a time
 
-// grid (ceil(nq / 8), nlane), 256 threads: one warp per charge; the CTA
-// stages (S_c, S_s, C(k), h) of EW_F_KCHUNK vectors at a time for its 8 warps
+// grid (ceil(nq / 8), EW_F_SPLIT, nlane), 256 threads: one warp per charge
+// over k range blockIdx.y; the CTA stages its 8 charges' tables and
+// (S_c, S_s, C(k), h) of EW_F_KCHUNK vectors at a time
+constexpr int EW_TAB_MAX = 3 * 16;   // 3 (hmax + 1) table entries per charge staged (hmax <= 15)
 __global__ void __launch_bounds__(256) ewald_force_kernel(KArgs a) {
-  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.y;
+  const int lane = (a.only_lane >= 0) ? a.only_lane : (int)blockIdx.z;
   if (lane >= a.nlane) return;
   const LaneDesc L = a.lanes[lane];
   const TopDesc T = a.tops[L.top];
@@ -129,14 +132,23 @@ __global__ void __launch_bounds__(256) ewald_force_kernel(KArgs a) {
   const int bead = qv ? a.q_bead[T.q0 + kq] : 0;
   const double q = qv ? a.b_charge[T.bead0 + bead] : 0.0;
   const double coefT = a.lab_coef[a.lstate[lane].label];
-  const double2 *t = (const double2 *)a.ew_tab + (size_t)(L.ew0 + (qv ? kq : 0)) * 3 * H;
   const double *S = a.ew_S + (size_t)lane * a.nqblk * a.nk * 2;
+  __shared__ double2 sT[8 * EW_TAB_MAX];
   __shared__ double2 sS[EW_F_KCHUNK];
   __shared__ double sC[EW_F_KCHUNK];
   __shared__ char4 sH[EW_F_KCHUNK];
+  const bool staged = 3 * H <= EW_TAB_MAX;
+  const double2 *t = staged ? sT + warp * EW_TAB_MAX
+                            : (const double2 *)a.ew_tab + (size_t)(L.ew0 + (qv ? kq : 0)) * 3 * H;
+  if (staged && qv) {
+    const double2 *g = (const double2 *)a.ew_tab + (size_t)(L.ew0 + kq) * 3 * H;
+    for (int e = lid; e < 3 * H; e += 32) sT[warp * EW_TAB_MAX + e] = g[e];
+  }
+  const int ka = (int)((long long)a.nk * blockIdx.y / EW_F_SPLIT);
+  const int kb = (int)((long long)a.nk * (blockIdx.y + 1) / EW_F_SPLIT);
   double fx = 0.0, fy = 0.0, fz = 0.0;
-  for (int k0 = 0; k0 < a.nk; k0 += EW_F_KCHUNK) {
-    const int nkc = min(EW_F_KCHUNK, a.nk - k0);
+  for (int k0 = ka; k0 < kb; k0 += EW_F_KCHUNK) {
+    const int nkc = min(EW_F_KCHUNK, kb - k0);
     __syncthreads();
     for (int e = threadIdx.x; e < nkc; e += blockDim.x) {
       const int k = k0 + e;
@@ -164,7 +176,7 @@ __global__ void __launch_bounds__(256) ewald_force_kernel(KArgs a) {
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
   if (qv && lid == 0) {
-    double *f = a.f_ext + 3 * (size_t)(L.state0 + bead);
+    double *f = a.f_ext + 3 * ((size_t)blockIdx.y * a.nbead_total + L.state0 + bead);
     f[0] = fx; f[1] = fy; f[2] = fz;
   }
 }
@@ -212,7 +224,7 @@ cudaError_t ewald_recip_launch(cudaStream_t st, const KArgs &a, int nq_max, bool
   ewald_tab_kernel<<<dim3((nq_max + 127) / 128, nl), 128, 0, st>>>(a);
   ewald_sk_kernel<<<dim3((a.nk + EW_SK_THREADS - 1) / EW_SK_THREADS, a.nqblk, nl), EW_SK_THREADS, 0, st>>>(a);
   if (a.nqblk > 1) ewald_sk_sum_kernel<<<dim3((a.nk + 255) / 256, nl), 256, 0, st>>>(a);
-  if (forces) ewald_force_kernel<<<dim3((nq_max + 7) / 8, nl), 256, 0, st>>>(a);
+  if (forces) ewald_force_kernel<<<dim3((nq_max + 7) / 8, EW_F_SPLIT, nl), 256, 0, st>>>(a);
   return cudaGetLastError();
 }
 

@@ -956,7 +956,8 @@ __device__ void force_pass(const KArgs &a, int lane, const LaneDesc &L, const To
     if (valid) {
       for (int d = g; d < 3; d += GA) {
         double f = d == 0 ? fx : (d == 1 ? fy : fz);
-        if (a.f_ext) f += a.f_ext[3 * (size_t)(L.state0 + i) + d];
+        if (a.f_ext)   // the reciprocal-space partial forces, in k-range order
+          for (int p = 0; p < EW_F_SPLIT; ++p) f += a.f_ext[3 * ((size_t)p * a.nbead_total + L.state0 + i) + d];
         sink(i, d, f);
       }
     }
