@@ -93,6 +93,31 @@ def test_ewald_trajectory_injected_noise(tis_lib, precision, tol):
     eng.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("skin", [False, True])
+def test_ewald_long_call_equals_one_step_calls(tis_lib, precision, skin):
+    """A call of n steps runs the x update of each next step in the launch of
+    the forces; it must give the one-step calls' state bit for bit (with
+    the skin rule: through several rebuilds)."""
+    s, par = c2_box()
+    par = dict(par, precision=precision, n_step_neighbor=0 if skin else 10, neigh_margin=2.0 if skin else 8.0)
+    nsteps = 60
+    out = []
+    for calls in ([nsteps], [1] * nsteps):
+        eng = Engine([s], par, [300.0])
+        eng.set_state(s["xyz"])
+        assert eng.time_integral_pre() >= 0
+        for n in calls:
+            assert eng.step(n) >= 0
+        out.append(eng.get_state() + (eng.get_pxyz(), eng.rebuild_info(1)))
+        eng.close()
+    for u, w in zip(out[0][:4], out[1][:4]):
+        assert np.array_equal(u, w)
+    assert out[0][4] == out[1][4]
+    if skin:
+        assert out[0][4][0] >= 3
+
+
 def test_ewald_rejects_non_cubic_box(tis_lib):
     from tis_b200.engine import TisError
     s, par = small_box()

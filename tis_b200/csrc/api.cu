@@ -1602,14 +1602,15 @@ int enqueue_steps(tis_ctx *c, int nsteps, const int *lane_n_dev) {
     if (rc < 0) return rc;
   } else {
     // the reciprocal sum needs every charge's new position: each step is
-    // x update -> reciprocal forces -> forces, v / a update
+    // x update -> reciprocal forces -> forces, v / a update; the x update
+    // of step k + 1 runs in the launch of step k's forces
+    KArgs x = make_args(c, KM_XSTEP, 1, -1);
+    x.lane_nsteps = a.lane_nsteps;
+    x.step_k = 0;
+    int rc = launch_lane(c, x);
+    if (rc < 0) return rc;
     for (int64_t k = 0; k < nsteps; ++k) {
-      KArgs x = make_args(c, KM_XSTEP, 1, -1);
-      x.lane_nsteps = a.lane_nsteps;
-      x.step_k = (int)k;
-      int rc = launch_lane(c, x);
-      if (rc < 0) return rc;
-      KArgs v = make_args(c, KM_VSTEP, 1, -1);
+      KArgs v = make_args(c, k + 1 < nsteps ? KM_VXSTEP : KM_VSTEP, 1, -1);
       v.lane_nsteps = a.lane_nsteps;
       v.step_k = (int)k;
       v.noise_base = c->noise_base + (int)k;

@@ -90,6 +90,7 @@ enum KMode {
   KM_STEP = 4,         // nsteps of time_integral
   KM_XSTEP = 5,        // first half of one step: trigger, rebuild, x update
   KM_VSTEP = 6,        // second half of one step: forces (+ f_ext), v / a update
+  KM_VXSTEP = 7,       // KM_VSTEP, then the KM_XSTEP of the next step
 };
 
 // Kernel arguments (all device pointers).

@@ -989,7 +989,9 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   if (lane >= a.nlane) return;
   if (CL == 2 && a.mode != KM_STEP) return;
   // replicas that have reached their exchange step wait (time_integral.F90:134)
-  if (a.lane_nsteps && (a.mode == KM_XSTEP || a.mode == KM_VSTEP) && a.step_k >= a.lane_nsteps[lane]) return;
+  if (a.lane_nsteps && (a.mode == KM_XSTEP || a.mode == KM_VSTEP || a.mode == KM_VXSTEP) &&
+      a.step_k >= a.lane_nsteps[lane])
+    return;
   const int lane_steps = (a.lane_nsteps && a.mode == KM_STEP) ? min(a.nsteps, a.lane_nsteps[lane]) : a.nsteps;
   const LaneDesc L = a.lanes[lane];
   const TopDesc T = a.tops[L.top];
@@ -1100,7 +1102,7 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   // are read after the cluster barrier below)
   bool skin_fire = false;
   double *red0 = s.red + ((CL == 2) ? 32 * (int)(istep0 & 1) : 0);
-  if (skin && (a.mode == KM_STEP || a.mode == KM_XSTEP)) {
+  if (skin && (a.mode == KM_STEP || a.mode == KM_XSTEP || a.mode == KM_VXSTEP)) {
     double m1 = 0.0, m2 = 0.0;
     for (int i = cu.lo + tid; i < cu.hi; i += nth) top2_add(m1, m2, disp2(s.DX[i], s.DY[i], s.DZ[i]));
     top2_store(m1, m2, red0);
@@ -1232,55 +1234,58 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
       const double n = (s.cst_on && a.noise_in_sweep) ? s.NX[d * N + i] : noise1(a, lane, L, i, is, a.noise_base, d);
       s.AX[d * N + i] = mad2<Real>(f, a.b_rcmass[T.bead0 + i], c1[i], n);
     });
-  } else {  // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step)
+  } else {
+    // KM_STEP (nsteps), KM_XSTEP and KM_VSTEP (the two halves of one step),
+    // KM_VXSTEP (the second half of one step and the first of the next)
+    auto xpart = [&](long long istep) {
+      // time_integral.F90:57-161: neighbour trigger, rebuild, x update
+      PHASE_T0(t_trig);
+      const bool rebuild = skin ? skin_fire : ((istep % a.n_step_neighbor) == 1 || istep == 1);
+      PHASE_ADD(0, t_trig);
+      PHASE_T0(t_reb);
+      if (rebuild) {
+        build_lists<Real, 1>(a, lane, L, T, s, cu, istep);
+        // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
+        if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
+        __syncthreads();
+      }
+      PHASE_ADD(1, t_reb);
+      PHASE_T0(t_xu);
+      // x update (time_integral.F90:152-161), each product rounded as the
+      // reference evaluates it; clear hbond-site counters
+      for (int i = tid; i < N; i += nth) {
+        const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
+        const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
+        const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
+        const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
+        s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
+        if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
+        if (skin) {
+          s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
+          const double d2 = disp2(s.DX[i], s.DY[i], s.DZ[i]);
+          s.DD[i] = d2;
+          atomicMax(&s.misc[MISC_DMAX], __float_as_int(__double2float_ru(d2)));   // order-preserving for d2 >= 0
+        }
+        set_pos<Real>(s, i);
+        if (s.near_on) {
+          const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
+                      ez = (float)s.A4[i].z - s.NR4[i].z;
+          const float e2 = ex * ex + ey * ey + ez * ez;
+          if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
+        }
+      }
+      for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
+      if (tid == 0) s.misc[MISC_EXCESS] = 0;
+      __syncthreads();
+      // the next step's trigger (MISC_DMAX is cleared after the force
+      // pass's first barrier, before the next x update)
+      if (skin) skin_fire = skin_trigger(s.misc[MISC_DMAX], s.DD, N, a.neigh_margin);
+      PHASE_ADD(2, t_xu);
+    };
     const int nloop = (a.mode == KM_STEP) ? lane_steps : 1;
     for (int step = 0; step < nloop; ++step) {
       const long long istep = st.istep + 1;
-      if (a.mode != KM_VSTEP) {
-        // time_integral.F90:57-161: neighbour trigger, rebuild, x update
-        PHASE_T0(t_trig);
-        const bool rebuild = skin ? skin_fire : ((istep % a.n_step_neighbor) == 1 || istep == 1);
-        PHASE_ADD(0, t_trig);
-        PHASE_T0(t_reb);
-        if (rebuild) {
-          build_lists<Real, 1>(a, lane, L, T, s, cu, istep);
-          // dxyz_mp(:,:,irep) = 0 after a skin-triggered rebuild (time_integral.F90:89)
-          if (skin) for (int i = tid; i < N; i += nth) { s.DX[i] = 0.0; s.DY[i] = 0.0; s.DZ[i] = 0.0; }
-          __syncthreads();
-        }
-        PHASE_ADD(1, t_reb);
-        PHASE_T0(t_xu);
-        // x update (time_integral.F90:152-161), each product rounded as the
-        // reference evaluates it; clear hbond-site counters
-        for (int i = tid; i < N; i += nth) {
-          const double c4 = s.cst_on ? s.C4[i] : a.b_c4[T.bead0 + i];
-          const double dx = mad2<Real>(c4, s.VX[i], a.tstep2, s.AX[i]);
-          const double dy = mad2<Real>(c4, s.VY[i], a.tstep2, s.AY[i]);
-          const double dz = mad2<Real>(c4, s.VZ[i], a.tstep2, s.AZ[i]);
-          s.X[i] += dx; s.Y[i] += dy; s.Z[i] += dz;
-          if (a.periodic) { s.PX[i] += dx; s.PY[i] += dy; s.PZ[i] += dz; }
-          if (skin) {
-            s.DX[i] += dx; s.DY[i] += dy; s.DZ[i] += dz;
-            const double d2 = disp2(s.DX[i], s.DY[i], s.DZ[i]);
-            s.DD[i] = d2;
-            atomicMax(&s.misc[MISC_DMAX], __float_as_int(__double2float_ru(d2)));   // order-preserving for d2 >= 0
-          }
-          set_pos<Real>(s, i);
-          if (s.near_on) {
-            const float ex = (float)s.A4[i].x - s.NR4[i].x, ey = (float)s.A4[i].y - s.NR4[i].y,
-                        ez = (float)s.A4[i].z - s.NR4[i].z;
-            const float e2 = ex * ex + ey * ey + ez * ez;
-            if (!(e2 <= NEAR_DISP_MAX * NEAR_DISP_MAX)) atomicMax(&s.misc[MISC_NEAR_DISP], 0x7f000000);
-          }
-        }
-        for (int k = tid; k < T.nsite; k += nth) exc[k] = 0;
-        if (tid == 0) s.misc[MISC_EXCESS] = 0;
-        __syncthreads();
-        // the next step's trigger (MISC_DMAX is cleared after the force
-        // pass's first barrier, before the next x update)
-        if (skin) skin_fire = skin_trigger(s.misc[MISC_DMAX], s.DD, N, a.neigh_margin);
-        PHASE_ADD(2, t_xu);
-      }
+      if (a.mode == KM_STEP || a.mode == KM_XSTEP) xpart(istep);
       if (a.mode != KM_XSTEP) {
         // time_integral.F90:162-183: forces (+ f_ext), v / a update
         const int nstep_noise = a.noise_base + step;
@@ -1290,6 +1295,8 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
         __syncthreads();
         PHASE_ADD(6, t_fp);
       }
+      // the next step's x update, unless this replica stops at this step
+      if (a.mode == KM_VXSTEP && (!a.lane_nsteps || a.step_k + 1 < a.lane_nsteps[lane])) xpart(istep + 1);
     }
   }
   __syncthreads();
