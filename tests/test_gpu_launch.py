@@ -112,3 +112,22 @@ def test_sweep_schedules_agree_bitwise(tis_lib, threads):
     for other in out[1:]:
         for a, b in zip(out[0], other):
             assert np.array_equal(a, b)
+
+
+def test_two_cta_layout_that_does_not_fit_runs_on_one_cta(tis_lib):
+    """The largest C4 chain (1,193 beads): its two-CTA layout (each CTA keeps
+    every bead's positions plus the next-step copies) needs more than the
+    227 KB of shared memory a CTA may use, so the context runs it on one CTA
+    even when two are asked for, and the steps run."""
+    systems, par, _ = synth.workload_c4()
+    s = max(systems, key=lambda x: x["nmp"])
+    assert s["nmp"] == 1193
+    for cfg in ({}, {"launch_ctas": 2}):
+        eng = Engine([s], dict(par, n_step_neighbor=0, **cfg), [300.0])
+        assert eng.status()["ctas_per_lane"] == 1
+        eng.set_state(s["xyz"])
+        assert eng.time_integral_pre() >= 0
+        assert eng.run(1, 20, exchange=False) >= 0
+        x, _, _ = eng.get_state()
+        assert np.isfinite(x).all()
+        eng.close()

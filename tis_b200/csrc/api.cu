@@ -30,7 +30,8 @@ size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool s
                        bool dbuf, int nsite);
 cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2);
 cudaError_t lane_kernel_launch_pair(int nlane, size_t smem, cudaStream_t st, const KArgs &a);
-size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit);
+size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
+                      bool dbuf);
 cudaError_t lane_kernel_launch(bool mixed, int grid, int block, size_t smem, cudaStream_t st, const KArgs &a);
 cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a);
 cudaError_t energy_pair_launch(int nlane, int max_nmp, cudaStream_t st, const KArgs &a, const KArgs &b);
@@ -836,6 +837,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
   const int real_size = (p.precision == TIS_PREC_MIXED) ? 4 : 8;
   size_t smem = 0, smem2 = 0;
   int minN = 1 << 30;
+  bool pair_fits = true;
   for (auto &d : c->tops) {
     // electrostatic row chunks: one per charged bead at least
     if (p.i_ele != TIS_ELE_NONE && d.nq > CHMAX) { tis_destroy(c); return TIS_E_UNSUPPORTED; }
@@ -843,7 +845,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     // the per-lane base layout must fit one CTA's shared memory (the
     // Brownian-HI path does not run the lane kernel)
     if (c->bdhi) continue;
-    if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit) + 64 > 227 * 1024) {
+    if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, false) + 64 > 227 * 1024) {
       tis_destroy(c);
       return TIS_E_UNSUPPORTED;
     }
@@ -852,6 +854,9 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     smem2 = std::max(smem2, smem_bytes_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, true,
                                             d.nsite));
     minN = std::min(minN, d.nmp);
+    // the two-CTA layout (next-step copies of the positions) must fit too
+    if (smem_base_host(d.nmp, d.nq, d.nslot, d.ninc, periodic, skin, real_size, d.nunit, true) + 64 > 227 * 1024)
+      pair_fits = false;
   }
   c->smem = smem;
   // launch configuration: caller fields, then the environment, then the
@@ -863,8 +868,7 @@ int init_impl(int32_t ntop, const tis_topology *tops, const tis_params *par, con
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const bool mixed = p.precision == TIS_PREC_MIXED;
-    const bool pair_ok = !c->bdhi && mixed && !periodic && p.i_ele != TIS_ELE_EWALD && minN >= 64 &&
-                         smem2 <= 227 * 1024;
+    const bool pair_ok = !c->bdhi && mixed && !periodic && p.i_ele != TIS_ELE_EWALD && minN >= 64 && pair_fits;
     LaunchCfg cfg;
     int source = 0;
     {
@@ -1341,6 +1345,8 @@ int check_lanes(tis_ctx *c) {
     if (ls[i].flags & LF_PMF)
       code = fail(c, TIS_E_PMF_RANGE, "Mg-P pair below the PMF table in lane " + std::to_string(i + 1));
     if (ls[i].flags & LF_OVERFLOW) code = fail(c, TIS_E_LIST_OVERFLOW, "hbond site list overflow");
+    if (ls[i].flags & LF_SMEM)
+      code = fail(c, TIS_E_UNSUPPORTED, "the shared-memory layout of lane " + std::to_string(i + 1) + " does not fit");
     if (ls[i].flags & (LF_UNIF_EXHAUSTED | LF_NOISE_EXHAUSTED))
       code = fail(c, TIS_E_NOISE_EXHAUSTED, "injected noise or uniforms exhausted");
     clamps += ls[i].nclamp - c->clamp_seen[i];

@@ -81,7 +81,8 @@ struct LaneState {
   int need_rebuild;
 };
 
-enum LaneFlags { LF_OVERFLOW = 1, LF_NAN = 2, LF_UNIF_EXHAUSTED = 4, LF_NOISE_EXHAUSTED = 8, LF_PMF = 16 };
+enum LaneFlags { LF_OVERFLOW = 1, LF_NAN = 2, LF_UNIF_EXHAUSTED = 4, LF_NOISE_EXHAUSTED = 8, LF_PMF = 16,
+                 LF_SMEM = 32 /* the lane's base layout did not fit the launch's shared memory: nothing ran */ };
 
 enum KMode {
   KM_NEIGHBOR = 1,     // rebuild lists (wrap pxyz if periodic)

@@ -129,6 +129,7 @@ struct Smem {
   int16_t *sched;           // fixed deal of the bonded sweep: warp w takes chunks sched[33 + sched[w] ..]
   int sched_cap;
   bool mask_smem, slots_smem, inc_smem, near_on, cst_on, exc_smem;
+  bool fits;                // the base layout fits the launch's dynamic shared memory
 };
 
 // Entries of the bonded sweep's fixed deal: 33 per-warp offsets, then the
@@ -230,6 +231,7 @@ __device__ Smem<Real> carve(unsigned char *base, int total, const KArgs &a, cons
   unsigned char *u = (unsigned char *)(s.sched + 33 + 2 * s.sched_cap);
   u = (unsigned char *)(((uintptr_t)u + 15) & ~(uintptr_t)15);
   size_t used = (size_t)(u - base);
+  s.fits = used <= (size_t)total;
   size_t left = (size_t)total > used ? (size_t)total - used : 0;
   s.W = (N + 31) >> 5;
   s.mask_smem = pl.mask <= MASK_SMEM_MAX && pl.mask <= left;

@@ -1002,6 +1002,12 @@ __global__ void __launch_bounds__(NT) lane_kernel(KArgs a) {
   const bool skin = (CL == 2) ? SKIN2 : a.n_step_neighbor <= 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<Real> s = carve<Real>(smem_raw, a.smem_total, a, L, T, a.periodic != 0, skin, CL == 2);
+  // a layout larger than the launch's shared memory (the host sizes the
+  // launch so this cannot happen) touches nothing: the lane is flagged
+  if (!s.fits) {
+    if (tid == 0) atomicOr(&a.lstate[lane].flags, LF_SMEM);
+    return;
+  }
   LaneState &st = a.lstate[lane];
   Clu cu;
   cu.nrank = CL;
@@ -1384,8 +1390,9 @@ size_t smem_bytes_host(int N, int nq, int nslot, int ninc, bool periodic, bool s
   return want < 227 * 1024 ? want : 227 * 1024;
 }
 
-size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit) {
-  return smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit).base;
+size_t smem_base_host(int N, int nq, int nslot, int ninc, bool periodic, bool skin, int real_size, int nunit,
+                      bool dbuf) {
+  return smem_plan(N, nq, nslot, ninc, periodic, skin, real_size, nunit, dbuf).base;
 }
 
 cudaError_t lane_kernel_set_smem(bool mixed, int bytes, int bytes2) {
