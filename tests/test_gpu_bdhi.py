@@ -50,6 +50,25 @@ def test_bdhi_forces_and_energy(tis_lib, n):
     eng.close()
 
 
+def test_energy_of_a_batch_with_a_lane_too_large_to_stage(tis_lib):
+    """The energy kernel stages pxyz in shared memory for lanes of up to
+    1,472 beads and reads the larger ones from global memory; in a batch of
+    both, each lane's energies equal the oracle's."""
+    systems = [synth.bead_chain(1500, 31), squeezed_chain(60, 32)]
+    par = synth.bdhi_params()
+    eng = Engine(systems, par, [300.0, 300.0])
+    eng.set_state(np.vstack([s["xyz"] for s in systems]))
+    for k, s in enumerate(systems):
+        orc = Oracle(s, par, [300.0])
+        orc.set_state(s["xyz"][None])
+        orc.neighbor()
+        e = eng.energy(k + 1)
+        er = orc.energy()
+        for t in (3, 23, 24):   # BOND (FENE), WCA_REP, WCA_ATT
+            assert abs(e[t - 1] - er[t - 1]) <= 1e-9 * max(1.0, abs(er[t - 1])), (k, t)
+    eng.close()
+
+
 @pytest.mark.parametrize("every", [1, 3])
 def test_bdhi_trajectory_injected_noise(tis_lib, every):
     ns = [30, 47, 64]

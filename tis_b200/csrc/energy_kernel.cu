@@ -28,7 +28,10 @@ __device__ __forceinline__ double wrapd(double d) {
 enum { ES_VELO, ES_BOND, ES_ANGLE, ES_STACK, ES_HB, ES_EXV, ES_ELE, ES_WREP, ES_WATT, ES_TST, ES_THB, ES_N };
 
 constexpr int EK_THREADS = 512;
-constexpr int EK_STAGE_MAX = 1536;   // beads whose (pxyz, charge) fit the 48 KB of default shared memory
+// beads whose (pxyz, charge) the energy kernels stage in shared memory:
+// 1472 x 32 bytes and the kernels' static arrays fit the 48 KB a launch gets
+// without opting in; larger lanes read pxyz from global memory
+constexpr int EK_STAGE_MAX = 1472;
 
 __device__ __forceinline__ void energy_lane(const KArgs &a, int lane) {
   const LaneDesc L = a.lanes[lane];
@@ -353,14 +356,18 @@ __global__ void __launch_bounds__(EK_THREADS) energy_pair_kernel(KArgs a, KArgs 
   else if (l < 2 * a.nlane) energy_lane(b, l - a.nlane);
 }
 
+// dynamic shared memory for the largest lane that stages (every lane with
+// N <= EK_STAGE_MAX stages, so the launch must hold min(max_nmp, EK_STAGE_MAX))
+inline size_t ek_smem(int max_nmp) { return (size_t)(max_nmp < EK_STAGE_MAX ? max_nmp : EK_STAGE_MAX) * sizeof(double4); }
+
 cudaError_t energy_kernel_launch(int grid, int max_nmp, cudaStream_t st, const KArgs &a) {
-  const size_t smem = (size_t)(max_nmp <= EK_STAGE_MAX ? max_nmp : 0) * sizeof(double4);
+  const size_t smem = ek_smem(max_nmp);
   energy_kernel<<<grid, EK_THREADS, smem, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t energy_pair_launch(int nlane, int max_nmp, cudaStream_t st, const KArgs &a, const KArgs &b) {
-  const size_t smem = (size_t)(max_nmp <= EK_STAGE_MAX ? max_nmp : 0) * sizeof(double4);
+  const size_t smem = ek_smem(max_nmp);
   energy_pair_kernel<<<2 * nlane, EK_THREADS, smem, st>>>(a, b);
   return cudaGetLastError();
 }
