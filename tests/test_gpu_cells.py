@@ -73,9 +73,10 @@ def compare_lists(eng, orc):
 @pytest.mark.parametrize("make", [long_chain, c2])
 def test_binned_lists_bit_exact(tis_lib, make):
     s, par = make()
-    assert binned(s, par)
     eng = Engine([s], par, [300.0])
-    assert eng.status()["ctas_per_lane"] == 1
+    st = eng.status()
+    assert st["ctas_per_lane"] == 1
+    assert binned(s, par, st["threads_per_cta"] // 32)
     orc = Oracle(s, dict(par, precision=0), [300.0])
     eng.set_state(s["xyz"])
     orc.set_state(s["xyz"][None])
@@ -94,8 +95,8 @@ def test_binned_lists_of_skin_rebuilds(tis_lib, make):
     GPU's pxyz, so both wrap the periodic box alike)."""
     s, par = make()
     par = dict(par, n_step_neighbor=0, neigh_margin=2.0)
-    assert binned(s, par)
     eng = Engine([s], par, [300.0])
+    assert binned(s, par, eng.status()["threads_per_cta"] // 32)
     eng.set_state(s["xyz"])
     eng.time_integral_pre()
     orc = Oracle(s, dict(par, precision=0), [300.0])
